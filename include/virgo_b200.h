@@ -1,0 +1,228 @@
+/* virgo_b200: B200 (sm_100a) kernels for the Virgo prover hot path, behind a
+ * plain C ABI.
+ *
+ * The drop-in C++ classes (zk_prover, poly_commit::poly_commit_prover, the
+ * fri:: functions, fast_fourier_transform, create_tree, my_hhash; headers under
+ * virgo_b200/host/include) are thin wrappers over these entry points; a caller
+ * in any language can bind them directly.
+ *
+ * Conventions
+ *  - Every entry point returns VG_OK (0) or a VG_ERR_* code; vg_last_error()
+ *    gives a message for the calling thread.
+ *  - vg_fe is the reference's prime_field::field_element layout: {img, real},
+ *    two uint64 in [0, 2^61 - 1).  vg_digest is __hhash_digest (32 bytes).
+ *  - "dev" pointers are device memory (vg_dev_alloc); "host" pointers are
+ *    ordinary host memory; "any" pointers may be either (detected per call).
+ *  - All work of one context is ordered on that context's CUDA stream.
+ *    Entry points that return values to host memory synchronise it.
+ */
+#ifndef VIRGO_B200_H
+#define VIRGO_B200_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { uint64_t img, real; } vg_fe;
+typedef struct { uint8_t bytes[32]; } vg_digest;
+
+enum {
+    VG_OK = 0,
+    VG_ERR_CUDA = 1,      /* a CUDA call failed (message has the CUDA error) */
+    VG_ERR_ARG = 2,       /* invalid argument (sizes, null pointers, ranges)  */
+    VG_ERR_OOM = 3,       /* device allocation failed                         */
+    VG_ERR_NO_DEVICE = 4, /* no CUDA device / extension not usable            */
+    VG_ERR_STATE = 5      /* call out of protocol order                        */
+};
+
+enum { VG_HASH_SHA3_256 = 0, VG_HASH_SHA256 = 1 };
+
+typedef struct vg_ctx vg_ctx;          /* device, stream, scratch, twiddle cache */
+typedef struct vg_circuit vg_circuit;  /* device-resident layered circuit        */
+typedef struct vg_gkr vg_gkr;          /* GKR prover state for one circuit       */
+typedef struct vg_pc vg_pc;            /* polynomial commitment + FRI state      */
+
+/* ---------------------------------------------------------------- context */
+const char *vg_last_error(void);
+/* Creates a context on `device` with its own stream.  Replaces the implicit
+ * global state of the reference (prime_field::init, prime_field.cpp:19-24;
+ * init_scratch_pad, RS_polynomial.cpp:8-16). */
+int vg_ctx_create(int device, vg_ctx **out);
+int vg_ctx_destroy(vg_ctx *ctx);
+/* Hash used for every Merkle commitment of this context.  The reference
+ * chooses it at build time (#define USESHA3, my_hhash.h:10); default SHA3-256. */
+int vg_ctx_set_hash(vg_ctx *ctx, int kind);
+int vg_ctx_get_hash(vg_ctx *ctx, int *kind);
+int vg_ctx_sync(vg_ctx *ctx);
+/* Number of kernels this context has launched since creation. */
+int vg_ctx_launch_count(vg_ctx *ctx, long long *count);
+
+/* ----------------------------------------------------------- device memory */
+int vg_dev_alloc(vg_ctx *ctx, size_t bytes, void **dev);
+int vg_dev_free(vg_ctx *ctx, void *dev);
+int vg_h2d(vg_ctx *ctx, void *dev, const void *host, size_t bytes);
+int vg_d2h(vg_ctx *ctx, void *host, const void *dev, size_t bytes);
+
+/* ------------------------------------------------------------------- field */
+/* Elementwise c = a op b on n elements, op 0 = add, 1 = sub, 2 = mul
+ * (prime_field::field_element operators, prime_field.h:114-165). dev. */
+int vg_fe_binop(vg_ctx *ctx, int op, const vg_fe *a, const vg_fe *b, vg_fe *c, long n);
+
+/* --------------------------------------------------------------------- NTT */
+/* Batched transform: for each of `batch` arrays, out = the evaluations of the
+ * polynomial with coefficients in[0..in_len) (zero beyond) at root^0 ..
+ * root^(n-1), n = 2^log_n, natural order; root must have order n.  With
+ * scale_inv_n != 0 the outputs are multiplied by n^-1.  in_len <= n.
+ * Replaces fast_fourier_transform (RS_polynomial.h:10, RS_polynomial.cpp:27)
+ * and, with the inverse root and scale_inv_n, inverse_fast_fourier_transform
+ * (RS_polynomial.h:16, RS_polynomial.cpp:169) for coef_len == order.
+ * in/out dev; in and out may not overlap unless in == out and in_len == n. */
+int vg_ntt(vg_ctx *ctx, const vg_fe *in, long in_len, long in_batch_stride,
+           vg_fe *out, int log_n, long out_batch_stride, int batch,
+           vg_fe root, int scale_inv_n);
+
+/* ------------------------------------------------------------------- hash */
+/* n independent hashes of 64-byte messages (my_hhash, my_hhash.h:28). dev. */
+int vg_hash64(vg_ctx *ctx, const void *msgs, void *digests, long n);
+/* Merkle tree over n leaves, tree = 2 * next_pow2(n) digests, tree[1] = root,
+ * leaves stored raw, padding leaves H(0^64), nodes H(left || right)
+ * (merkle_tree::merkle_tree_prover::create_tree, merkle_tree.h:12,
+ * merkle_tree.cpp:4-57). dev. */
+int vg_merkle_tree(vg_ctx *ctx, const vg_digest *leaves, long n, vg_digest *tree);
+/* Leaf hash chains of a slice-major codeword set (n_slices slices of length
+ * n): leaf k < n/2 is h = H((c[s][k], c[s][k+n/2]) || h) over s from h = 0
+ * (the leaf loops of fri::request_init_commit, fri.cpp:97-126, and
+ * fri::commit_phase_step, fri.cpp:394-420). dev. */
+int vg_leaf_chain(vg_ctx *ctx, const vg_fe *codewords, int n_slices, long n, vg_digest *leaves);
+
+/* --------------------------------------------------------------- circuits */
+/* Uploads a layered circuit: layer i has 2^bit_length[i] gates given as
+ * ty[i][g] (gate type 0..13), u[i][g], v[i][g] (host arrays, the fields of
+ * `gate`, circuit_fast_track.h:6-14).  Layer 0 is the input layer (its u is
+ * the input value, read through int as zk_prover::evaluate does,
+ * zk_prover.cpp:57-66).  Mirrors layered_circuit after
+ * zk_verifier::read_circuit (zk_verifier.cpp:15-217). */
+int vg_circuit_upload(vg_ctx *ctx, int depth, const int *bit_length,
+                      const uint8_t *const *ty, const int64_t *const *u, const int64_t *const *v,
+                      vg_circuit **out);
+int vg_circuit_destroy(vg_circuit *c);
+int vg_circuit_depth(const vg_circuit *c, int *depth);
+
+/* ------------------------------------------------------------------- GKR */
+/* State for proving one circuit; buffers are sized for its widest layer
+ * (zk_prover::init_array, zk_prover.cpp:337-350). */
+int vg_gkr_create(vg_ctx *ctx, const vg_circuit *c, vg_gkr **out);
+int vg_gkr_destroy(vg_gkr *g);
+/* All layer values (zk_prover::evaluate, zk_prover.cpp:54-157). */
+int vg_gkr_evaluate(vg_gkr *g);
+/* Device pointer to the 2^bit_length values of a layer (after evaluate). */
+int vg_gkr_layer_values(vg_gkr *g, int layer, const vg_fe **dev_values);
+/* Multilinear extension of the output layer at r (r_len = its bit length)
+ * (zk_prover::V_res, zk_prover.cpp:30-52).  r host, out host. */
+int vg_gkr_v_res(vg_gkr *g, const vg_fe *r, int r_len, vg_fe *out);
+/* Multilinear extension of vals (any, 2^log_n entries) at r (host, log_n
+ * entries; bit b of the index pairs with r[b]), the fold of V_res
+ * (zk_prover.cpp:37-44).  out host. */
+int vg_mle_eval(vg_ctx *ctx, const vg_fe *vals, long n, const vg_fe *r, int log_n, vg_fe *out);
+/* Phase-1 bookkeeping of layer `layer` (zk_prover::sumcheck_phase1_init,
+ * zk_prover.cpp:375-592): beta_g = alpha*eq(r0,g) + beta*eq(r1,g) over
+ * length_g bits, then the gate scatter into add_mult_sum / addV_array by u.
+ * r0, r1 host (length_g entries). */
+int vg_gkr_phase1_init(vg_gkr *g, int layer, const vg_fe *r0, const vg_fe *r1, int length_g,
+                       vg_fe alpha, vg_fe beta);
+/* Phase-2 bookkeeping (zk_prover::sumcheck_phase2_init, zk_prover.cpp:789-972):
+ * scatter by v with beta_g * eq(r_u, u) and the claimed value v_u.
+ * r_u host (length_u entries). */
+int vg_gkr_phase2_init(vg_gkr *g, const vg_fe *r_u, int length_u, vg_fe v_u);
+/* One sumcheck round over the three bookkeeping tables (the array loop of
+ * sumcheck_phase{1,2}_update[lastbit], zk_prover.cpp:600-633, 684-717,
+ * 992-1025, 1075-1108): folds the tables with previous_random (unless
+ * current_bit == 0), returns the round sums (a, b, c) before the mask terms
+ * in out3, and, when two entries remain, the folded tables in last6 as
+ * {V[0], V[1], addV[0], addV[1], add_mult[0], add_mult[1]} (may be NULL).
+ * out3, last6 host. */
+int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, vg_fe *out3, vg_fe *last6);
+
+/* ------------------------------------------------ polynomial commitment */
+int vg_pc_create(vg_ctx *ctx, vg_pc **out);
+int vg_pc_destroy(vg_pc *pc);
+/* poly_commit_prover::commit_private_array (poly_commit.h:42-116): RS-encodes
+ * 64 slices of the private array (any, 2^log_len entries) and the mask (host,
+ * n_mask entries, zero-padded to the next power of two M that divides the
+ * slice evenly) at rate 1/32 into l_eval (65 slices of S = 2^(log_len-1)).
+ * *mask_len (host, may be NULL) receives M. */
+int vg_pc_encode_private(vg_pc *pc, const vg_fe *priv, int log_len, const vg_fe *mask, long n_mask, long *mask_len);
+/* poly_commit_prover::commit_public_array (poly_commit.h:125-342): RS-encodes
+ * the public array (any, 2^log_len) and the public mask (host, n_mask <= M,
+ * zero-padded to M), forms l*q, divides out the vanishing polynomial (h) and
+ * builds the virtual oracle.  all_sum (host, 65 entries) is written;
+ * *inner_product (host, may be NULL) receives <l, q> + <mask_l, mask_q> over
+ * the committed points, the value the reference asserts equal to target_sum
+ * (poly_commit.h:179-193). */
+int vg_pc_encode_public(vg_pc *pc, const vg_fe *pub, const vg_fe *pub_mask, long n_mask, vg_fe *all_sum,
+                        vg_fe *inner_product);
+/* fri::request_init_commit (fri.cpp:36-139): leaf hash chains and Merkle tree
+ * of oracle 0 (l_eval) or 1 (h_eval); *root host. */
+int vg_pc_init_commit(vg_pc *pc, int oracle, vg_digest *root);
+/* Public array eq(r, .) over log_len bits: pub[x] = prod_b (x_b ? r_b : 1 - r_b),
+ * the table the reference verifier builds with dfs_for_public_eval
+ * (zk_verifier.cpp:838-847).  r host, pub dev (2^log_len entries). */
+int vg_eq_table(vg_ctx *ctx, const vg_fe *r, int log_len, vg_fe *pub);
+/* fri::commit_phase_step (fri.cpp:291-430): folds the current codeword set
+ * with r, hashes the new leaf chains and Merkle tree; root host. */
+int vg_pc_fri_step(vg_pc *pc, vg_fe r, vg_digest *root);
+/* fri::commit_phase_final (fri.cpp:432-438): the last folded codeword set in
+ * the reference's interleaved layout, data[(j << 7) | (s << 1) | b] and
+ * mask[2j + b] for j < n/2 (n = final per-slice length), host.  n host. */
+int vg_pc_fri_final(vg_pc *pc, vg_fe *data, vg_fe *mask, long *n);
+/* fri::request_init_value_with_merkle (fri.cpp:148-201) without the proof-size
+ * bookkeeping: the 65 value pairs at (pow0, pow0 + S/2) of oracle 0 (l) or 1 (h)
+ * and the authentication path (path[0..depth-1] siblings bottom-up,
+ * path[depth] the leaf; depth = log_len - 2).  values (130 entries) and path
+ * (depth + 1 entries) host. */
+int vg_pc_query_init(vg_pc *pc, long pow0, int oracle, vg_fe *values, vg_digest *path);
+/* fri::request_step_commit (fri.cpp:227-289) without the proof-size
+ * bookkeeping: the 65 value pairs of FRI level lvl at position pow and its
+ * authentication path (siblings bottom-up, then the leaf). host. */
+int vg_pc_query_step(vg_pc *pc, int lvl, long pow, vg_fe *values, vg_digest *path, int *path_len);
+/* Sizes of the current commitment: log_len, slice size S, FRI levels so far. */
+int vg_pc_info(vg_pc *pc, int *log_len, long *slice_size, int *levels);
+
+/* ------------------------------------------------------------ whole proofs */
+/* A session holds one circuit on the device and proves it on request.  Each
+ * proof replays the reference verifier's challenge draws (glibc rand() after
+ * srand(seed), zk_verifier.cpp:910-1253, vpd_verifier.cpp:80-312) and calls
+ * the prover in the verifier's order, so the messages, roots and query
+ * answers equal those of the reference prover run by the reference verifier
+ * with that seed (the fft_gkr side proof is not part of it). */
+typedef struct vg_session vg_session;
+typedef struct {
+    double evaluate_s, gkr_s, commit_s, fri_s, query_s, total_s;   /* wall time per stage */
+    double prove_time;      /* zk_prover::total_time + poly_commit_prover::total_time */
+    long long proof_size;   /* bytes by the reference's accounting, without fft_gkr */
+    long long launches;     /* kernels launched for this proof */
+} vg_proof_stats;
+/* From file-level layers as in the circuit text format (src/linear_gkr/README.md):
+ * d layers, the input layer first (types 2/3, u = value), layer i has n[i]
+ * gates ty[i][g], u[i][g], v[i][g] (host).  The input layer is padded and a
+ * relay layer inserted as zk_verifier::read_circuit does
+ * (zk_verifier.cpp:24-191). */
+int vg_session_create(int d, const long *n, const uint8_t *const *ty, const int64_t *const *u,
+                      const int64_t *const *v, vg_session **out);
+/* Reads the circuit text format. */
+int vg_session_from_file(const char *circuit_path, vg_session **out);
+int vg_session_destroy(vg_session *s);
+/* depth of the prover's circuit (file layers + 1) and log2 of the padded input */
+int vg_session_depth(vg_session *s, int *depth, int *input_log);
+/* One proof.  With want_transcript, *transcript (free with vg_free) receives
+ * the records: tag byte, uint32 count of 16-byte units, the units. */
+int vg_session_prove(vg_session *s, unsigned seed, int want_transcript, vg_proof_stats *stats,
+                     uint8_t **transcript, size_t *transcript_len);
+void vg_free(void *p);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,130 @@
+"""Generates the golden fixtures in this directory from the reference itself.
+
+Run in a container where the reference sources are present:
+    make -C oracle ref && python tests/golden/make_golden.py
+It runs the reference prover + verifier (oracle/_ref/zk_proof_ref, compiled
+from the reference's own sources with the transcript recorder wrapped around
+every prover entry point) on seeded synthetic circuits, and single reference
+routines (oracle/_ref/libvirgo_refkern.so) on seeded inputs, and writes:
+  transcripts.json  per case: circuit generator and parameters, prover seed,
+                    the number of records, a digest of all prover records,
+                    the tag and a short SHA-256 of every record, and the raw
+                    records of the first GKR layer (hex)
+  kernels.json      FFT / inverse FFT outputs, Merkle roots and hashes
+"""
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+from virgo_b200 import circuits, transcript  # noqa: E402
+
+REF = os.path.join(ROOT, "oracle", "_ref")
+P = (1 << 61) - 1
+
+CASES = [
+    # name, generator, params, prover seed
+    ("matmul16_seed1", "matmul_addtree", {"n": 16, "bits": 16, "seed": 1}, 1),
+    ("matmul16_seed7", "matmul_addtree", {"n": 16, "bits": 16, "seed": 2}, 7),
+    ("mixed_gates", "mixed_gates", {"seed": 3}, 5),
+    ("random_5layer", "random_layered", {"log_widths": [10, 12, 11, 12, 9], "seed": 4}, 11),
+    ("random_3layer_pad15", "random_layered", {"log_widths": [8, 9, 8], "seed": 5}, 3),
+    ("matmul8_32bit", "matmul_addtree", {"n": 8, "bits": 32, "seed": 6}, 2),
+]
+
+
+def make_circuit(gen, params):
+    return getattr(circuits, gen)(**params)
+
+
+def run_ref(layers, seed, workdir):
+    c, m = os.path.join(workdir, "c.txt"), os.path.join(workdir, "m.txt")
+    circuits.write_text(layers, c, m)
+    fft = os.path.join(workdir, "fft_gkr")
+    if not os.path.exists(fft):
+        os.symlink(os.path.join(REF, "fft_gkr"), fft)
+    tr = os.path.join(workdir, "tr.bin")
+    out = subprocess.run([os.path.join(REF, "zk_proof_ref"), c, m, os.path.join(workdir, "r.txt"), str(seed), tr],
+                         cwd=workdir, capture_output=True, text=True)
+    assert out.returncode == 0 and "Pass" in out.stdout, out.stdout[-500:] + out.stderr[-500:]
+    return transcript.read(tr)
+
+
+def transcripts():
+    res = []
+    for name, gen, params, seed in CASES:
+        with tempfile.TemporaryDirectory() as d:
+            recs = run_ref(make_circuit(gen, params), seed, d)
+        pr = transcript.prover_records(recs)
+        first_layer = []
+        for tag, data in pr[1:]:
+            first_layer.append([tag, data.hex()])
+            if tag == "h":
+                break
+        res.append({
+            "name": name, "generator": gen, "params": params, "seed": seed,
+            "n_records": len(pr), "digest": transcript.digest(pr),
+            "records": [[t, h] for t, h in transcript.record_hashes(pr)],
+            "v_res": pr[0][1].hex(), "first_layer": first_layer,
+            "verdict": [recs[-1][0], recs[-1][1].hex()],
+        })
+        print(name, len(pr), res[-1]["digest"][:16])
+    return res
+
+
+def fe_random(seed, n):
+    """Seeded canonical field elements, shape (n, 2) as (img, real)."""
+    rng = np.random.default_rng(seed)
+    a = np.empty((n, 2), dtype=np.uint64)
+    a[:, 0] = rng.integers(0, P, n, dtype=np.uint64)
+    a[:, 1] = rng.integers(0, P, n, dtype=np.uint64)
+    return a
+
+
+def kernels():
+    """Inputs are regenerated from their seeds by the tests (fe_random, or
+    numpy default_rng bytes); outputs are stored whole when small and as a
+    SHA-256 otherwise."""
+    import hashlib
+    L = ctypes.CDLL(os.path.join(REF, "libvirgo_refkern.so"))
+    L.ref_init()
+    out = {"fft": [], "ifft": [], "tree": [], "hash": []}
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    keep = lambda a: a.tobytes().hex() if a.nbytes <= 4096 else "sha256:" + hashlib.sha256(a.tobytes()).hexdigest()  # noqa: E731
+    for k, (lc, lo) in enumerate([(0, 3), (1, 1), (3, 3), (3, 6), (5, 9), (9, 9), (6, 12), (11, 11), (10, 15)]):
+        co = fe_random(1000 + k, 1 << lc)
+        r = np.zeros((1 << lo, 2), np.uint64)
+        L.ref_fft(vp(co), 1 << lc, 1 << lo, lo, vp(r))
+        out["fft"].append({"coef_len": 1 << lc, "order": 1 << lo, "seed": 1000 + k, "output": keep(r)})
+        ev = fe_random(2000 + k, 1 << lo)
+        ri = np.zeros((1 << lc, 2), np.uint64)
+        L.ref_ifft(vp(ev), 1 << lc, 1 << lo, lo, vp(ri))
+        out["ifft"].append({"coef_len": 1 << lc, "order": 1 << lo, "seed": 2000 + k, "output": keep(ri)})
+    for k, n in enumerate([1, 2, 3, 5, 64, 100, 1000]):
+        lv = np.random.default_rng(3000 + k).integers(0, 256, (n, 32), dtype=np.uint8)
+        sz = 1
+        while sz < n:
+            sz *= 2
+        t = np.zeros((2 * sz, 32), np.uint8)
+        L.ref_create_tree(vp(lv), n, vp(t))
+        out["tree"].append({"n": n, "seed": 3000 + k, "root": t[1].tobytes().hex(), "tree": keep(t[1:])})
+    for k in range(8):
+        m = np.random.default_rng(4000 + k).integers(0, 256, 64, dtype=np.uint8)
+        d = np.zeros(32, np.uint8)
+        L.ref_hash64(vp(m), vp(d))
+        out["hash"].append({"seed": 4000 + k, "sha3_256": d.tobytes().hex()})
+    return out
+
+
+if __name__ == "__main__":
+    here = os.path.dirname(os.path.abspath(__file__))
+    with open(os.path.join(here, "kernels.json"), "w") as f:
+        json.dump(kernels(), f)
+    with open(os.path.join(here, "transcripts.json"), "w") as f:
+        json.dump(transcripts(), f, indent=0)

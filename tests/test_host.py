@@ -1,0 +1,117 @@
+"""Host-side checks that need no GPU: the library builds and exports the C
+ABI, fails loudly without a device, the circuit generators and transcript
+format, and glibc's rand stream reproduction."""
+import ctypes
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+import virgo_b200 as vb
+from virgo_b200 import circuits, transcript
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+@pytest.fixture(scope="module")
+def built():
+    if not os.path.exists(vb.LIB_PATH):
+        subprocess.run(["make", "-C", os.path.join(ROOT, "virgo_b200"), "-j8"], check=True, capture_output=True)
+    return vb.lib()
+
+
+def test_library_exports_every_declared_function(built):
+    names = vb.header_functions()
+    assert len(names) > 30
+    missing = [n for n in names if not hasattr(built, n)]
+    assert not missing, missing
+
+
+def test_no_device_fails_loudly(built):
+    try:
+        import torch
+        if torch.cuda.is_available():
+            pytest.skip("a GPU is present")
+    except ImportError:
+        pass
+    h = ctypes.c_void_p()
+    rc = built.vg_ctx_create(0, ctypes.byref(h))
+    assert rc == 4   # VG_ERR_NO_DEVICE: no CPU fallback exists
+    assert b"CUDA" in built.vg_last_error() or b"device" in built.vg_last_error()
+
+
+def test_matmul_generator_shapes():
+    L = circuits.matmul_addtree(4, 16, seed=0)
+    assert [len(t) for t, _, _ in L] == [32, 64, 32, 16]
+    ty, u, v = L[1]
+    # gate (i, j, k) multiplies A[i][k] and B[k][j]
+    g = (1 * 4 + 2) * 4 + 3
+    assert ty[g] == 1 and u[g] == 1 * 4 + 3 and v[g] == 16 + 3 * 4 + 2
+    ty, u, v = L[2]
+    assert (u == 2 * np.arange(32)).all() and (v == u + 1).all() and (ty == 0).all()
+    assert circuits.total_gates(circuits.matmul_addtree(256, 32, 1)) == 2 * 65536 + sum(1 << k for k in range(16, 25))
+
+
+def test_random_layered_wires_in_range():
+    L = circuits.random_layered([6, 8, 5, 7], seed=3)
+    prev = 64
+    for ty, u, v in L[1:]:
+        assert set(np.unique(ty)) <= {0, 1}
+        assert u.max() < prev and v.max() < prev and u.min() >= 0
+        prev = len(ty)
+
+
+def test_text_format_roundtrip(tmp_path):
+    L = circuits.mixed_gates(9, log_width=4)
+    c, m = str(tmp_path / "c.txt"), str(tmp_path / "m.txt")
+    circuits.write_text(L, c, m)
+    toks = open(c).read().split()
+    d = int(toks[0])
+    assert d == len(L)
+    pos = 1
+    for ty, u, v in L:
+        n = int(toks[pos])
+        rows = np.array(toks[pos + 1:pos + 1 + 4 * n], dtype=np.int64).reshape(n, 4)
+        assert (rows[:, 0] == ty).all() and (rows[:, 1] == np.arange(n)).all()
+        assert (rows[:, 2] == u).all() and (rows[:, 3] == v).all()
+        pos += 1 + 4 * n
+    assert open(m).read().count("0 0 1 0 0") == d
+
+
+def test_transcript_parse_roundtrip():
+    blob = b"R" + (1).to_bytes(4, "little") + bytes(range(16)) + b"C" + (2).to_bytes(4, "little") + bytes(32)
+    recs = transcript.parse(blob)
+    assert [t for t, _ in recs] == ["R", "C"] and len(recs[1][1]) == 32
+    assert transcript.first_difference(recs, recs) is None
+
+
+def test_golden_transcripts_are_consistent():
+    with open(os.path.join(ROOT, "tests", "golden", "transcripts.json")) as f:
+        cases = json.load(f)
+    assert len(cases) >= 5
+    for c in cases:
+        tags = [t for t, _ in c["records"]]
+        assert tags[0] == "R" and tags.count("C") == 2 and "X" in tags
+        assert c["verdict"][0] == "V"
+        # 33 query repetitions, each: two init answers (l, h) and L-6 step answers
+        assert tags.count("I") == 66
+
+
+def test_glibc_random_r_reproduces_rand():
+    """Per-proof random streams (initstate_r + random_r with a 128-byte state)
+    reproduce srand(seed)/rand(), the stream the reference draws from."""
+    libc = ctypes.CDLL(None)
+    for seed in [1, 7, 123456]:
+        libc.srand(seed)
+        a = [libc.rand() for _ in range(1000)]
+        buf = ctypes.create_string_buffer(64)
+        state = ctypes.create_string_buffer(128)
+        assert libc.initstate_r(ctypes.c_uint(seed), state, ctypes.c_size_t(128), buf) == 0
+        out = ctypes.c_int32()
+        b = []
+        for _ in range(1000):
+            libc.random_r(buf, ctypes.byref(out))
+            b.append(out.value)
+        assert a == b

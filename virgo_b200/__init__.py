@@ -1,0 +1,234 @@
+"""virgo_b200: B200-native Virgo prover hot path.
+
+The product is the shared library lib/libvirgo_b200.so (CUDA kernels for
+sm_100a behind the C ABI of include/virgo_b200.h, plus the drop-in C++ prover
+classes).  This module binds the C ABI with ctypes for tests, benchmarks and
+Python callers.  There is no CPU fallback: if the library or a CUDA device is
+missing, every call raises.
+
+Field elements are numpy uint64 arrays of shape (n, 2) holding (img, real),
+the memory layout of the reference's prime_field::field_element.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libvirgo_b200.so")
+HEADER = os.path.join(os.path.dirname(_HERE), "include", "virgo_b200.h")
+P = (1 << 61) - 1
+
+_lib = None
+
+
+class VirgoError(RuntimeError):
+    pass
+
+
+class vg_fe(ctypes.Structure):
+    _fields_ = [("img", ctypes.c_uint64), ("real", ctypes.c_uint64)]
+
+
+class vg_proof_stats(ctypes.Structure):
+    _fields_ = [
+        ("evaluate_s", ctypes.c_double), ("gkr_s", ctypes.c_double), ("commit_s", ctypes.c_double),
+        ("fri_s", ctypes.c_double), ("query_s", ctypes.c_double), ("total_s", ctypes.c_double),
+        ("prove_time", ctypes.c_double), ("proof_size", ctypes.c_longlong), ("launches", ctypes.c_longlong),
+    ]
+
+
+def lib():
+    """Loads the library (raises VirgoError when it has not been built)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise VirgoError("libvirgo_b200.so not built: run `make -C virgo_b200` (or __graft_entry__.build())")
+        L = ctypes.CDLL(LIB_PATH)
+        c_p, c_i, c_l, c_sz = ctypes.c_void_p, ctypes.c_int, ctypes.c_long, ctypes.c_size_t
+        sig = {
+            "vg_last_error": (ctypes.c_char_p, []),
+            "vg_ctx_create": (c_i, [c_i, ctypes.POINTER(c_p)]),
+            "vg_ctx_destroy": (c_i, [c_p]),
+            "vg_ctx_set_hash": (c_i, [c_p, c_i]),
+            "vg_ctx_sync": (c_i, [c_p]),
+            "vg_ctx_launch_count": (c_i, [c_p, ctypes.POINTER(ctypes.c_longlong)]),
+            "vg_dev_alloc": (c_i, [c_p, c_sz, ctypes.POINTER(c_p)]),
+            "vg_dev_free": (c_i, [c_p, c_p]),
+            "vg_h2d": (c_i, [c_p, c_p, c_p, c_sz]),
+            "vg_d2h": (c_i, [c_p, c_p, c_p, c_sz]),
+            "vg_fe_binop": (c_i, [c_p, c_i, c_p, c_p, c_p, c_l]),
+            "vg_ntt": (c_i, [c_p, c_p, c_l, c_l, c_p, c_i, c_l, c_i, vg_fe, c_i]),
+            "vg_hash64": (c_i, [c_p, c_p, c_p, c_l]),
+            "vg_merkle_tree": (c_i, [c_p, c_p, c_l, c_p]),
+            "vg_leaf_chain": (c_i, [c_p, c_p, c_i, c_l, c_p]),
+            "vg_circuit_upload": (c_i, [c_p, c_i, c_p, c_p, c_p, c_p, ctypes.POINTER(c_p)]),
+            "vg_circuit_destroy": (c_i, [c_p]),
+            "vg_gkr_create": (c_i, [c_p, c_p, ctypes.POINTER(c_p)]),
+            "vg_gkr_destroy": (c_i, [c_p]),
+            "vg_gkr_evaluate": (c_i, [c_p]),
+            "vg_gkr_layer_values": (c_i, [c_p, c_i, ctypes.POINTER(c_p)]),
+            "vg_gkr_v_res": (c_i, [c_p, c_p, c_i, c_p]),
+            "vg_mle_eval": (c_i, [c_p, c_p, c_l, c_p, c_i, c_p]),
+            "vg_gkr_phase1_init": (c_i, [c_p, c_i, c_p, c_p, c_i, vg_fe, vg_fe]),
+            "vg_gkr_phase2_init": (c_i, [c_p, c_p, c_i, vg_fe]),
+            "vg_gkr_round": (c_i, [c_p, vg_fe, c_i, c_p, c_p]),
+            "vg_pc_create": (c_i, [c_p, ctypes.POINTER(c_p)]),
+            "vg_pc_destroy": (c_i, [c_p]),
+            "vg_pc_encode_private": (c_i, [c_p, c_p, c_i, c_p, c_l, ctypes.POINTER(c_l)]),
+            "vg_pc_encode_public": (c_i, [c_p, c_p, c_p, c_l, c_p, c_p]),
+            "vg_pc_init_commit": (c_i, [c_p, c_i, c_p]),
+            "vg_eq_table": (c_i, [c_p, c_p, c_i, c_p]),
+            "vg_pc_fri_step": (c_i, [c_p, vg_fe, c_p]),
+            "vg_pc_fri_final": (c_i, [c_p, c_p, c_p, ctypes.POINTER(c_l)]),
+            "vg_pc_query_init": (c_i, [c_p, c_l, c_i, c_p, c_p]),
+            "vg_pc_query_step": (c_i, [c_p, c_i, c_l, c_p, c_p, ctypes.POINTER(c_i)]),
+            "vg_pc_info": (c_i, [c_p, ctypes.POINTER(c_i), ctypes.POINTER(c_l), ctypes.POINTER(c_i)]),
+            "vg_session_create": (c_i, [c_i, c_p, c_p, c_p, c_p, ctypes.POINTER(c_p)]),
+            "vg_session_from_file": (c_i, [ctypes.c_char_p, ctypes.POINTER(c_p)]),
+            "vg_session_destroy": (c_i, [c_p]),
+            "vg_session_depth": (c_i, [c_p, ctypes.POINTER(c_i), ctypes.POINTER(c_i)]),
+            "vg_session_prove": (c_i, [c_p, ctypes.c_uint, c_i, ctypes.POINTER(vg_proof_stats),
+                                       ctypes.POINTER(c_p), ctypes.POINTER(c_sz)]),
+            "vg_free": (None, [c_p]),
+        }
+        for name, (res, args) in sig.items():
+            f = getattr(L, name)
+            f.restype = res
+            f.argtypes = args
+        _lib = L
+    return _lib
+
+
+def check(rc: int, what: str = ""):
+    if rc != 0:
+        msg = lib().vg_last_error().decode(errors="replace")
+        raise VirgoError("%s failed (%d): %s" % (what, rc, msg))
+
+
+def fe_array(n: int) -> np.ndarray:
+    return np.zeros((n, 2), dtype=np.uint64)
+
+
+def to_fe(x) -> vg_fe:
+    """(img, real) pair or numpy row -> vg_fe"""
+    return vg_fe(int(x[0]), int(x[1]))
+
+
+def ptr(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class DeviceBuffer:
+    def __init__(self, ctx: "Context", nbytes: int):
+        self.ctx = ctx
+        self.nbytes = nbytes
+        p = ctypes.c_void_p()
+        check(lib().vg_dev_alloc(ctx.h, nbytes, ctypes.byref(p)), "vg_dev_alloc")
+        self.p = p
+
+    def upload(self, arr: np.ndarray):
+        arr = np.ascontiguousarray(arr)
+        assert arr.nbytes <= self.nbytes
+        check(lib().vg_h2d(self.ctx.h, self.p, ptr(arr), arr.nbytes), "vg_h2d")
+
+    def download(self, arr: np.ndarray):
+        check(lib().vg_d2h(self.ctx.h, ptr(arr), self.p, arr.nbytes), "vg_d2h")
+        return arr
+
+    def free(self):
+        if self.p:
+            lib().vg_dev_free(self.ctx.h, self.p)
+            self.p = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Context:
+    """A device context (vg_ctx): one CUDA stream plus caches."""
+
+    def __init__(self, device: int = 0, hash_kind: int = 0):
+        h = ctypes.c_void_p()
+        check(lib().vg_ctx_create(device, ctypes.byref(h)), "vg_ctx_create")
+        self.h = h
+        check(lib().vg_ctx_set_hash(h, hash_kind), "vg_ctx_set_hash")
+
+    def close(self):
+        if self.h:
+            lib().vg_ctx_destroy(self.h)
+            self.h = None
+
+    def buffer(self, arr_or_nbytes) -> DeviceBuffer:
+        if isinstance(arr_or_nbytes, np.ndarray):
+            b = DeviceBuffer(self, max(16, arr_or_nbytes.nbytes))
+            b.upload(arr_or_nbytes)
+            return b
+        return DeviceBuffer(self, max(16, int(arr_or_nbytes)))
+
+    def sync(self):
+        check(lib().vg_ctx_sync(self.h), "vg_ctx_sync")
+
+    def launches(self) -> int:
+        c = ctypes.c_longlong()
+        check(lib().vg_ctx_launch_count(self.h, ctypes.byref(c)), "vg_ctx_launch_count")
+        return c.value
+
+
+class Session:
+    """One circuit resident on the GPU (default context of the drop-in
+    classes); prove() runs a whole proof for a seed."""
+
+    def __init__(self, layers=None, circuit_path: str | None = None):
+        h = ctypes.c_void_p()
+        if circuit_path is not None:
+            check(lib().vg_session_from_file(circuit_path.encode(), ctypes.byref(h)), "vg_session_from_file")
+        else:
+            d = len(layers)
+            ns = np.array([len(t) for t, _, _ in layers], dtype=np.int64)
+            self._keep = []
+            tys = (ctypes.c_void_p * d)()
+            us = (ctypes.c_void_p * d)()
+            vs = (ctypes.c_void_p * d)()
+            for i, (t, u, v) in enumerate(layers):
+                t = np.ascontiguousarray(t, dtype=np.uint8)
+                u = np.ascontiguousarray(u, dtype=np.int64)
+                v = np.ascontiguousarray(v, dtype=np.int64)
+                self._keep += [t, u, v]
+                tys[i], us[i], vs[i] = t.ctypes.data, u.ctypes.data, v.ctypes.data
+            self._keep.append(ns)
+            check(lib().vg_session_create(d, ptr(ns), tys, us, vs, ctypes.byref(h)), "vg_session_create")
+        self.h = h
+
+    def depth(self):
+        d, li = ctypes.c_int(), ctypes.c_int()
+        check(lib().vg_session_depth(self.h, ctypes.byref(d), ctypes.byref(li)), "vg_session_depth")
+        return d.value, li.value
+
+    def prove(self, seed: int, transcript: bool = True):
+        st = vg_proof_stats()
+        buf = ctypes.c_void_p()
+        n = ctypes.c_size_t()
+        check(lib().vg_session_prove(self.h, seed, 1 if transcript else 0, ctypes.byref(st), ctypes.byref(buf),
+                                     ctypes.byref(n)), "vg_session_prove")
+        data = ctypes.string_at(buf, n.value) if (transcript and n.value) else b""
+        lib().vg_free(buf)
+        return st, data
+
+    def close(self):
+        if self.h:
+            lib().vg_session_destroy(self.h)
+            self.h = None
+
+
+def header_functions(path: str = HEADER) -> list:
+    """Names of the functions declared in include/virgo_b200.h."""
+    import re
+    src = open(path).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(vg_[a-z0-9_]+)\s*\(", src)))

@@ -1,0 +1,119 @@
+"""Seeded synthetic layered circuits in the reference's text format.
+
+A circuit is a list of file-level layers, input layer first; each layer is a
+tuple (ty, u, v) of numpy arrays (uint8, int64, int64) with one entry per gate.
+The input layer has type 3 gates whose u is the input value.  The text format
+is the one of the reference's src/linear_gkr/README.md; the meta file holds
+one "is_parallel block_size repeat_num log_block_size log_repeat_num" line per
+layer, written as "0 0 1 0 0" (no data-parallel blocks), like the reference's
+tests/matmul/gen.cpp.
+
+Generators:
+  matmul_addtree(n, bits, seed)  n x n matrix product: n^3 product gates, then
+                                 log2(n) layers of pairwise add gates (the
+                                 matmul circuits of the benchmark configs)
+  random_layered(log_widths, seed, p_mult)  random add/mult layers with wires
+                                 uniform over the previous layer
+  mixed_gates(seed)              small circuit with every interior gate type
+"""
+from __future__ import annotations
+
+import numpy as np
+
+Layer = tuple  # (ty: uint8[n], u: int64[n], v: int64[n])
+
+
+def matmul_addtree(n: int, bits: int, seed: int) -> list:
+    assert n >= 2 and n & (n - 1) == 0
+    rng = np.random.default_rng(seed)
+    a = rng.integers(0, 1 << bits, size=n * n, dtype=np.int64)
+    b = rng.integers(0, 1 << bits, size=n * n, dtype=np.int64)
+    vals = np.concatenate([a, b])
+    layers = [(np.full(2 * n * n, 3, np.uint8), vals, np.zeros(2 * n * n, np.int64))]
+    i, j, k = np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing="ij")
+    # product gate (i, j, k) at g = (i n + j) n + k multiplies A[i][k] by B[k][j]
+    u = (i * n + k).ravel().astype(np.int64)
+    v = (n * n + k * n + j).ravel().astype(np.int64)
+    layers.append((np.ones(n ** 3, np.uint8), u, v))
+    width = n ** 3
+    while width > n * n:
+        width //= 2
+        g = np.arange(width, dtype=np.int64)
+        layers.append((np.zeros(width, np.uint8), 2 * g, 2 * g + 1))
+    return layers
+
+
+def random_layered(log_widths: list, seed: int, p_mult: float = 0.5, input_bits: int = 31) -> list:
+    """log_widths[0] is the input layer; every other layer draws its gates
+    add/mult with probability p_mult of mult and wires uniform over the
+    previous layer."""
+    rng = np.random.default_rng(seed)
+    n0 = 1 << log_widths[0]
+    vals = rng.integers(0, 1 << input_bits, size=n0, dtype=np.int64)
+    layers = [(np.full(n0, 3, np.uint8), vals, np.zeros(n0, np.int64))]
+    prev = n0
+    for lw in log_widths[1:]:
+        n = 1 << lw
+        ty = (rng.random(n) < p_mult).astype(np.uint8)
+        u = rng.integers(0, prev, size=n, dtype=np.int64)
+        v = rng.integers(0, prev, size=n, dtype=np.int64)
+        layers.append((ty, u, v))
+        prev = n
+    return layers
+
+
+def mixed_gates(seed: int, log_width: int = 6) -> list:
+    """Every gate type the reference proves in interior layers (0-2, 5-10,
+    12, 13; type 3 constants are only evaluated, zk_prover.cpp:581-584 has no
+    bookkeeping for them, and 4 is inserted by the reader) in each layer."""
+    rng = np.random.default_rng(seed)
+    n = 1 << log_width
+    vals = rng.integers(0, 1 << 20, size=n, dtype=np.int64)
+    vals[0] = -5  # negative input exercises the int truncation of evaluate()
+    layers = [(np.full(n, 3, np.uint8), vals, np.zeros(n, np.int64))]
+    types = [0, 1, 2, 5, 6, 7, 8, 9, 10, 12, 13]
+    prev = n
+    for _layer in range(3):
+        ty = np.array([types[g % len(types)] for g in range(n)], np.uint8)
+        u = rng.integers(0, prev, size=n, dtype=np.int64)
+        v = rng.integers(0, prev, size=n, dtype=np.int64)
+        for g in range(n):
+            t = ty[g]
+            if t == 2:
+                u[g] = v[g] = 0
+            elif t == 5:
+                lo = int(rng.integers(0, prev - 4))
+                u[g], v[g] = lo, lo + int(rng.integers(1, 4))
+            elif t == 12:
+                lo = int(rng.integers(0, prev - 8))
+                u[g], v[g] = lo, lo + int(rng.integers(0, 7))
+            elif t in (6, 10):
+                v[g] = 0
+            elif t == 13:
+                v[g] = u[g]
+        layers.append((ty, u, v))
+        prev = n
+    return layers
+
+
+def write_text(layers: list, circuit_path: str, meta_path: str) -> None:
+    """Writes the reference text format (one line per layer)."""
+    with open(circuit_path, "w") as f:
+        f.write("%d\n" % len(layers))
+        for ty, u, v in layers:
+            n = len(ty)
+            rows = np.empty((n, 4), dtype=np.int64)
+            rows[:, 0] = ty
+            rows[:, 1] = np.arange(n)
+            rows[:, 2] = u
+            rows[:, 3] = v
+            f.write("%d " % n)
+            f.write(" ".join(map(str, rows.ravel().tolist())))
+            f.write("\n")
+    with open(meta_path, "w") as f:
+        for _ in layers:
+            f.write("0 0 1 0 0\n")
+
+
+def total_gates(layers: list) -> int:
+    return int(sum(len(t) for t, _, _ in layers))

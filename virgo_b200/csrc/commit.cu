@@ -1,0 +1,515 @@
+// Polynomial commitment and FRI commit phase on the device.
+//
+// Data layout in HBM: every codeword set is slice-major, 65 slices (64 data +
+// 1 mask) of the per-slice length n, slice s at base + s * n.  The reference
+// stores the same values interleaved ((j << 7) | (s << 1) | b, fri.cpp:86-96,
+// 345-362); slice-major keeps every kernel's loads coalesced (a warp reads 32
+// consecutive positions of one slice) and the interleaved form is produced
+// only for the small final level the verifier reads.
+//
+// Per commitment of an input of 2^L elements (S = 2^(L-1), R = S/32):
+//   l_eval, h_eval       65 x S      kept for query answers
+//   q_eval, virtual oracle 65 x S    temporaries (freed after use)
+//   FRI level t          65 x S/2^(t+1) codewords + Merkle tree
+#include "common.cuh"
+#include "merkle.cuh"
+#include "hash.cuh"
+#include <cstring>
+
+namespace {
+
+struct FriLevel {
+    fe *cw = nullptr;        // 65 x n
+    long n = 0;
+    uint64_t *tree = nullptr;  // n digests (n/2 leaves)
+};
+
+__device__ __forceinline__ uint64_t halfp(uint64_t x) { return (x & 1) ? ((x + vg::P) >> 1) : (x >> 1); }
+__device__ __forceinline__ fe half_fe(fe x) { return vg::fe_make(halfp(x.real), halfp(x.img)); }
+
+__device__ __forceinline__ fe tw_pow(const fe *__restrict__ lo, const fe *__restrict__ hi, uint64_t e)
+{
+    fe a = lo[e & 4095];
+    uint64_t h = e >> 12;
+    if (h) a = a * hi[h];
+    return a;
+}
+
+// lq[s][j] = l[s][j * stride] * q[s][j * stride], j < 2m (poly_commit.h:211-218, 271-278)
+__global__ void k_lq_sample(const fe *__restrict__ l, const fe *__restrict__ q, long S, long m, long stride,
+                            int nslices, fe *__restrict__ lq)
+{
+    long total = (long)nslices * 2 * m;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        long s = i / (2 * m), j = i % (2 * m);
+        long src = s * S + j * stride;
+        lq[i] = l[src] * q[src];
+    }
+}
+
+// Virtual oracle (poly_commit.h:241-263 mask slice, 298-322 data slices):
+// vo[s][j] = (l q - (x^m - 1) h - c0_s) * m * x^-1 at x = w_S^j, where
+// c0_s = lq_coef[s][0] + lq_coef[s][m] is the constant term of g + h.
+// tw_f/tw_i are the twiddle tables of w_S and w_S^-1.
+__global__ void k_virtual_oracle(const fe *__restrict__ l, const fe *__restrict__ q, const fe *__restrict__ h,
+                                 const fe *__restrict__ lq_coef, long S, long m, int logS, int slice0, int nslices,
+                                 const fe *__restrict__ twf_lo, const fe *__restrict__ twf_hi,
+                                 const fe *__restrict__ twi_lo, const fe *__restrict__ twi_hi, fe *__restrict__ vo)
+{
+    const uint64_t mask = (uint64_t)S - 1;
+    const fe mm = vg::fe_make((uint64_t)m % vg::P, 0);
+    long total = (long)nslices * S;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        long s = i >> logS, j = i & mask;
+        long off = (long)(slice0 + s) * S + j;
+        fe c0 = lq_coef[s * 2 * m] + lq_coef[s * 2 * m + m];
+        fe xm = tw_pow(twf_lo, twf_hi, ((uint64_t)j * (uint64_t)m) & mask);
+        fe g = l[off] * q[off] - (xm - vg::fe_one()) * h[off];
+        fe xinv = tw_pow(twi_lo, twi_hi, (uint64_t)j);
+        vo[off] = ((g - c0) * mm) * xinv;
+    }
+}
+
+// all_sum[s] = (lq_coef[s][0] + lq_coef[s][m]) * m  (poly_commit.h:264, 326)
+__global__ void k_all_sum(const fe *__restrict__ lq_coef, long m, int slice0, int nslices, fe *__restrict__ out)
+{
+    int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= nslices) return;
+    fe c0 = lq_coef[(long)s * 2 * m] + lq_coef[(long)s * 2 * m + m];
+    out[slice0 + s] = c0 * vg::fe_make((uint64_t)m % vg::P, 0);
+}
+
+// sum over data positions (stride 32 in every data slice) and mask positions
+// (stride gap in the mask slice) of l * q  (poly_commit.h:179-193)
+__global__ void k_inner_product(const fe *__restrict__ l, const fe *__restrict__ q, long S, long gap,
+                                fe *__restrict__ parts)
+{
+    __shared__ fe sm[32];
+    const long R = S >> 5;
+    const long n_data = 64 * R, n_mask = S / gap;
+    fe acc[1] = {vg::fe_zero()};
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n_data + n_mask; i += (long)gridDim.x * blockDim.x) {
+        long pos = i < n_data ? (i << 5) : (64 * S + (i - n_data) * gap);
+        acc[0] = acc[0] + l[pos] * q[pos];
+    }
+    block_sum<1>(acc, sm);
+    if (threadIdx.x == 0) parts[blockIdx.x] = acc[0];
+}
+
+// One FRI fold fused with the next level's leaf hash chains.
+// Input codeword set (per-slice length n, domain <w>, w = w_S^(2^t)):
+//   out[s][i] = ((a + b) + r w^-i (a - b)) / 2,  a = c[s][i], b = c[s][i + n/2]
+// (fri.cpp:321-340 data, 367-379 mask).  Thread k < n/4 produces out[s][k] and
+// out[s][k + n/4], which are exactly the pair hashed into leaf k of the new
+// level (fri.cpp:394-420), so the fold output is never re-read.
+template <int KIND>
+__global__ void __launch_bounds__(128) k_fri_fold_leaf(const fe *__restrict__ c, long n, int t, fe r,
+                                                       const fe *__restrict__ twi_lo, const fe *__restrict__ twi_hi,
+                                                       fe *__restrict__ out, uint64_t *__restrict__ leaves)
+{
+    const long q4 = n >> 2, half = n >> 1, nh = n >> 1;
+    long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (k >= q4) return;
+    fe t0 = r * tw_pow(twi_lo, twi_hi, (uint64_t)k << t);
+    fe t1 = r * tw_pow(twi_lo, twi_hi, (uint64_t)(k + q4) << t);
+    uint64_t h[4] = {0, 0, 0, 0};
+    for (int s = 0; s < 65; ++s) {
+        const fe *cs = c + (long)s * n;
+        fe a0 = cs[k], b0 = cs[k + half], a1 = cs[k + q4], b1 = cs[k + q4 + half];
+        fe y0 = half_fe((a0 + b0) + t0 * (a0 - b0));
+        fe y1 = half_fe((a1 + b1) + t1 * (a1 - b1));
+        out[(long)s * nh + k] = y0;
+        out[(long)s * nh + k + q4] = y1;
+        uint64_t w[8] = {y0.img, y0.real, y1.img, y1.real, h[0], h[1], h[2], h[3]};
+        vg::hash64<KIND>(w, h);
+    }
+    ulonglong2 *o = (ulonglong2 *)(leaves + 4 * k);
+    o[0] = make_ulonglong2(h[0], h[1]);
+    o[1] = make_ulonglong2(h[2], h[3]);
+}
+
+// gather of query answers: 65 value pairs at (p, p + n/2) and a tree path
+__global__ void k_gather_query(const fe *__restrict__ cw, long n, long p, const uint64_t *__restrict__ tree,
+                               long leaf_node, int depth, fe *__restrict__ vals, uint64_t *__restrict__ path)
+{
+    int i = threadIdx.x;
+    if (i < 65) {
+        vals[2 * i] = cw[(long)i * n + p];
+        vals[2 * i + 1] = cw[(long)i * n + p + n / 2];
+    }
+    if (i <= depth) {
+        long node = leaf_node;
+        uint64_t src;
+        if (i < depth) {
+            node >>= i;
+            src = (uint64_t)(node ^ 1);
+        } else {
+            src = (uint64_t)leaf_node;
+        }
+        for (int w = 0; w < 4; ++w) path[4 * i + w] = tree[4 * src + w];
+    }
+}
+
+long mask_gap(long S, long n_mask)
+{
+    long gap = S / n_mask, g = 1;
+    while (g * 2 <= gap) g *= 2;
+    return g;
+}
+
+int ilog2l(long x)
+{
+    int k = 0;
+    while ((1L << k) < x) ++k;
+    return k;
+}
+
+}  // namespace
+
+struct vg_pc {
+    vg_ctx *ctx = nullptr;
+    int log_len = 0;
+    long S = 0, R = 0, gap = 0, M = 0;
+    fe *l_eval = nullptr, *h_eval = nullptr, *vo = nullptr;
+    uint64_t *tree_l = nullptr, *tree_h = nullptr;
+    std::vector<FriLevel> levels;
+    bool have_private = false, have_public = false;
+};
+
+static void pc_free(vg_pc *pc)
+{
+    cudaFree(pc->l_eval);
+    cudaFree(pc->h_eval);
+    cudaFree(pc->vo);
+    cudaFree(pc->tree_l);
+    cudaFree(pc->tree_h);
+    for (auto &L : pc->levels) {
+        cudaFree(L.cw);
+        cudaFree(L.tree);
+    }
+    pc->l_eval = pc->h_eval = pc->vo = nullptr;
+    pc->tree_l = pc->tree_h = nullptr;
+    pc->levels.clear();
+    pc->have_private = pc->have_public = false;
+}
+
+static int dalloc(void **p, size_t bytes)
+{
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return vg_fail(VG_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    }
+    return VG_OK;
+}
+
+static fe root_of(int log_order) { return vg::fe_root_of_unity(log_order); }
+static vg_fe to_vg(fe x) { vg_fe r; r.img = x.img; r.real = x.real; return r; }
+
+// RS encoding of `batch` slices of m values (stride m) into length S (stride S):
+// interpolate on <w_m>, evaluate on <w_S>  (poly_commit.h:107-108, 152-153)
+static int rs_encode(vg_ctx *c, const fe *vals, long m, int batch, fe *out, long S, fe *coef_tmp)
+{
+    int lm = ilog2l(m), lS = ilog2l(S);
+    VG_TRY(vg_ntt(c, (const vg_fe *)vals, m, m, (vg_fe *)coef_tmp, lm, m, batch, to_vg(vg::fe_inv(root_of(lm))), 1));
+    VG_TRY(vg_ntt(c, (const vg_fe *)coef_tmp, m, m, (vg_fe *)out, lS, S, batch, to_vg(root_of(lS)), 0));
+    return VG_OK;
+}
+
+static int commit_tree(vg_ctx *c, const fe *cw, long S, uint64_t **tree, vg_digest *root)
+{
+    long nleaves = S >> 1;
+    if (!*tree) VG_TRY(dalloc((void **)tree, 2 * nleaves * 32));
+    VG_TRY(vg_leaf_chain_dev(c, cw, 65, S, *tree + 4 * nleaves));
+    VG_TRY(vg_merkle_build(c, *tree, nleaves));
+    if (root) {
+        VG_CHECK_CUDA(cudaMemcpyAsync(root, *tree + 4, 32, cudaMemcpyDeviceToHost, c->stream));
+        VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    }
+    return VG_OK;
+}
+
+extern "C" int vg_pc_create(vg_ctx *ctx, vg_pc **out)
+{
+    if (!ctx || !out) return vg_fail(VG_ERR_ARG, "vg_pc_create: null argument");
+    vg_pc *pc = new vg_pc();
+    pc->ctx = ctx;
+    *out = pc;
+    return VG_OK;
+}
+
+extern "C" int vg_pc_destroy(vg_pc *pc)
+{
+    if (!pc) return VG_OK;
+    cudaStreamSynchronize(pc->ctx->stream);
+    pc_free(pc);
+    delete pc;
+    return VG_OK;
+}
+
+extern "C" int vg_pc_info(vg_pc *pc, int *log_len, long *slice_size, int *levels)
+{
+    if (!pc) return vg_fail(VG_ERR_ARG, "null pc");
+    if (log_len) *log_len = pc->log_len;
+    if (slice_size) *slice_size = pc->S;
+    if (levels) *levels = (int)pc->levels.size();
+    return VG_OK;
+}
+
+extern "C" int vg_pc_encode_private(vg_pc *pc, const vg_fe *priv, int log_len, const vg_fe *mask, long n_mask,
+                                    long *mask_len)
+{
+    if (!pc || !priv || !mask || n_mask < 1 || log_len < 7 || log_len > 28)
+        return vg_fail(VG_ERR_ARG, "vg_pc_encode_private: bad argument (log_len=%d n_mask=%ld)", log_len, n_mask);
+    vg_ctx *c = pc->ctx;
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    pc_free(pc);
+    pc->log_len = log_len;
+    pc->S = 1L << (log_len - 1);
+    pc->R = pc->S >> 5;
+    if (n_mask > pc->S) return vg_fail(VG_ERR_ARG, "mask longer than a slice (%ld > %ld)", n_mask, pc->S);
+    pc->gap = mask_gap(pc->S, n_mask);
+    pc->M = pc->S / pc->gap;
+    const long S = pc->S, R = pc->R, M = pc->M, N = 1L << log_len;
+
+    VG_TRY(dalloc((void **)&pc->l_eval, 65 * S * sizeof(fe)));
+    const fe *priv_d = (const fe *)priv;
+    fe *staging = nullptr;
+    if (!vg_is_device_ptr(priv)) {
+        VG_TRY(dalloc((void **)&staging, N * sizeof(fe)));
+        VG_CHECK_CUDA(cudaMemcpyAsync(staging, priv, N * sizeof(fe), cudaMemcpyHostToDevice, c->stream));
+        priv_d = staging;
+    }
+    fe *coef;
+    VG_TRY(vg_scratch2(c, 64 * R * sizeof(fe), (void **)&coef));
+    int rc = rs_encode(c, priv_d, R, 64, pc->l_eval, S, coef);
+    // mask slice: padded to M with zeros (poly_commit.h:66-70, 80-88)
+    if (rc == VG_OK) {
+        std::vector<fe> pm(M);
+        for (long i = 0; i < M; ++i) pm[i] = i < n_mask ? vg::fe_make(mask[i].real, mask[i].img) : vg::fe_zero();
+        fe *md = nullptr;
+        rc = dalloc((void **)&md, M * sizeof(fe));
+        if (rc == VG_OK) {
+            cudaMemcpyAsync(md, pm.data(), M * sizeof(fe), cudaMemcpyHostToDevice, c->stream);
+            rc = rs_encode(c, md, M, 1, pc->l_eval + 64 * S, S, coef);
+            cudaStreamSynchronize(c->stream);
+            cudaFree(md);
+        }
+    }
+    if (staging) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(staging);
+    }
+    VG_TRY(rc);
+    if (mask_len) *mask_len = M;
+    pc->have_private = true;
+    return VG_OK;
+}
+
+extern "C" int vg_pc_encode_public(vg_pc *pc, const vg_fe *pub, const vg_fe *pub_mask, long n_mask, vg_fe *all_sum,
+                                   vg_fe *inner_product)
+{
+    if (!pc || !pub || !pub_mask || !all_sum) return vg_fail(VG_ERR_ARG, "vg_pc_encode_public: null argument");
+    if (!pc->have_private) return vg_fail(VG_ERR_STATE, "commit_public before commit_private");
+    if (n_mask > pc->M) return vg_fail(VG_ERR_ARG, "public mask longer than the padded private mask (%ld > %ld)", n_mask, pc->M);
+    vg_ctx *c = pc->ctx;
+    const long S = pc->S, R = pc->R, M = pc->M, N = 1L << pc->log_len;
+    const int logS = ilog2l(S);
+    if (pc->gap == 1) return vg_fail(VG_ERR_ARG, "mask fills the whole slice (mask_position_gap == 1)");
+
+    fe *q_eval = nullptr, *lq = nullptr, *lqc = nullptr;
+    VG_TRY(dalloc((void **)&q_eval, 65 * S * sizeof(fe)));
+    if (!pc->h_eval) VG_TRY(dalloc((void **)&pc->h_eval, 65 * S * sizeof(fe)));
+    if (!pc->vo) VG_TRY(dalloc((void **)&pc->vo, 65 * S * sizeof(fe)));
+    long lq_len = 64 * 2 * R + 2 * M;
+    VG_TRY(dalloc((void **)&lq, lq_len * sizeof(fe)));
+    VG_TRY(dalloc((void **)&lqc, lq_len * sizeof(fe)));
+
+    const fe *pub_d = (const fe *)pub;
+    fe *staging = nullptr;
+    if (!vg_is_device_ptr(pub)) {
+        VG_TRY(dalloc((void **)&staging, N * sizeof(fe)));
+        VG_CHECK_CUDA(cudaMemcpyAsync(staging, pub, N * sizeof(fe), cudaMemcpyHostToDevice, c->stream));
+        pub_d = staging;
+    }
+    fe *coef;
+    VG_TRY(vg_scratch2(c, 64 * R * sizeof(fe), (void **)&coef));
+    VG_TRY(rs_encode(c, pub_d, R, 64, q_eval, S, coef));
+    std::vector<fe> pm(M);
+    for (long i = 0; i < M; ++i) pm[i] = i < n_mask ? vg::fe_make(pub_mask[i].real, pub_mask[i].img) : vg::fe_zero();
+    fe *md;
+    VG_TRY(dalloc((void **)&md, M * sizeof(fe)));
+    VG_CHECK_CUDA(cudaMemcpyAsync(md, pm.data(), M * sizeof(fe), cudaMemcpyHostToDevice, c->stream));
+    VG_TRY(rs_encode(c, md, M, 1, q_eval + 64 * S, S, coef));
+
+    // inner product check value
+    fe *parts;
+    const int nb = 148 * 4;
+    VG_TRY(vg_partials(c, nb + 1 + 65, &parts));   // block partials, <l,q>, all_sum[65]
+    k_inner_product<<<nb, 256, 0, c->stream>>>(pc->l_eval, q_eval, S, pc->gap, parts);
+    VG_LAUNCHED(c);
+    VG_TRY(vg_reduce_partials(c, parts, nb, 1, parts + nb));
+
+    // lq samples, their interpolation and the quotient h
+    fe *lq_m = lq + 64 * 2 * R, *lqc_m = lqc + 64 * 2 * R;
+    k_lq_sample<<<148 * 8, 256, 0, c->stream>>>(pc->l_eval, q_eval, S, R, S / (2 * R), 64, lq);
+    VG_LAUNCHED(c);
+    k_lq_sample<<<grid_for(2 * M, 256), 256, 0, c->stream>>>(pc->l_eval + 64 * S, q_eval + 64 * S, S, M, S / (2 * M), 1, lq_m);
+    VG_LAUNCHED(c);
+    int l2R = ilog2l(2 * R), l2M = ilog2l(2 * M);
+    VG_TRY(vg_ntt(c, (const vg_fe *)lq, 2 * R, 2 * R, (vg_fe *)lqc, l2R, 2 * R, 64, to_vg(vg::fe_inv(root_of(l2R))), 1));
+    VG_TRY(vg_ntt(c, (const vg_fe *)lq_m, 2 * M, 2 * M, (vg_fe *)lqc_m, l2M, 2 * M, 1, to_vg(vg::fe_inv(root_of(l2M))), 1));
+    VG_TRY(vg_ntt(c, (const vg_fe *)(lqc + R), R, 2 * R, (vg_fe *)pc->h_eval, logS, S, 64, to_vg(root_of(logS)), 0));
+    VG_TRY(vg_ntt(c, (const vg_fe *)(lqc_m + M), M, 2 * M, (vg_fe *)(pc->h_eval + 64 * S), logS, S, 1, to_vg(root_of(logS)), 0));
+
+    // virtual oracle and all_sum
+    const fe *tf_lo, *tf_hi, *ti_lo, *ti_hi;
+    VG_TRY(vg_twiddles(c, root_of(logS), logS, &tf_lo, &tf_hi));
+    VG_TRY(vg_twiddles(c, vg::fe_inv(root_of(logS)), logS, &ti_lo, &ti_hi));
+    k_virtual_oracle<<<148 * 16, 256, 0, c->stream>>>(pc->l_eval, q_eval, pc->h_eval, lqc, S, R, logS, 0, 64,
+                                                      tf_lo, tf_hi, ti_lo, ti_hi, pc->vo);
+    VG_LAUNCHED(c);
+    k_virtual_oracle<<<grid_for(S, 256), 256, 0, c->stream>>>(pc->l_eval, q_eval, pc->h_eval, lqc_m, S, M, logS, 64, 1,
+                                                             tf_lo, tf_hi, ti_lo, ti_hi, pc->vo);
+    VG_LAUNCHED(c);
+    fe *sums_d = parts + nb + 1;
+    k_all_sum<<<1, 64, 0, c->stream>>>(lqc, R, 0, 64, sums_d);
+    VG_LAUNCHED(c);
+    k_all_sum<<<1, 1, 0, c->stream>>>(lqc_m, M, 64, 1, sums_d);
+    VG_LAUNCHED(c);
+
+    fe host[66];
+    VG_CHECK_CUDA(cudaMemcpyAsync(host, parts + nb, 66 * sizeof(fe), cudaMemcpyDeviceToHost, c->stream));
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < 65; ++i) all_sum[i] = to_vg(host[1 + i]);
+    if (inner_product) *inner_product = to_vg(host[0]);
+    cudaFree(q_eval);
+    cudaFree(lq);
+    cudaFree(lqc);
+    cudaFree(md);
+    if (staging) cudaFree(staging);
+    pc->have_public = true;
+    return VG_OK;
+}
+
+extern "C" int vg_pc_init_commit(vg_pc *pc, int oracle, vg_digest *root)
+{
+    if (!pc || !root || (oracle != 0 && oracle != 1)) return vg_fail(VG_ERR_ARG, "vg_pc_init_commit: bad argument");
+    if (oracle == 0 && !pc->have_private) return vg_fail(VG_ERR_STATE, "init_commit(0) before encode_private");
+    if (oracle == 1 && !pc->have_public) return vg_fail(VG_ERR_STATE, "init_commit(1) before encode_public");
+    if (oracle == 0) {   // a new private commitment restarts the FRI levels
+        for (auto &L : pc->levels) {
+            cudaFree(L.cw);
+            cudaFree(L.tree);
+        }
+        pc->levels.clear();
+    }
+    return commit_tree(pc->ctx, oracle == 0 ? pc->l_eval : pc->h_eval, pc->S, oracle == 0 ? &pc->tree_l : &pc->tree_h, root);
+}
+
+extern "C" int vg_eq_table(vg_ctx *c, const vg_fe *r, int log_len, vg_fe *pub);
+
+extern "C" int vg_pc_fri_step(vg_pc *pc, vg_fe r_, vg_digest *root)
+{
+    if (!pc || !root) return vg_fail(VG_ERR_ARG, "vg_pc_fri_step: null argument");
+    if (!pc->have_public) return vg_fail(VG_ERR_STATE, "fri step before commit_public");
+    vg_ctx *c = pc->ctx;
+    const int t = (int)pc->levels.size();
+    const fe *in = t == 0 ? pc->vo : pc->levels.back().cw;
+    const long n = pc->S >> t;
+    if (n < 8) return vg_fail(VG_ERR_STATE, "FRI folded below 8 elements per slice");
+    FriLevel L;
+    L.n = n >> 1;
+    VG_TRY(dalloc((void **)&L.cw, 65 * L.n * sizeof(fe)));
+    VG_TRY(dalloc((void **)&L.tree, L.n * 32));
+    const int logS = ilog2l(pc->S);
+    const fe *ti_lo, *ti_hi;
+    VG_TRY(vg_twiddles(c, vg::fe_inv(root_of(logS)), logS, &ti_lo, &ti_hi));
+    fe r = vg::fe_make(r_.real, r_.img);
+    long q4 = n >> 2;
+    long nleaves = L.n >> 1;
+    if (c->hash_kind == VG_HASH_SHA256)
+        k_fri_fold_leaf<VG_HASH_SHA256><<<grid_for(q4, 128), 128, 0, c->stream>>>(in, n, t, r, ti_lo, ti_hi, L.cw, L.tree + 4 * nleaves);
+    else
+        k_fri_fold_leaf<VG_HASH_SHA3_256><<<grid_for(q4, 128), 128, 0, c->stream>>>(in, n, t, r, ti_lo, ti_hi, L.cw, L.tree + 4 * nleaves);
+    VG_LAUNCHED(c);
+    VG_TRY(vg_merkle_build(c, L.tree, nleaves));
+    pc->levels.push_back(L);
+    VG_CHECK_CUDA(cudaMemcpyAsync(root, L.tree + 4, 32, cudaMemcpyDeviceToHost, c->stream));
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    if (t == 0) {
+        cudaFree(pc->vo);   // the virtual oracle is never queried directly
+        pc->vo = nullptr;
+    }
+    return VG_OK;
+}
+
+extern "C" int vg_pc_fri_final(vg_pc *pc, vg_fe *data, vg_fe *mask, long *n_out)
+{
+    if (!pc || pc->levels.empty()) return vg_fail(VG_ERR_STATE, "vg_pc_fri_final: no FRI level");
+    const FriLevel &L = pc->levels.back();
+    const long n = L.n, h = n >> 1;
+    if (n_out) *n_out = n;
+    if (!data && !mask) return VG_OK;
+    std::vector<fe> buf(65 * n);
+    VG_CHECK_CUDA(cudaMemcpyAsync(buf.data(), L.cw, 65 * n * sizeof(fe), cudaMemcpyDeviceToHost, pc->ctx->stream));
+    VG_CHECK_CUDA(cudaStreamSynchronize(pc->ctx->stream));
+    // interleaved layout of fri.cpp:348-363 and 382-388
+    for (long j = 0; j < h; ++j) {
+        for (int s = 0; s < 64; ++s) {
+            if (data) {
+                data[(j << 7) | (s << 1) | 0] = to_vg(buf[s * n + j]);
+                data[(j << 7) | (s << 1) | 1] = to_vg(buf[s * n + j + h]);
+            }
+        }
+        if (mask) {
+            mask[2 * j] = to_vg(buf[64 * n + j]);
+            mask[2 * j + 1] = to_vg(buf[64 * n + j + h]);
+        }
+    }
+    return VG_OK;
+}
+
+static int gather(vg_pc *pc, const fe *cw, long n, long p, const uint64_t *tree, long leaf_node, int depth,
+                  vg_fe *values, vg_digest *path)
+{
+    vg_ctx *c = pc->ctx;
+    fe *buf;
+    VG_TRY(vg_partials(c, 130 + 2 * (depth + 1) + 1, &buf));
+    k_gather_query<<<1, 160, 0, c->stream>>>(cw, n, p, tree, leaf_node, depth, buf, (uint64_t *)(buf + 130));
+    VG_LAUNCHED(c);
+    fe *host;
+    VG_TRY(vg_pinned(c, 130 + 2 * (depth + 1), &host));
+    VG_CHECK_CUDA(cudaMemcpyAsync(host, buf, (130 + 2 * (depth + 1)) * sizeof(fe), cudaMemcpyDeviceToHost, c->stream));
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    memcpy(values, host, 130 * sizeof(fe));
+    memcpy(path, host + 130, (depth + 1) * 32);
+    return VG_OK;
+}
+
+extern "C" int vg_pc_query_init(vg_pc *pc, long pow0, int oracle, vg_fe *values, vg_digest *path)
+{
+    if (!pc || !values || !path || (oracle != 0 && oracle != 1)) return vg_fail(VG_ERR_ARG, "vg_pc_query_init: bad argument");
+    const long S = pc->S;
+    if (pow0 < 0 || pow0 >= S / 2) return vg_fail(VG_ERR_ARG, "query position %ld out of range [0, %ld)", pow0, S / 2);
+    if (oracle == 0 && !pc->have_private) return vg_fail(VG_ERR_STATE, "no private commitment");
+    if (oracle == 1 && !pc->have_public) return vg_fail(VG_ERR_STATE, "no public commitment");
+    const fe *cw = oracle == 0 ? pc->l_eval : pc->h_eval;
+    const uint64_t *tree = oracle == 0 ? pc->tree_l : pc->tree_h;
+    int depth = pc->log_len - 2;
+    return gather(pc, cw, S, pow0, tree, pow0 + S / 2, depth, values, path);
+}
+
+extern "C" int vg_pc_query_step(vg_pc *pc, int lvl, long pow, vg_fe *values, vg_digest *path, int *path_len)
+{
+    if (!pc || !values || !path || lvl < 0 || lvl >= (int)pc->levels.size())
+        return vg_fail(VG_ERR_ARG, "vg_pc_query_step: bad argument (lvl %d)", lvl);
+    const FriLevel &L = pc->levels[lvl];
+    const long h = L.n >> 1;
+    if (pow < 0) return vg_fail(VG_ERR_ARG, "negative query position");
+    long p = pow % h;
+    int depth = ilog2l(h);
+    if (path_len) *path_len = depth + 1;
+    return gather(pc, L.cw, L.n, p, L.tree, p + h, depth, values, path);
+}

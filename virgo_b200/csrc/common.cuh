@@ -1,0 +1,113 @@
+// Shared definitions for the virgo_b200 CUDA library: the context object,
+// error reporting and launch bookkeeping, and block reductions over F_{p^2}.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <string>
+#include <vector>
+#include "fp2.cuh"
+#include "virgo_b200.h"
+
+using vg::fe;
+
+struct TwEntry {
+    uint64_t key_real, key_img;  // the root
+    int logn;
+    fe *lo;   // w^i, i < 4096
+    fe *hi;   // w^(4096 j), j < max(1, n / 4096)
+};
+
+struct vg_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    int hash_kind = VG_HASH_SHA3_256;
+    long long launches = 0;
+    std::vector<TwEntry> tw_cache;
+    // reusable device scratch (grown on demand, freed with the context)
+    void *scratch = nullptr;
+    size_t scratch_cap = 0;
+    void *scratch2 = nullptr;
+    size_t scratch2_cap = 0;
+    fe *partials = nullptr;  // block partial sums of reductions
+    size_t partials_cap = 0;
+    fe *pinned = nullptr;    // pinned host staging for small results
+    size_t pinned_cap = 0;
+};
+
+// ---- errors ----
+int vg_fail(int code, const char *fmt, ...);
+#define VG_CHECK_CUDA(call)                                                              \
+    do {                                                                                 \
+        cudaError_t e_ = (call);                                                         \
+        if (e_ != cudaSuccess)                                                           \
+            return vg_fail(VG_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #call,        \
+                           cudaGetErrorString(e_));                                      \
+    } while (0)
+#define VG_TRY(expr)                   \
+    do {                               \
+        int rc_ = (expr);              \
+        if (rc_ != VG_OK) return rc_;  \
+    } while (0)
+#define VG_LAUNCHED(ctx)                                                                   \
+    do {                                                                                   \
+        (ctx)->launches++;                                                                 \
+        cudaError_t e_ = cudaGetLastError();                                               \
+        if (e_ != cudaSuccess)                                                             \
+            return vg_fail(VG_ERR_CUDA, "%s:%d launch: %s", __FILE__, __LINE__,             \
+                           cudaGetErrorString(e_));                                        \
+    } while (0)
+
+// scratch buffers owned by the context; contents do not survive other calls
+int vg_scratch(vg_ctx *ctx, size_t bytes, void **p);
+int vg_scratch2(vg_ctx *ctx, size_t bytes, void **p);
+int vg_partials(vg_ctx *ctx, size_t n, fe **p);
+int vg_pinned(vg_ctx *ctx, size_t n, fe **p);
+int vg_twiddles(vg_ctx *ctx, fe root, int logn, const fe **lo, const fe **hi);
+bool vg_is_device_ptr(const void *p);
+
+static inline unsigned grid_for(long n, int threads)
+{
+    long g = (n + threads - 1) / threads;
+    return (unsigned)(g < 1 ? 1 : g);
+}
+
+// ---- reductions ----
+__device__ __forceinline__ fe shfl_down_fe(fe x, int off)
+{
+    fe r;
+    r.real = __shfl_down_sync(0xffffffffu, x.real, off);
+    r.img = __shfl_down_sync(0xffffffffu, x.img, off);
+    return r;
+}
+__device__ __forceinline__ fe warp_sum(fe x)
+{
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) x = x + shfl_down_fe(x, off);
+    return x;
+}
+// Sum of K values over the block; result valid in thread 0.  sm holds
+// K * 32 elements.  Field addition is exact and commutative, so the result is
+// independent of the reduction order.
+template <int K>
+__device__ __forceinline__ void block_sum(fe (&v)[K], fe *sm)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) sm[k * 32 + wid] = v[k];
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            fe x = lane < nw ? sm[k * 32 + lane] : vg::fe_zero();
+            v[k] = warp_sum(x);
+        }
+    }
+}
+
+// sum of `nparts` groups of K partials (layout [part][K]) into out[K]
+int vg_reduce_partials(vg_ctx *ctx, const fe *parts, int nparts, int K, fe *out_dev);

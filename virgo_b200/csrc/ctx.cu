@@ -1,0 +1,235 @@
+// Context, device memory, error reporting, elementwise field ops and the
+// generic partial-sum reduction.
+#include "common.cuh"
+#include <mutex>
+
+static thread_local std::string g_err;
+
+int vg_fail(int code, const char *fmt, ...)
+{
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+extern "C" const char *vg_last_error(void) { return g_err.c_str(); }
+
+extern "C" int vg_ctx_create(int device, vg_ctx **out)
+{
+    if (!out) return vg_fail(VG_ERR_ARG, "vg_ctx_create: null out");
+    int n = 0;
+    cudaError_t e = cudaGetDeviceCount(&n);
+    if (e != cudaSuccess || n == 0)
+        return vg_fail(VG_ERR_NO_DEVICE, "no CUDA device (%s)", cudaGetErrorString(e));
+    if (device < 0 || device >= n) return vg_fail(VG_ERR_ARG, "device %d out of range (%d)", device, n);
+    VG_CHECK_CUDA(cudaSetDevice(device));
+    vg_ctx *c = new vg_ctx();
+    c->device = device;
+    e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) {
+        delete c;
+        return vg_fail(VG_ERR_CUDA, "cudaStreamCreate: %s", cudaGetErrorString(e));
+    }
+    *out = c;
+    return VG_OK;
+}
+
+extern "C" int vg_ctx_destroy(vg_ctx *c)
+{
+    if (!c) return VG_OK;
+    cudaSetDevice(c->device);
+    cudaStreamSynchronize(c->stream);
+    for (auto &t : c->tw_cache) {
+        cudaFree(t.lo);
+        cudaFree(t.hi);
+    }
+    if (c->scratch) cudaFree(c->scratch);
+    if (c->scratch2) cudaFree(c->scratch2);
+    if (c->partials) cudaFree(c->partials);
+    if (c->pinned) cudaFreeHost(c->pinned);
+    cudaStreamDestroy(c->stream);
+    delete c;
+    return VG_OK;
+}
+
+extern "C" int vg_ctx_set_hash(vg_ctx *c, int kind)
+{
+    if (!c) return vg_fail(VG_ERR_ARG, "null ctx");
+    if (kind != VG_HASH_SHA3_256 && kind != VG_HASH_SHA256) return vg_fail(VG_ERR_ARG, "unknown hash kind %d", kind);
+    c->hash_kind = kind;
+    return VG_OK;
+}
+extern "C" int vg_ctx_get_hash(vg_ctx *c, int *kind)
+{
+    if (!c || !kind) return vg_fail(VG_ERR_ARG, "null argument");
+    *kind = c->hash_kind;
+    return VG_OK;
+}
+
+extern "C" int vg_ctx_sync(vg_ctx *c)
+{
+    if (!c) return vg_fail(VG_ERR_ARG, "null ctx");
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    return VG_OK;
+}
+
+extern "C" int vg_ctx_launch_count(vg_ctx *c, long long *count)
+{
+    if (!c || !count) return vg_fail(VG_ERR_ARG, "null argument");
+    *count = c->launches;
+    return VG_OK;
+}
+
+static int grow(void **p, size_t *cap, size_t bytes)
+{
+    if (bytes <= *cap) return VG_OK;
+    if (*p) cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    cudaError_t e = cudaMalloc(p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return vg_fail(VG_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    }
+    *cap = bytes;
+    return VG_OK;
+}
+
+int vg_scratch(vg_ctx *c, size_t bytes, void **p)
+{
+    if (bytes > c->scratch_cap) VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    VG_TRY(grow(&c->scratch, &c->scratch_cap, bytes));
+    *p = c->scratch;
+    return VG_OK;
+}
+int vg_scratch2(vg_ctx *c, size_t bytes, void **p)
+{
+    if (bytes > c->scratch2_cap) VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    VG_TRY(grow(&c->scratch2, &c->scratch2_cap, bytes));
+    *p = c->scratch2;
+    return VG_OK;
+}
+int vg_partials(vg_ctx *c, size_t n, fe **p)
+{
+    if (n * sizeof(fe) > c->partials_cap) VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    void *q = c->partials;
+    VG_TRY(grow(&q, &c->partials_cap, n * sizeof(fe)));
+    c->partials = (fe *)q;
+    *p = c->partials;
+    return VG_OK;
+}
+int vg_pinned(vg_ctx *c, size_t n, fe **p)
+{
+    size_t bytes = n * sizeof(fe);
+    if (bytes > c->pinned_cap) {
+        VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+        if (c->pinned) cudaFreeHost(c->pinned);
+        c->pinned = nullptr;
+        c->pinned_cap = 0;
+        size_t cap = bytes < 65536 ? 65536 : bytes;
+        VG_CHECK_CUDA(cudaMallocHost((void **)&c->pinned, cap));
+        c->pinned_cap = cap;
+    }
+    *p = c->pinned;
+    return VG_OK;
+}
+
+bool vg_is_device_ptr(const void *p)
+{
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+extern "C" int vg_dev_alloc(vg_ctx *c, size_t bytes, void **dev)
+{
+    if (!c || !dev) return vg_fail(VG_ERR_ARG, "null argument");
+    cudaError_t e = cudaMalloc(dev, bytes ? bytes : 16);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        *dev = nullptr;
+        return vg_fail(VG_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    }
+    return VG_OK;
+}
+extern "C" int vg_dev_free(vg_ctx *c, void *dev)
+{
+    if (!c) return vg_fail(VG_ERR_ARG, "null ctx");
+    if (dev) {
+        VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+        VG_CHECK_CUDA(cudaFree(dev));
+    }
+    return VG_OK;
+}
+extern "C" int vg_h2d(vg_ctx *c, void *dev, const void *host, size_t bytes)
+{
+    if (!c) return vg_fail(VG_ERR_ARG, "null ctx");
+    VG_CHECK_CUDA(cudaMemcpyAsync(dev, host, bytes, cudaMemcpyDefault, c->stream));
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    return VG_OK;
+}
+extern "C" int vg_d2h(vg_ctx *c, void *host, const void *dev, size_t bytes)
+{
+    if (!c) return vg_fail(VG_ERR_ARG, "null ctx");
+    VG_CHECK_CUDA(cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDefault, c->stream));
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    return VG_OK;
+}
+
+// ------------------------------------------------------------ field binop
+__global__ void k_binop(int op, const fe *__restrict__ a, const fe *__restrict__ b, fe *__restrict__ c, long n)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n; i += (long)gridDim.x * blockDim.x) {
+        fe x = a[i], y = b[i];
+        c[i] = op == 0 ? x + y : (op == 1 ? x - y : x * y);
+    }
+}
+
+extern "C" int vg_fe_binop(vg_ctx *c, int op, const vg_fe *a, const vg_fe *b, vg_fe *out, long n)
+{
+    if (!c || !a || !b || !out || n < 0 || op < 0 || op > 2) return vg_fail(VG_ERR_ARG, "vg_fe_binop: bad argument");
+    if (n == 0) return VG_OK;
+    unsigned g = grid_for(n, 256);
+    if (g > 148 * 32) g = 148 * 32;
+    k_binop<<<g, 256, 0, c->stream>>>(op, (const fe *)a, (const fe *)b, (fe *)out, n);
+    VG_LAUNCHED(c);
+    return VG_OK;
+}
+
+// ------------------------------------------------------- partial reductions
+template <int K>
+__global__ void k_reduce_parts(const fe *__restrict__ parts, int nparts, fe *__restrict__ out)
+{
+    __shared__ fe sm[K * 32];
+    fe v[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = vg::fe_zero();
+    for (int i = threadIdx.x; i < nparts; i += blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = v[k] + parts[(long)i * K + k];
+    }
+    block_sum<K>(v, sm);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) out[k] = v[k];
+    }
+}
+
+int vg_reduce_partials(vg_ctx *c, const fe *parts, int nparts, int K, fe *out_dev)
+{
+    switch (K) {
+    case 1: k_reduce_parts<1><<<1, 1024, 0, c->stream>>>(parts, nparts, out_dev); break;
+    case 3: k_reduce_parts<3><<<1, 1024, 0, c->stream>>>(parts, nparts, out_dev); break;
+    default: return vg_fail(VG_ERR_ARG, "vg_reduce_partials: K=%d unsupported", K);
+    }
+    VG_LAUNCHED(c);
+    return VG_OK;
+}

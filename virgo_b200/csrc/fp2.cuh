@@ -1,0 +1,136 @@
+// F_{p^2} arithmetic, p = 2^61 - 1, i^2 = -1, shared by device kernels and
+// host code.
+//
+// Element layout is {img, real} (two uint64, img first), the in-memory layout
+// of prime_field::field_element (reference include/linear_gkr/prime_field.h:93),
+// so buffers cross the C ABI unchanged.  Every operation returns a canonical
+// value in [0, p) for canonical inputs; the reference's operators do the same
+// (prime_field.h:114-172), so results agree bit for bit whatever the order of
+// evaluation.
+#pragma once
+#include <stdint.h>
+
+#if defined(__CUDACC__)
+#define VG_HD __host__ __device__ __forceinline__
+#else
+#define VG_HD inline
+#endif
+
+namespace vg {
+
+constexpr uint64_t P = 0x1FFFFFFFFFFFFFFFull;  // 2^61 - 1
+
+struct alignas(16) fe {
+    uint64_t img, real;
+};
+
+VG_HD fe fe_make(uint64_t real, uint64_t img) { fe r; r.real = real; r.img = img; return r; }
+VG_HD fe fe_zero() { return fe_make(0, 0); }
+VG_HD fe fe_one() { return fe_make(1, 0); }
+VG_HD bool fe_eq(fe a, fe b) { return a.real == b.real && a.img == b.img; }
+VG_HD bool fe_is_zero(fe a) { return (a.real | a.img) == 0; }
+
+// ---- F_p ----
+VG_HD uint64_t addp(uint64_t a, uint64_t b)
+{
+    uint64_t s = a + b;
+    return s >= P ? s - P : s;
+}
+VG_HD uint64_t subp(uint64_t a, uint64_t b) { return a >= b ? a - b : a + P - b; }
+VG_HD uint64_t negp(uint64_t a) { return a ? P - a : 0; }
+
+VG_HD void mul64wide(uint64_t a, uint64_t b, uint64_t &lo, uint64_t &hi)
+{
+#if defined(__CUDA_ARCH__)
+    lo = a * b;
+    hi = __umul64hi(a, b);
+#else
+    unsigned __int128 x = (unsigned __int128)a * b;
+    lo = (uint64_t)x;
+    hi = (uint64_t)(x >> 64);
+#endif
+}
+
+// a*b mod p for a, b < 2^61 (canonical).  x = hi*2^64 + lo < 2^122, and
+// x = (x >> 61) * 2^61 + (x & p) == (x >> 61) + (x & p) (mod p); both terms are
+// below 2^61, so one conditional subtraction makes the sum canonical.
+VG_HD uint64_t mulp(uint64_t a, uint64_t b)
+{
+    uint64_t lo, hi;
+    mul64wide(a, b, lo, hi);
+    uint64_t r = (lo & P) + ((hi << 3) | (lo >> 61));
+    return r >= P ? r - P : r;
+}
+
+// a*b mod p for a, b < 2^62 (sums of two canonical values): x < 2^124 and the
+// first fold leaves a value below 2^64, folded once more.
+VG_HD uint64_t mulp_wide(uint64_t a, uint64_t b)
+{
+    uint64_t lo, hi;
+    mul64wide(a, b, lo, hi);
+    uint64_t r = (lo & P) + ((hi << 3) | (lo >> 61));
+    r = (r & P) + (r >> 61);
+    return r >= P ? r - P : r;
+}
+
+// ---- F_{p^2} ----
+VG_HD fe operator+(fe a, fe b) { return fe_make(addp(a.real, b.real), addp(a.img, b.img)); }
+VG_HD fe operator-(fe a, fe b) { return fe_make(subp(a.real, b.real), subp(a.img, b.img)); }
+VG_HD fe operator-(fe a) { return fe_make(negp(a.real), negp(a.img)); }
+
+// (ar + i ai)(br + i bi) = (ar br - ai bi) + i((ar + ai)(br + bi) - ar br - ai bi)
+VG_HD fe operator*(fe a, fe b)
+{
+    uint64_t ac = mulp(a.real, b.real);
+    uint64_t bd = mulp(a.img, b.img);
+    uint64_t t = mulp_wide(a.real + a.img, b.real + b.img);
+    return fe_make(subp(ac, bd), subp(t, addp(ac, bd)));
+}
+
+VG_HD fe fe_double(fe a) { return a + a; }
+
+// multiplication by an element of F_p (img = 0)
+VG_HD fe fe_scale(fe a, uint64_t s) { return fe_make(mulp(a.real, s), mulp(a.img, s)); }
+
+VG_HD fe fe_pow(fe x, uint64_t e)
+{
+    fe r = fe_one();
+    while (e) {
+        if (e & 1) r = r * x;
+        x = x * x;
+        e >>= 1;
+    }
+    return r;
+}
+
+// x^(p^2 - 2) = x^-1; p^2 - 2 does not fit 64 bits, so exponentiate by the
+// 128-bit value with two 64-bit words.
+VG_HD fe fe_inv(fe x)
+{
+    // p^2 - 2 = (2^61-1)^2 - 2 = 2^122 - 2^62 - 1
+    const uint64_t e_hi = (1ull << 58) - 1;            // bits 64..121 of 2^122 - 2^62 - 1
+    const uint64_t e_lo = 0xBFFFFFFFFFFFFFFFull;       // low 64 bits
+    fe r = fe_one();
+    fe b = x;
+    for (int i = 0; i < 64; ++i) {
+        if ((e_lo >> i) & 1) r = r * b;
+        b = b * b;
+    }
+    for (int i = 0; i < 58; ++i) {
+        if ((e_hi >> i) & 1) r = r * b;
+        b = b * b;
+    }
+    return r;
+}
+
+// Root of unity of order 2^log_order: the generator of the 2-adic subgroup of
+// order 2^62 (real 2^31, img 1033321771269002680), squared 62 - log_order times.
+// Same construction as the reference (src/linear_gkr/prime_field.cpp:60-73).
+VG_HD fe fe_root_of_unity(int log_order)
+{
+    fe r = fe_make(2147483648ull, 1033321771269002680ull);
+    for (int i = 0; i < 62 - log_order; ++i) r = r * r;
+    return r;
+}
+
+}  // namespace vg

@@ -1,0 +1,742 @@
+// GKR prover kernels: layered-circuit evaluation, V_res, the phase-1/phase-2
+// bookkeeping scatters and the per-round sumcheck fold + reduction.
+//
+// Gate records live on the device as three arrays per layer (ty: uint8,
+// u, v: uint32 bit patterns; 9 bytes per gate instead of the reference's
+// 24-byte AoS `gate`).
+//
+// Bookkeeping tables.  The reference keeps linear polynomials {a, b} (32 B per
+// entry) and, at each round, evaluates the previous round's polynomial at the
+// verifier's challenge (zk_prover.cpp:616-626).  Here each table is the list of
+// values W (16 B per entry): at round t the entries are folded with the
+// previous challenge, W'[k] = W[2k] + r (W[2k+1] - W[2k]), which is exactly
+// V_mult_add[k].eval(r) of the reference, and the round sums read the pair
+// (W'[2i], W'[2i+1]) as b = W'[2i], a = W'[2i+1] - W'[2i].  One fused kernel
+// per round reads 4 entries of each table per thread, writes the 2 folded
+// ones, and reduces the three round sums per block (exact field addition, so
+// the sum does not depend on the order).
+//
+// Scatters.  phase*_init add gate contributions into table entries chosen by
+// the gate's u (phase 1) or v (phase 2).  Field additions are done exactly with
+// 64-bit integer atomics: a canonical value x < 2^61 is split into
+// x mod 2^32 and x >> 32, each accumulated in its own uint64 (at most 2^30
+// contributions per entry keeps both below 2^64), and a finalise pass folds
+// lo + hi * 2^32 back into a canonical element.
+#include "common.cuh"
+#include <algorithm>
+#include <cstring>
+
+namespace {
+
+constexpr int GKR_THREADS = 256;
+
+struct DevLayer {
+    int bl = 0;
+    long n = 0;
+    uint8_t *ty = nullptr;
+    uint32_t *u = nullptr, *v = nullptr;
+};
+
+__device__ __forceinline__ fe from_int32(int32_t x)
+{
+    uint64_t val = (uint64_t)(int64_t)x;   // zk_prover.cpp:60-65 (int) then field_element(unsigned long long)
+    uint64_t r = (val & vg::P) + (val >> 61);
+    return vg::fe_make(r >= vg::P ? r - vg::P : r, 0);
+}
+
+// --------------------------------------------------------------- evaluate
+__global__ void k_eval_input(const int64_t *__restrict__ u, long n, fe *__restrict__ out)
+{
+    long g = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (g < n) out[g] = from_int32((int32_t)u[g]);
+}
+
+// zk_prover::evaluate, one layer (zk_prover.cpp:68-150)
+__global__ void k_eval_layer(const uint8_t *__restrict__ ty, const uint32_t *__restrict__ uu,
+                             const uint32_t *__restrict__ vv, long n, const fe *__restrict__ prev,
+                             fe *__restrict__ out)
+{
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < n; g += (long)gridDim.x * blockDim.x) {
+        const uint32_t u = uu[g], v = vv[g];
+        fe r = vg::fe_zero();
+        switch (ty[g]) {
+        case 0: r = prev[u] + prev[v]; break;
+        case 1: r = prev[u] * prev[v]; break;
+        case 3: r = from_int32((int32_t)u); break;
+        case 4:
+        case 10: r = prev[u]; break;
+        case 5:
+            for (uint32_t k = u; k < v; ++k) r = r + prev[k];
+            break;
+        case 6: r = vg::fe_one() - prev[u]; break;
+        case 7: r = prev[u] - prev[v]; break;
+        case 8: {
+            fe x = prev[u], y = prev[v], xy = x * y;
+            r = (x + y) - (xy + xy);
+        } break;
+        case 9: {
+            fe x = prev[u], y = prev[v];
+            r = y - x * y;
+        } break;
+        case 12:   // sum_k prev[k] 2^(k-u), Horner from the top
+            for (long k = (long)v; k >= (long)u; --k) r = (r + r) + prev[k];
+            break;
+        case 13: r = prev[u] * (vg::fe_one() - prev[v]); break;
+        default: break;   // 2 (dummy) and unknown types evaluate to 0
+        }
+        out[g] = r;
+    }
+}
+
+// ------------------------------------------------------------ eq tables
+// out[i] = scale * prod_{b < nbits} (bit b of i ? r[b] : 1 - r[b])
+__global__ void k_eq_half(const fe *__restrict__ r, int nbits, fe scale, fe *__restrict__ out)
+{
+    long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i >= (1L << nbits)) return;
+    fe x = scale;
+    for (int b = 0; b < nbits; ++b) x = x * (((i >> b) & 1) ? r[b] : vg::fe_one() - r[b]);
+    out[i] = x;
+}
+
+// out[x] = lo[x & mask] * hi[x >> fh]
+__global__ void k_eq_combine(const fe *__restrict__ lo, const fe *__restrict__ hi, int fh, long n, fe *__restrict__ out)
+{
+    const long mask = (1L << fh) - 1;
+    for (long x = blockIdx.x * (long)blockDim.x + threadIdx.x; x < n; x += (long)gridDim.x * blockDim.x)
+        out[x] = lo[x & mask] * hi[x >> fh];
+}
+
+// sum_x vals[x] * lo[x & mask] * hi[x >> fh]  (V_res as an inner product with eq)
+__global__ void k_eq_dot(const fe *__restrict__ vals, const fe *__restrict__ lo, const fe *__restrict__ hi, int fh,
+                         long n, fe *__restrict__ parts)
+{
+    __shared__ fe sm[32];
+    const long mask = (1L << fh) - 1;
+    fe acc[1] = {vg::fe_zero()};
+    for (long x = blockIdx.x * (long)blockDim.x + threadIdx.x; x < n; x += (long)gridDim.x * blockDim.x)
+        acc[0] = acc[0] + vals[x] * (lo[x & mask] * hi[x >> fh]);
+    block_sum<1>(acc, sm);
+    if (threadIdx.x == 0) parts[blockIdx.x] = acc[0];
+}
+
+// ---------------------------------------------------------- accumulators
+struct BetaG {
+    const fe *f0, *s0, *f1, *s1;   // alpha*eq(r0 low half), eq(r0 high half), beta*..., eq(r1 high)
+    int fh;
+    long mask;
+    __device__ __forceinline__ fe at(long i) const
+    {
+        return f0[i & mask] * s0[i >> fh] + f1[i & mask] * s1[i >> fh];
+    }
+};
+struct BetaU {
+    const fe *f, *s;
+    int fh;
+    long mask;
+    __device__ __forceinline__ fe at(long i) const { return f[i & mask] * s[i >> fh]; }
+};
+
+__device__ __forceinline__ void acc_add(unsigned long long *acc, long j, fe x)
+{
+    unsigned long long *p = acc + 4 * j;
+    atomicAdd(p + 0, (unsigned long long)(x.real & 0xffffffffull));
+    atomicAdd(p + 1, (unsigned long long)(x.real >> 32));
+    atomicAdd(p + 2, (unsigned long long)(x.img & 0xffffffffull));
+    atomicAdd(p + 3, (unsigned long long)(x.img >> 32));
+}
+__device__ __forceinline__ void acc_sub(unsigned long long *acc, long j, fe x) { acc_add(acc, j, -x); }
+
+__device__ __forceinline__ uint64_t fold_split(uint64_t lo, uint64_t hi)
+{
+    uint64_t a = (lo & vg::P) + (lo >> 61);
+    a = a >= vg::P ? a - vg::P : a;
+    uint64_t b = (hi & vg::P) + (hi >> 61);
+    b = b >= vg::P ? b - vg::P : b;
+    return vg::addp(a, vg::mulp(b, 1ull << 32));
+}
+
+__global__ void k_acc_finalize(const unsigned long long *__restrict__ acc, long n, fe *__restrict__ out)
+{
+    for (long j = blockIdx.x * (long)blockDim.x + threadIdx.x; j < n; j += (long)gridDim.x * blockDim.x) {
+        const unsigned long long *p = acc + 4 * j;
+        out[j] = vg::fe_make(fold_split(p[0], p[1]), fold_split(p[2], p[3]));
+    }
+}
+
+// add a block's sum of `x` into acc entry j with 4 atomics from thread 0
+__device__ __forceinline__ void block_acc_add(unsigned long long *acc, long j, fe x, fe *sm)
+{
+    fe v[1] = {x};
+    block_sum<1>(v, sm);
+    if (threadIdx.x == 0 && !vg::fe_is_zero(v[0])) acc_add(acc, j, v[0]);
+}
+
+// sumcheck_phase1_init gate scatter (zk_prover.cpp:422-587).  am/av are the
+// accumulators of add_mult_sum[.].b and addV_array[.].b.
+__global__ void __launch_bounds__(GKR_THREADS) k_phase1_scatter(const uint8_t *__restrict__ ty, const uint32_t *__restrict__ uu,
+                                                                const uint32_t *__restrict__ vv, long ng, BetaG bg,
+                                                                const fe *__restrict__ prev, unsigned long long *am,
+                                                                unsigned long long *av)
+{
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < ng; i += (long)gridDim.x * blockDim.x) {
+        const int t = ty[i];
+        if (t == 2 || t == 3 || t == 11 || t > 13) continue;
+        const uint32_t u = uu[i], v = vv[i];
+        if (t == 4) {   // direct relay: beta taken at u (zk_prover.cpp:496-497)
+            acc_add(am, u, bg.at(u));
+            continue;
+        }
+        fe tmp = bg.at(i);
+        switch (t) {
+        case 0: acc_add(av, u, prev[v] * tmp); acc_add(am, u, tmp); break;
+        case 1: acc_add(am, u, prev[v] * tmp); break;
+        case 5:
+            for (uint32_t j = u; j < v; ++j) acc_add(am, j, tmp);
+            break;
+        case 12:
+            for (uint32_t j = u; j <= v; ++j) {
+                acc_add(am, j, tmp);
+                tmp = tmp + tmp;
+            }
+            break;
+        case 6: acc_sub(am, u, tmp); acc_add(av, u, tmp); break;
+        case 7: acc_sub(av, u, prev[v] * tmp); acc_add(am, u, tmp); break;
+        case 8: {
+            fe tv = tmp * prev[v];
+            acc_add(av, u, tv);
+            acc_add(am, u, tmp - (tv + tv));
+        } break;
+        case 13: {
+            fe tv = tmp * prev[v];
+            acc_add(am, u, tmp - tv);
+        } break;
+        case 9: {
+            fe tv = tmp * prev[v];
+            acc_add(av, u, tv);
+            acc_sub(am, u, tv);
+        } break;
+        case 10: acc_add(am, u, tmp); break;
+        default: break;
+        }
+    }
+}
+
+// sumcheck_phase2_init gate scatter (zk_prover.cpp:845-972).  Summation gates
+// (5, 12) all add into addV_array[0]: those contributions are summed per block
+// first and added with one set of atomics per block.
+__global__ void __launch_bounds__(GKR_THREADS) k_phase2_scatter(const uint8_t *__restrict__ ty, const uint32_t *__restrict__ uu,
+                                                                const uint32_t *__restrict__ vv, long ng, BetaG bg, BetaU bu,
+                                                                fe vu, unsigned long long *am, unsigned long long *av)
+{
+    __shared__ fe sm[32];
+    fe zero_acc = vg::fe_zero();
+    const long stride = (long)gridDim.x * blockDim.x;
+    const long start = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    const long iters = (ng + stride - 1) / stride;
+    for (long it = 0; it < iters; ++it) {
+        long i = start + it * stride;
+        if (i >= ng) continue;
+        const int t = ty[i];
+        if (t == 2 || t == 3 || t == 4 || t == 11 || t > 13) continue;
+        const uint32_t u = uu[i], v = vv[i];
+        fe tg = bg.at(i);
+        switch (t) {
+        case 1: acc_add(am, v, (tg * bu.at(u)) * vu); break;
+        case 0: {
+            fe tgu = tg * bu.at(u);
+            acc_add(am, v, tgu);
+            acc_add(av, v, tgu * vu);
+        } break;
+        case 5: {
+            fe tvu = tg * vu;
+            for (uint32_t j = u; j < v; ++j) zero_acc = zero_acc + tvu * bu.at(j);
+        } break;
+        case 12: {
+            fe tvu = tg * vu;
+            for (uint32_t j = u; j <= v; ++j) {
+                zero_acc = zero_acc + tvu * bu.at(j);
+                tvu = tvu + tvu;
+            }
+        } break;
+        case 6: {
+            fe tgu = tg * bu.at(u);
+            acc_add(av, v, tgu - tgu * vu);
+        } break;
+        case 7: {
+            fe tgu = tg * bu.at(u);
+            acc_sub(am, v, tgu);
+            acc_add(av, v, tgu * vu);
+        } break;
+        case 8: {
+            fe tgu = tg * bu.at(u), tv = tgu * vu;
+            acc_add(am, v, tgu - (tv + tv));
+            acc_add(av, v, tv);
+        } break;
+        case 13: {
+            fe tv = (tg * bu.at(u)) * vu;
+            acc_sub(am, v, tv);
+            acc_add(av, v, tv);
+        } break;
+        case 9: {
+            fe tgu = tg * bu.at(u);
+            acc_add(am, v, tgu - vu * tgu);
+        } break;
+        case 10: acc_add(av, v, (tg * bu.at(u)) * vu); break;
+        default: break;
+        }
+    }
+    block_acc_add(av, 0, zero_acc, sm);
+}
+
+// ------------------------------------------------------------ round kernel
+__device__ __forceinline__ fe fold(fe x0, fe x1, fe r) { return x0 + r * (x1 - x0); }
+
+template <bool FOLD>
+__global__ void __launch_bounds__(GKR_THREADS) k_round(const fe *__restrict__ xV, const fe *__restrict__ xAV,
+                                                       const fe *__restrict__ xAM, long npairs, fe r,
+                                                       fe *__restrict__ yV, fe *__restrict__ yAV, fe *__restrict__ yAM,
+                                                       fe *__restrict__ parts)
+{
+    __shared__ fe sm[3 * 32];
+    fe acc[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < npairs; i += (long)gridDim.x * blockDim.x) {
+        fe v0, v1, a0, a1, m0, m1;
+        if (FOLD) {
+            const long b = 4 * i;
+            v0 = fold(xV[b], xV[b + 1], r);
+            v1 = fold(xV[b + 2], xV[b + 3], r);
+            a0 = fold(xAV[b], xAV[b + 1], r);
+            a1 = fold(xAV[b + 2], xAV[b + 3], r);
+            m0 = fold(xAM[b], xAM[b + 1], r);
+            m1 = fold(xAM[b + 2], xAM[b + 3], r);
+            yV[2 * i] = v0; yV[2 * i + 1] = v1;
+            yAV[2 * i] = a0; yAV[2 * i + 1] = a1;
+            yAM[2 * i] = m0; yAM[2 * i + 1] = m1;
+        } else {
+            v0 = xV[2 * i]; v1 = xV[2 * i + 1];
+            a0 = xAV[2 * i]; a1 = xAV[2 * i + 1];
+            m0 = xAM[2 * i]; m1 = xAM[2 * i + 1];
+        }
+        const fe va = v1 - v0, aa = a1 - a0, ma = m1 - m0;
+        acc[0] = acc[0] + ma * va;
+        acc[1] = acc[1] + (ma * v0 + m0 * va) + aa;
+        acc[2] = acc[2] + m0 * v0 + a0;
+    }
+    block_sum<3>(acc, sm);
+    if (threadIdx.x == 0) {
+        parts[3 * blockIdx.x + 0] = acc[0];
+        parts[3 * blockIdx.x + 1] = acc[1];
+        parts[3 * blockIdx.x + 2] = acc[2];
+    }
+}
+
+vg::fe tofe(vg_fe x) { return vg::fe_make(x.real, x.img); }
+vg_fe tovg(vg::fe x) { vg_fe r; r.real = x.real; r.img = x.img; return r; }
+
+}  // namespace
+
+struct vg_circuit {
+    vg_ctx *ctx = nullptr;
+    int depth = 0;
+    int max_bl = 0;
+    std::vector<DevLayer> L;
+    fe *input = nullptr;   // layer 0 values
+};
+
+struct vg_gkr {
+    vg_ctx *ctx = nullptr;
+    const vg_circuit *C = nullptr;
+    std::vector<fe *> vals;
+    fe *buf[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};   // ping-pong V, AV, AM
+    unsigned long long *acc = nullptr;   // 2 tables x 4 words x 2^max_bl
+    fe *eq = nullptr;                    // half tables
+    fe *rbuf = nullptr;                  // challenges (device copy)
+    long eq_half = 0;
+    int layer = -1, length_g = 0;
+    long n = 0;                          // current table length
+    const fe *cur[3] = {nullptr, nullptr, nullptr};
+    int next_buf = 1;
+    bool round0_pending = false;
+    BetaG bg{};
+};
+
+// ------------------------------------------------------------------ circuit
+extern "C" int vg_circuit_upload(vg_ctx *ctx, int depth, const int *bit_length, const uint8_t *const *ty,
+                                 const int64_t *const *u, const int64_t *const *v, vg_circuit **out)
+{
+    if (!ctx || !out || depth < 2 || !bit_length || !ty || !u || !v)
+        return vg_fail(VG_ERR_ARG, "vg_circuit_upload: bad argument (depth %d)", depth);
+    for (int i = 0; i < depth; ++i)
+        if (bit_length[i] < 0 || bit_length[i] > 30) return vg_fail(VG_ERR_ARG, "layer %d: bit length %d", i, bit_length[i]);
+    // validate every gate against the previous layer (zk_verifier.cpp:70-102)
+    for (int i = 1; i < depth; ++i) {
+        const long n = 1L << bit_length[i], np = 1L << bit_length[i - 1];
+        for (long g = 0; g < n; ++g) {
+            const int t = ty[i][g];
+            const int64_t a = u[i][g], b = v[i][g];
+            bool ok = true;
+            if (t > 13 || t == 11) ok = false;
+            else if (t == 3 || t == 2) ok = true;
+            else if (t == 5) ok = a >= 0 && a < np && b > a && b <= np;
+            else if (t == 12) ok = a >= 0 && b >= a && b < np && b - a + 1 <= 60;
+            else if (t == 6 || t == 10 || t == 4) ok = a >= 0 && a < np;
+            else ok = a >= 0 && a < np && b >= 0 && b < np && (t != 13 || a == b);
+            if (t == 4 && a >= n) ok = false;   // relay reads beta at u over this layer's bits
+            if (!ok)
+                return vg_fail(VG_ERR_ARG, "layer %d gate %ld: type %d u %lld v %lld invalid for previous width %ld",
+                               i, g, t, (long long)a, (long long)b, np);
+        }
+    }
+    vg_circuit *c = new vg_circuit();
+    c->ctx = ctx;
+    c->depth = depth;
+    c->L.resize(depth);
+    auto fail = [&](int rc) { vg_circuit_destroy(c); return rc; };
+    for (int i = 0; i < depth; ++i) {
+        DevLayer &D = c->L[i];
+        D.bl = bit_length[i];
+        D.n = 1L << D.bl;
+        c->max_bl = std::max(c->max_bl, D.bl);
+        if (i == 0) {
+            int64_t *tmp;
+            if (cudaMalloc(&c->input, D.n * sizeof(fe)) != cudaSuccess || cudaMalloc(&tmp, D.n * 8) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(vg_fail(VG_ERR_OOM, "circuit input allocation"));
+            }
+            cudaMemcpyAsync(tmp, u[0], D.n * 8, cudaMemcpyHostToDevice, ctx->stream);
+            k_eval_input<<<grid_for(D.n, 256), 256, 0, ctx->stream>>>(tmp, D.n, c->input);
+            ctx->launches++;
+            cudaStreamSynchronize(ctx->stream);
+            cudaFree(tmp);
+            continue;
+        }
+        std::vector<uint32_t> hu(D.n), hv(D.n);
+        for (long g = 0; g < D.n; ++g) {
+            hu[g] = (uint32_t)u[i][g];
+            hv[g] = (ty[i][g] == 6 || ty[i][g] == 10) ? 0u : (uint32_t)v[i][g];   // zk_verifier.cpp:87-98
+        }
+        if (cudaMalloc(&D.ty, D.n) != cudaSuccess || cudaMalloc(&D.u, D.n * 4) != cudaSuccess ||
+            cudaMalloc(&D.v, D.n * 4) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(vg_fail(VG_ERR_OOM, "circuit layer %d allocation", i));
+        }
+        cudaMemcpyAsync(D.ty, ty[i], D.n, cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync(D.u, hu.data(), D.n * 4, cudaMemcpyHostToDevice, ctx->stream);
+        cudaMemcpyAsync(D.v, hv.data(), D.n * 4, cudaMemcpyHostToDevice, ctx->stream);
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) return fail(vg_fail(VG_ERR_CUDA, "circuit upload: %s", cudaGetErrorString(e)));
+    }
+    *out = c;
+    return VG_OK;
+}
+
+extern "C" int vg_circuit_destroy(vg_circuit *c)
+{
+    if (!c) return VG_OK;
+    cudaStreamSynchronize(c->ctx->stream);
+    for (auto &D : c->L) {
+        cudaFree(D.ty);
+        cudaFree(D.u);
+        cudaFree(D.v);
+    }
+    cudaFree(c->input);
+    delete c;
+    return VG_OK;
+}
+
+extern "C" int vg_circuit_depth(const vg_circuit *c, int *depth)
+{
+    if (!c || !depth) return vg_fail(VG_ERR_ARG, "null argument");
+    *depth = c->depth;
+    return VG_OK;
+}
+
+// ---------------------------------------------------------------------- GKR
+extern "C" int vg_gkr_create(vg_ctx *ctx, const vg_circuit *c, vg_gkr **out)
+{
+    if (!ctx || !c || !out) return vg_fail(VG_ERR_ARG, "vg_gkr_create: null argument");
+    vg_gkr *g = new vg_gkr();
+    g->ctx = ctx;
+    g->C = c;
+    g->vals.assign(c->depth, nullptr);
+    const long N = 1L << c->max_bl;
+    auto fail = [&](const char *what) {
+        cudaGetLastError();
+        vg_gkr_destroy(g);
+        return vg_fail(VG_ERR_OOM, "vg_gkr_create: %s allocation failed", what);
+    };
+    for (int i = 1; i < c->depth; ++i)
+        if (cudaMalloc(&g->vals[i], c->L[i].n * sizeof(fe)) != cudaSuccess) return fail("layer values");
+    g->vals[0] = c->input;
+    for (int b = 0; b < 2; ++b)
+        for (int k = 0; k < 3; ++k)
+            if (cudaMalloc(&g->buf[b][k], (b == 0 ? N : N / 2 + 1) * sizeof(fe)) != cudaSuccess) return fail("tables");
+    if (cudaMalloc(&g->acc, 2 * 4 * N * sizeof(unsigned long long)) != cudaSuccess) return fail("accumulators");
+    g->eq_half = 1L << (c->max_bl / 2 + 1);
+    if (cudaMalloc(&g->eq, 6 * g->eq_half * sizeof(fe)) != cudaSuccess) return fail("eq tables");
+    if (cudaMalloc(&g->rbuf, 3 * 64 * sizeof(fe)) != cudaSuccess) return fail("challenges");
+    *out = g;
+    return VG_OK;
+}
+
+extern "C" int vg_gkr_destroy(vg_gkr *g)
+{
+    if (!g) return VG_OK;
+    cudaStreamSynchronize(g->ctx->stream);
+    for (size_t i = 1; i < g->vals.size(); ++i) cudaFree(g->vals[i]);
+    for (int b = 0; b < 2; ++b)
+        for (int k = 0; k < 3; ++k) cudaFree(g->buf[b][k]);
+    cudaFree(g->acc);
+    cudaFree(g->eq);
+    cudaFree(g->rbuf);
+    delete g;
+    return VG_OK;
+}
+
+extern "C" int vg_gkr_evaluate(vg_gkr *g)
+{
+    if (!g) return vg_fail(VG_ERR_ARG, "null gkr");
+    vg_ctx *c = g->ctx;
+    for (int i = 1; i < g->C->depth; ++i) {
+        const DevLayer &D = g->C->L[i];
+        unsigned grid = std::min<unsigned>(grid_for(D.n, GKR_THREADS), 148u * 64u);
+        k_eval_layer<<<grid, GKR_THREADS, 0, c->stream>>>(D.ty, D.u, D.v, D.n, g->vals[i - 1], g->vals[i]);
+        VG_LAUNCHED(c);
+    }
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    return VG_OK;
+}
+
+extern "C" int vg_gkr_layer_values(vg_gkr *g, int layer, const vg_fe **dev_values)
+{
+    if (!g || !dev_values || layer < 0 || layer >= g->C->depth) return vg_fail(VG_ERR_ARG, "vg_gkr_layer_values: bad layer");
+    *dev_values = (const vg_fe *)g->vals[layer];
+    return VG_OK;
+}
+
+// eq half tables for bits r[0..len): low half (len >> 1 bits, scaled) and high half
+static int build_halves(vg_gkr *g, const fe *r_dev, int len, fe scale, fe *lo, fe *hi, int *fh)
+{
+    vg_ctx *c = g->ctx;
+    int f = len >> 1, s = len - f;
+    k_eq_half<<<grid_for(1L << f, 256), 256, 0, c->stream>>>(r_dev, f, scale, lo);
+    VG_LAUNCHED(c);
+    k_eq_half<<<grid_for(1L << s, 256), 256, 0, c->stream>>>(r_dev + f, s, vg::fe_one(), hi);
+    VG_LAUNCHED(c);
+    *fh = f;
+    return VG_OK;
+}
+
+static int upload_r(vg_gkr *g, int slot, const vg_fe *r, int len)
+{
+    if (len > 64) return vg_fail(VG_ERR_ARG, "challenge vector longer than 64");
+    if (len == 0) return VG_OK;
+    VG_CHECK_CUDA(cudaMemcpyAsync(g->rbuf + 64 * slot, r, len * sizeof(fe), cudaMemcpyHostToDevice, g->ctx->stream));
+    return VG_OK;
+}
+
+extern "C" int vg_gkr_v_res(vg_gkr *g, const vg_fe *r, int r_len, vg_fe *out)
+{
+    if (!g || !r || !out) return vg_fail(VG_ERR_ARG, "vg_gkr_v_res: null argument");
+    const int last = g->C->depth - 1;
+    if (r_len != g->C->L[last].bl) return vg_fail(VG_ERR_ARG, "r_len %d != output bit length %d", r_len, g->C->L[last].bl);
+    vg_ctx *c = g->ctx;
+    VG_TRY(upload_r(g, 0, r, r_len));
+    fe *lo = g->eq, *hi = g->eq + g->eq_half;
+    int fh;
+    VG_TRY(build_halves(g, g->rbuf, r_len, vg::fe_one(), lo, hi, &fh));
+    fe *parts;
+    const int nb = 148 * 2;
+    VG_TRY(vg_partials(c, nb + 1, &parts));
+    const long n = 1L << r_len;
+    k_eq_dot<<<nb, 256, 0, c->stream>>>(g->vals[last], lo, hi, fh, n, parts);
+    VG_LAUNCHED(c);
+    VG_TRY(vg_reduce_partials(c, parts, nb, 1, parts + nb));
+    VG_CHECK_CUDA(cudaMemcpyAsync(out, parts + nb, sizeof(fe), cudaMemcpyDeviceToHost, c->stream));
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    return VG_OK;
+}
+
+extern "C" int vg_mle_eval(vg_ctx *c, const vg_fe *vals, long n, const vg_fe *r, int log_n, vg_fe *out)
+{
+    if (!c || !vals || !r || !out || log_n < 0 || log_n > 30 || n < (1L << log_n))
+        return vg_fail(VG_ERR_ARG, "vg_mle_eval: bad argument (n=%ld log_n=%d)", n, log_n);
+    const long m = 1L << log_n;
+    int f = log_n >> 1, s = log_n - f;
+    fe *tmp;
+    VG_CHECK_CUDA(cudaMalloc(&tmp, ((1L << f) + (1L << s) + 64 + (vg_is_device_ptr(vals) ? 0 : m)) * sizeof(fe)));
+    fe *lo = tmp, *hi = tmp + (1L << f), *rd = hi + (1L << s);
+    const fe *v = (const fe *)vals;
+    if (!vg_is_device_ptr(vals)) {
+        fe *vd = rd + 64;
+        cudaMemcpyAsync(vd, vals, m * sizeof(fe), cudaMemcpyHostToDevice, c->stream);
+        v = vd;
+    }
+    if (log_n) cudaMemcpyAsync(rd, r, log_n * sizeof(fe), cudaMemcpyHostToDevice, c->stream);
+    k_eq_half<<<grid_for(1L << f, 256), 256, 0, c->stream>>>(rd, f, vg::fe_one(), lo);
+    c->launches++;
+    k_eq_half<<<grid_for(1L << s, 256), 256, 0, c->stream>>>(rd + f, s, vg::fe_one(), hi);
+    c->launches++;
+    fe *parts;
+    const int nb = 148 * 2;
+    int rc = vg_partials(c, nb + 1, &parts);
+    if (rc != VG_OK) {
+        cudaFree(tmp);
+        return rc;
+    }
+    k_eq_dot<<<nb, 256, 0, c->stream>>>(v, lo, hi, f, m, parts);
+    c->launches++;
+    rc = vg_reduce_partials(c, parts, nb, 1, parts + nb);
+    if (rc == VG_OK) {
+        cudaMemcpyAsync(out, parts + nb, sizeof(fe), cudaMemcpyDeviceToHost, c->stream);
+        cudaError_t e = cudaStreamSynchronize(c->stream);
+        if (e != cudaSuccess) rc = vg_fail(VG_ERR_CUDA, "vg_mle_eval: %s", cudaGetErrorString(e));
+    }
+    cudaFree(tmp);
+    return rc;
+}
+
+extern "C" int vg_eq_table(vg_ctx *c, const vg_fe *r, int log_len, vg_fe *pub)
+{
+    if (!c || !r || !pub || log_len < 1 || log_len > 30) return vg_fail(VG_ERR_ARG, "vg_eq_table: bad argument");
+    fe *tmp;
+    int f = log_len >> 1, s = log_len - f;
+    VG_CHECK_CUDA(cudaMalloc(&tmp, ((1L << f) + (1L << s) + 64) * sizeof(fe)));
+    fe *lo = tmp, *hi = tmp + (1L << f), *rd = hi + (1L << s);
+    cudaMemcpyAsync(rd, r, log_len * sizeof(fe), cudaMemcpyHostToDevice, c->stream);
+    k_eq_half<<<grid_for(1L << f, 256), 256, 0, c->stream>>>(rd, f, vg::fe_one(), lo);
+    c->launches++;
+    k_eq_half<<<grid_for(1L << s, 256), 256, 0, c->stream>>>(rd + f, s, vg::fe_one(), hi);
+    c->launches++;
+    long n = 1L << log_len;
+    k_eq_combine<<<std::min<unsigned>(grid_for(n, 256), 148u * 32u), 256, 0, c->stream>>>(lo, hi, f, n, (fe *)pub);
+    VG_LAUNCHED(c);
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    cudaFree(tmp);
+    return VG_OK;
+}
+
+static int finalize_tables(vg_gkr *g, long N)
+{
+    vg_ctx *c = g->ctx;
+    const long maxN = 1L << g->C->max_bl;
+    unsigned grid = std::min<unsigned>(grid_for(N, 256), 148u * 32u);
+    k_acc_finalize<<<grid, 256, 0, c->stream>>>(g->acc, N, g->buf[0][2]);   // add_mult_sum
+    VG_LAUNCHED(c);
+    k_acc_finalize<<<grid, 256, 0, c->stream>>>(g->acc + 4 * maxN, N, g->buf[0][1]);   // addV_array
+    VG_LAUNCHED(c);
+    g->n = N;
+    g->cur[1] = g->buf[0][1];
+    g->cur[2] = g->buf[0][2];
+    g->next_buf = 1;
+    g->round0_pending = true;
+    return VG_OK;
+}
+
+extern "C" int vg_gkr_phase1_init(vg_gkr *g, int layer, const vg_fe *r0, const vg_fe *r1, int length_g, vg_fe alpha,
+                                  vg_fe beta)
+{
+    if (!g || !r0 || !r1) return vg_fail(VG_ERR_ARG, "vg_gkr_phase1_init: null argument");
+    if (layer < 1 || layer >= g->C->depth) return vg_fail(VG_ERR_ARG, "layer %d out of range", layer);
+    if (length_g != g->C->L[layer].bl) return vg_fail(VG_ERR_ARG, "length_g %d != layer bit length %d", length_g, g->C->L[layer].bl);
+    vg_ctx *c = g->ctx;
+    const DevLayer &D = g->C->L[layer];
+    const long N = g->C->L[layer - 1].n, maxN = 1L << g->C->max_bl;
+    g->layer = layer;
+    g->length_g = length_g;
+    VG_TRY(upload_r(g, 0, r0, length_g));
+    VG_TRY(upload_r(g, 1, r1, length_g));
+    fe *e = g->eq;
+    const long H = g->eq_half;
+    int fh;
+    VG_TRY(build_halves(g, g->rbuf, length_g, tofe(alpha), e, e + H, &fh));
+    VG_TRY(build_halves(g, g->rbuf + 64, length_g, tofe(beta), e + 2 * H, e + 3 * H, &fh));
+    g->bg.f0 = e;
+    g->bg.s0 = e + H;
+    g->bg.f1 = e + 2 * H;
+    g->bg.s1 = e + 3 * H;
+    g->bg.fh = fh;
+    g->bg.mask = (1L << fh) - 1;
+    VG_CHECK_CUDA(cudaMemsetAsync(g->acc, 0, N * 4 * sizeof(unsigned long long), c->stream));
+    VG_CHECK_CUDA(cudaMemsetAsync(g->acc + 4 * maxN, 0, N * 4 * sizeof(unsigned long long), c->stream));
+    unsigned grid = std::min<unsigned>(grid_for(D.n, GKR_THREADS), 148u * 32u);
+    k_phase1_scatter<<<grid, GKR_THREADS, 0, c->stream>>>(D.ty, D.u, D.v, D.n, g->bg, g->vals[layer - 1], g->acc,
+                                                         g->acc + 4 * maxN);
+    VG_LAUNCHED(c);
+    g->cur[0] = g->vals[layer - 1];
+    return finalize_tables(g, N);
+}
+
+extern "C" int vg_gkr_phase2_init(vg_gkr *g, const vg_fe *r_u, int length_u, vg_fe v_u)
+{
+    if (!g || !r_u) return vg_fail(VG_ERR_ARG, "vg_gkr_phase2_init: null argument");
+    if (g->layer < 1) return vg_fail(VG_ERR_STATE, "phase2_init before phase1_init");
+    const int layer = g->layer;
+    if (length_u != g->C->L[layer - 1].bl) return vg_fail(VG_ERR_ARG, "length_u %d != previous layer bit length %d", length_u, g->C->L[layer - 1].bl);
+    vg_ctx *c = g->ctx;
+    const DevLayer &D = g->C->L[layer];
+    const long N = g->C->L[layer - 1].n, maxN = 1L << g->C->max_bl;
+    VG_TRY(upload_r(g, 2, r_u, length_u));
+    fe *e = g->eq + 4 * g->eq_half;
+    int fh;
+    VG_TRY(build_halves(g, g->rbuf + 128, length_u, vg::fe_one(), e, e + g->eq_half, &fh));
+    BetaU bu;
+    bu.f = e;
+    bu.s = e + g->eq_half;
+    bu.fh = fh;
+    bu.mask = (1L << fh) - 1;
+    VG_CHECK_CUDA(cudaMemsetAsync(g->acc, 0, N * 4 * sizeof(unsigned long long), c->stream));
+    VG_CHECK_CUDA(cudaMemsetAsync(g->acc + 4 * maxN, 0, N * 4 * sizeof(unsigned long long), c->stream));
+    unsigned grid = std::min<unsigned>(grid_for(D.n, GKR_THREADS), 148u * 32u);
+    k_phase2_scatter<<<grid, GKR_THREADS, 0, c->stream>>>(D.ty, D.u, D.v, D.n, g->bg, bu, tofe(v_u), g->acc,
+                                                         g->acc + 4 * maxN);
+    VG_LAUNCHED(c);
+    g->cur[0] = g->vals[layer - 1];
+    return finalize_tables(g, N);
+}
+
+extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, vg_fe *out3, vg_fe *last6)
+{
+    if (!g || !out3) return vg_fail(VG_ERR_ARG, "vg_gkr_round: null argument");
+    if (g->layer < 1 || g->n < 2) return vg_fail(VG_ERR_STATE, "sumcheck round without tables (n=%ld)", g->n);
+    const bool fold = current_bit != 0;
+    if (!fold && !g->round0_pending) return vg_fail(VG_ERR_STATE, "current_bit 0 only directly after an init");
+    if (fold && g->round0_pending) return vg_fail(VG_ERR_STATE, "first round after an init must have current_bit 0");
+    if (fold && g->n < 4) return vg_fail(VG_ERR_STATE, "no variables left to fold");
+    vg_ctx *c = g->ctx;
+    const long n_out = fold ? g->n / 2 : g->n;   // table length the sums are taken over
+    const long npairs = n_out / 2;
+    unsigned grid = std::min<unsigned>(grid_for(npairs, GKR_THREADS), 148u * 8u);
+    fe *parts;
+    VG_TRY(vg_partials(c, 3 * (size_t)grid + 3 + 6, &parts));
+    fe *y[3] = {g->buf[g->next_buf][0], g->buf[g->next_buf][1], g->buf[g->next_buf][2]};
+    fe r = tofe(previous_random);
+    if (fold)
+        k_round<true><<<grid, GKR_THREADS, 0, c->stream>>>(g->cur[0], g->cur[1], g->cur[2], npairs, r, y[0], y[1], y[2], parts);
+    else
+        k_round<false><<<grid, GKR_THREADS, 0, c->stream>>>(g->cur[0], g->cur[1], g->cur[2], npairs, r, nullptr, nullptr, nullptr, parts);
+    VG_LAUNCHED(c);
+    VG_TRY(vg_reduce_partials(c, parts, (int)grid, 3, parts + 3 * grid));
+    if (fold) {
+        g->cur[0] = y[0];
+        g->cur[1] = y[1];
+        g->cur[2] = y[2];
+        g->next_buf ^= 1;
+        g->n = n_out;
+    }
+    g->round0_pending = false;
+    fe *host;
+    VG_TRY(vg_pinned(c, 9, &host));
+    VG_CHECK_CUDA(cudaMemcpyAsync(host, parts + 3 * grid, 3 * sizeof(fe), cudaMemcpyDeviceToHost, c->stream));
+    const bool want_last = last6 && g->n == 2;
+    if (want_last) {
+        for (int k = 0; k < 3; ++k)
+            VG_CHECK_CUDA(cudaMemcpyAsync(host + 3 + 2 * k, g->cur[k], 2 * sizeof(fe), cudaMemcpyDeviceToHost, c->stream));
+    }
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    for (int k = 0; k < 3; ++k) out3[k] = tovg(host[k]);
+    if (want_last)
+        for (int k = 0; k < 6; ++k) last6[k] = tovg(host[3 + k]);
+    return VG_OK;
+}

@@ -1,0 +1,571 @@
+// Whole proofs without the reference verifier in the loop.
+//
+// The protocol is interactive, but every verifier challenge comes from the
+// same glibc rand() stream as the prover's masks and never depends on a
+// prover message.  A session therefore replays the verifier's draws in the
+// reference's order (src/linear_gkr/zk_verifier.cpp:910-1253 and
+// src/VPD/vpd_verifier.cpp:80-335) and calls the prover exactly as the
+// verifier would, producing the same messages, roots and query answers.
+// The verifier's own checks and its predicate evaluation are not run; the
+// one prover input that comes from the predicates, the general value of
+// sumcheck_finalround (zk_verifier.cpp:1149), is fixed by the sumcheck claim
+// itself: finalround(0) + finalround(1) + direct_relay * v_u must equal the
+// running claim, and the general value enters finalround's linear
+// coefficient only, so it is that difference.
+//
+// The transcript has the record layout of the oracle's recorder: 1 byte tag,
+// uint32 count of 16-byte units, the units.
+#include <stdlib.h>
+#include <algorithm>
+#include <chrono>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+#include "device.h"
+#include "linear_gkr/zk_prover.h"
+#include "poly_commitment/poly_commit.h"
+
+typedef prime_field::field_element F;
+using clk = std::chrono::high_resolution_clock;
+
+static double since(clk::time_point t0)
+{
+    return std::chrono::duration_cast<std::chrono::duration<double>>(clk::now() - t0).count();
+}
+
+namespace
+{
+struct Transcript {
+    std::vector<uint8_t> bytes;
+    bool on = true;
+    void put(char tag, const void *units, uint32_t n16)
+    {
+        if (!on) return;
+        size_t o = bytes.size();
+        bytes.resize(o + 5 + 16 * (size_t)n16);
+        bytes[o] = (uint8_t)tag;
+        memcpy(&bytes[o + 1], &n16, 4);
+        if (n16) memcpy(&bytes[o + 5], units, 16 * (size_t)n16);
+    }
+    void fe(char tag, const F &x) { put(tag, &x, 1); }
+    void answer(char tag, const std::pair<std::vector<std::pair<F, F> >, std::vector<__hhash_digest> > &a, int new_size)
+    {
+        std::vector<uint8_t> buf(16 + a.first.size() * 32 + a.second.size() * 32);
+        int64_t hdr[2] = {(int64_t)new_size, (int64_t)((a.first.size() << 16) | a.second.size())};
+        memcpy(buf.data(), hdr, 16);
+        size_t off = 16;
+        for (auto &pv : a.first) {
+            memcpy(&buf[off], &pv.first, 16);
+            memcpy(&buf[off + 16], &pv.second, 16);
+            off += 32;
+        }
+        for (auto &h : a.second) {
+            memcpy(&buf[off], &h, 32);
+            off += 32;
+        }
+        put(tag, buf.data(), (uint32_t)(buf.size() / 16));
+    }
+};
+
+std::vector<F> draws(int n)
+{
+    std::vector<F> r(n);
+    for (int i = 0; i < n; ++i) r[i] = prime_field::random();
+    return r;
+}
+
+// zk_verifier.cpp:608-619
+F direct_relay(const layered_circuit &C, int depth, const F *r_g, const F *r_u)
+{
+    if (depth != 1) return F(0);
+    F ret(1);
+    for (int i = 0; i < C.circuit[depth].bit_length; ++i)
+        ret = ret * (F(1) - r_g[i] - r_u[i] + F(2) * r_g[i] * r_u[i]);
+    return ret;
+}
+}  // namespace
+
+struct vg_session {
+    layered_circuit C;
+    std::vector<std::vector<gate> > storage;
+    vg_circuit *dev = nullptr;
+    zk_prover *p = nullptr;
+};
+
+// ----------------------------------------------------------- circuit build
+// The file-level layers (input layer first) turned into the prover's circuit
+// the way zk_verifier::read_circuit does (zk_verifier.cpp:24-191): the input
+// layer becomes layer 0 (values) plus a relay layer 1, padded to 2^17 gates
+// when there are more than three file layers and to 2^15 otherwise.
+static int build_circuit(vg_session *s, int d, const long *n, const uint8_t *const *ty, const int64_t *const *u,
+                         const int64_t *const *v, std::string &err)
+{
+    if (d < 1) {
+        err = "circuit needs at least one layer";
+        return VG_ERR_ARG;
+    }
+    layered_circuit &C = s->C;
+    C.total_depth = d + 1;
+    C.circuit = new layer[d + 1];
+    s->storage.assign(d + 1, std::vector<gate>());
+    const int pad_log = d > 3 ? 17 : 15;
+    for (int i = 1; i <= d; ++i) {
+        long cnt = n[i - 1];
+        if (cnt < 1) {
+            err = "empty layer";
+            return VG_ERR_ARG;
+        }
+        long padded = cnt;
+        if (i == 1 && cnt < (1L << pad_log)) padded = 1L << pad_log;
+        int bl = 0;
+        while ((1L << bl) < padded) ++bl;
+        if (padded == 1) bl = 1;   // a single gate gets a dummy partner
+        const long full = 1L << bl;
+        const int prev_bl = i == 1 ? 0 : C.circuit[i - 1].bit_length;
+        for (long g = 0; g < cnt; ++g) {
+            const int t = ty[i - 1][g];
+            const long long a = u[i - 1][g], b = v[i - 1][g];
+            if (i == 1) {
+                if (t != 2 && t != 3) {
+                    err = "input layer gates must have type 2 or 3";
+                    return VG_ERR_ARG;
+                }
+                continue;
+            }
+            const long long np = 1LL << prev_bl;
+            bool ok;
+            if (t == 3 || t == 2) ok = true;
+            else if (t == 5) ok = a >= 0 && a < np && b > a && b <= np;
+            else if (t == 12) ok = a >= 0 && a <= b && b < np && b - a + 1 <= 60;
+            else if (t == 6 || t == 10) ok = a >= 0 && a < np;
+            else if (t > 13 || t == 11) ok = false;
+            else ok = a >= 0 && a < np && b >= 0 && b < np && (t != 13 || a == b) && (t != 4 || a < (1LL << bl));
+            if (!ok) {
+                char buf[200];
+                snprintf(buf, sizeof buf, "layer %d gate %ld: type %d u %lld v %lld invalid", i, g, t, a, b);
+                err = buf;
+                return VG_ERR_ARG;
+            }
+        }
+        if (i == 1) {
+            auto &in = s->storage[0];
+            auto &relay = s->storage[1];
+            in.assign(full, gate(2, 0, 0));
+            relay.assign(full, gate(2, 0, 0));
+            for (long g = 0; g < cnt; ++g) {
+                in[g] = gate(ty[0][g], u[0][g], v[0][g]);
+                relay[g] = gate(4, g, 0);
+            }
+            for (long g = cnt; g < padded; ++g) {
+                in[g] = gate(3, 0, 0);
+                relay[g] = gate(4, g, 0);
+            }
+            if (padded == 1) relay[1] = gate(4, 1, 0);
+            C.circuit[0].gates = in.data();
+            C.circuit[1].gates = relay.data();
+            C.circuit[0].bit_length = C.circuit[1].bit_length = bl;
+        } else {
+            auto &L = s->storage[i];
+            L.assign(full, gate(2, 0, 0));
+            for (long g = 0; g < cnt; ++g) {
+                const int t = ty[i - 1][g];
+                L[g] = gate(t, u[i - 1][g], (t == 6 || t == 10) ? 0 : v[i - 1][g]);
+            }
+            C.circuit[i].gates = L.data();
+            C.circuit[i].bit_length = bl;
+        }
+    }
+    return VG_OK;
+}
+
+static int session_finish(vg_session *s)
+{
+    const int depth = s->C.total_depth;
+    std::vector<int> bl(depth);
+    std::vector<std::vector<uint8_t> > ty(depth);
+    std::vector<std::vector<int64_t> > u(depth), v(depth);
+    std::vector<const uint8_t *> pty(depth);
+    std::vector<const int64_t *> pu(depth), pv(depth);
+    for (int i = 0; i < depth; ++i) {
+        bl[i] = s->C.circuit[i].bit_length;
+        const long nn = 1L << bl[i];
+        ty[i].resize(nn);
+        u[i].resize(nn);
+        v[i].resize(nn);
+        for (long k = 0; k < nn; ++k) {
+            ty[i][k] = (uint8_t)s->C.circuit[i].gates[k].ty;
+            u[i][k] = s->C.circuit[i].gates[k].u;
+            v[i][k] = s->C.circuit[i].gates[k].v;
+        }
+        pty[i] = ty[i].data();
+        pu[i] = u[i].data();
+        pv[i] = v[i].data();
+    }
+    int rc = vg_circuit_upload(virgo::ctx(), depth, bl.data(), pty.data(), pu.data(), pv.data(), &s->dev);
+    if (rc != VG_OK) return rc;
+    s->p = new zk_prover();
+    s->p->attach_circuit(s->C, s->dev);
+    return VG_OK;
+}
+
+extern "C" int vg_session_create(int d, const long *n, const uint8_t *const *ty, const int64_t *const *u,
+                                 const int64_t *const *v, vg_session **out)
+{
+    if (!n || !ty || !u || !v || !out) return VG_ERR_ARG;
+    vg_session *s = new vg_session();
+    std::string err;
+    int rc = build_circuit(s, d, n, ty, u, v, err);
+    if (rc == VG_OK) rc = session_finish(s);
+    if (rc != VG_OK) {
+        if (!err.empty()) fprintf(stderr, "vg_session_create: %s\n", err.c_str());
+        vg_session_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return VG_OK;
+}
+
+// text circuit format of src/linear_gkr/README.md (the meta file is only
+// needed by the verifier's predicate evaluation and is not read here)
+extern "C" int vg_session_from_file(const char *circuit_path, vg_session **out)
+{
+    FILE *f = fopen(circuit_path, "rb");
+    if (!f) return VG_ERR_ARG;
+    fseek(f, 0, SEEK_END);
+    long sz = ftell(f);
+    fseek(f, 0, SEEK_SET);
+    std::vector<char> buf(sz + 1);
+    size_t got = fread(buf.data(), 1, sz, f);
+    fclose(f);
+    buf[got] = 0;
+    const char *p = buf.data();
+    auto next = [&](long long &x) -> bool {
+        while (*p && (*p < '0' || *p > '9') && *p != '-') ++p;
+        if (!*p) return false;
+        bool neg = false;
+        if (*p == '-') {
+            neg = true;
+            ++p;
+        }
+        long long r = 0;
+        while (*p >= '0' && *p <= '9') r = r * 10 + (*p++ - '0');
+        x = neg ? -r : r;
+        return true;
+    };
+    long long d;
+    if (!next(d) || d < 1 || d > 100000) return VG_ERR_ARG;
+    std::vector<long> n(d);
+    std::vector<std::vector<uint8_t> > ty(d);
+    std::vector<std::vector<int64_t> > u(d), v(d);
+    for (long long i = 0; i < d; ++i) {
+        long long cnt;
+        if (!next(cnt) || cnt < 1) return VG_ERR_ARG;
+        n[i] = (long)cnt;
+        ty[i].resize(cnt);
+        u[i].resize(cnt);
+        v[i].resize(cnt);
+        for (long long j = 0; j < cnt; ++j) {
+            long long t, g, a, b;
+            if (!next(t) || !next(g) || !next(a) || !next(b)) return VG_ERR_ARG;
+            if (g != j) {
+                fprintf(stderr, "Error, gates must be in sorted order, and full [0, 2^n - 1]. %lld %lld %lld\n", i + 1, j, g);
+                return VG_ERR_ARG;
+            }
+            ty[i][j] = (uint8_t)t;
+            u[i][j] = a;
+            v[i][j] = b;
+        }
+    }
+    std::vector<const uint8_t *> pty(d);
+    std::vector<const int64_t *> pu(d), pv(d);
+    for (long long i = 0; i < d; ++i) {
+        pty[i] = ty[i].data();
+        pu[i] = u[i].data();
+        pv[i] = v[i].data();
+    }
+    return vg_session_create((int)d, n.data(), pty.data(), pu.data(), pv.data(), out);
+}
+
+extern "C" int vg_session_destroy(vg_session *s)
+{
+    if (!s) return VG_OK;
+    if (s->p) {
+        s->p->delete_self();
+        delete s->p;
+    }
+    if (s->dev) vg_circuit_destroy(s->dev);
+    delete[] s->C.circuit;
+    delete s;
+    return VG_OK;
+}
+
+extern "C" int vg_session_depth(vg_session *s, int *depth, int *input_log)
+{
+    if (!s) return VG_ERR_ARG;
+    if (depth) *depth = s->C.total_depth;
+    if (input_log) *input_log = s->C.circuit[0].bit_length;
+    return VG_OK;
+}
+
+extern "C" void vg_free(void *p) { free(p); }
+
+extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcript, vg_proof_stats *stats,
+                                uint8_t **transcript, size_t *transcript_len)
+{
+    if (!s || !s->p) return VG_ERR_ARG;
+    auto t_all = clk::now();
+    vg_proof_stats st;
+    memset(&st, 0, sizeof st);
+    long long launches0 = 0;
+    vg_ctx_launch_count(virgo::ctx(), &launches0);
+
+    // the reference's rand() stream after srand(seed), private to this thread
+    struct random_data rd;
+    int32_t statebuf[32];   // 128 bytes: glibc's default TYPE_3 state, as srand() uses
+    memset(&rd, 0, sizeof rd);
+    memset(statebuf, 0, sizeof statebuf);
+    initstate_r(seed, (char *)statebuf, sizeof statebuf, &rd);
+    prime_field::set_thread_random_state(&rd);
+    auto rand_int = [&]() {
+        int32_t r;
+        random_r(&rd, &r);
+        return (int)r;
+    };
+
+    Transcript tr;
+    tr.on = want_transcript != 0;
+    zk_prover &p = *s->p;
+    layered_circuit &C = s->C;
+    p.reset_proof();
+    int proof_size = 0;
+
+    // ---------------- GKR (zk_verifier.cpp:919-1207) ----------------
+    auto t0 = clk::now();
+    F *result = p.evaluate();
+    st.evaluate_s = since(t0);
+    t0 = clk::now();
+    F alpha(1), beta(0);
+    const int out_bl = C.circuit[C.total_depth - 1].bit_length;
+    std::vector<F> r_0 = draws(out_bl), r_1 = draws(out_bl);
+    std::vector<F> omr_0(out_bl), omr_1(out_bl);
+    for (int i = 0; i < out_bl; ++i) {
+        omr_0[i] = F(1) - r_0[i];
+        omr_1[i] = F(1) - r_1[i];
+    }
+    F a_0 = p.V_res(omr_0.data(), r_0.data(), result, out_bl, 1 << out_bl);
+    tr.fe('R', a_0);
+    F alpha_beta_sum = alpha * a_0;
+    std::vector<F> all_pub_mask;
+    F all_mask_sum(0);
+
+    for (int i = C.total_depth - 1; i >= 1; --i) {
+        const int ll = C.circuit[i - 1].bit_length;
+        F rho = prime_field::random();
+        p.sumcheck_init(i, C.circuit[i].bit_length, ll, ll, alpha, beta, r_0.data(), r_1.data(), omr_0.data(), omr_1.data());
+        p.generate_maskpoly_pre_rho(ll * 2 + 1, 2);
+        p.rho = rho;
+        p.generate_maskpoly_after_rho(ll * 2 + 1, 2);
+        tr.fe('S', p.maskpoly_sumc);
+        alpha_beta_sum = alpha_beta_sum + p.maskpoly_sumc;
+        p.sumcheck_phase1_init();
+        F previous_random(0);
+        std::vector<F> r_u = draws(ll), r_v = draws(ll);
+        F direct_relay_value = alpha * direct_relay(C, i, r_0.data(), r_u.data()) + beta * direct_relay(C, i, r_1.data(), r_u.data());
+        F r_c = prime_field::random();
+        if (i == 1) {
+            for (int j = 0; j < ll; ++j) r_v[j] = F(0);
+            r_c = F(0);
+        }
+        F random_combine = prime_field::random();
+        F linear_coeff = prime_field::random();
+        // public coefficients of the R mask at preu1 / prev1 (zk_verifier.cpp:983-990)
+        const F pu1 = p.prepreu1, pv1 = p.preprev1, one(1);
+        all_pub_mask.push_back(one * random_combine + linear_coeff * one * random_combine);
+        all_pub_mask.push_back(pu1 * random_combine + linear_coeff * pv1 * random_combine);
+        all_pub_mask.push_back(pu1 * pu1 * random_combine + linear_coeff * pv1 * pv1 * random_combine);
+        all_pub_mask.push_back(r_c * random_combine + linear_coeff * r_c * random_combine);
+        all_pub_mask.push_back(r_c * r_c * random_combine + linear_coeff * r_c * r_c * random_combine);
+        all_pub_mask.push_back(pu1 * r_c * random_combine + linear_coeff * pv1 * r_c * random_combine);
+        // public coefficients of the sumcheck mask polynomial (zk_verifier.cpp:1002-1025)
+        F linear_combine = prime_field::random();
+        for (int k = 0; k < ll; ++k) {
+            all_pub_mask.push_back(linear_combine * r_u[k] * r_u[k] * rho);
+            all_pub_mask.push_back(linear_combine * r_u[k] * rho);
+        }
+        for (int k = 0; k < ll; ++k) {
+            all_pub_mask.push_back(linear_combine * r_v[k] * r_v[k] * rho);
+            all_pub_mask.push_back(linear_combine * r_v[k] * rho);
+        }
+        all_pub_mask.push_back(linear_combine * r_c * r_c * rho);
+        all_pub_mask.push_back(linear_combine * r_c * rho);
+        all_pub_mask.push_back(linear_combine * one * rho);
+        const F ul = r_u[ll - 1], vl = r_v[ll - 1];
+        all_pub_mask.push_back(linear_combine * ul * ul * ul * ul * ul * rho);
+        all_pub_mask.push_back(linear_combine * ul * ul * ul * ul * rho);
+        all_pub_mask.push_back(linear_combine * ul * ul * ul * rho);
+        all_pub_mask.push_back(linear_combine * vl * vl * vl * vl * vl * rho);
+        all_pub_mask.push_back(linear_combine * vl * vl * vl * vl * rho);
+        all_pub_mask.push_back(linear_combine * vl * vl * vl * rho);
+        std::vector<F> omr_u(ll), omr_v(ll);
+        for (int j = 0; j < ll; ++j) {
+            omr_u[j] = F(1) - r_u[j];
+            omr_v[j] = F(1) - r_v[j];
+        }
+        // phase 1
+        for (int j = 0; j < ll; ++j) {
+            if (j == ll - 1) {
+                quintuple_poly poly = p.sumcheck_phase1_updatelastbit(previous_random, j);
+                proof_size += sizeof(quintuple_poly);
+                F u6[6] = {poly.a, poly.b, poly.c, poly.d, poly.e, poly.f};
+                tr.put('p', u6, 6);
+                alpha_beta_sum = poly.eval(r_u[j]);
+            } else {
+                quadratic_poly poly = p.sumcheck_phase1_update(previous_random, j);
+                proof_size += sizeof(quadratic_poly);
+                F u3[3] = {poly.a, poly.b, poly.c};
+                tr.put('q', u3, 3);
+                alpha_beta_sum = poly.eval(r_u[j]);
+            }
+            previous_random = r_u[j];
+        }
+        p.sumcheck_phase2_init(previous_random, r_u.data(), omr_u.data());
+        tr.fe('u', p.v_u);
+        previous_random = F(0);
+        for (int j = 0; j < ll; ++j) {
+            if (i == 1) r_v[j] = F(0);
+            if (j == ll - 1) {
+                quintuple_poly poly = p.sumcheck_phase2_updatelastbit(previous_random, j);
+                proof_size += sizeof(quintuple_poly);
+                F u6[6] = {poly.a, poly.b, poly.c, poly.d, poly.e, poly.f};
+                tr.put('P', u6, 6);
+                alpha_beta_sum = poly.eval(r_v[j]) + direct_relay_value * p.v_u;
+            } else {
+                quadratic_poly poly = p.sumcheck_phase2_update(previous_random, j);
+                proof_size += sizeof(quadratic_poly);
+                F u3[3] = {poly.a, poly.b, poly.c};
+                tr.put('Q', u3, 3);
+                alpha_beta_sum = poly.eval(r_v[j]) + direct_relay_value * p.v_u;
+            }
+            previous_random = r_v[j];
+        }
+        auto claims = p.sumcheck_finalize(previous_random);
+        F cl[2] = {claims.first, claims.second};
+        tr.put('z', cl, 2);
+        const F v_u = claims.first;
+        // final round with the general value implied by the claim
+        quadratic_poly fin = p.sumcheck_finalround(previous_random, ll << 1, F(0));
+        F general = alpha_beta_sum - direct_relay_value * v_u - (fin.a + fin.b + fin.c + fin.c);
+        fin.b = fin.b + general;
+        F u3[3] = {fin.a, fin.b, fin.c};
+        tr.put('f', u3, 3);
+        if (i == 1) r_c = F(0);
+        alpha_beta_sum = fin.eval(r_c) + direct_relay_value * p.v_u;
+        F mv = p.query(r_u.data(), r_v.data(), r_c);
+        tr.fe('y', mv);
+        F g1 = p.queryRg1(r_c);
+        tr.fe('g', g1);
+        F g2 = p.queryRg2(r_c);
+        tr.fe('h', g2);
+        all_mask_sum = all_mask_sum + g1 * random_combine + linear_coeff * g2 * random_combine + linear_combine * mv;
+        alpha = prime_field::random();
+        beta = prime_field::random();
+        alpha_beta_sum = i != 1 ? alpha * v_u + beta * claims.second : v_u;
+        r_0 = r_u;
+        r_1 = r_v;
+        omr_0 = omr_u;
+        omr_1 = omr_v;
+    }
+    all_pub_mask.push_back(p.Zu);
+    all_pub_mask.push_back(p.Zu * p.preu1);
+    p.all_pri_mask.push_back(p.maskr[0]);
+    p.all_pri_mask.push_back(p.maskr[1]);
+    all_mask_sum = all_mask_sum + p.Zu * p.sumRc.eval(p.preu1);
+    st.gkr_s = since(t0);
+
+    // ---------------- commitments (zk_verifier.cpp:1210-1219) ----------------
+    t0 = clk::now();
+    const int L = C.circuit[0].bit_length;
+    __hhash_digest root_l = p.poly_prover.commit_private_array(p.circuit_value[0], L, p.all_pri_mask);
+    tr.put('C', &root_l, 2);
+    void *pub = nullptr;
+    virgo::check(vg_dev_alloc(virgo::ctx(), ((size_t)1 << L) * sizeof(F), &pub), "vg_dev_alloc");
+    virgo::check(vg_eq_table(virgo::ctx(), (const vg_fe *)r_0.data(), L, (vg_fe *)pub), "vg_eq_table");
+    F all_sum[slice_number + 1];
+    F target = alpha_beta_sum - p.Zu * p.sumRc.eval(p.preu1) + all_mask_sum;
+    __hhash_digest root_h = p.poly_prover.commit_public_array(all_pub_mask, (F *)pub, L, target, all_sum);
+    tr.put('C', &root_h, 2);
+    vg_dev_free(virgo::ctx(), pub);
+    proof_size += 2 * sizeof(__hhash_digest);
+    tr.put('A', all_sum, slice_number + 1);
+    __hhash_digest lh[2] = {root_l, root_h};
+    tr.put('B', lh, 4);
+    st.commit_s = since(t0);
+
+    // ---------------- FRI commit phase (vpd_verifier.cpp:46-78, 101) ----------------
+    t0 = clk::now();
+    const int saved = fri::log_current_witness_size_per_slice;
+    int codeword_size = 1 << (L + rs_code_rate - log_slice_number);
+    int levels = 0;
+    while (codeword_size > (1 << rs_code_rate)) {
+        F r = prime_field::random();
+        __hhash_digest h = fri::commit_phase_step(r);
+        tr.put('T', &h, 2);
+        codeword_size /= 2;
+        ++levels;
+    }
+    F *final_cw = fri::commit_phase_final();
+    {
+        const int nfin = 1 << fri::log_current_witness_size_per_slice;
+        tr.put('X', final_cw, (uint32_t)(nfin * slice_number));
+        tr.put('x', fri::cpd.rs_codeword_msk[fri::current_step_no - 1], (uint32_t)nfin);
+    }
+    fri::log_current_witness_size_per_slice = saved;
+    st.fri_s = since(t0);
+
+    // ---------------- query answers (vpd_verifier.cpp:105-312) ----------------
+    t0 = clk::now();
+    for (int rep = 0; rep < ldt_repeat_num; ++rep) {
+        long long pow = 0;
+        for (int i = 0; i < L - log_slice_number; ++i) {
+            const int lw = L + rs_code_rate - log_slice_number - i;
+            int new_size = 0;
+            if (i == 0) {
+                do {
+                    pow = rand_int() % (1 << lw);
+                } while (pow < (1 << (L - log_slice_number - i)) || pow % 2 == 1);
+                const long long s0 = pow / 2, s1 = (pow + (1LL << lw)) / 2;
+                auto al = fri::request_init_value_with_merkle(s0, s1, new_size, 0);
+                tr.answer('I', al, new_size);
+                auto ah = fri::request_init_value_with_merkle(s0, s1, new_size, 1);
+                tr.answer('I', ah, new_size);
+                proof_size += new_size;
+                auto b = fri::request_step_commit(0, pow / 2, new_size);
+                tr.answer('J', b, new_size);
+                proof_size += new_size;
+            } else {
+                pow = pow % (1 << lw);
+                auto b = fri::request_step_commit(i, pow / 2, new_size);
+                tr.answer('J', b, new_size);
+                proof_size += new_size;
+            }
+        }
+    }
+    st.query_s = since(t0);
+    prime_field::set_thread_random_state(nullptr);
+
+    st.prove_time = p.total_time + p.poly_prover.total_time;
+    st.total_s = since(t_all);
+    st.proof_size = proof_size;
+    long long launches1 = 0;
+    vg_ctx_launch_count(virgo::ctx(), &launches1);
+    st.launches = launches1 - launches0;
+    (void)levels;
+    if (stats) *stats = st;
+    if (transcript && transcript_len) {
+        *transcript_len = tr.bytes.size();
+        *transcript = (uint8_t *)malloc(tr.bytes.size() ? tr.bytes.size() : 1);
+        if (tr.bytes.size()) memcpy(*transcript, tr.bytes.data(), tr.bytes.size());
+    }
+    return VG_OK;
+}
