@@ -45,7 +45,7 @@ __device__ __forceinline__ fe tw_pow(const fe *__restrict__ lo, const fe *__rest
     return a;
 }
 
-__device__ __forceinline__ int bitrev(int x, int bits) { return (int)(__brev((unsigned)x) >> (32 - bits)); }
+__device__ __forceinline__ int bitrev(int x, int bits) { return bits ? (int)(__brev((unsigned)x) >> (32 - bits)) : 0; }
 
 __global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(PassArgs a)
 {
