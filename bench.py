@@ -1,0 +1,377 @@
+#!/usr/bin/env python
+"""Virgo prover benchmark: whole proofs of the 256 x 256 matrix-product circuit
+(2^24 product gates, then 8 add-tree layers, seeded uniform 32-bit entries).
+
+One step = one complete proof: layer evaluation, GKR sumcheck over every
+layer, the polynomial commitment of the input (RS encoding, virtual oracle,
+Merkle trees), the FRI commit phase and the answers to the verifier's 33 query
+repetitions -- the prover side of the reference's zk_proof run.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+ours:       `value` = proofs/s with the circuit resident on the GPU (device
+            time between CUDA events on the prover's stream, max over ranks);
+            `e2e` = the same through the C ABI from pinned host buffers, the
+            circuit upload and the proof transcript download inside each step.
+reference:  the reference prover (compiled from its sources, oracle/_ref) on
+            the host cores, one single-threaded proof per core, proofs/s from
+            its own timers (Prove Time without the fft_gkr side proof, plus
+            evaluate).
+Multi-GPU: replicas only (independent proofs per GPU, no collective on the
+data path), launched by torchrun with one rank per GPU.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "matmul256_addtree_32bit"
+METRIC = "proofs/s (256x256 matmul circuit, 2^24 product gates, full prover)"
+REF_BIN = os.path.join(ROOT, "oracle", "_ref", "zk_proof_ref")
+FFT_BIN = os.path.join(ROOT, "oracle", "_ref", "fft_gkr")
+FAMILIES = ["ntt_pass", "leaf_chain", "merkle_level", "fri_fold_leaf", "virtual_oracle", "eval_layer",
+            "phase1_scatter", "phase2_scatter", "acc_finalize", "sumcheck_round", "reduce", "other"]
+HBM_BOUND = {"ntt_pass", "virtual_oracle", "eval_layer", "phase1_scatter", "phase2_scatter", "acc_finalize",
+             "sumcheck_round", "reduce"}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def make_workload(args):
+    from virgo_b200 import circuits
+    if args.workload == "matmul256":
+        return circuits.matmul_addtree(256, 32, seed=1)
+    if args.workload == "matmul16":
+        return circuits.matmul_addtree(16, 16, seed=1)
+    raise SystemExit("unknown workload " + args.workload)
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (clocks and throttle reasons)."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.rows = []
+        self.stop = threading.Event()
+
+    def _run(self):
+        while not self.stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                for line in out.stdout.strip().splitlines():
+                    self.rows.append([x.strip() for x in line.split(",")])
+            except Exception:
+                pass
+            self.stop.wait(0.2)
+
+    def __enter__(self):
+        self.t = threading.Thread(target=self._run, daemon=True)
+        self.t.start()
+        return self
+
+    def __exit__(self, *a):
+        self.stop.set()
+        self.t.join(timeout=10)
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+# ------------------------------------------------------------- reference arm
+def ref_prover_seconds(workdir):
+    err = open(os.path.join(workdir, "err.txt")).read()
+    ev = float(re.search(r"total evaluation time: ([0-9.eE+-]+)", err).group(1))
+    prove = float(re.search(r"^Prove Time ([0-9.eE+-]+)", err, re.M).group(1))
+    gkr = float(re.search(r"GKR Prove Time ([0-9.eE+-]+)", err).group(1))
+    fft = float(open(os.path.join(workdir, "log_fftgkr.txt")).read().split()[2])
+    return ev + prove - fft, {"evaluate_s": ev, "gkr_s": gkr, "prove_time_s": prove, "fft_gkr_s": fft}
+
+
+def run_reference_proofs(circuit, meta, count, seed0):
+    """`count` concurrent single-threaded reference proofs; returns per-proof
+    prover seconds and stage details."""
+    procs = []
+    for k in range(count):
+        d = tempfile.mkdtemp(prefix="virgo_ref_")
+        os.symlink(FFT_BIN, os.path.join(d, "fft_gkr"))
+        p = subprocess.Popen([REF_BIN, circuit, meta, os.path.join(d, "res.txt"), str(seed0 + k)], cwd=d,
+                             stdout=open(os.path.join(d, "out.txt"), "w"), stderr=open(os.path.join(d, "err.txt"), "w"))
+        procs.append((p, d))
+    res = []
+    for p, d in procs:
+        p.wait()
+        ok = "Pass" in open(os.path.join(d, "out.txt")).read()
+        secs, detail = ref_prover_seconds(d)
+        detail["verified"] = ok
+        res.append((secs, detail))
+    return res
+
+
+def write_circuit_text(layers, circuit, meta):
+    import virgo_b200 as vb
+    L = vb.lib()
+    L.vg_circuit_write_text.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p]
+    d = len(layers)
+    ns = np.array([len(t) for t, _, _ in layers], np.int64)
+    tys, us, vs = (ctypes.c_void_p * d)(), (ctypes.c_void_p * d)(), (ctypes.c_void_p * d)()
+    for i, (t, u, v) in enumerate(layers):
+        tys[i], us[i], vs[i] = t.ctypes.data, u.ctypes.data, v.ctypes.data
+    vb.check(L.vg_circuit_write_text(d, ns.ctypes.data, tys, us, vs, circuit.encode(), meta.encode()), "write text")
+
+
+def reference_arm(args, layers):
+    cores = os.cpu_count() or 1
+    try:
+        mem_gb = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES") / 2 ** 30
+    except Exception:
+        mem_gb = 64
+    if not os.path.exists(REF_BIN):
+        return {"impl": "reference", "unavailable": "reference prover not compiled (oracle/_ref missing)"}
+    tmp = tempfile.mkdtemp(prefix="virgo_circ_")
+    circuit, meta = os.path.join(tmp, "c.txt"), os.path.join(tmp, "m.txt")
+    write_circuit_text(layers, circuit, meta)
+    per_proof_gb = 5.0 if args.workload == "matmul256" else 1.0
+    width = max(1, min(cores, int(mem_gb // per_proof_gb), args.steps + args.warmup))
+    # warm-up proofs run in the same wave when cores allow; only the last K count
+    t0 = time.time()
+    results = run_reference_proofs(circuit, meta, width, seed0=1)
+    measured = results[-args.steps:] if len(results) > args.steps else results
+    wall = time.time() - t0
+    secs = [s for s, _ in measured]
+    value = sum(1.0 / s for s in secs)
+    return {
+        "metric": METRIC, "value": value, "unit": "proofs/s", "impl": "reference",
+        "n_gpus": args.gpus, "steps": len(measured), "warmup": len(results) - len(measured),
+        "ms_per_step": 1000.0 * statistics.mean(secs), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u64 (F_{p^2}, p = 2^61 - 1)", "data": "synthetic (seeded)",
+        "config": {"workload": WORKLOAD if args.workload == "matmul256" else args.workload, "circuit_gates": int(sum(len(t) for t, _, _ in layers)),
+                   "concurrent_proofs": width, "input_log2": 17, "hash": "sha3-256"},
+        "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": width, "kind": "reference",
+                         "sample": "%d concurrent single-threaded reference proofs of the workload, each timed by "
+                                   "its own Prove Time without fft_gkr plus evaluate" % width},
+        "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "reference_detail": [d for _, d in measured], "wall_s": wall,
+    }
+
+
+# -------------------------------------------------------------------- ours
+def session_arrays(layers):
+    """pinned host copies of the file-level layer arrays"""
+    import torch
+    pinned = []
+    for t, u, v in layers:
+        pt = torch.from_numpy(np.ascontiguousarray(t)).pin_memory()
+        pu = torch.from_numpy(np.ascontiguousarray(u)).pin_memory()
+        pv = torch.from_numpy(np.ascontiguousarray(v)).pin_memory()
+        pinned.append((pt, pu, pv))
+    return pinned
+
+
+def create_session_from_pinned(pinned):
+    import virgo_b200 as vb
+    d = len(pinned)
+    ns = np.array([t.numel() for t, _, _ in pinned], np.int64)
+    tys, us, vs = (ctypes.c_void_p * d)(), (ctypes.c_void_p * d)(), (ctypes.c_void_p * d)()
+    for i, (t, u, v) in enumerate(pinned):
+        tys[i], us[i], vs[i] = t.data_ptr(), u.data_ptr(), v.data_ptr()
+    h = ctypes.c_void_p()
+    vb.check(vb.lib().vg_session_create(d, ns.ctypes.data, tys, us, vs, ctypes.byref(h)), "vg_session_create")
+    s = vb.Session.__new__(vb.Session)
+    s.h = h
+    return s
+
+
+def ours(args, layers, rank, world):
+    import virgo_b200 as vb
+    L = vb.lib()
+    L.vg_default_ctx.argtypes = [ctypes.POINTER(ctypes.c_void_p)]
+    L.vg_ctx_profile.argtypes = [ctypes.c_void_p, ctypes.c_int]
+    L.vg_ctx_profile_read.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.POINTER(ctypes.c_longlong),
+                                      ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    L.vg_timer_start.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_void_p)]
+    L.vg_timer_stop.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_double)]
+    L.vg_ctx_launch_count.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_longlong)]
+
+    session = vb.Session(layers)
+    ctx = ctypes.c_void_p()
+    vb.check(L.vg_default_ctx(ctypes.byref(ctx)))
+    seed0 = 1000 * rank + 1
+    for w in range(args.warmup):
+        session.prove(seed0 + w, transcript=True)
+
+    def launches():
+        c = ctypes.c_longlong()
+        L.vg_ctx_launch_count(ctx, ctypes.byref(c))
+        return c.value
+
+    barrier(world)
+    # ---- timed: resident circuit, K proofs ----
+    stages = {"evaluate_s": 0.0, "gkr_s": 0.0, "commit_s": 0.0, "fri_s": 0.0, "query_s": 0.0}
+    vb.check(L.vg_ctx_profile(ctx, 1))
+    l0 = launches()
+    timer = ctypes.c_void_p()
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks:
+        vb.check(L.vg_timer_start(ctx, ctypes.byref(timer)))
+        for k in range(args.steps):
+            st, _ = session.prove(seed0 + 100 + k, transcript=True)
+            for key in stages:
+                stages[key] += getattr(st, key)
+        ms = ctypes.c_double()
+        vb.check(L.vg_timer_stop(ctx, timer, ctypes.byref(ms)))
+    n_launch = launches() - l0
+    fam = {}
+    for i, name in enumerate(FAMILIES):
+        n, t, b = ctypes.c_longlong(), ctypes.c_double(), ctypes.c_double()
+        vb.check(L.vg_ctx_profile_read(ctx, i, ctypes.byref(n), ctypes.byref(t), ctypes.byref(b)))
+        if n.value:
+            fam[name] = {"launches": n.value, "ms": t.value, "bytes": b.value}
+    vb.check(L.vg_ctx_profile(ctx, 0))
+    t_dev = max_over_ranks(ms.value / 1000.0, world)
+
+    # ---- e2e: circuit from pinned host buffers through the C ABI each step ----
+    pinned = session_arrays(layers)
+    h2d = int(sum(t.numel() * 1 + u.numel() * 8 + v.numel() * 8 for t, u, v in pinned))
+    d2h = 0
+    barrier(world)
+    t0 = time.perf_counter()
+    for k in range(args.steps):
+        s = create_session_from_pinned(pinned)
+        st, blob = s.prove(seed0 + 200 + k, transcript=True)
+        d2h = len(blob)
+        s.close()
+    t_e2e = max_over_ranks(time.perf_counter() - t0, world)
+    session.close()
+    return {"t_dev": t_dev, "t_e2e": t_e2e, "clocks": clocks.summary(), "families": fam, "launches": n_launch,
+            "stages": {k: v / args.steps for k, v in stages.items()}, "h2d": h2d, "d2h": d2h}
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(x, world):
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def roofline(fam, hbm_peak, peak_kind):
+    mem = {k: v for k, v in fam.items() if k in HBM_BOUND}
+    if not mem:
+        return None
+    top = max(mem, key=lambda k: mem[k]["ms"])
+    f = mem[top]
+    gbs = f["bytes"] / (f["ms"] / 1000.0) / 1e9 if f["ms"] > 0 else 0.0
+    return {"bound": "hbm", "kernel": top, "achieved": round(gbs, 1), "peak": hbm_peak, "unit": "GB/s",
+            "frac": round(gbs / hbm_peak, 4), "traffic": None, "peak_source": peak_kind,
+            "launches": f["launches"], "avg_launch_us": round(1000.0 * f["ms"] / f["launches"], 2),
+            "bytes_per_launch": f["bytes"] / f["launches"]}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["matmul256", "matmul16"], default="matmul256")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    layers = make_workload(args)
+
+    if args.impl == "reference":
+        if rank == 0:
+            print(json.dumps(reference_arm(args, layers)))
+        return
+
+    os.environ["VIRGO_DEVICE"] = str(local)
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    r = ours(args, layers, rank, world)
+    if rank == 0:
+        hbm, kind = peaks()
+        total_ms = sum(f["ms"] for f in r["families"].values()) or 1.0
+        fam = {k: dict(v, share=round(v["ms"] / total_ms, 4)) for k, v in r["families"].items()}
+        line = {
+            "metric": METRIC, "value": args.steps * world / r["t_dev"], "unit": "proofs/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * r["t_dev"] / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u64 (F_{p^2}, p = 2^61 - 1)", "data": "synthetic (seeded)",
+            "config": {"workload": WORKLOAD if args.workload == "matmul256" else args.workload, "circuit_gates": int(sum(len(t) for t, _, _ in layers)),
+                       "input_log2": 17, "hash": "sha3-256", "parallelism": "replicas" if world > 1 else "1 gpu",
+                       "l2": "inputs larger than L2 (circuit + tables > 1 GB per proof)"},
+            "e2e": {"value": args.steps * world / r["t_e2e"], "unit": "proofs/s", "h2d_bytes_per_step": r["h2d"],
+                    "d2h_bytes_per_step": r["d2h"]},
+            "gpu_launches": r["launches"],
+            "clocks": r["clocks"],
+            "roofline": roofline(r["families"], hbm, kind),
+            "stages_s": r["stages"],
+            "kernel_families": fam,
+        }
+        if not args.no_cpu_baseline and world >= 1 and os.path.exists(REF_BIN):
+            tmp = tempfile.mkdtemp(prefix="virgo_circ_")
+            c, m = os.path.join(tmp, "c.txt"), os.path.join(tmp, "m.txt")
+            write_circuit_text(layers, c, m)
+            (secs, detail), = run_reference_proofs(c, m, 1, seed0=1)
+            line["cpu_baseline"] = {"value": 1.0 / secs, "unit": "proofs/s", "cores": 1, "kind": "reference",
+                                    "sample": "one reference proof of the workload on 1 core (Prove Time without "
+                                              "fft_gkr, plus evaluate)", "detail": detail}
+        else:
+            line["cpu_baseline"] = None
+        print(json.dumps(line))
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

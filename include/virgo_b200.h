@@ -59,6 +59,21 @@ int vg_ctx_sync(vg_ctx *ctx);
 /* Number of kernels this context has launched since creation. */
 int vg_ctx_launch_count(vg_ctx *ctx, long long *count);
 
+/* Per-launch profiler.  While enabled, every kernel launch of the context is
+ * bracketed by CUDA events on its stream (no extra synchronisation);
+ * vg_ctx_profile_read returns, for one kernel family, the launches, their
+ * summed device time and their summed algorithmic bytes (bytes the kernel
+ * must move by its definition, not measured traffic).  Families: 0 NTT pass,
+ * 1 leaf hash chain, 2 Merkle level, 3 FRI fold + leaf chain, 4 virtual
+ * oracle, 5 layer evaluation, 6 phase-1 scatter, 7 phase-2 scatter,
+ * 8 accumulator finalise, 9 sumcheck round, 10 partial-sum reduction,
+ * 11 other.  Enabling resets the counters. */
+int vg_ctx_profile(vg_ctx *ctx, int enable);
+int vg_ctx_profile_read(vg_ctx *ctx, int family, long long *launches, double *ms, double *bytes);
+/* Device time between two points of the context's stream. */
+int vg_timer_start(vg_ctx *ctx, void **timer);
+int vg_timer_stop(vg_ctx *ctx, void *timer, double *ms);
+
 /* ----------------------------------------------------------- device memory */
 int vg_dev_alloc(vg_ctx *ctx, size_t bytes, void **dev);
 int vg_dev_free(vg_ctx *ctx, void *dev);
@@ -214,6 +229,13 @@ int vg_session_create(int d, const long *n, const uint8_t *const *ty, const int6
 /* Reads the circuit text format. */
 int vg_session_from_file(const char *circuit_path, vg_session **out);
 int vg_session_destroy(vg_session *s);
+/* The context the drop-in classes and sessions run on (created on first use,
+ * device $VIRGO_DEVICE, default 0). */
+int vg_default_ctx(vg_ctx **out);
+/* Writes file-level layers (as for vg_session_create) in the circuit text
+ * format, and a meta file with one "0 0 1 0 0" line per layer.  Host only. */
+int vg_circuit_write_text(int d, const long *n, const uint8_t *const *ty, const int64_t *const *u,
+                          const int64_t *const *v, const char *circuit_path, const char *meta_path);
 /* depth of the prover's circuit (file layers + 1) and log2 of the padded input */
 int vg_session_depth(vg_session *s, int *depth, int *input_log);
 /* One proof.  With want_transcript, *transcript (free with vg_free) receives

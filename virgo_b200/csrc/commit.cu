@@ -367,8 +367,11 @@ extern "C" int vg_pc_encode_public(vg_pc *pc, const vg_fe *pub, const vg_fe *pub
     const fe *tf_lo, *tf_hi, *ti_lo, *ti_hi;
     VG_TRY(vg_twiddles(c, root_of(logS), logS, &tf_lo, &tf_hi));
     VG_TRY(vg_twiddles(c, vg::fe_inv(root_of(logS)), logS, &ti_lo, &ti_hi));
-    k_virtual_oracle<<<148 * 16, 256, 0, c->stream>>>(pc->l_eval, q_eval, pc->h_eval, lqc, S, R, logS, 0, 64,
-                                                      tf_lo, tf_hi, ti_lo, ti_hi, pc->vo);
+    {
+        ProfScope ps(c, KF_VIRTUAL_ORACLE, 64.0 * 64.0 * (double)S);
+        k_virtual_oracle<<<148 * 16, 256, 0, c->stream>>>(pc->l_eval, q_eval, pc->h_eval, lqc, S, R, logS, 0, 64,
+                                                          tf_lo, tf_hi, ti_lo, ti_hi, pc->vo);
+    }
     VG_LAUNCHED(c);
     k_virtual_oracle<<<grid_for(S, 256), 256, 0, c->stream>>>(pc->l_eval, q_eval, pc->h_eval, lqc_m, S, M, logS, 64, 1,
                                                              tf_lo, tf_hi, ti_lo, ti_hi, pc->vo);
@@ -429,10 +432,13 @@ extern "C" int vg_pc_fri_step(vg_pc *pc, vg_fe r_, vg_digest *root)
     fe r = vg::fe_make(r_.real, r_.img);
     long q4 = n >> 2;
     long nleaves = L.n >> 1;
+    {
+    ProfScope ps(c, KF_FRI_FOLD, 16.0 * 65.0 * (double)n * 1.5 + 32.0 * (double)q4);
     if (c->hash_kind == VG_HASH_SHA256)
         k_fri_fold_leaf<VG_HASH_SHA256><<<grid_for(q4, 128), 128, 0, c->stream>>>(in, n, t, r, ti_lo, ti_hi, L.cw, L.tree + 4 * nleaves);
     else
         k_fri_fold_leaf<VG_HASH_SHA3_256><<<grid_for(q4, 128), 128, 0, c->stream>>>(in, n, t, r, ti_lo, ti_hi, L.cw, L.tree + 4 * nleaves);
+    }
     VG_LAUNCHED(c);
     VG_TRY(vg_merkle_build(c, L.tree, nleaves));
     pc->levels.push_back(L);

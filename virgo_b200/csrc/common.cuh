@@ -18,6 +18,17 @@ struct TwEntry {
     fe *hi;   // w^(4096 j), j < max(1, n / 4096)
 };
 
+// Kernel families timed by the optional per-launch profiler (vg_ctx_profile).
+enum KernelFamily {
+    KF_NTT = 0, KF_LEAF_CHAIN, KF_MERKLE, KF_FRI_FOLD, KF_VIRTUAL_ORACLE, KF_EVAL, KF_SCATTER1, KF_SCATTER2,
+    KF_FINALIZE, KF_ROUND, KF_REDUCE, KF_OTHER, KF_COUNT
+};
+struct ProfRec {
+    int fam;
+    cudaEvent_t a, b;
+    double bytes;
+};
+
 struct vg_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -33,6 +44,32 @@ struct vg_ctx {
     size_t partials_cap = 0;
     fe *pinned = nullptr;    // pinned host staging for small results
     size_t pinned_cap = 0;
+    // per-launch profiler: event pairs around launches of each kernel family
+    bool profiling = false;
+    std::vector<ProfRec> prof;
+    std::vector<cudaEvent_t> event_pool;
+    long long prof_launches[KF_COUNT] = {0};
+    double prof_ms[KF_COUNT] = {0}, prof_bytes[KF_COUNT] = {0};
+};
+
+// Profiler hooks around one launch: no-ops unless profiling is on.  Events are
+// recorded on the context stream without synchronising; vg_ctx_profile_read
+// resolves them.
+void vg_prof_begin(vg_ctx *c, int fam, ProfRec *r);
+void vg_prof_end(vg_ctx *c, ProfRec *r, double bytes);
+struct ProfScope {
+    vg_ctx *c;
+    ProfRec r;
+    double bytes;
+    bool on;
+    ProfScope(vg_ctx *ctx, int fam, double b) : c(ctx), bytes(b), on(ctx->profiling)
+    {
+        if (on) vg_prof_begin(c, fam, &r);
+    }
+    ~ProfScope()
+    {
+        if (on) vg_prof_end(c, &r, bytes);
+    }
 };
 
 // ---- errors ----

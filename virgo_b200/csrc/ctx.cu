@@ -38,11 +38,119 @@ extern "C" int vg_ctx_create(int device, vg_ctx **out)
     return VG_OK;
 }
 
+static cudaEvent_t get_event(vg_ctx *c)
+{
+    if (!c->event_pool.empty()) {
+        cudaEvent_t e = c->event_pool.back();
+        c->event_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void vg_prof_begin(vg_ctx *c, int fam, ProfRec *r)
+{
+    r->fam = fam;
+    r->a = get_event(c);
+    r->b = get_event(c);
+    cudaEventRecord(r->a, c->stream);
+}
+
+void vg_prof_end(vg_ctx *c, ProfRec *r, double bytes)
+{
+    cudaEventRecord(r->b, c->stream);
+    r->bytes = bytes;
+    c->prof.push_back(*r);
+    if (c->prof.size() > 4096) {   // resolve in batches to bound the event count
+        cudaStreamSynchronize(c->stream);
+        for (auto &p : c->prof) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, p.a, p.b);
+            c->prof_launches[p.fam]++;
+            c->prof_ms[p.fam] += ms;
+            c->prof_bytes[p.fam] += p.bytes;
+            c->event_pool.push_back(p.a);
+            c->event_pool.push_back(p.b);
+        }
+        c->prof.clear();
+    }
+}
+
+extern "C" int vg_ctx_profile(vg_ctx *c, int enable)
+{
+    if (!c) return vg_fail(VG_ERR_ARG, "null ctx");
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    c->profiling = enable != 0;
+    for (auto &p : c->prof) {
+        c->event_pool.push_back(p.a);
+        c->event_pool.push_back(p.b);
+    }
+    c->prof.clear();
+    for (int k = 0; k < KF_COUNT; ++k) {
+        c->prof_launches[k] = 0;
+        c->prof_ms[k] = c->prof_bytes[k] = 0;
+    }
+    return VG_OK;
+}
+
+extern "C" int vg_ctx_profile_read(vg_ctx *c, int family, long long *launches, double *ms, double *bytes)
+{
+    if (!c || family < 0 || family >= KF_COUNT) return vg_fail(VG_ERR_ARG, "vg_ctx_profile_read: bad family");
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    for (auto &p : c->prof) {
+        float t = 0;
+        cudaEventElapsedTime(&t, p.a, p.b);
+        c->prof_launches[p.fam]++;
+        c->prof_ms[p.fam] += t;
+        c->prof_bytes[p.fam] += p.bytes;
+        c->event_pool.push_back(p.a);
+        c->event_pool.push_back(p.b);
+    }
+    c->prof.clear();
+    if (launches) *launches = c->prof_launches[family];
+    if (ms) *ms = c->prof_ms[family];
+    if (bytes) *bytes = c->prof_bytes[family];
+    return VG_OK;
+}
+
+extern "C" int vg_timer_start(vg_ctx *c, void **timer)
+{
+    if (!c || !timer) return vg_fail(VG_ERR_ARG, "null argument");
+    cudaEvent_t *ev = new cudaEvent_t[2];
+    VG_CHECK_CUDA(cudaEventCreate(&ev[0]));
+    VG_CHECK_CUDA(cudaEventCreate(&ev[1]));
+    VG_CHECK_CUDA(cudaEventRecord(ev[0], c->stream));
+    *timer = ev;
+    return VG_OK;
+}
+
+extern "C" int vg_timer_stop(vg_ctx *c, void *timer, double *ms)
+{
+    if (!c || !timer || !ms) return vg_fail(VG_ERR_ARG, "null argument");
+    cudaEvent_t *ev = (cudaEvent_t *)timer;
+    VG_CHECK_CUDA(cudaEventRecord(ev[1], c->stream));
+    VG_CHECK_CUDA(cudaEventSynchronize(ev[1]));
+    float t = 0;
+    VG_CHECK_CUDA(cudaEventElapsedTime(&t, ev[0], ev[1]));
+    *ms = t;
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    delete[] ev;
+    return VG_OK;
+}
+
 extern "C" int vg_ctx_destroy(vg_ctx *c)
 {
     if (!c) return VG_OK;
     cudaSetDevice(c->device);
     cudaStreamSynchronize(c->stream);
+    for (auto &p : c->prof) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    for (auto e : c->event_pool) cudaEventDestroy(e);
     for (auto &t : c->tw_cache) {
         cudaFree(t.lo);
         cudaFree(t.hi);
@@ -225,6 +333,7 @@ __global__ void k_reduce_parts(const fe *__restrict__ parts, int nparts, fe *__r
 
 int vg_reduce_partials(vg_ctx *c, const fe *parts, int nparts, int K, fe *out_dev)
 {
+    ProfScope ps(c, KF_REDUCE, 16.0 * (double)nparts * K);
     switch (K) {
     case 1: k_reduce_parts<1><<<1, 1024, 0, c->stream>>>(parts, nparts, out_dev); break;
     case 3: k_reduce_parts<3><<<1, 1024, 0, c->stream>>>(parts, nparts, out_dev); break;

@@ -501,7 +501,10 @@ extern "C" int vg_gkr_evaluate(vg_gkr *g)
     for (int i = 1; i < g->C->depth; ++i) {
         const DevLayer &D = g->C->L[i];
         unsigned grid = std::min<unsigned>(grid_for(D.n, GKR_THREADS), 148u * 64u);
-        k_eval_layer<<<grid, GKR_THREADS, 0, c->stream>>>(D.ty, D.u, D.v, D.n, g->vals[i - 1], g->vals[i]);
+        {
+            ProfScope ps(c, KF_EVAL, 57.0 * (double)D.n);   // gate record, two operands, one result
+            k_eval_layer<<<grid, GKR_THREADS, 0, c->stream>>>(D.ty, D.u, D.v, D.n, g->vals[i - 1], g->vals[i]);
+        }
         VG_LAUNCHED(c);
     }
     VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
@@ -622,9 +625,15 @@ static int finalize_tables(vg_gkr *g, long N)
     vg_ctx *c = g->ctx;
     const long maxN = 1L << g->C->max_bl;
     unsigned grid = std::min<unsigned>(grid_for(N, 256), 148u * 32u);
-    k_acc_finalize<<<grid, 256, 0, c->stream>>>(g->acc, N, g->buf[0][2]);   // add_mult_sum
+    {
+        ProfScope ps(c, KF_FINALIZE, 48.0 * (double)N);
+        k_acc_finalize<<<grid, 256, 0, c->stream>>>(g->acc, N, g->buf[0][2]);   // add_mult_sum
+    }
     VG_LAUNCHED(c);
-    k_acc_finalize<<<grid, 256, 0, c->stream>>>(g->acc + 4 * maxN, N, g->buf[0][1]);   // addV_array
+    {
+        ProfScope ps(c, KF_FINALIZE, 48.0 * (double)N);
+        k_acc_finalize<<<grid, 256, 0, c->stream>>>(g->acc + 4 * maxN, N, g->buf[0][1]);   // addV_array
+    }
     VG_LAUNCHED(c);
     g->n = N;
     g->cur[1] = g->buf[0][1];
@@ -661,8 +670,12 @@ extern "C" int vg_gkr_phase1_init(vg_gkr *g, int layer, const vg_fe *r0, const v
     VG_CHECK_CUDA(cudaMemsetAsync(g->acc, 0, N * 4 * sizeof(unsigned long long), c->stream));
     VG_CHECK_CUDA(cudaMemsetAsync(g->acc + 4 * maxN, 0, N * 4 * sizeof(unsigned long long), c->stream));
     unsigned grid = std::min<unsigned>(grid_for(D.n, GKR_THREADS), 148u * 32u);
-    k_phase1_scatter<<<grid, GKR_THREADS, 0, c->stream>>>(D.ty, D.u, D.v, D.n, g->bg, g->vals[layer - 1], g->acc,
-                                                         g->acc + 4 * maxN);
+    {
+        // gate record, one operand gather, two 32-byte accumulator updates
+        ProfScope ps(c, KF_SCATTER1, 89.0 * (double)D.n);
+        k_phase1_scatter<<<grid, GKR_THREADS, 0, c->stream>>>(D.ty, D.u, D.v, D.n, g->bg, g->vals[layer - 1], g->acc,
+                                                             g->acc + 4 * maxN);
+    }
     VG_LAUNCHED(c);
     g->cur[0] = g->vals[layer - 1];
     return finalize_tables(g, N);
@@ -689,8 +702,11 @@ extern "C" int vg_gkr_phase2_init(vg_gkr *g, const vg_fe *r_u, int length_u, vg_
     VG_CHECK_CUDA(cudaMemsetAsync(g->acc, 0, N * 4 * sizeof(unsigned long long), c->stream));
     VG_CHECK_CUDA(cudaMemsetAsync(g->acc + 4 * maxN, 0, N * 4 * sizeof(unsigned long long), c->stream));
     unsigned grid = std::min<unsigned>(grid_for(D.n, GKR_THREADS), 148u * 32u);
-    k_phase2_scatter<<<grid, GKR_THREADS, 0, c->stream>>>(D.ty, D.u, D.v, D.n, g->bg, bu, tofe(v_u), g->acc,
-                                                         g->acc + 4 * maxN);
+    {
+        ProfScope ps(c, KF_SCATTER2, 73.0 * (double)D.n);   // gate record, two accumulator updates
+        k_phase2_scatter<<<grid, GKR_THREADS, 0, c->stream>>>(D.ty, D.u, D.v, D.n, g->bg, bu, tofe(v_u), g->acc,
+                                                             g->acc + 4 * maxN);
+    }
     VG_LAUNCHED(c);
     g->cur[0] = g->vals[layer - 1];
     return finalize_tables(g, N);
@@ -712,10 +728,14 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
     VG_TRY(vg_partials(c, 3 * (size_t)grid + 3 + 6, &parts));
     fe *y[3] = {g->buf[g->next_buf][0], g->buf[g->next_buf][1], g->buf[g->next_buf][2]};
     fe r = tofe(previous_random);
-    if (fold)
-        k_round<true><<<grid, GKR_THREADS, 0, c->stream>>>(g->cur[0], g->cur[1], g->cur[2], npairs, r, y[0], y[1], y[2], parts);
-    else
-        k_round<false><<<grid, GKR_THREADS, 0, c->stream>>>(g->cur[0], g->cur[1], g->cur[2], npairs, r, nullptr, nullptr, nullptr, parts);
+    {
+        // fold: read 3 tables x 4 entries, write 3 x 2 per pair; else read 3 x 2
+        ProfScope ps(c, KF_ROUND, (fold ? 288.0 : 96.0) * (double)npairs);
+        if (fold)
+            k_round<true><<<grid, GKR_THREADS, 0, c->stream>>>(g->cur[0], g->cur[1], g->cur[2], npairs, r, y[0], y[1], y[2], parts);
+        else
+            k_round<false><<<grid, GKR_THREADS, 0, c->stream>>>(g->cur[0], g->cur[1], g->cur[2], npairs, r, nullptr, nullptr, nullptr, parts);
+    }
     VG_LAUNCHED(c);
     VG_TRY(vg_reduce_partials(c, parts, (int)grid, 3, parts + 3 * grid));
     if (fold) {

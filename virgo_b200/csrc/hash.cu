@@ -106,6 +106,7 @@ int vg_merkle_build(vg_ctx *c, uint64_t *tree, long n_leaves_padded)
     const long TOP = 1024;
     long cnt = n_leaves_padded >> 1;
     while (cnt > TOP) {
+        ProfScope ps(c, KF_MERKLE, 96.0 * (double)cnt);
         if (c->hash_kind == VG_HASH_SHA256)
             k_merkle_level<VG_HASH_SHA256><<<grid_for(cnt, HASH_THREADS), HASH_THREADS, 0, c->stream>>>(tree, cnt, cnt);
         else
@@ -114,6 +115,7 @@ int vg_merkle_build(vg_ctx *c, uint64_t *tree, long n_leaves_padded)
         cnt >>= 1;
     }
     if (cnt >= 1) {
+        ProfScope ps(c, KF_MERKLE, 96.0 * (double)(2 * cnt));
         if (c->hash_kind == VG_HASH_SHA256)
             k_merkle_top<VG_HASH_SHA256><<<1, 512, 0, c->stream>>>(tree, cnt);
         else
@@ -127,6 +129,7 @@ int vg_leaf_chain_dev(vg_ctx *c, const fe *cw, int n_slices, long n, uint64_t *l
 {
     long half = n >> 1;
     if (half < 1) return VG_OK;
+    ProfScope ps(c, KF_LEAF_CHAIN, 16.0 * (double)n_slices * (double)n + 32.0 * (double)half);
     if (c->hash_kind == VG_HASH_SHA256)
         k_leaf_chain<VG_HASH_SHA256><<<grid_for(half, HASH_THREADS), HASH_THREADS, 0, c->stream>>>(cw, n_slices, n, leaves);
     else

@@ -229,7 +229,10 @@ static int launch_pass(vg_ctx *c, PassArgs &a, long nblocks, int batch)
     size_t sm = ((size_t)m * G + (m >> 1)) * sizeof(fe);
     if (sm > 48 * 1024) VG_CHECK_CUDA(cudaFuncSetAttribute(k_ntt_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     dim3 grid((unsigned)nblocks, (unsigned)batch);
-    k_ntt_pass<<<grid, NTT_THREADS, sm, c->stream>>>(a);
+    {
+        ProfScope ps(c, KF_NTT, 2.0 * 16.0 * (double)batch * (double)(1L << a.logn));
+        k_ntt_pass<<<grid, NTT_THREADS, sm, c->stream>>>(a);
+    }
     VG_LAUNCHED(c);
     return VG_OK;
 }

@@ -310,6 +310,70 @@ extern "C" int vg_session_depth(vg_session *s, int *depth, int *input_log)
 
 extern "C" void vg_free(void *p) { free(p); }
 
+extern "C" int vg_default_ctx(vg_ctx **out)
+{
+    if (!out) return VG_ERR_ARG;
+    *out = virgo::ctx();
+    return VG_OK;
+}
+
+// decimal digits of x into p (x >= 0 or negative), returns the end
+static char *put_int(char *p, long long x)
+{
+    char tmp[24];
+    int n = 0;
+    unsigned long long ux = x < 0 ? 0ULL - (unsigned long long)x : (unsigned long long)x;
+    do {
+        tmp[n++] = (char)('0' + ux % 10);
+        ux /= 10;
+    } while (ux);
+    if (x < 0) *p++ = '-';
+    while (n) *p++ = tmp[--n];
+    return p;
+}
+
+extern "C" int vg_circuit_write_text(int d, const long *n, const uint8_t *const *ty, const int64_t *const *u,
+                                     const int64_t *const *v, const char *circuit_path, const char *meta_path)
+{
+    if (d < 1 || !n || !ty || !u || !v || !circuit_path) return VG_ERR_ARG;
+    FILE *f = fopen(circuit_path, "wb");
+    if (!f) return VG_ERR_ARG;
+    std::vector<char> buf(1 << 22);
+    char *p = buf.data();
+    char *end = buf.data() + buf.size() - 128;
+    auto flush = [&]() {
+        fwrite(buf.data(), 1, p - buf.data(), f);
+        p = buf.data();
+    };
+    p = put_int(p, d);
+    *p++ = '\n';
+    for (int i = 0; i < d; ++i) {
+        p = put_int(p, n[i]);
+        *p++ = ' ';
+        for (long g = 0; g < n[i]; ++g) {
+            if (p > end) flush();
+            p = put_int(p, ty[i][g]);
+            *p++ = ' ';
+            p = put_int(p, g);
+            *p++ = ' ';
+            p = put_int(p, u[i][g]);
+            *p++ = ' ';
+            p = put_int(p, v[i][g]);
+            if (g + 1 < n[i]) *p++ = ' ';
+        }
+        *p++ = '\n';
+    }
+    flush();
+    fclose(f);
+    if (meta_path) {
+        FILE *m = fopen(meta_path, "wb");
+        if (!m) return VG_ERR_ARG;
+        for (int i = 0; i < d; ++i) fputs("0 0 1 0 0\n", m);
+        fclose(m);
+    }
+    return VG_OK;
+}
+
 extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcript, vg_proof_stats *stats,
                                 uint8_t **transcript, size_t *transcript_len)
 {
