@@ -141,6 +141,19 @@ int vg_gkr_v_res(vg_gkr *g, const vg_fe *r, int r_len, vg_fe *out);
  * entries; bit b of the index pairs with r[b]), the fold of V_res
  * (zk_prover.cpp:37-44).  out host. */
 int vg_mle_eval(vg_ctx *ctx, const vg_fe *vals, long n, const vg_fe *r, int log_n, vg_fe *out);
+/* vg_mle_eval for callers that cannot allocate device memory (a host whose
+ * pool already holds the GPU, a latency-critical path that must not take
+ * cudaFree's device-wide synchronisation, a fixed memory budget).  No
+ * counterpart in the reference.  It allocates nothing: its scratch (eq tables,
+ * block partials) is one file-scope device array of 268,160 bytes that every
+ * GPU loading this library keeps until exit.  vals device (n >= 2^log_n), r and
+ * out host; log_n <= 26, larger is rejected with VG_ERR_ARG.  The first call on
+ * a device looks up the array's address (cudaGetSymbolAddress, that device
+ * current): make it before any stream capture.  All calls share the array,
+ * which keeps the last call's contents (each call writes what it reads);
+ * calls that overlap on the GPU race.  Runs on the legacy default stream and
+ * returns after *out is written. */
+int vg_mle_eval_noalloc(const vg_fe *vals, long n, const vg_fe *r, int log_n, vg_fe *out);
 /* Phase-1 bookkeeping of layer `layer` (zk_prover::sumcheck_phase1_init,
  * zk_prover.cpp:375-592): beta_g = alpha*eq(r0,g) + beta*eq(r1,g) over
  * length_g bits, then the gate scatter into add_mult_sum / addV_array by u.
