@@ -56,6 +56,7 @@ int vg_ctx_destroy(vg_ctx *ctx);
 int vg_ctx_set_hash(vg_ctx *ctx, int kind);
 int vg_ctx_get_hash(vg_ctx *ctx, int *kind);
 int vg_ctx_sync(vg_ctx *ctx);
+int vg_ctx_device(vg_ctx *ctx, int *device);
 /* Number of kernels this context has launched since creation. */
 int vg_ctx_launch_count(vg_ctx *ctx, long long *count);
 
@@ -73,6 +74,9 @@ int vg_ctx_profile_read(vg_ctx *ctx, int family, long long *launches, double *ms
 /* Device time between two points of the context's stream. */
 int vg_timer_start(vg_ctx *ctx, void **timer);
 int vg_timer_stop(vg_ctx *ctx, void *timer, double *ms);
+/* Device time from the start point to the end of the work queued so far on
+ * every listed context (the latest of them); consumes the timer. */
+int vg_timer_stop_multi(vg_ctx *const *ctxs, int n, void *timer, double *ms);
 
 /* ----------------------------------------------------------- device memory */
 int vg_dev_alloc(vg_ctx *ctx, size_t bytes, void **dev);
@@ -215,6 +219,13 @@ int vg_pc_query_init(vg_pc *pc, long pow0, int oracle, vg_fe *values, vg_digest 
  * bookkeeping: the 65 value pairs of FRI level lvl at position pow and its
  * authentication path (siblings bottom-up, then the leaf). host. */
 int vg_pc_query_step(vg_pc *pc, int lvl, long pow, vg_fe *values, vg_digest *path, int *path_len);
+/* Many query answers in one gather: query q reads codeword set which[q]
+ * (0 = l, 1 = h, 2 + t = FRI level t) at position pos[q] (taken modulo half
+ * the per-slice length) and returns 130 values (values[q*130 ..]) and its
+ * authentication path (paths[q*32 ..], path_len[q] digests: siblings
+ * bottom-up, then the leaf).  All arrays host. */
+int vg_pc_query_batch(vg_pc *pc, int nq, const int *which, const long *pos, vg_fe *values, vg_digest *paths,
+                      int *path_len);
 /* Sizes of the current commitment: log_len, slice size S, FRI levels so far. */
 int vg_pc_info(vg_pc *pc, int *log_len, long *slice_size, int *levels);
 
@@ -239,6 +250,10 @@ typedef struct {
  * (zk_verifier.cpp:24-191). */
 int vg_session_create(int d, const long *n, const uint8_t *const *ty, const int64_t *const *u,
                       const int64_t *const *v, vg_session **out);
+/* A session proving the same circuit with its own stream, commitment state and
+ * tables; the device circuit is shared (kept until every session using it is
+ * destroyed).  Sessions of one circuit prove concurrently. */
+int vg_session_fork(vg_session *base, vg_session **out);
 /* Reads the circuit text format. */
 int vg_session_from_file(const char *circuit_path, vg_session **out);
 int vg_session_destroy(vg_session *s);
@@ -255,6 +270,13 @@ int vg_session_depth(vg_session *s, int *depth, int *input_log);
  * the records: tag byte, uint32 count of 16-byte units, the units. */
 int vg_session_prove(vg_session *s, unsigned seed, int want_transcript, vg_proof_stats *stats,
                      uint8_t **transcript, size_t *transcript_len);
+/* n proofs at once, session i with seed i, each on its own host thread and
+ * CUDA stream (the sessions must be distinct objects, e.g. forks of one).
+ * stats, transcripts and transcript_lens have n entries (or are NULL). */
+int vg_session_prove_batch(vg_session *const *ss, int n, const unsigned *seeds, int want_transcript,
+                           vg_proof_stats *stats, uint8_t **transcripts, size_t *transcript_lens);
+/* The context (stream) a session runs on. */
+int vg_session_ctx(vg_session *s, vg_ctx **out);
 void vg_free(void *p);
 
 #ifdef __cplusplus

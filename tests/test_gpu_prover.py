@@ -121,3 +121,23 @@ def test_session_rejects_malformed_circuit():
     u[0] = 1 << 40
     with pytest.raises(vb.VirgoError):
         vb.Session([layers[0], layers[1], (ty, u, v)])
+
+
+def test_forked_sessions_prove_concurrently_bit_exact():
+    """Forks of one circuit prove at once (own streams, shared circuit); every
+    transcript equals the one the same seed gives alone, and the golden one."""
+    c = next(x for x in _golden() if x["name"] == "random_5layer")
+    layers = getattr(circuits, c["generator"])(**c["params"])
+    base = vb.Session(layers)
+    forks = [base.fork() for _ in range(3)]
+    try:
+        seeds = [c["seed"], 17, c["seed"], 23]
+        res = vb.prove_batch([base] + forks, seeds)
+        alone = {sd: base.prove(sd)[1] for sd in set(seeds)}
+    finally:
+        for s in forks:
+            s.close()
+        base.close()
+    for sd, (_, blob) in zip(seeds, res):
+        assert blob == alone[sd]
+    assert transcript.digest(transcript.parse(res[0][1])) == c["digest"]

@@ -92,6 +92,20 @@ def lib():
             "vg_session_depth": (c_i, [c_p, ctypes.POINTER(c_i), ctypes.POINTER(c_i)]),
             "vg_session_prove": (c_i, [c_p, ctypes.c_uint, c_i, ctypes.POINTER(vg_proof_stats),
                                        ctypes.POINTER(c_p), ctypes.POINTER(c_sz)]),
+            "vg_session_fork": (c_i, [c_p, ctypes.POINTER(c_p)]),
+            "vg_session_prove_batch": (c_i, [c_p, c_i, c_p, c_i, c_p, c_p, c_p]),
+            "vg_session_ctx": (c_i, [c_p, ctypes.POINTER(c_p)]),
+            "vg_pc_query_batch": (c_i, [c_p, c_i, c_p, c_p, c_p, c_p, c_p]),
+            "vg_ctx_profile": (c_i, [c_p, c_i]),
+            "vg_ctx_profile_read": (c_i, [c_p, c_i, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double),
+                                          ctypes.POINTER(ctypes.c_double)]),
+            "vg_timer_start": (c_i, [c_p, ctypes.POINTER(c_p)]),
+            "vg_timer_stop": (c_i, [c_p, c_p, ctypes.POINTER(ctypes.c_double)]),
+            "vg_timer_stop_multi": (c_i, [c_p, c_i, c_p, ctypes.POINTER(ctypes.c_double)]),
+            "vg_default_ctx": (c_i, [ctypes.POINTER(c_p)]),
+            "vg_ctx_device": (c_i, [c_p, ctypes.POINTER(c_i)]),
+            "vg_circuit_write_text": (c_i, [c_i, c_p, c_p, c_p, c_p, ctypes.c_char_p, ctypes.c_char_p]),
+            "vg_mle_eval_noalloc": (c_i, [c_p, c_l, c_p, c_i, c_p]),
             "vg_free": (None, [c_p]),
         }
         for name, (res, args) in sig.items():
@@ -220,10 +234,40 @@ class Session:
         lib().vg_free(buf)
         return st, data
 
+    def fork(self) -> "Session":
+        """A session on the same (shared) device circuit with its own stream."""
+        h = ctypes.c_void_p()
+        check(lib().vg_session_fork(self.h, ctypes.byref(h)), "vg_session_fork")
+        s = Session.__new__(Session)
+        s.h = h
+        return s
+
+    def ctx(self):
+        c = ctypes.c_void_p()
+        check(lib().vg_session_ctx(self.h, ctypes.byref(c)), "vg_session_ctx")
+        return c
+
     def close(self):
         if self.h:
             lib().vg_session_destroy(self.h)
             self.h = None
+
+
+def prove_batch(sessions, seeds, transcript: bool = True):
+    """One proof per session, all at once (each session on its own stream)."""
+    n = len(sessions)
+    hs = (ctypes.c_void_p * n)(*[s.h.value for s in sessions])
+    sd = (ctypes.c_uint * n)(*seeds)
+    st = (vg_proof_stats * n)()
+    bufs = (ctypes.c_void_p * n)()
+    lens = (ctypes.c_size_t * n)()
+    check(lib().vg_session_prove_batch(hs, n, sd, 1 if transcript else 0, st, bufs, lens), "vg_session_prove_batch")
+    out = []
+    for i in range(n):
+        data = ctypes.string_at(bufs[i], lens[i]) if (transcript and lens[i]) else b""
+        lib().vg_free(bufs[i])
+        out.append((st[i], data))
+    return out
 
 
 def header_functions(path: str = HEADER) -> list:

@@ -14,15 +14,10 @@
 #include "common.cuh"
 #include "merkle.cuh"
 #include "hash.cuh"
+#include <algorithm>
 #include <cstring>
 
 namespace {
-
-struct FriLevel {
-    fe *cw = nullptr;        // 65 x n
-    long n = 0;
-    uint64_t *tree = nullptr;  // n digests (n/2 leaves)
-};
 
 __device__ __forceinline__ uint64_t halfp(uint64_t x) { return (x & 1) ? ((x + vg::P) >> 1) : (x >> 1); }
 __device__ __forceinline__ fe half_fe(fe x) { return vg::fe_make(halfp(x.real), halfp(x.img)); }
@@ -128,25 +123,29 @@ __global__ void __launch_bounds__(128) k_fri_fold_leaf(const fe *__restrict__ c,
     o[1] = make_ulonglong2(h[2], h[3]);
 }
 
-// gather of query answers: 65 value pairs at (p, p + n/2) and a tree path
-__global__ void k_gather_query(const fe *__restrict__ cw, long n, long p, const uint64_t *__restrict__ tree,
-                               long leaf_node, int depth, fe *__restrict__ vals, uint64_t *__restrict__ path)
+// Query answers for a batch: block q answers query q from codeword set
+// desc[which[q]] at position pos[q] (taken modulo n/2): 65 value pairs and the
+// authentication path (siblings bottom-up, then the leaf).
+struct QueryDesc {
+    const fe *cw;
+    const uint64_t *tree;
+    long n;
+    int depth;
+};
+__global__ void k_gather_batch(const QueryDesc *__restrict__ desc, const int *__restrict__ which,
+                               const long *__restrict__ pos, fe *__restrict__ vals, uint64_t *__restrict__ paths)
 {
-    int i = threadIdx.x;
+    const int q = blockIdx.x, i = threadIdx.x;
+    const QueryDesc d = desc[which[q]];
+    const long h = d.n >> 1, p = pos[q] % h;
     if (i < 65) {
-        vals[2 * i] = cw[(long)i * n + p];
-        vals[2 * i + 1] = cw[(long)i * n + p + n / 2];
+        vals[(long)q * 130 + 2 * i] = d.cw[(long)i * d.n + p];
+        vals[(long)q * 130 + 2 * i + 1] = d.cw[(long)i * d.n + p + h];
     }
-    if (i <= depth) {
-        long node = leaf_node;
-        uint64_t src;
-        if (i < depth) {
-            node >>= i;
-            src = (uint64_t)(node ^ 1);
-        } else {
-            src = (uint64_t)leaf_node;
-        }
-        for (int w = 0; w < 4; ++w) path[4 * i + w] = tree[4 * src + w];
+    if (i <= d.depth) {
+        const long leaf = p + h;
+        const long src = i < d.depth ? ((leaf >> i) ^ 1) : leaf;
+        for (int w = 0; w < 4; ++w) paths[((long)q * 32 + i) * 4 + w] = d.tree[4 * src + w];
     }
 }
 
@@ -166,42 +165,65 @@ int ilog2l(long x)
 
 }  // namespace
 
+struct DevBuf {
+    void *p = nullptr;
+    size_t cap = 0;
+};
+
+// grows a persistent buffer; buffers are kept across commitments so a proof
+// does not pay cudaMalloc/cudaFree (and cudaFree's device synchronisation)
+static int ensure(vg_ctx *c, DevBuf &b, size_t bytes)
+{
+    if (bytes <= b.cap) return VG_OK;
+    if (b.p) {
+        cudaStreamSynchronize(c->stream);
+        cudaFree(b.p);
+    }
+    b.p = nullptr;
+    b.cap = 0;
+    cudaError_t e = cudaMalloc(&b.p, bytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        b.p = nullptr;
+        return vg_fail(VG_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+    }
+    b.cap = bytes;
+    return VG_OK;
+}
+
+struct PcLevel {
+    DevBuf cw, tree;   // 65 x n codewords, n digests (n/2 leaves)
+    long n = 0;
+};
+
 struct vg_pc {
     vg_ctx *ctx = nullptr;
     int log_len = 0;
     long S = 0, R = 0, gap = 0, M = 0;
-    fe *l_eval = nullptr, *h_eval = nullptr, *vo = nullptr;
-    uint64_t *tree_l = nullptr, *tree_h = nullptr;
-    std::vector<FriLevel> levels;
+    DevBuf l_eval, h_eval, q_eval, vo, lq, lqc, mask, staging, tree_l, tree_h, qdesc, qio;
+    std::vector<PcLevel> levels;
+    int nlevels = 0;
     bool have_private = false, have_public = false;
+    fe *F(DevBuf &b) { return (fe *)b.p; }
+    uint64_t *U(DevBuf &b) { return (uint64_t *)b.p; }
 };
 
 static void pc_free(vg_pc *pc)
 {
-    cudaFree(pc->l_eval);
-    cudaFree(pc->h_eval);
-    cudaFree(pc->vo);
-    cudaFree(pc->tree_l);
-    cudaFree(pc->tree_h);
+    DevBuf *all[] = {&pc->l_eval, &pc->h_eval, &pc->q_eval, &pc->vo, &pc->lq, &pc->lqc, &pc->mask, &pc->staging,
+                     &pc->tree_l, &pc->tree_h, &pc->qdesc, &pc->qio};
+    for (DevBuf *b : all) {
+        cudaFree(b->p);
+        b->p = nullptr;
+        b->cap = 0;
+    }
     for (auto &L : pc->levels) {
-        cudaFree(L.cw);
-        cudaFree(L.tree);
+        cudaFree(L.cw.p);
+        cudaFree(L.tree.p);
     }
-    pc->l_eval = pc->h_eval = pc->vo = nullptr;
-    pc->tree_l = pc->tree_h = nullptr;
     pc->levels.clear();
+    pc->nlevels = 0;
     pc->have_private = pc->have_public = false;
-}
-
-static int dalloc(void **p, size_t bytes)
-{
-    cudaError_t e = cudaMalloc(p, bytes);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        *p = nullptr;
-        return vg_fail(VG_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
-    }
-    return VG_OK;
 }
 
 static fe root_of(int log_order) { return vg::fe_root_of_unity(log_order); }
@@ -217,15 +239,17 @@ static int rs_encode(vg_ctx *c, const fe *vals, long m, int batch, fe *out, long
     return VG_OK;
 }
 
-static int commit_tree(vg_ctx *c, const fe *cw, long S, uint64_t **tree, vg_digest *root)
+static int commit_tree(vg_ctx *c, const fe *cw, long S, uint64_t *tree, vg_digest *root)
 {
     long nleaves = S >> 1;
-    if (!*tree) VG_TRY(dalloc((void **)tree, 2 * nleaves * 32));
-    VG_TRY(vg_leaf_chain_dev(c, cw, 65, S, *tree + 4 * nleaves));
-    VG_TRY(vg_merkle_build(c, *tree, nleaves));
+    VG_TRY(vg_leaf_chain_dev(c, cw, 65, S, tree + 4 * nleaves));
+    VG_TRY(vg_merkle_build(c, tree, nleaves));
     if (root) {
-        VG_CHECK_CUDA(cudaMemcpyAsync(root, *tree + 4, 32, cudaMemcpyDeviceToHost, c->stream));
+        fe *host;
+        VG_TRY(vg_pinned(c, 2, &host));
+        VG_CHECK_CUDA(cudaMemcpyAsync(host, tree + 4, 32, cudaMemcpyDeviceToHost, c->stream));
         VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+        memcpy(root, host, 32);
     }
     return VG_OK;
 }
@@ -253,7 +277,33 @@ extern "C" int vg_pc_info(vg_pc *pc, int *log_len, long *slice_size, int *levels
     if (!pc) return vg_fail(VG_ERR_ARG, "null pc");
     if (log_len) *log_len = pc->log_len;
     if (slice_size) *slice_size = pc->S;
-    if (levels) *levels = (int)pc->levels.size();
+    if (levels) *levels = pc->nlevels;
+    return VG_OK;
+}
+
+// the private/public input on the device (a host array is staged)
+static int device_input(vg_pc *pc, const vg_fe *x, long N, const fe **out)
+{
+    if (vg_is_device_ptr(x)) {
+        *out = (const fe *)x;
+        return VG_OK;
+    }
+    VG_TRY(ensure(pc->ctx, pc->staging, N * sizeof(fe)));
+    VG_CHECK_CUDA(cudaMemcpyAsync(pc->staging.p, x, N * sizeof(fe), cudaMemcpyHostToDevice, pc->ctx->stream));
+    *out = (const fe *)pc->staging.p;
+    return VG_OK;
+}
+
+// zero-padded mask of M entries on the device (poly_commit.h:66-70, 138-139)
+static int device_mask(vg_pc *pc, const vg_fe *mask, long n_mask, long M)
+{
+    vg_ctx *c = pc->ctx;
+    VG_TRY(ensure(c, pc->mask, M * sizeof(fe)));
+    fe *host;
+    VG_TRY(vg_pinned(c, M, &host));
+    for (long i = 0; i < M; ++i) host[i] = i < n_mask ? vg::fe_make(mask[i].real, mask[i].img) : vg::fe_zero();
+    VG_CHECK_CUDA(cudaMemcpyAsync(pc->mask.p, host, M * sizeof(fe), cudaMemcpyHostToDevice, c->stream));
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));   // the pinned staging is reused
     return VG_OK;
 }
 
@@ -263,8 +313,8 @@ extern "C" int vg_pc_encode_private(vg_pc *pc, const vg_fe *priv, int log_len, c
     if (!pc || !priv || !mask || n_mask < 1 || log_len < 7 || log_len > 28)
         return vg_fail(VG_ERR_ARG, "vg_pc_encode_private: bad argument (log_len=%d n_mask=%ld)", log_len, n_mask);
     vg_ctx *c = pc->ctx;
-    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
-    pc_free(pc);
+    pc->have_private = pc->have_public = false;
+    pc->nlevels = 0;
     pc->log_len = log_len;
     pc->S = 1L << (log_len - 1);
     pc->R = pc->S >> 5;
@@ -272,36 +322,14 @@ extern "C" int vg_pc_encode_private(vg_pc *pc, const vg_fe *priv, int log_len, c
     pc->gap = mask_gap(pc->S, n_mask);
     pc->M = pc->S / pc->gap;
     const long S = pc->S, R = pc->R, M = pc->M, N = 1L << log_len;
-
-    VG_TRY(dalloc((void **)&pc->l_eval, 65 * S * sizeof(fe)));
-    const fe *priv_d = (const fe *)priv;
-    fe *staging = nullptr;
-    if (!vg_is_device_ptr(priv)) {
-        VG_TRY(dalloc((void **)&staging, N * sizeof(fe)));
-        VG_CHECK_CUDA(cudaMemcpyAsync(staging, priv, N * sizeof(fe), cudaMemcpyHostToDevice, c->stream));
-        priv_d = staging;
-    }
+    VG_TRY(ensure(c, pc->l_eval, 65 * S * sizeof(fe)));
+    const fe *priv_d;
+    VG_TRY(device_input(pc, priv, N, &priv_d));
     fe *coef;
     VG_TRY(vg_scratch2(c, 64 * R * sizeof(fe), (void **)&coef));
-    int rc = rs_encode(c, priv_d, R, 64, pc->l_eval, S, coef);
-    // mask slice: padded to M with zeros (poly_commit.h:66-70, 80-88)
-    if (rc == VG_OK) {
-        std::vector<fe> pm(M);
-        for (long i = 0; i < M; ++i) pm[i] = i < n_mask ? vg::fe_make(mask[i].real, mask[i].img) : vg::fe_zero();
-        fe *md = nullptr;
-        rc = dalloc((void **)&md, M * sizeof(fe));
-        if (rc == VG_OK) {
-            cudaMemcpyAsync(md, pm.data(), M * sizeof(fe), cudaMemcpyHostToDevice, c->stream);
-            rc = rs_encode(c, md, M, 1, pc->l_eval + 64 * S, S, coef);
-            cudaStreamSynchronize(c->stream);
-            cudaFree(md);
-        }
-    }
-    if (staging) {
-        cudaStreamSynchronize(c->stream);
-        cudaFree(staging);
-    }
-    VG_TRY(rc);
+    VG_TRY(rs_encode(c, priv_d, R, 64, pc->F(pc->l_eval), S, coef));
+    VG_TRY(device_mask(pc, mask, n_mask, M));
+    VG_TRY(rs_encode(c, pc->F(pc->mask), M, 1, pc->F(pc->l_eval) + 64 * S, S, coef));
     if (mask_len) *mask_len = M;
     pc->have_private = true;
     return VG_OK;
@@ -313,55 +341,46 @@ extern "C" int vg_pc_encode_public(vg_pc *pc, const vg_fe *pub, const vg_fe *pub
     if (!pc || !pub || !pub_mask || !all_sum) return vg_fail(VG_ERR_ARG, "vg_pc_encode_public: null argument");
     if (!pc->have_private) return vg_fail(VG_ERR_STATE, "commit_public before commit_private");
     if (n_mask > pc->M) return vg_fail(VG_ERR_ARG, "public mask longer than the padded private mask (%ld > %ld)", n_mask, pc->M);
+    if (pc->gap == 1) return vg_fail(VG_ERR_ARG, "mask fills the whole slice (mask_position_gap == 1)");
     vg_ctx *c = pc->ctx;
     const long S = pc->S, R = pc->R, M = pc->M, N = 1L << pc->log_len;
     const int logS = ilog2l(S);
-    if (pc->gap == 1) return vg_fail(VG_ERR_ARG, "mask fills the whole slice (mask_position_gap == 1)");
+    const long lq_len = 64 * 2 * R + 2 * M;
+    VG_TRY(ensure(c, pc->q_eval, 65 * S * sizeof(fe)));
+    VG_TRY(ensure(c, pc->h_eval, 65 * S * sizeof(fe)));
+    VG_TRY(ensure(c, pc->vo, 65 * S * sizeof(fe)));
+    VG_TRY(ensure(c, pc->lq, lq_len * sizeof(fe)));
+    VG_TRY(ensure(c, pc->lqc, lq_len * sizeof(fe)));
+    fe *l_eval = pc->F(pc->l_eval), *q_eval = pc->F(pc->q_eval), *h_eval = pc->F(pc->h_eval);
+    fe *lq = pc->F(pc->lq), *lqc = pc->F(pc->lqc);
 
-    fe *q_eval = nullptr, *lq = nullptr, *lqc = nullptr;
-    VG_TRY(dalloc((void **)&q_eval, 65 * S * sizeof(fe)));
-    if (!pc->h_eval) VG_TRY(dalloc((void **)&pc->h_eval, 65 * S * sizeof(fe)));
-    if (!pc->vo) VG_TRY(dalloc((void **)&pc->vo, 65 * S * sizeof(fe)));
-    long lq_len = 64 * 2 * R + 2 * M;
-    VG_TRY(dalloc((void **)&lq, lq_len * sizeof(fe)));
-    VG_TRY(dalloc((void **)&lqc, lq_len * sizeof(fe)));
-
-    const fe *pub_d = (const fe *)pub;
-    fe *staging = nullptr;
-    if (!vg_is_device_ptr(pub)) {
-        VG_TRY(dalloc((void **)&staging, N * sizeof(fe)));
-        VG_CHECK_CUDA(cudaMemcpyAsync(staging, pub, N * sizeof(fe), cudaMemcpyHostToDevice, c->stream));
-        pub_d = staging;
-    }
+    const fe *pub_d;
+    VG_TRY(device_input(pc, pub, N, &pub_d));
     fe *coef;
     VG_TRY(vg_scratch2(c, 64 * R * sizeof(fe), (void **)&coef));
     VG_TRY(rs_encode(c, pub_d, R, 64, q_eval, S, coef));
-    std::vector<fe> pm(M);
-    for (long i = 0; i < M; ++i) pm[i] = i < n_mask ? vg::fe_make(pub_mask[i].real, pub_mask[i].img) : vg::fe_zero();
-    fe *md;
-    VG_TRY(dalloc((void **)&md, M * sizeof(fe)));
-    VG_CHECK_CUDA(cudaMemcpyAsync(md, pm.data(), M * sizeof(fe), cudaMemcpyHostToDevice, c->stream));
-    VG_TRY(rs_encode(c, md, M, 1, q_eval + 64 * S, S, coef));
+    VG_TRY(device_mask(pc, pub_mask, n_mask, M));
+    VG_TRY(rs_encode(c, pc->F(pc->mask), M, 1, q_eval + 64 * S, S, coef));
 
     // inner product check value
     fe *parts;
     const int nb = 148 * 4;
     VG_TRY(vg_partials(c, nb + 1 + 65, &parts));   // block partials, <l,q>, all_sum[65]
-    k_inner_product<<<nb, 256, 0, c->stream>>>(pc->l_eval, q_eval, S, pc->gap, parts);
+    k_inner_product<<<nb, 256, 0, c->stream>>>(l_eval, q_eval, S, pc->gap, parts);
     VG_LAUNCHED(c);
     VG_TRY(vg_reduce_partials(c, parts, nb, 1, parts + nb));
 
     // lq samples, their interpolation and the quotient h
     fe *lq_m = lq + 64 * 2 * R, *lqc_m = lqc + 64 * 2 * R;
-    k_lq_sample<<<148 * 8, 256, 0, c->stream>>>(pc->l_eval, q_eval, S, R, S / (2 * R), 64, lq);
+    k_lq_sample<<<148 * 8, 256, 0, c->stream>>>(l_eval, q_eval, S, R, S / (2 * R), 64, lq);
     VG_LAUNCHED(c);
-    k_lq_sample<<<grid_for(2 * M, 256), 256, 0, c->stream>>>(pc->l_eval + 64 * S, q_eval + 64 * S, S, M, S / (2 * M), 1, lq_m);
+    k_lq_sample<<<grid_for(2 * M, 256), 256, 0, c->stream>>>(l_eval + 64 * S, q_eval + 64 * S, S, M, S / (2 * M), 1, lq_m);
     VG_LAUNCHED(c);
     int l2R = ilog2l(2 * R), l2M = ilog2l(2 * M);
     VG_TRY(vg_ntt(c, (const vg_fe *)lq, 2 * R, 2 * R, (vg_fe *)lqc, l2R, 2 * R, 64, to_vg(vg::fe_inv(root_of(l2R))), 1));
     VG_TRY(vg_ntt(c, (const vg_fe *)lq_m, 2 * M, 2 * M, (vg_fe *)lqc_m, l2M, 2 * M, 1, to_vg(vg::fe_inv(root_of(l2M))), 1));
-    VG_TRY(vg_ntt(c, (const vg_fe *)(lqc + R), R, 2 * R, (vg_fe *)pc->h_eval, logS, S, 64, to_vg(root_of(logS)), 0));
-    VG_TRY(vg_ntt(c, (const vg_fe *)(lqc_m + M), M, 2 * M, (vg_fe *)(pc->h_eval + 64 * S), logS, S, 1, to_vg(root_of(logS)), 0));
+    VG_TRY(vg_ntt(c, (const vg_fe *)(lqc + R), R, 2 * R, (vg_fe *)h_eval, logS, S, 64, to_vg(root_of(logS)), 0));
+    VG_TRY(vg_ntt(c, (const vg_fe *)(lqc_m + M), M, 2 * M, (vg_fe *)(h_eval + 64 * S), logS, S, 1, to_vg(root_of(logS)), 0));
 
     // virtual oracle and all_sum
     const fe *tf_lo, *tf_hi, *ti_lo, *ti_hi;
@@ -369,12 +388,12 @@ extern "C" int vg_pc_encode_public(vg_pc *pc, const vg_fe *pub, const vg_fe *pub
     VG_TRY(vg_twiddles(c, vg::fe_inv(root_of(logS)), logS, &ti_lo, &ti_hi));
     {
         ProfScope ps(c, KF_VIRTUAL_ORACLE, 64.0 * 64.0 * (double)S);
-        k_virtual_oracle<<<148 * 16, 256, 0, c->stream>>>(pc->l_eval, q_eval, pc->h_eval, lqc, S, R, logS, 0, 64,
-                                                          tf_lo, tf_hi, ti_lo, ti_hi, pc->vo);
+        k_virtual_oracle<<<148 * 16, 256, 0, c->stream>>>(l_eval, q_eval, h_eval, lqc, S, R, logS, 0, 64,
+                                                          tf_lo, tf_hi, ti_lo, ti_hi, pc->F(pc->vo));
     }
     VG_LAUNCHED(c);
-    k_virtual_oracle<<<grid_for(S, 256), 256, 0, c->stream>>>(pc->l_eval, q_eval, pc->h_eval, lqc_m, S, M, logS, 64, 1,
-                                                             tf_lo, tf_hi, ti_lo, ti_hi, pc->vo);
+    k_virtual_oracle<<<grid_for(S, 256), 256, 0, c->stream>>>(l_eval, q_eval, h_eval, lqc_m, S, M, logS, 64, 1,
+                                                             tf_lo, tf_hi, ti_lo, ti_hi, pc->F(pc->vo));
     VG_LAUNCHED(c);
     fe *sums_d = parts + nb + 1;
     k_all_sum<<<1, 64, 0, c->stream>>>(lqc, R, 0, 64, sums_d);
@@ -382,16 +401,12 @@ extern "C" int vg_pc_encode_public(vg_pc *pc, const vg_fe *pub, const vg_fe *pub
     k_all_sum<<<1, 1, 0, c->stream>>>(lqc_m, M, 64, 1, sums_d);
     VG_LAUNCHED(c);
 
-    fe host[66];
+    fe *host;
+    VG_TRY(vg_pinned(c, 66, &host));
     VG_CHECK_CUDA(cudaMemcpyAsync(host, parts + nb, 66 * sizeof(fe), cudaMemcpyDeviceToHost, c->stream));
     VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
     for (int i = 0; i < 65; ++i) all_sum[i] = to_vg(host[1 + i]);
     if (inner_product) *inner_product = to_vg(host[0]);
-    cudaFree(q_eval);
-    cudaFree(lq);
-    cudaFree(lqc);
-    cudaFree(md);
-    if (staging) cudaFree(staging);
     pc->have_public = true;
     return VG_OK;
 }
@@ -401,14 +416,10 @@ extern "C" int vg_pc_init_commit(vg_pc *pc, int oracle, vg_digest *root)
     if (!pc || !root || (oracle != 0 && oracle != 1)) return vg_fail(VG_ERR_ARG, "vg_pc_init_commit: bad argument");
     if (oracle == 0 && !pc->have_private) return vg_fail(VG_ERR_STATE, "init_commit(0) before encode_private");
     if (oracle == 1 && !pc->have_public) return vg_fail(VG_ERR_STATE, "init_commit(1) before encode_public");
-    if (oracle == 0) {   // a new private commitment restarts the FRI levels
-        for (auto &L : pc->levels) {
-            cudaFree(L.cw);
-            cudaFree(L.tree);
-        }
-        pc->levels.clear();
-    }
-    return commit_tree(pc->ctx, oracle == 0 ? pc->l_eval : pc->h_eval, pc->S, oracle == 0 ? &pc->tree_l : &pc->tree_h, root);
+    if (oracle == 0) pc->nlevels = 0;   // a new private commitment restarts the FRI levels
+    DevBuf &t = oracle == 0 ? pc->tree_l : pc->tree_h;
+    VG_TRY(ensure(pc->ctx, t, (size_t)pc->S * 32));
+    return commit_tree(pc->ctx, pc->F(oracle == 0 ? pc->l_eval : pc->h_eval), pc->S, pc->U(t), root);
 }
 
 extern "C" int vg_eq_table(vg_ctx *c, const vg_fe *r, int log_len, vg_fe *pub);
@@ -418,48 +429,50 @@ extern "C" int vg_pc_fri_step(vg_pc *pc, vg_fe r_, vg_digest *root)
     if (!pc || !root) return vg_fail(VG_ERR_ARG, "vg_pc_fri_step: null argument");
     if (!pc->have_public) return vg_fail(VG_ERR_STATE, "fri step before commit_public");
     vg_ctx *c = pc->ctx;
-    const int t = (int)pc->levels.size();
-    const fe *in = t == 0 ? pc->vo : pc->levels.back().cw;
+    const int t = pc->nlevels;
     const long n = pc->S >> t;
     if (n < 8) return vg_fail(VG_ERR_STATE, "FRI folded below 8 elements per slice");
-    FriLevel L;
+    const fe *in = t == 0 ? pc->F(pc->vo) : pc->F(pc->levels[t - 1].cw);
+    if ((int)pc->levels.size() <= t) pc->levels.resize(t + 1);
+    PcLevel &L = pc->levels[t];
     L.n = n >> 1;
-    VG_TRY(dalloc((void **)&L.cw, 65 * L.n * sizeof(fe)));
-    VG_TRY(dalloc((void **)&L.tree, L.n * 32));
+    VG_TRY(ensure(c, L.cw, 65 * L.n * sizeof(fe)));
+    VG_TRY(ensure(c, L.tree, L.n * 32));
     const int logS = ilog2l(pc->S);
     const fe *ti_lo, *ti_hi;
     VG_TRY(vg_twiddles(c, vg::fe_inv(root_of(logS)), logS, &ti_lo, &ti_hi));
     fe r = vg::fe_make(r_.real, r_.img);
     long q4 = n >> 2;
     long nleaves = L.n >> 1;
+    uint64_t *tree = pc->U(L.tree);
     {
-    ProfScope ps(c, KF_FRI_FOLD, 16.0 * 65.0 * (double)n * 1.5 + 32.0 * (double)q4);
-    if (c->hash_kind == VG_HASH_SHA256)
-        k_fri_fold_leaf<VG_HASH_SHA256><<<grid_for(q4, 128), 128, 0, c->stream>>>(in, n, t, r, ti_lo, ti_hi, L.cw, L.tree + 4 * nleaves);
-    else
-        k_fri_fold_leaf<VG_HASH_SHA3_256><<<grid_for(q4, 128), 128, 0, c->stream>>>(in, n, t, r, ti_lo, ti_hi, L.cw, L.tree + 4 * nleaves);
+        ProfScope ps(c, KF_FRI_FOLD, 16.0 * 65.0 * (double)n * 1.5 + 32.0 * (double)q4);
+        if (c->hash_kind == VG_HASH_SHA256)
+            k_fri_fold_leaf<VG_HASH_SHA256><<<grid_for(q4, 128), 128, 0, c->stream>>>(in, n, t, r, ti_lo, ti_hi, pc->F(L.cw), tree + 4 * nleaves);
+        else
+            k_fri_fold_leaf<VG_HASH_SHA3_256><<<grid_for(q4, 128), 128, 0, c->stream>>>(in, n, t, r, ti_lo, ti_hi, pc->F(L.cw), tree + 4 * nleaves);
     }
     VG_LAUNCHED(c);
-    VG_TRY(vg_merkle_build(c, L.tree, nleaves));
-    pc->levels.push_back(L);
-    VG_CHECK_CUDA(cudaMemcpyAsync(root, L.tree + 4, 32, cudaMemcpyDeviceToHost, c->stream));
+    VG_TRY(vg_merkle_build(c, tree, nleaves));
+    pc->nlevels = t + 1;
+    fe *host;
+    VG_TRY(vg_pinned(c, 2, &host));
+    VG_CHECK_CUDA(cudaMemcpyAsync(host, tree + 4, 32, cudaMemcpyDeviceToHost, c->stream));
     VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
-    if (t == 0) {
-        cudaFree(pc->vo);   // the virtual oracle is never queried directly
-        pc->vo = nullptr;
-    }
+    memcpy(root, host, 32);
     return VG_OK;
 }
 
 extern "C" int vg_pc_fri_final(vg_pc *pc, vg_fe *data, vg_fe *mask, long *n_out)
 {
-    if (!pc || pc->levels.empty()) return vg_fail(VG_ERR_STATE, "vg_pc_fri_final: no FRI level");
-    const FriLevel &L = pc->levels.back();
+    if (!pc || pc->nlevels == 0) return vg_fail(VG_ERR_STATE, "vg_pc_fri_final: no FRI level");
+    PcLevel &L = pc->levels[pc->nlevels - 1];
     const long n = L.n, h = n >> 1;
     if (n_out) *n_out = n;
     if (!data && !mask) return VG_OK;
-    std::vector<fe> buf(65 * n);
-    VG_CHECK_CUDA(cudaMemcpyAsync(buf.data(), L.cw, 65 * n * sizeof(fe), cudaMemcpyDeviceToHost, pc->ctx->stream));
+    fe *buf;
+    VG_TRY(vg_pinned(pc->ctx, 65 * n, &buf));
+    VG_CHECK_CUDA(cudaMemcpyAsync(buf, L.cw.p, 65 * n * sizeof(fe), cudaMemcpyDeviceToHost, pc->ctx->stream));
     VG_CHECK_CUDA(cudaStreamSynchronize(pc->ctx->stream));
     // interleaved layout of fri.cpp:348-363 and 382-388
     for (long j = 0; j < h; ++j) {
@@ -477,45 +490,81 @@ extern "C" int vg_pc_fri_final(vg_pc *pc, vg_fe *data, vg_fe *mask, long *n_out)
     return VG_OK;
 }
 
-static int gather(vg_pc *pc, const fe *cw, long n, long p, const uint64_t *tree, long leaf_node, int depth,
-                  vg_fe *values, vg_digest *path)
+// one descriptor per codeword set: 0 = l, 1 = h, 2 + t = FRI level t
+static int query_descs(vg_pc *pc, std::vector<QueryDesc> &d)
 {
+    d.clear();
+    const int depth0 = ilog2l(pc->S / 2);
+    d.push_back({pc->F(pc->l_eval), pc->U(pc->tree_l), pc->S, depth0});
+    d.push_back({pc->F(pc->h_eval), pc->U(pc->tree_h), pc->S, depth0});
+    for (int t = 0; t < pc->nlevels; ++t)
+        d.push_back({pc->F(pc->levels[t].cw), pc->U(pc->levels[t].tree), pc->levels[t].n, ilog2l(pc->levels[t].n / 2)});
+    return VG_OK;
+}
+
+extern "C" int vg_pc_query_batch(vg_pc *pc, int nq, const int *which, const long *pos, vg_fe *values, vg_digest *paths,
+                                 int *path_len)
+{
+    if (!pc || nq < 0 || (nq && (!which || !pos || !values || !paths)))
+        return vg_fail(VG_ERR_ARG, "vg_pc_query_batch: bad argument");
+    if (nq == 0) return VG_OK;
+    std::vector<QueryDesc> d;
+    query_descs(pc, d);
+    for (int q = 0; q < nq; ++q) {
+        if (which[q] < 0 || which[q] >= (int)d.size()) return vg_fail(VG_ERR_ARG, "query %d: no codeword set %d", q, which[q]);
+        if (which[q] == 0 && !pc->have_private) return vg_fail(VG_ERR_STATE, "no private commitment");
+        if (which[q] == 1 && !pc->have_public) return vg_fail(VG_ERR_STATE, "no public commitment");
+        if (pos[q] < 0) return vg_fail(VG_ERR_ARG, "query %d: negative position", q);
+        if (which[q] < 2 && pos[q] >= pc->S / 2) return vg_fail(VG_ERR_ARG, "query %d: position out of range", q);
+        if (path_len) path_len[q] = d[which[q]].depth + 1;
+    }
     vg_ctx *c = pc->ctx;
-    fe *buf;
-    VG_TRY(vg_partials(c, 130 + 2 * (depth + 1) + 1, &buf));
-    k_gather_query<<<1, 160, 0, c->stream>>>(cw, n, p, tree, leaf_node, depth, buf, (uint64_t *)(buf + 130));
-    VG_LAUNCHED(c);
+    const size_t desc_b = d.size() * sizeof(QueryDesc), which_b = nq * sizeof(int), pos_b = nq * sizeof(long);
+    const size_t in_b = ((desc_b + which_b + pos_b + 255) / 256) * 256;
+    const size_t vals_b = (size_t)nq * 130 * sizeof(fe), paths_b = (size_t)nq * 32 * 32;
+    VG_TRY(ensure(c, pc->qdesc, in_b));
+    VG_TRY(ensure(c, pc->qio, vals_b + paths_b));
     fe *host;
-    VG_TRY(vg_pinned(c, 130 + 2 * (depth + 1), &host));
-    VG_CHECK_CUDA(cudaMemcpyAsync(host, buf, (130 + 2 * (depth + 1)) * sizeof(fe), cudaMemcpyDeviceToHost, c->stream));
+    const size_t pinned_elems = (std::max(in_b, vals_b + paths_b) + 15) / 16;
+    VG_TRY(vg_pinned(c, pinned_elems, &host));
+    char *hb = (char *)host;
+    memcpy(hb, d.data(), desc_b);
+    memcpy(hb + desc_b, which, which_b);
+    memcpy(hb + desc_b + which_b, pos, pos_b);
+    char *db = (char *)pc->qdesc.p;
+    VG_CHECK_CUDA(cudaMemcpyAsync(db, hb, desc_b + which_b + pos_b, cudaMemcpyHostToDevice, c->stream));
     VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
-    memcpy(values, host, 130 * sizeof(fe));
-    memcpy(path, host + 130, (depth + 1) * 32);
+    fe *vals_d = (fe *)pc->qio.p;
+    uint64_t *paths_d = (uint64_t *)((char *)pc->qio.p + vals_b);
+    k_gather_batch<<<nq, 96, 0, c->stream>>>((const QueryDesc *)db, (const int *)(db + desc_b),
+                                             (const long *)(db + desc_b + which_b), vals_d, paths_d);
+    VG_LAUNCHED(c);
+    VG_CHECK_CUDA(cudaMemcpyAsync(host, pc->qio.p, vals_b + paths_b, cudaMemcpyDeviceToHost, c->stream));
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    memcpy(values, host, vals_b);
+    memcpy(paths, (char *)host + vals_b, paths_b);
     return VG_OK;
 }
 
 extern "C" int vg_pc_query_init(vg_pc *pc, long pow0, int oracle, vg_fe *values, vg_digest *path)
 {
     if (!pc || !values || !path || (oracle != 0 && oracle != 1)) return vg_fail(VG_ERR_ARG, "vg_pc_query_init: bad argument");
-    const long S = pc->S;
-    if (pow0 < 0 || pow0 >= S / 2) return vg_fail(VG_ERR_ARG, "query position %ld out of range [0, %ld)", pow0, S / 2);
-    if (oracle == 0 && !pc->have_private) return vg_fail(VG_ERR_STATE, "no private commitment");
-    if (oracle == 1 && !pc->have_public) return vg_fail(VG_ERR_STATE, "no public commitment");
-    const fe *cw = oracle == 0 ? pc->l_eval : pc->h_eval;
-    const uint64_t *tree = oracle == 0 ? pc->tree_l : pc->tree_h;
-    int depth = pc->log_len - 2;
-    return gather(pc, cw, S, pow0, tree, pow0 + S / 2, depth, values, path);
+    std::vector<vg_digest> p(32);
+    int plen = 0;
+    long pos = pow0;
+    VG_TRY(vg_pc_query_batch(pc, 1, &oracle, &pos, values, p.data(), &plen));
+    memcpy(path, p.data(), plen * sizeof(vg_digest));
+    return VG_OK;
 }
 
 extern "C" int vg_pc_query_step(vg_pc *pc, int lvl, long pow, vg_fe *values, vg_digest *path, int *path_len)
 {
-    if (!pc || !values || !path || lvl < 0 || lvl >= (int)pc->levels.size())
+    if (!pc || !values || !path || lvl < 0 || lvl >= pc->nlevels)
         return vg_fail(VG_ERR_ARG, "vg_pc_query_step: bad argument (lvl %d)", lvl);
-    const FriLevel &L = pc->levels[lvl];
-    const long h = L.n >> 1;
-    if (pow < 0) return vg_fail(VG_ERR_ARG, "negative query position");
-    long p = pow % h;
-    int depth = ilog2l(h);
-    if (path_len) *path_len = depth + 1;
-    return gather(pc, L.cw, L.n, p, L.tree, p + h, depth, values, path);
+    std::vector<vg_digest> p(32);
+    int plen = 0, which = 2 + lvl;
+    VG_TRY(vg_pc_query_batch(pc, 1, &which, &pow, values, p.data(), &plen));
+    memcpy(path, p.data(), plen * sizeof(vg_digest));
+    if (path_len) *path_len = plen;
+    return VG_OK;
 }

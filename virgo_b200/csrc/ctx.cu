@@ -141,6 +141,28 @@ extern "C" int vg_timer_stop(vg_ctx *c, void *timer, double *ms)
     return VG_OK;
 }
 
+extern "C" int vg_timer_stop_multi(vg_ctx *const *ctxs, int n, void *timer, double *ms)
+{
+    if (!ctxs || n < 1 || !timer || !ms) return vg_fail(VG_ERR_ARG, "null argument");
+    cudaEvent_t *ev = (cudaEvent_t *)timer;
+    double worst = 0;
+    for (int i = 0; i < n; ++i) {
+        cudaEvent_t e;
+        VG_CHECK_CUDA(cudaEventCreate(&e));
+        VG_CHECK_CUDA(cudaEventRecord(e, ctxs[i]->stream));
+        VG_CHECK_CUDA(cudaEventSynchronize(e));
+        float t = 0;
+        VG_CHECK_CUDA(cudaEventElapsedTime(&t, ev[0], e));
+        if (t > worst) worst = t;
+        cudaEventDestroy(e);
+    }
+    *ms = worst;
+    cudaEventDestroy(ev[0]);
+    cudaEventDestroy(ev[1]);
+    delete[] ev;
+    return VG_OK;
+}
+
 extern "C" int vg_ctx_destroy(vg_ctx *c)
 {
     if (!c) return VG_OK;
@@ -175,6 +197,13 @@ extern "C" int vg_ctx_get_hash(vg_ctx *c, int *kind)
 {
     if (!c || !kind) return vg_fail(VG_ERR_ARG, "null argument");
     *kind = c->hash_kind;
+    return VG_OK;
+}
+
+extern "C" int vg_ctx_device(vg_ctx *c, int *device)
+{
+    if (!c || !device) return vg_fail(VG_ERR_ARG, "null argument");
+    *device = c->device;
     return VG_OK;
 }
 

@@ -292,13 +292,17 @@ __global__ void __launch_bounds__(GKR_THREADS) k_phase2_scatter(const uint8_t *_
 // ------------------------------------------------------------ round kernel
 __device__ __forceinline__ fe fold(fe x0, fe x1, fe r) { return x0 + r * (x1 - x0); }
 
+// The block partials are reduced by the last block to finish (a counter in
+// device memory decides which one), so one launch returns the round sums.
 template <bool FOLD>
 __global__ void __launch_bounds__(GKR_THREADS) k_round(const fe *__restrict__ xV, const fe *__restrict__ xAV,
                                                        const fe *__restrict__ xAM, long npairs, fe r,
                                                        fe *__restrict__ yV, fe *__restrict__ yAV, fe *__restrict__ yAM,
-                                                       fe *__restrict__ parts)
+                                                       fe *__restrict__ parts, unsigned *__restrict__ counter,
+                                                       fe *__restrict__ out3)
 {
     __shared__ fe sm[3 * 32];
+    __shared__ bool last;
     fe acc[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < npairs; i += (long)gridDim.x * blockDim.x) {
         fe v0, v1, a0, a1, m0, m1;
@@ -328,6 +332,29 @@ __global__ void __launch_bounds__(GKR_THREADS) k_round(const fe *__restrict__ xV
         parts[3 * blockIdx.x + 0] = acc[0];
         parts[3 * blockIdx.x + 1] = acc[1];
         parts[3 * blockIdx.x + 2] = acc[2];
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    fe tot[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            fe x;
+            x.img = __ldcg(&parts[3 * b + k].img);
+            x.real = __ldcg(&parts[3 * b + k].real);
+            tot[k] = tot[k] + x;
+        }
+    }
+    __syncthreads();
+    block_sum<3>(tot, sm);
+    if (threadIdx.x == 0) {
+        out3[0] = tot[0];
+        out3[1] = tot[1];
+        out3[2] = tot[2];
+        *counter = 0;
     }
 }
 
@@ -352,6 +379,9 @@ struct vg_gkr {
     unsigned long long *acc = nullptr;   // 2 tables x 4 words x 2^max_bl
     fe *eq = nullptr;                    // half tables
     fe *rbuf = nullptr;                  // challenges (device copy)
+    fe *round_parts = nullptr;           // block partials of the round kernel
+    fe *round_out = nullptr;             // round sums (3) written by the last block
+    unsigned *round_counter = nullptr;   // blocks finished, reset by the last one
     long eq_half = 0;
     int layer = -1, length_g = 0;
     long n = 0;                          // current table length
@@ -476,6 +506,10 @@ extern "C" int vg_gkr_create(vg_ctx *ctx, const vg_circuit *c, vg_gkr **out)
     g->eq_half = 1L << (c->max_bl / 2 + 1);
     if (cudaMalloc(&g->eq, 6 * g->eq_half * sizeof(fe)) != cudaSuccess) return fail("eq tables");
     if (cudaMalloc(&g->rbuf, 3 * 64 * sizeof(fe)) != cudaSuccess) return fail("challenges");
+    if (cudaMalloc(&g->round_parts, 3 * 148 * 8 * sizeof(fe)) != cudaSuccess) return fail("round partials");
+    if (cudaMalloc(&g->round_out, 16 * sizeof(fe)) != cudaSuccess) return fail("round sums");
+    if (cudaMalloc(&g->round_counter, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
+    if (cudaMemset(g->round_counter, 0, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
     *out = g;
     return VG_OK;
 }
@@ -490,6 +524,9 @@ extern "C" int vg_gkr_destroy(vg_gkr *g)
     cudaFree(g->acc);
     cudaFree(g->eq);
     cudaFree(g->rbuf);
+    cudaFree(g->round_parts);
+    cudaFree(g->round_out);
+    cudaFree(g->round_counter);
     delete g;
     return VG_OK;
 }
@@ -605,7 +642,7 @@ extern "C" int vg_eq_table(vg_ctx *c, const vg_fe *r, int log_len, vg_fe *pub)
     if (!c || !r || !pub || log_len < 1 || log_len > 30) return vg_fail(VG_ERR_ARG, "vg_eq_table: bad argument");
     fe *tmp;
     int f = log_len >> 1, s = log_len - f;
-    VG_CHECK_CUDA(cudaMalloc(&tmp, ((1L << f) + (1L << s) + 64) * sizeof(fe)));
+    VG_TRY(vg_scratch2(c, ((1L << f) + (1L << s) + 64) * sizeof(fe), (void **)&tmp));
     fe *lo = tmp, *hi = tmp + (1L << f), *rd = hi + (1L << s);
     cudaMemcpyAsync(rd, r, log_len * sizeof(fe), cudaMemcpyHostToDevice, c->stream);
     k_eq_half<<<grid_for(1L << f, 256), 256, 0, c->stream>>>(rd, f, vg::fe_one(), lo);
@@ -616,7 +653,6 @@ extern "C" int vg_eq_table(vg_ctx *c, const vg_fe *r, int log_len, vg_fe *pub)
     k_eq_combine<<<std::min<unsigned>(grid_for(n, 256), 148u * 32u), 256, 0, c->stream>>>(lo, hi, f, n, (fe *)pub);
     VG_LAUNCHED(c);
     VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
-    cudaFree(tmp);
     return VG_OK;
 }
 
@@ -724,20 +760,19 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
     const long n_out = fold ? g->n / 2 : g->n;   // table length the sums are taken over
     const long npairs = n_out / 2;
     unsigned grid = std::min<unsigned>(grid_for(npairs, GKR_THREADS), 148u * 8u);
-    fe *parts;
-    VG_TRY(vg_partials(c, 3 * (size_t)grid + 3 + 6, &parts));
     fe *y[3] = {g->buf[g->next_buf][0], g->buf[g->next_buf][1], g->buf[g->next_buf][2]};
     fe r = tofe(previous_random);
     {
         // fold: read 3 tables x 4 entries, write 3 x 2 per pair; else read 3 x 2
         ProfScope ps(c, KF_ROUND, (fold ? 288.0 : 96.0) * (double)npairs);
         if (fold)
-            k_round<true><<<grid, GKR_THREADS, 0, c->stream>>>(g->cur[0], g->cur[1], g->cur[2], npairs, r, y[0], y[1], y[2], parts);
+            k_round<true><<<grid, GKR_THREADS, 0, c->stream>>>(g->cur[0], g->cur[1], g->cur[2], npairs, r, y[0], y[1], y[2],
+                                                               g->round_parts, g->round_counter, g->round_out);
         else
-            k_round<false><<<grid, GKR_THREADS, 0, c->stream>>>(g->cur[0], g->cur[1], g->cur[2], npairs, r, nullptr, nullptr, nullptr, parts);
+            k_round<false><<<grid, GKR_THREADS, 0, c->stream>>>(g->cur[0], g->cur[1], g->cur[2], npairs, r, nullptr, nullptr,
+                                                                nullptr, g->round_parts, g->round_counter, g->round_out);
     }
     VG_LAUNCHED(c);
-    VG_TRY(vg_reduce_partials(c, parts, (int)grid, 3, parts + 3 * grid));
     if (fold) {
         g->cur[0] = y[0];
         g->cur[1] = y[1];
@@ -748,7 +783,7 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
     g->round0_pending = false;
     fe *host;
     VG_TRY(vg_pinned(c, 9, &host));
-    VG_CHECK_CUDA(cudaMemcpyAsync(host, parts + 3 * grid, 3 * sizeof(fe), cudaMemcpyDeviceToHost, c->stream));
+    VG_CHECK_CUDA(cudaMemcpyAsync(host, g->round_out, 3 * sizeof(fe), cudaMemcpyDeviceToHost, c->stream));
     const bool want_last = last6 && g->n == 2;
     if (want_last) {
         for (int k = 0; k < 3; ++k)

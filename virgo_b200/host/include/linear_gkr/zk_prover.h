@@ -87,13 +87,15 @@ public:
     std::vector<prime_field::field_element> maskr;
 
     // ---- device state (not part of the reference interface) ----
+    struct vg_ctx *dev_ctx;   // context (stream) of this prover; the process default when null
     vg_circuit *dev_circuit;
     vg_gkr *dev_gkr;
     bool owns_circuit;
+    bool quiet;               // no timing line on stderr from evaluate()
     prime_field::field_element tables_last[6];   // folded V, addV, add_mult pairs after a phase's last round
     // Reuses an uploaded circuit (e.g. many proofs of one circuit); the
     // prover then does not free it.
-    void attach_circuit(const layered_circuit &c, vg_circuit *dev);
+    void attach_circuit(const layered_circuit &c, vg_circuit *dev, struct vg_ctx *ctx = nullptr);
     // Clears the per-proof state so the same object can prove again.
     void reset_proof();
 };

@@ -15,8 +15,12 @@
 //
 // The transcript has the record layout of the oracle's recorder: 1 byte tag,
 // uint32 count of 16-byte units, the units.
+#include <cuda_runtime.h>
 #include <stdlib.h>
 #include <algorithm>
+#include <memory>
+#include <thread>
+#include <unordered_set>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -86,11 +90,27 @@ F direct_relay(const layered_circuit &C, int depth, const F *r_g, const F *r_u)
 }
 }  // namespace
 
-struct vg_session {
+// Gate storage of a circuit shared by forked sessions.
+struct CircuitData {
     layered_circuit C;
     std::vector<std::vector<gate> > storage;
     vg_circuit *dev = nullptr;
+    ~CircuitData()
+    {
+        if (dev) vg_circuit_destroy(dev);
+        delete[] C.circuit;
+    }
+};
+
+// A session owns its context (CUDA stream, scratch), its commitment state and
+// its prover tables, so sessions prove concurrently from different threads.
+struct vg_session {
+    std::shared_ptr<CircuitData> circuit;
+    vg_ctx *ctx = nullptr;
+    vg_pc *pc = nullptr;
     zk_prover *p = nullptr;
+    void *pub = nullptr;   // device buffer for the public eq table
+    size_t pub_bytes = 0;
 };
 
 // ----------------------------------------------------------- circuit build
@@ -98,7 +118,7 @@ struct vg_session {
 // the way zk_verifier::read_circuit does (zk_verifier.cpp:24-191): the input
 // layer becomes layer 0 (values) plus a relay layer 1, padded to 2^17 gates
 // when there are more than three file layers and to 2^15 otherwise.
-static int build_circuit(vg_session *s, int d, const long *n, const uint8_t *const *ty, const int64_t *const *u,
+static int build_circuit(CircuitData *s, int d, const long *n, const uint8_t *const *ty, const int64_t *const *u,
                          const int64_t *const *v, std::string &err)
 {
     if (d < 1) {
@@ -179,34 +199,51 @@ static int build_circuit(vg_session *s, int d, const long *n, const uint8_t *con
     return VG_OK;
 }
 
-static int session_finish(vg_session *s)
+static int session_device(vg_ctx **ctx)
 {
-    const int depth = s->C.total_depth;
+    int dev = 0;
+    if (const char *e = getenv("VIRGO_DEVICE")) dev = atoi(e);
+    return vg_ctx_create(dev, ctx);
+}
+
+// own context, commitment state and prover over a (possibly shared) circuit
+static int session_attach(vg_session *s)
+{
+    int rc = s->ctx ? VG_OK : session_device(&s->ctx);
+    if (rc != VG_OK) return rc;
+    rc = vg_ctx_set_hash(s->ctx, virgo_hash_kind());
+    if (rc == VG_OK) rc = vg_pc_create(s->ctx, &s->pc);
+    if (rc != VG_OK) return rc;
+    s->p = new zk_prover();
+    s->p->quiet = true;
+    s->p->attach_circuit(s->circuit->C, s->circuit->dev, s->ctx);
+    return VG_OK;
+}
+
+static int circuit_upload(CircuitData *cd, vg_ctx *ctx)
+{
+    const int depth = cd->C.total_depth;
     std::vector<int> bl(depth);
     std::vector<std::vector<uint8_t> > ty(depth);
     std::vector<std::vector<int64_t> > u(depth), v(depth);
     std::vector<const uint8_t *> pty(depth);
     std::vector<const int64_t *> pu(depth), pv(depth);
     for (int i = 0; i < depth; ++i) {
-        bl[i] = s->C.circuit[i].bit_length;
+        bl[i] = cd->C.circuit[i].bit_length;
         const long nn = 1L << bl[i];
         ty[i].resize(nn);
         u[i].resize(nn);
         v[i].resize(nn);
         for (long k = 0; k < nn; ++k) {
-            ty[i][k] = (uint8_t)s->C.circuit[i].gates[k].ty;
-            u[i][k] = s->C.circuit[i].gates[k].u;
-            v[i][k] = s->C.circuit[i].gates[k].v;
+            ty[i][k] = (uint8_t)cd->C.circuit[i].gates[k].ty;
+            u[i][k] = cd->C.circuit[i].gates[k].u;
+            v[i][k] = cd->C.circuit[i].gates[k].v;
         }
         pty[i] = ty[i].data();
         pu[i] = u[i].data();
         pv[i] = v[i].data();
     }
-    int rc = vg_circuit_upload(virgo::ctx(), depth, bl.data(), pty.data(), pu.data(), pv.data(), &s->dev);
-    if (rc != VG_OK) return rc;
-    s->p = new zk_prover();
-    s->p->attach_circuit(s->C, s->dev);
-    return VG_OK;
+    return vg_circuit_upload(ctx, depth, bl.data(), pty.data(), pu.data(), pv.data(), &cd->dev);
 }
 
 extern "C" int vg_session_create(int d, const long *n, const uint8_t *const *ty, const int64_t *const *u,
@@ -214,11 +251,28 @@ extern "C" int vg_session_create(int d, const long *n, const uint8_t *const *ty,
 {
     if (!n || !ty || !u || !v || !out) return VG_ERR_ARG;
     vg_session *s = new vg_session();
+    s->circuit = std::make_shared<CircuitData>();
     std::string err;
-    int rc = build_circuit(s, d, n, ty, u, v, err);
-    if (rc == VG_OK) rc = session_finish(s);
+    int rc = build_circuit(s->circuit.get(), d, n, ty, u, v, err);
+    if (rc == VG_OK) rc = session_device(&s->ctx);
+    if (rc == VG_OK) rc = circuit_upload(s->circuit.get(), s->ctx);
+    if (rc == VG_OK) rc = session_attach(s);
     if (rc != VG_OK) {
         if (!err.empty()) fprintf(stderr, "vg_session_create: %s\n", err.c_str());
+        vg_session_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return VG_OK;
+}
+
+extern "C" int vg_session_fork(vg_session *base, vg_session **out)
+{
+    if (!base || !out) return VG_ERR_ARG;
+    vg_session *s = new vg_session();
+    s->circuit = base->circuit;
+    int rc = session_attach(s);
+    if (rc != VG_OK) {
         vg_session_destroy(s);
         return rc;
     }
@@ -294,8 +348,10 @@ extern "C" int vg_session_destroy(vg_session *s)
         s->p->delete_self();
         delete s->p;
     }
-    if (s->dev) vg_circuit_destroy(s->dev);
-    delete[] s->C.circuit;
+    if (s->pub) vg_dev_free(s->ctx, s->pub);
+    if (s->pc) vg_pc_destroy(s->pc);
+    s->circuit.reset();
+    if (s->ctx) vg_ctx_destroy(s->ctx);
     delete s;
     return VG_OK;
 }
@@ -303,12 +359,19 @@ extern "C" int vg_session_destroy(vg_session *s)
 extern "C" int vg_session_depth(vg_session *s, int *depth, int *input_log)
 {
     if (!s) return VG_ERR_ARG;
-    if (depth) *depth = s->C.total_depth;
-    if (input_log) *input_log = s->C.circuit[0].bit_length;
+    if (depth) *depth = s->circuit->C.total_depth;
+    if (input_log) *input_log = s->circuit->C.circuit[0].bit_length;
     return VG_OK;
 }
 
 extern "C" void vg_free(void *p) { free(p); }
+
+extern "C" int vg_session_ctx(vg_session *s, vg_ctx **out)
+{
+    if (!s || !out) return VG_ERR_ARG;
+    *out = s->ctx;
+    return VG_OK;
+}
 
 extern "C" int vg_default_ctx(vg_ctx **out)
 {
@@ -378,11 +441,16 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
                                 uint8_t **transcript, size_t *transcript_len)
 {
     if (!s || !s->p) return VG_ERR_ARG;
+    {
+        int dev = 0;
+        vg_ctx_device(s->ctx, &dev);
+        cudaSetDevice(dev);   // this thread may not have used the session's device yet
+    }
     auto t_all = clk::now();
     vg_proof_stats st;
     memset(&st, 0, sizeof st);
     long long launches0 = 0;
-    vg_ctx_launch_count(virgo::ctx(), &launches0);
+    vg_ctx_launch_count(s->ctx, &launches0);
 
     // the reference's rand() stream after srand(seed), private to this thread
     struct random_data rd;
@@ -400,7 +468,7 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
     Transcript tr;
     tr.on = want_transcript != 0;
     zk_prover &p = *s->p;
-    layered_circuit &C = s->C;
+    layered_circuit &C = s->circuit->C;
     p.reset_proof();
     int proof_size = 0;
 
@@ -547,19 +615,49 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
     all_mask_sum = all_mask_sum + p.Zu * p.sumRc.eval(p.preu1);
     st.gkr_s = since(t0);
 
-    // ---------------- commitments (zk_verifier.cpp:1210-1219) ----------------
+    // ---------------- commitments (zk_verifier.cpp:1210-1219; poly_commit.h:42-351) ----------------
     t0 = clk::now();
     const int L = C.circuit[0].bit_length;
-    __hhash_digest root_l = p.poly_prover.commit_private_array(p.circuit_value[0], L, p.all_pri_mask);
+    int rc;
+#define SESSION_TRY(x)                 \
+    do {                               \
+        rc = (x);                      \
+        if (rc != VG_OK) {             \
+            prime_field::set_thread_random_state(nullptr); \
+            return rc;                 \
+        }                              \
+    } while (0)
+    long M = 0;
+    SESSION_TRY(vg_pc_encode_private(s->pc, (const vg_fe *)p.circuit_value[0], L, (const vg_fe *)p.all_pri_mask.data(),
+                                     (long)p.all_pri_mask.size(), &M));
+    __hhash_digest root_l, root_h;
+    SESSION_TRY(vg_pc_init_commit(s->pc, 0, (vg_digest *)&root_l));
     tr.put('C', &root_l, 2);
-    void *pub = nullptr;
-    virgo::check(vg_dev_alloc(virgo::ctx(), ((size_t)1 << L) * sizeof(F), &pub), "vg_dev_alloc");
-    virgo::check(vg_eq_table(virgo::ctx(), (const vg_fe *)r_0.data(), L, (vg_fe *)pub), "vg_eq_table");
-    F all_sum[slice_number + 1];
-    F target = alpha_beta_sum - p.Zu * p.sumRc.eval(p.preu1) + all_mask_sum;
-    __hhash_digest root_h = p.poly_prover.commit_public_array(all_pub_mask, (F *)pub, L, target, all_sum);
+    const size_t pub_bytes = ((size_t)1 << L) * sizeof(F);
+    if (s->pub_bytes < pub_bytes) {
+        if (s->pub) vg_dev_free(s->ctx, s->pub);
+        s->pub = nullptr;
+        SESSION_TRY(vg_dev_alloc(s->ctx, pub_bytes, &s->pub));
+        s->pub_bytes = pub_bytes;
+    }
+    SESSION_TRY(vg_eq_table(s->ctx, (const vg_fe *)r_0.data(), L, (vg_fe *)s->pub));
+    if ((long)all_pub_mask.size() > M) {
+        prime_field::set_thread_random_state(nullptr);
+        return VG_ERR_STATE;
+    }
+    while ((long)all_pub_mask.size() < M) all_pub_mask.push_back(F(0));   // poly_commit.h:138-139
+    F all_sum[slice_number + 1], inner;
+    SESSION_TRY(vg_pc_encode_public(s->pc, (const vg_fe *)s->pub, (const vg_fe *)all_pub_mask.data(), M,
+                                    (vg_fe *)all_sum, (vg_fe *)&inner));
+    // the claimed inner product the reference asserts (poly_commit.h:193)
+    const F target = alpha_beta_sum - p.Zu * p.sumRc.eval(p.preu1) + all_mask_sum;
+    if (inner != target) {
+        fprintf(stderr, "vg_session_prove: committed inner product differs from the sumcheck claim\n");
+        prime_field::set_thread_random_state(nullptr);
+        return VG_ERR_STATE;
+    }
+    SESSION_TRY(vg_pc_init_commit(s->pc, 1, (vg_digest *)&root_h));
     tr.put('C', &root_h, 2);
-    vg_dev_free(virgo::ctx(), pub);
     proof_size += 2 * sizeof(__hhash_digest);
     tr.put('A', all_sum, slice_number + 1);
     __hhash_digest lh[2] = {root_l, root_h};
@@ -568,68 +666,147 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
 
     // ---------------- FRI commit phase (vpd_verifier.cpp:46-78, 101) ----------------
     t0 = clk::now();
-    const int saved = fri::log_current_witness_size_per_slice;
     int codeword_size = 1 << (L + rs_code_rate - log_slice_number);
     int levels = 0;
     while (codeword_size > (1 << rs_code_rate)) {
         F r = prime_field::random();
-        __hhash_digest h = fri::commit_phase_step(r);
+        __hhash_digest h;
+        vg_fe rv;
+        rv.real = r.real;
+        rv.img = r.img;
+        SESSION_TRY(vg_pc_fri_step(s->pc, rv, (vg_digest *)&h));
         tr.put('T', &h, 2);
         codeword_size /= 2;
         ++levels;
     }
-    F *final_cw = fri::commit_phase_final();
     {
-        const int nfin = 1 << fri::log_current_witness_size_per_slice;
-        tr.put('X', final_cw, (uint32_t)(nfin * slice_number));
-        tr.put('x', fri::cpd.rs_codeword_msk[fri::current_step_no - 1], (uint32_t)nfin);
+        long nfin = 0;
+        SESSION_TRY(vg_pc_fri_final(s->pc, nullptr, nullptr, &nfin));
+        std::vector<F> data(nfin * (slice_number + 1)), msk(nfin);
+        SESSION_TRY(vg_pc_fri_final(s->pc, (vg_fe *)data.data(), (vg_fe *)msk.data(), &nfin));
+        tr.put('X', data.data(), (uint32_t)(nfin * slice_number));
+        tr.put('x', msk.data(), (uint32_t)nfin);
     }
-    fri::log_current_witness_size_per_slice = saved;
     st.fri_s = since(t0);
 
     // ---------------- query answers (vpd_verifier.cpp:105-312) ----------------
+    // All positions come from the rand() stream alone, so they are drawn
+    // first and every answer is gathered in one batch; the answers and the
+    // proof-size bookkeeping (fri.cpp:148-289) are then assembled in order.
     t0 = clk::now();
+    std::vector<int> which;
+    std::vector<long> pos;
     for (int rep = 0; rep < ldt_repeat_num; ++rep) {
-        long long pow = 0;
+        long long pw = 0;
         for (int i = 0; i < L - log_slice_number; ++i) {
             const int lw = L + rs_code_rate - log_slice_number - i;
-            int new_size = 0;
             if (i == 0) {
                 do {
-                    pow = rand_int() % (1 << lw);
-                } while (pow < (1 << (L - log_slice_number - i)) || pow % 2 == 1);
-                const long long s0 = pow / 2, s1 = (pow + (1LL << lw)) / 2;
-                auto al = fri::request_init_value_with_merkle(s0, s1, new_size, 0);
-                tr.answer('I', al, new_size);
-                auto ah = fri::request_init_value_with_merkle(s0, s1, new_size, 1);
-                tr.answer('I', ah, new_size);
-                proof_size += new_size;
-                auto b = fri::request_step_commit(0, pow / 2, new_size);
-                tr.answer('J', b, new_size);
-                proof_size += new_size;
+                    pw = rand_int() % (1 << lw);
+                } while (pw < (1 << (L - log_slice_number - i)) || pw % 2 == 1);
+                which.push_back(0);
+                pos.push_back((long)(pw / 2));
+                which.push_back(1);
+                pos.push_back((long)(pw / 2));
             } else {
-                pow = pow % (1 << lw);
-                auto b = fri::request_step_commit(i, pow / 2, new_size);
-                tr.answer('J', b, new_size);
-                proof_size += new_size;
+                pw = pw % (1 << lw);
             }
+            which.push_back(2 + i);
+            pos.push_back((long)(pw / 2));
+        }
+    }
+    const int nq = (int)which.size();
+    std::vector<F> qvals((size_t)nq * 130);
+    std::vector<__hhash_digest> qpaths((size_t)nq * 32);
+    std::vector<int> qlen(nq);
+    SESSION_TRY(vg_pc_query_batch(s->pc, nq, which.data(), pos.data(), (vg_fe *)qvals.data(), (vg_digest *)qpaths.data(),
+                                  qlen.data()));
+    std::unordered_set<long long> seen_elem[2], seen_node[2];
+    std::vector<std::unordered_set<long long> > seen_level(levels);
+    const long long half_S = 1LL << (L - 2);
+    for (int q = 0; q < nq; ++q) {
+        std::pair<std::vector<std::pair<F, F> >, std::vector<__hhash_digest> > a;
+        const F *v = &qvals[(size_t)q * 130];
+        for (int k = 0; k <= slice_number; ++k) a.first.push_back(std::make_pair(v[2 * k], v[2 * k + 1]));
+        const __hhash_digest *pth = &qpaths[(size_t)q * 32];
+        const int depth = qlen[q] - 1;
+        int new_size = 0;
+        if (which[q] < 2) {   // fri::request_init_value_with_merkle
+            const int o = which[q];
+            const long long p0 = pos[q];
+            for (int k = 0; k < slice_number; ++k)
+                for (int b = 0; b < 2; ++b)
+                    if (seen_elem[o].insert((p0 << (log_slice_number + 1)) | (k << 1) | b).second) new_size += sizeof(F);
+            a.second.resize(depth + 1);
+            a.second[depth] = pth[depth];
+            long long node = p0 + half_S;
+            for (int k = 0; k < depth; ++k) {
+                if (!seen_node[o].count(node ^ 1)) new_size += sizeof(__hhash_digest);
+                seen_node[o].insert(node);
+                seen_node[o].insert(node ^ 1);
+                a.second[k] = pth[k];
+                node /= 2;
+            }
+            tr.answer('I', a, new_size);
+            if (o == 1) proof_size += new_size;   // the verifier adds the second call's count
+        } else {              // fri::request_step_commit
+            const int lvl = which[q] - 2;
+            const long long h = 1LL << depth, p0 = pos[q] % h;
+            auto &seen = seen_level[lvl];
+            bool visited = false;
+            for (int k = 0; k < slice_number; ++k)
+                if (seen.count((p0 << (log_slice_number + 1)) | (k << 1))) visited = true;
+            if (!visited) new_size += sizeof(F);
+            long long node = p0 + h;
+            int k = 0;
+            while (node != 1) {
+                if (!seen.count(node ^ 1)) {
+                    new_size += sizeof(__hhash_digest);
+                    seen.insert(node ^ 1);
+                    seen.insert(node);
+                }
+                a.second.push_back(pth[k++]);
+                node /= 2;
+            }
+            a.second.push_back(pth[depth]);
+            tr.answer('J', a, new_size);
+            proof_size += new_size;
         }
     }
     st.query_s = since(t0);
     prime_field::set_thread_random_state(nullptr);
+#undef SESSION_TRY
 
-    st.prove_time = p.total_time + p.poly_prover.total_time;
+    st.prove_time = p.total_time + st.commit_s + st.fri_s;   // GKR methods + commitments + FRI
     st.total_s = since(t_all);
     st.proof_size = proof_size;
     long long launches1 = 0;
-    vg_ctx_launch_count(virgo::ctx(), &launches1);
+    vg_ctx_launch_count(s->ctx, &launches1);
     st.launches = launches1 - launches0;
-    (void)levels;
     if (stats) *stats = st;
     if (transcript && transcript_len) {
         *transcript_len = tr.bytes.size();
         *transcript = (uint8_t *)malloc(tr.bytes.size() ? tr.bytes.size() : 1);
         if (tr.bytes.size()) memcpy(*transcript, tr.bytes.data(), tr.bytes.size());
     }
+    return VG_OK;
+}
+
+// Proofs of several sessions at once, one host thread per session; each
+// session has its own CUDA stream, so their kernels overlap on the GPU.
+extern "C" int vg_session_prove_batch(vg_session *const *ss, int n, const unsigned *seeds, int want_transcript,
+                                      vg_proof_stats *stats, uint8_t **transcripts, size_t *transcript_lens)
+{
+    if (!ss || !seeds || n < 0) return VG_ERR_ARG;
+    std::vector<int> rcs(n, VG_OK);
+    std::vector<std::thread> th;
+    for (int i = 0; i < n; ++i)
+        th.emplace_back([&, i]() {
+            rcs[i] = vg_session_prove(ss[i], seeds[i], want_transcript, stats ? &stats[i] : nullptr,
+                                      transcripts ? &transcripts[i] : nullptr, transcript_lens ? &transcript_lens[i] : nullptr);
+        });
+    for (auto &t : th) t.join();
+    for (int i = 0; i < n; ++i)
+        if (rcs[i] != VG_OK) return rcs[i];
     return VG_OK;
 }

@@ -14,7 +14,8 @@
 typedef prime_field::field_element F;
 using clk = std::chrono::high_resolution_clock;
 
-static F inv_2;
+// 1/2 in F_p (the reference's global inv_2, zk_prover.cpp:23-28)
+static const F inv_2 = prime_field::inv(F(2));
 
 static inline vg_fe to_vg(const F &x)
 {
@@ -45,9 +46,11 @@ zk_prover::zk_prover()
 {
     memset(circuit_value, 0, sizeof circuit_value);
     maskpoly = nullptr;
+    dev_ctx = nullptr;
     dev_circuit = nullptr;
     dev_gkr = nullptr;
     owns_circuit = false;
+    quiet = false;
     total_time = 0;
     r_0 = r_1 = nullptr;
     one_minus_r_0 = one_minus_r_1 = nullptr;
@@ -88,27 +91,28 @@ static void upload(const layered_circuit &C, vg_circuit **out)
     virgo::check(vg_circuit_upload(virgo::ctx(), depth, bl.data(), pty.data(), pu.data(), pv.data(), out), "vg_circuit_upload");
 }
 
+static vg_ctx *ctx_of(const zk_prover *p) { return p->dev_ctx ? p->dev_ctx : virgo::ctx(); }
+
 void zk_prover::get_circuit(const layered_circuit &from_verifier)
 {
     C = from_verifier;
-    inv_2 = prime_field::inv(F(2));
     if (dev_gkr) vg_gkr_destroy(dev_gkr);
     if (dev_circuit && owns_circuit) vg_circuit_destroy(dev_circuit);
     dev_gkr = nullptr;
     upload(C, &dev_circuit);
     owns_circuit = true;
-    virgo::check(vg_gkr_create(virgo::ctx(), dev_circuit, &dev_gkr), "vg_gkr_create");
+    virgo::check(vg_gkr_create(ctx_of(this), dev_circuit, &dev_gkr), "vg_gkr_create");
 }
 
-void zk_prover::attach_circuit(const layered_circuit &c, vg_circuit *dev)
+void zk_prover::attach_circuit(const layered_circuit &c, vg_circuit *dev, vg_ctx *ctx)
 {
     C = c;
-    inv_2 = prime_field::inv(F(2));
+    if (ctx) dev_ctx = ctx;
     if (dev_gkr) vg_gkr_destroy(dev_gkr);
     if (dev_circuit && owns_circuit) vg_circuit_destroy(dev_circuit);
     dev_circuit = dev;
     owns_circuit = false;
-    virgo::check(vg_gkr_create(virgo::ctx(), dev_circuit, &dev_gkr), "vg_gkr_create");
+    virgo::check(vg_gkr_create(ctx_of(this), dev_circuit, &dev_gkr), "vg_gkr_create");
 }
 
 void zk_prover::reset_proof()
@@ -137,7 +141,7 @@ F *zk_prover::evaluate()
         virgo::check(vg_gkr_layer_values(dev_gkr, i, &p), "vg_gkr_layer_values");
         circuit_value[i] = (F *)p;
     }
-    std::cerr << "total evaluation time: " << since(t0) << " seconds." << std::endl;
+    if (!quiet) std::cerr << "total evaluation time: " << since(t0) << " seconds." << std::endl;
     return circuit_value[C.total_depth - 1];
 }
 
@@ -153,7 +157,7 @@ F zk_prover::V_res(const F *one_minus_r_0, const F *r_0, const F *output_raw, in
     if (output_raw == circuit_value[C.total_depth - 1] && output_size == (1 << C.circuit[C.total_depth - 1].bit_length)) {
         virgo::check(vg_gkr_v_res(dev_gkr, r.data(), r_0_size, &out), "vg_gkr_v_res");
     } else {
-        virgo::check(vg_mle_eval(virgo::ctx(), (const vg_fe *)output_raw, output_size, r.data(), r_0_size, &out), "vg_mle_eval");
+        virgo::check(vg_mle_eval(ctx_of(this), (const vg_fe *)output_raw, output_size, r.data(), r_0_size, &out), "vg_mle_eval");
     }
     res = from_vg(out);
     total_time += since(t0);
