@@ -519,8 +519,11 @@ extern "C" int vg_pc_query_batch(vg_pc *pc, int nq, const int *which, const long
         if (path_len) path_len[q] = d[which[q]].depth + 1;
     }
     vg_ctx *c = pc->ctx;
-    const size_t desc_b = d.size() * sizeof(QueryDesc), which_b = nq * sizeof(int), pos_b = nq * sizeof(long);
-    const size_t in_b = ((desc_b + which_b + pos_b + 255) / 256) * 256;
+    // sections of the upload, each starting on a 16-byte boundary:
+    // descriptors (8-byte members), positions (long), codeword-set indices (int)
+    auto up16 = [](size_t x) { return (x + 15) / 16 * 16; };
+    const size_t desc_b = d.size() * sizeof(QueryDesc), pos_b = nq * sizeof(long), which_b = nq * sizeof(int);
+    const size_t off_pos = up16(desc_b), off_which = off_pos + up16(pos_b), in_b = off_which + up16(which_b);
     const size_t vals_b = (size_t)nq * 130 * sizeof(fe), paths_b = (size_t)nq * 32 * 32;
     VG_TRY(ensure(c, pc->qdesc, in_b));
     VG_TRY(ensure(c, pc->qio, vals_b + paths_b));
@@ -529,15 +532,15 @@ extern "C" int vg_pc_query_batch(vg_pc *pc, int nq, const int *which, const long
     VG_TRY(vg_pinned(c, pinned_elems, &host));
     char *hb = (char *)host;
     memcpy(hb, d.data(), desc_b);
-    memcpy(hb + desc_b, which, which_b);
-    memcpy(hb + desc_b + which_b, pos, pos_b);
+    memcpy(hb + off_pos, pos, pos_b);
+    memcpy(hb + off_which, which, which_b);
     char *db = (char *)pc->qdesc.p;
-    VG_CHECK_CUDA(cudaMemcpyAsync(db, hb, desc_b + which_b + pos_b, cudaMemcpyHostToDevice, c->stream));
+    VG_CHECK_CUDA(cudaMemcpyAsync(db, hb, in_b, cudaMemcpyHostToDevice, c->stream));
     VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
     fe *vals_d = (fe *)pc->qio.p;
     uint64_t *paths_d = (uint64_t *)((char *)pc->qio.p + vals_b);
-    k_gather_batch<<<nq, 96, 0, c->stream>>>((const QueryDesc *)db, (const int *)(db + desc_b),
-                                             (const long *)(db + desc_b + which_b), vals_d, paths_d);
+    k_gather_batch<<<nq, 96, 0, c->stream>>>((const QueryDesc *)db, (const int *)(db + off_which),
+                                             (const long *)(db + off_pos), vals_d, paths_d);
     VG_LAUNCHED(c);
     VG_CHECK_CUDA(cudaMemcpyAsync(host, pc->qio.p, vals_b + paths_b, cudaMemcpyDeviceToHost, c->stream));
     VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
