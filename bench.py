@@ -11,8 +11,9 @@ repetitions -- the prover side of the reference's zk_proof run.
 
 ours:       `value` = proofs/s with the circuit resident on the GPU (device
             time between CUDA events on the prover's stream, max over ranks);
-            `e2e` = the same through the C ABI from pinned host buffers, the
-            circuit upload and the proof transcript download inside each step.
+            `e2e` = the same through the C ABI from pinned host buffers, wall
+            clock: every proof loads its circuit (vg_session_load, uint32
+            wires) and downloads its transcript inside the step.
 reference:  the reference prover (compiled from its sources, oracle/_ref) on
             the host cores, one single-threaded proof per core, proofs/s from
             its own timers (Prove Time without the fft_gkr side proof, plus
@@ -24,6 +25,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes
+from concurrent.futures import ThreadPoolExecutor
 import json
 import os
 import re
@@ -190,30 +192,30 @@ def reference_arm(args, layers):
 
 
 # -------------------------------------------------------------------- ours
-def session_arrays(layers):
-    """pinned host copies of the file-level layer arrays"""
+def session_arrays(layers, index_bytes=4):
+    """pinned host copies of the layer arrays in the vg_session_load format:
+    uint8 gate types, wires as uint32 (index_bytes=4) except the input
+    layer's, whose u holds the int64 input values"""
     import torch
     pinned = []
-    for t, u, v in layers:
-        pt = torch.from_numpy(np.ascontiguousarray(t)).pin_memory()
-        pu = torch.from_numpy(np.ascontiguousarray(u)).pin_memory()
-        pv = torch.from_numpy(np.ascontiguousarray(v)).pin_memory()
+    for i, (t, u, v) in enumerate(layers):
+        dt = np.int64 if (i == 0 or index_bytes == 8) else np.uint32
+        pt = torch.from_numpy(np.ascontiguousarray(t, np.uint8)).pin_memory()
+        pu = torch.from_numpy(np.ascontiguousarray(u, dt).view(np.uint8)).pin_memory()
+        pv = torch.from_numpy(np.ascontiguousarray(v, dt).view(np.uint8)).pin_memory()
         pinned.append((pt, pu, pv))
     return pinned
 
 
-def create_session_from_pinned(pinned):
+def load_from_pinned(session, pinned, index_bytes=4):
+    """vg_session_load straight from pinned host buffers"""
     import virgo_b200 as vb
     d = len(pinned)
     ns = np.array([t.numel() for t, _, _ in pinned], np.int64)
     tys, us, vs = (ctypes.c_void_p * d)(), (ctypes.c_void_p * d)(), (ctypes.c_void_p * d)()
     for i, (t, u, v) in enumerate(pinned):
         tys[i], us[i], vs[i] = t.data_ptr(), u.data_ptr(), v.data_ptr()
-    h = ctypes.c_void_p()
-    vb.check(vb.lib().vg_session_create(d, ns.ctypes.data, tys, us, vs, ctypes.byref(h)), "vg_session_create")
-    s = vb.Session.__new__(vb.Session)
-    s.h = h
-    return s
+    vb.check(vb.lib().vg_session_load(session.h, d, ns.ctypes.data, tys, us, vs, index_bytes), "vg_session_load")
 
 
 def ours(args, layers, rank, world):
@@ -283,19 +285,34 @@ def ours(args, layers, rank, world):
     for s in sessions[1:]:
         s.close()
 
-    # ---- e2e: circuit from pinned host buffers through the C ABI each step ----
-    pinned = session_arrays(layers)
-    h2d = int(sum(t.numel() * 1 + u.numel() * 8 + v.numel() * 8 for t, u, v in pinned))
-    d2h = 0
+    # ---- e2e: every step, each of the `batch` sessions loads its circuit from
+    # pinned host buffers (built and validated on the GPU), proves it and
+    # downloads the transcript: host -> device -> host through the C ABI ----
+    pinned = session_arrays(layers, 4)
+    h2d_one = int(sum(t.numel() + u.numel() + v.numel() for t, u, v in pinned))
+    sessions = [base] + [base.fork() for _ in range(args.batch - 1)]
+    pool = ThreadPoolExecutor(len(sessions))
+
+    def one(i, seed):
+        load_from_pinned(sessions[i], pinned, 4)
+        return len(sessions[i].prove(seed, transcript=True)[1])
+
+    def e2e_step(seed):
+        return sum(pool.map(one, range(len(sessions)), [seed + i for i in range(len(sessions))]))
+
+    for w in range(args.warmup):
+        e2e_step(seed0 + 700 + w * args.batch)
     barrier(world)
+    d2h = 0
     t0 = time.perf_counter()
     for k in range(args.steps):
-        s = create_session_from_pinned(pinned)
-        st, blob = s.prove(seed0 + 200 + k, transcript=True)
-        d2h = len(blob)
-        s.close()
+        d2h = e2e_step(seed0 + 200 + k * args.batch)
     t_e2e = max_over_ranks(time.perf_counter() - t0, world)
+    pool.shutdown()
+    for s in sessions[1:]:
+        s.close()
     base.close()
+    h2d = h2d_one * args.batch
     return {"t_plain": t_plain, "t_batch": t_batch, "t_e2e": t_e2e, "clocks": clocks.summary(), "families": fam,
             "launches": n_launch, "stages": {k: v / args.steps for k, v in stages.items()}, "h2d": h2d, "d2h": d2h}
 
@@ -375,9 +392,11 @@ def main():
             "plain": {"value": args.steps * world / r["t_plain"], "unit": "proofs/s",
                       "ms_per_proof": 1000.0 * r["t_plain"] / args.steps,
                       "note": "one proof at a time on one stream, CUDA-event device time"},
-            "e2e": {"value": args.steps * world / r["t_e2e"], "unit": "proofs/s", "h2d_bytes_per_step": r["h2d"],
-                    "d2h_bytes_per_step": r["d2h"],
-                    "note": "one proof per step: circuit upload from pinned host buffers, proof, transcript download"},
+            "e2e": {"value": args.steps * args.batch * world / r["t_e2e"], "unit": "proofs/s",
+                    "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
+                    "note": "%d proofs per step, wall clock: each loads its circuit from pinned host buffers "
+                            "(uint32 wires, built and validated on the GPU), proves, downloads its transcript"
+                            % args.batch},
             "gpu_launches": r["launches"],
             "clocks": r["clocks"],
             "roofline": roofline(r["families"], hbm, kind),

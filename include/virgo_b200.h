@@ -126,6 +126,17 @@ int vg_leaf_chain(vg_ctx *ctx, const vg_fe *codewords, int n_slices, long n, vg_
 int vg_circuit_upload(vg_ctx *ctx, int depth, const int *bit_length,
                       const uint8_t *const *ty, const int64_t *const *u, const int64_t *const *v,
                       vg_circuit **out);
+/* Builds the prover's circuit on the device from file-level layers, as
+ * zk_verifier::read_circuit does on the host (zk_verifier.cpp:24-191): the
+ * input layer (u = values, int64) becomes layer 0 padded to 2^17 gates (2^15
+ * for at most three file layers) plus a relay layer, wires are checked
+ * against the previous layer and narrowed to 32 bits, gates above a layer's
+ * count become dummies.  index_bytes is the width of u and v of the other
+ * layers in host memory: 8 (int64, as in the text format) or 4 (uint32).
+ * *inout is reused (its buffers grown as needed) when non-NULL.
+ * bit_lengths (host, d + 1 entries, may be NULL) receives the layer widths. */
+int vg_circuit_build(vg_ctx *ctx, int d, const long *n, const uint8_t *const *ty, const void *const *u,
+                     const void *const *v, int index_bytes, vg_circuit **inout, int *bit_lengths);
 int vg_circuit_destroy(vg_circuit *c);
 int vg_circuit_depth(const vg_circuit *c, int *depth);
 
@@ -254,6 +265,11 @@ int vg_session_create(int d, const long *n, const uint8_t *const *ty, const int6
  * tables; the device circuit is shared (kept until every session using it is
  * destroyed).  Sessions of one circuit prove concurrently. */
 int vg_session_fork(vg_session *base, vg_session **out);
+/* Replaces a session's circuit, reusing its device buffers when the new
+ * circuit fits them (the file-level layers as for vg_session_create;
+ * index_bytes as for vg_circuit_build).  Forks keep the old circuit. */
+int vg_session_load(vg_session *s, int d, const long *n, const uint8_t *const *ty, const void *const *u,
+                    const void *const *v, int index_bytes);
 /* Reads the circuit text format. */
 int vg_session_from_file(const char *circuit_path, vg_session **out);
 int vg_session_destroy(vg_session *s);

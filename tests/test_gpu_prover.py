@@ -141,3 +141,49 @@ def test_forked_sessions_prove_concurrently_bit_exact():
     for sd, (_, blob) in zip(seeds, res):
         assert blob == alone[sd]
     assert transcript.digest(transcript.parse(res[0][1])) == c["digest"]
+
+
+def test_session_load_reuses_buffers_and_matches():
+    """vg_session_load: the 32-bit wire format, the 64-bit one and a fresh
+    session give the same proof; a different circuit loads into the same
+    session; a circuit of the same shape reuses the device buffers."""
+    a = circuits.random_layered([10, 12, 11, 12, 9], seed=4)
+    b = circuits.matmul_addtree(8, 20, seed=3)
+    c = next(x for x in _golden() if x["name"] == "random_5layer")
+    s = vb.Session(b)
+    try:
+        s.load(a, index_bytes=4)
+        t32 = s.prove(c["seed"])[1]
+        s.load(a, index_bytes=8)
+        t64 = s.prove(c["seed"])[1]
+        s.load(b)
+        tb = s.prove(5)[1]
+        a2 = [(t, u, v) for t, u, v in a]
+        t, u, v = a2[2]
+        a2[2] = (t, u.copy(), v)
+        s.load(a2, index_bytes=4)   # same shape
+        t_again = s.prove(c["seed"])[1]
+    finally:
+        s.close()
+    assert t32 == t64 == t_again
+    assert transcript.digest(transcript.parse(t32)) == c["digest"]
+    fresh = vb.Session(b)
+    try:
+        assert fresh.prove(5)[1] == tb
+    finally:
+        fresh.close()
+    bad = [(t, u, v) for t, u, v in a]
+    t, u, v = bad[3]
+    u = u.copy()
+    u[5] = 1 << 20
+    bad[3] = (t, u, v)
+    s = vb.Session(a)
+    try:
+        with pytest.raises(vb.VirgoError):
+            s.load(bad, index_bytes=4)
+        with pytest.raises(vb.VirgoError):   # no circuit after a failed load
+            s.prove(c["seed"])
+        s.load(a, index_bytes=4)
+        assert s.prove(c["seed"])[1] == t32
+    finally:
+        s.close()

@@ -106,6 +106,8 @@ def lib():
             "vg_ctx_device": (c_i, [c_p, ctypes.POINTER(c_i)]),
             "vg_circuit_write_text": (c_i, [c_i, c_p, c_p, c_p, c_p, ctypes.c_char_p, ctypes.c_char_p]),
             "vg_mle_eval_noalloc": (c_i, [c_p, c_l, c_p, c_i, c_p]),
+            "vg_session_load": (c_i, [c_p, c_i, c_p, c_p, c_p, c_p, c_i]),
+            "vg_circuit_build": (c_i, [c_p, c_i, c_p, c_p, c_p, c_p, c_i, ctypes.POINTER(c_p), c_p]),
             "vg_free": (None, [c_p]),
         }
         for name, (res, args) in sig.items():
@@ -233,6 +235,23 @@ class Session:
         data = ctypes.string_at(buf, n.value) if (transcript and n.value) else b""
         lib().vg_free(buf)
         return st, data
+
+    def load(self, layers, index_bytes: int = 8):
+        """Replaces the circuit (device buffers reused when it fits).  layers
+        are (ty, u, v) arrays; with index_bytes=4 the wires of layers >= 1 are
+        passed as uint32 (the input layer's u, its values, stay int64)."""
+        d = len(layers)
+        ns = np.array([len(t) for t, _, _ in layers], dtype=np.int64)
+        keep = [ns]
+        tys, us, vs = (ctypes.c_void_p * d)(), (ctypes.c_void_p * d)(), (ctypes.c_void_p * d)()
+        for i, (t, u, v) in enumerate(layers):
+            dt = np.int64 if (i == 0 or index_bytes == 8) else np.uint32
+            t = t if isinstance(t, np.ndarray) and t.dtype == np.uint8 and t.flags.c_contiguous else np.ascontiguousarray(t, np.uint8)
+            u = u if getattr(u, "dtype", None) == dt and u.flags.c_contiguous else np.ascontiguousarray(u, dt)
+            v = v if getattr(v, "dtype", None) == dt and v.flags.c_contiguous else np.ascontiguousarray(v, dt)
+            keep += [t, u, v]
+            tys[i], us[i], vs[i] = t.ctypes.data, u.ctypes.data, v.ctypes.data
+        check(lib().vg_session_load(self.h, d, ptr(ns), tys, us, vs, index_bytes), "vg_session_load")
 
     def fork(self) -> "Session":
         """A session on the same (shared) device circuit with its own stream."""

@@ -361,6 +361,67 @@ __global__ void __launch_bounds__(GKR_THREADS) k_round(const fe *__restrict__ xV
 vg::fe tofe(vg_fe x) { return vg::fe_make(x.real, x.img); }
 vg_fe tovg(vg::fe x) { vg_fe r; r.real = x.real; r.img = x.img; return r; }
 
+// ---------------------------------------------------- device circuit build
+// Input layer: values from the file's u (read through int, zk_prover.cpp:60-65)
+// and the padding gates (3, 0, 0), i.e. value 0, up to 2^bl; types must be 2 or 3.
+__global__ void k_build_input(const uint8_t *__restrict__ ty, const int64_t *__restrict__ u, long n, long width,
+                              fe *__restrict__ vals, unsigned long long *__restrict__ err)
+{
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < width; g += (long)gridDim.x * blockDim.x) {
+        if (g < n) {
+            const int t = ty[g];
+            if (t != 2 && t != 3) atomicMin(err, (0ull << 40) | (unsigned long long)g);
+            vals[g] = from_int32((int32_t)u[g]);
+        } else {
+            vals[g] = vg::fe_zero();
+        }
+    }
+}
+
+// the relay layer the reader inserts above the input (zk_verifier.cpp:114, 123):
+// relay gates (4, g, 0) over the padded input, dummies (2, 0, 0) above it
+__global__ void k_build_relay(long padded, long width, uint8_t *__restrict__ ty, uint32_t *__restrict__ u,
+                              uint32_t *__restrict__ v)
+{
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < width; g += (long)gridDim.x * blockDim.x) {
+        ty[g] = g < padded ? 4 : 2;
+        u[g] = g < padded ? (uint32_t)g : 0u;
+        v[g] = 0;
+    }
+}
+
+// One file layer into prover layer `li`: wires narrowed to uint32, checked
+// against the previous layer's width (the reader's asserts,
+// zk_verifier.cpp:70-102), v cleared for NOT and relay gates, dummy (2, 0, 0)
+// gates above n.  The first bad gate is reported as (li << 40) | g.
+template <typename IDX>
+__global__ void k_build_layer(const uint8_t *__restrict__ ty_in, const IDX *__restrict__ u_in, const IDX *__restrict__ v_in,
+                              long n, long width, long prev_width, int li, uint8_t *__restrict__ ty, uint32_t *__restrict__ u,
+                              uint32_t *__restrict__ v, unsigned long long *__restrict__ err)
+{
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < width; g += (long)gridDim.x * blockDim.x) {
+        if (g >= n) {
+            ty[g] = 2;
+            u[g] = 0;
+            v[g] = 0;
+            continue;
+        }
+        const int t = ty_in[g];
+        const long long a = (long long)u_in[g], b = (long long)v_in[g];
+        bool ok;
+        if (t == 2 || t == 3) ok = true;
+        else if (t == 5) ok = a >= 0 && a < prev_width && b > a && b <= prev_width;
+        else if (t == 12) ok = a >= 0 && a <= b && b < prev_width && b - a + 1 <= 60;
+        else if (t == 6 || t == 10) ok = a >= 0 && a < prev_width;
+        else if (t > 13 || t == 11) ok = false;
+        else ok = a >= 0 && a < prev_width && b >= 0 && b < prev_width && (t != 13 || a == b) && (t != 4 || a < width);
+        if (!ok) atomicMin(err, ((unsigned long long)li << 40) | (unsigned long long)g);
+        ty[g] = ok ? (uint8_t)t : (uint8_t)2;
+        u[g] = ok ? (uint32_t)a : 0u;
+        v[g] = ok && t != 6 && t != 10 ? (uint32_t)b : 0u;
+    }
+}
+
 }  // namespace
 
 struct vg_circuit {
@@ -369,6 +430,12 @@ struct vg_circuit {
     int max_bl = 0;
     std::vector<DevLayer> L;
     fe *input = nullptr;   // layer 0 values
+    // capacities (entries) of the arrays above, for reuse by vg_circuit_build
+    std::vector<long> cap;
+    long input_cap = 0;
+    void *staging = nullptr;   // upload staging for one layer
+    size_t staging_cap = 0;
+    unsigned long long *err = nullptr;
 };
 
 struct vg_gkr {
@@ -471,7 +538,143 @@ extern "C" int vg_circuit_destroy(vg_circuit *c)
         cudaFree(D.v);
     }
     cudaFree(c->input);
+    cudaFree(c->staging);
+    cudaFree(c->err);
     delete c;
+    return VG_OK;
+}
+
+static int grow_dev(void **p, size_t *cap, size_t bytes)
+{
+    if (bytes <= *cap) return VG_OK;
+    cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    if (cudaMalloc(p, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return vg_fail(VG_ERR_OOM, "cudaMalloc(%zu) failed", bytes);
+    }
+    *cap = bytes;
+    return VG_OK;
+}
+
+// log2 of the layer width the reader gives n gates (zk_verifier.cpp:129-169)
+static int width_log(long n)
+{
+    int bl = 0;
+    while ((1L << bl) < n) ++bl;
+    return n == 1 ? 1 : bl;
+}
+
+extern "C" int vg_circuit_build(vg_ctx *ctx, int d, const long *n, const uint8_t *const *ty, const void *const *u,
+                                const void *const *v, int index_bytes, vg_circuit **inout, int *bit_lengths)
+{
+    if (!ctx || d < 1 || !n || !ty || !u || !v || !inout || (index_bytes != 4 && index_bytes != 8))
+        return vg_fail(VG_ERR_ARG, "vg_circuit_build: bad argument");
+    for (int i = 0; i < d; ++i)
+        if (n[i] < 1 || n[i] > (1L << 30)) return vg_fail(VG_ERR_ARG, "layer %d: %ld gates", i, n[i]);
+    // prover layers: 0 input values, 1 relay, 1 + i for file layer i >= 1
+    const int depth = d + 1;
+    std::vector<int> bl(depth);
+    const long pad = 1L << (d > 3 ? 17 : 15);   // zk_verifier.cpp:32-41
+    bl[0] = bl[1] = width_log(std::max(n[0], pad));
+    for (int i = 1; i < d; ++i) bl[i + 1] = width_log(n[i]);
+    vg_circuit *c = *inout;
+    if (!c) {
+        c = new vg_circuit();
+        c->ctx = ctx;
+    }
+    c->ctx = ctx;
+    c->depth = depth;
+    c->max_bl = 0;
+    c->L.resize(depth);
+    c->cap.resize(depth, 0);
+    auto fail = [&](int rc) {
+        if (!*inout) vg_circuit_destroy(c);
+        return rc;
+    };
+    if (!c->err && cudaMalloc(&c->err, sizeof(unsigned long long)) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(vg_fail(VG_ERR_OOM, "circuit error flag"));
+    }
+    VG_CHECK_CUDA(cudaMemsetAsync(c->err, 0xff, sizeof(unsigned long long), ctx->stream));
+    for (int i = 0; i < depth; ++i) {
+        DevLayer &D = c->L[i];
+        D.bl = bl[i];
+        D.n = 1L << bl[i];
+        c->max_bl = std::max(c->max_bl, D.bl);
+        if (i == 0) {
+            size_t capb = c->input_cap * sizeof(fe);
+            int rc = grow_dev((void **)&c->input, &capb, D.n * sizeof(fe));
+            if (rc != VG_OK) return fail(rc);
+            c->input_cap = (long)(capb / sizeof(fe));
+            continue;
+        }
+        if (c->cap[i] < D.n) {
+            cudaFree(D.ty);
+            cudaFree(D.u);
+            cudaFree(D.v);
+            D.ty = nullptr;
+            D.u = D.v = nullptr;
+            if (cudaMalloc(&D.ty, D.n) != cudaSuccess || cudaMalloc(&D.u, D.n * 4) != cudaSuccess ||
+                cudaMalloc(&D.v, D.n * 4) != cudaSuccess) {
+                cudaGetLastError();
+                return fail(vg_fail(VG_ERR_OOM, "circuit layer %d allocation", i));
+            }
+            c->cap[i] = D.n;
+        }
+    }
+    // staging for the largest file layer: types, then u and v
+    long nmax = 0;
+    for (int i = 0; i < d; ++i) nmax = std::max(nmax, n[i]);
+    const size_t stage_b = ((size_t)nmax + 255) / 256 * 256 + 2 * (size_t)nmax * 8;
+    int rc = grow_dev(&c->staging, &c->staging_cap, stage_b);
+    if (rc != VG_OK) return fail(rc);
+    const unsigned grid_cap = 148u * 32u;
+    for (int fi = 0; fi < d; ++fi) {
+        const long cnt = n[fi];
+        const size_t wb = fi == 0 ? 8 : (size_t)index_bytes;   // the input layer's u are values (int64)
+        uint8_t *sty = (uint8_t *)c->staging;
+        char *su = (char *)c->staging + ((size_t)nmax + 255) / 256 * 256;
+        char *sv = su + (size_t)nmax * 8;
+        VG_CHECK_CUDA(cudaMemcpyAsync(sty, ty[fi], cnt, cudaMemcpyHostToDevice, ctx->stream));
+        VG_CHECK_CUDA(cudaMemcpyAsync(su, u[fi], cnt * wb, cudaMemcpyHostToDevice, ctx->stream));
+        if (fi > 0) VG_CHECK_CUDA(cudaMemcpyAsync(sv, v[fi], cnt * wb, cudaMemcpyHostToDevice, ctx->stream));
+        if (fi == 0) {
+            const long width = c->L[0].n;
+            k_build_input<<<std::min<unsigned>(grid_for(width, 256), grid_cap), 256, 0, ctx->stream>>>(
+                sty, (const int64_t *)su, cnt, width, c->input, c->err);
+            VG_LAUNCHED(ctx);
+            DevLayer &R = c->L[1];
+            k_build_relay<<<std::min<unsigned>(grid_for(R.n, 256), grid_cap), 256, 0, ctx->stream>>>(
+                std::max(cnt, pad), R.n, R.ty, R.u, R.v);
+            VG_LAUNCHED(ctx);
+        } else {
+            const int li = fi + 1;
+            DevLayer &D = c->L[li];
+            const long prev = c->L[li - 1].n;
+            const unsigned grid = std::min<unsigned>(grid_for(D.n, 256), grid_cap);
+            if (index_bytes == 8)
+                k_build_layer<int64_t><<<grid, 256, 0, ctx->stream>>>(sty, (const int64_t *)su, (const int64_t *)sv, cnt, D.n,
+                                                                      prev, li, D.ty, D.u, D.v, c->err);
+            else
+                k_build_layer<uint32_t><<<grid, 256, 0, ctx->stream>>>(sty, (const uint32_t *)su, (const uint32_t *)sv, cnt,
+                                                                       D.n, prev, li, D.ty, D.u, D.v, c->err);
+            VG_LAUNCHED(ctx);
+        }
+    }
+    unsigned long long e = 0;
+    VG_CHECK_CUDA(cudaMemcpyAsync(&e, c->err, sizeof e, cudaMemcpyDeviceToHost, ctx->stream));
+    VG_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (e != ~0ull) {
+        const int li = (int)(e >> 40);
+        const long gi = (long)(e & ((1ull << 40) - 1));
+        return fail(vg_fail(VG_ERR_ARG, "file layer %d gate %ld: invalid type or wire", li == 0 ? 0 : li - 1, gi));
+    }
+    if (bit_lengths)
+        for (int i = 0; i < depth; ++i) bit_lengths[i] = bl[i];
+    *inout = c;
     return VG_OK;
 }
 

@@ -16,6 +16,8 @@
 // hi[e >> 12], built once per root and cached in the context.
 #include "common.cuh"
 #include <algorithm>
+#include <mutex>
+#include <vector>
 
 namespace {
 
@@ -223,11 +225,31 @@ int vg_twiddles(vg_ctx *c, fe root, int logn, const fe **lo, const fe **hi)
     return VG_OK;
 }
 
+// Largest dynamic shared memory of a pass: m * G <= 4096 items (pick_logG)
+// plus m / 2 <= 512 twiddles.  The kernel attribute is process-wide per
+// device, so it is raised once to this bound: setting it per launch to the
+// launch's own size races with other threads' launches of other sizes.
+constexpr size_t NTT_MAX_SMEM = (4096 + 512) * sizeof(fe);
+
+static int ntt_smem_attribute(int dev)
+{
+    static std::mutex mu;
+    static std::vector<bool> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= (int)done.size()) done.resize(dev + 1, false);
+    if (!done[dev]) {
+        VG_CHECK_CUDA(cudaFuncSetAttribute(k_ntt_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)NTT_MAX_SMEM));
+        done[dev] = true;
+    }
+    return VG_OK;
+}
+
 static int launch_pass(vg_ctx *c, PassArgs &a, long nblocks, int batch)
 {
     const int m = 1 << a.lm, G = 1 << a.logG;
     size_t sm = ((size_t)m * G + (m >> 1)) * sizeof(fe);
-    if (sm > 48 * 1024) VG_CHECK_CUDA(cudaFuncSetAttribute(k_ntt_pass, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    if (sm > NTT_MAX_SMEM) return vg_fail(VG_ERR_ARG, "ntt pass: %zu bytes of shared memory", sm);
+    if (sm > 48 * 1024) VG_TRY(ntt_smem_attribute(c->device));
     dim3 grid((unsigned)nblocks, (unsigned)batch);
     {
         ProfScope ps(c, KF_NTT, 2.0 * 16.0 * (double)batch * (double)(1L << a.logn));

@@ -33,6 +33,8 @@
 typedef prime_field::field_element F;
 using clk = std::chrono::high_resolution_clock;
 
+int vg_fail(int code, const char *fmt, ...);   // sets vg_last_error()
+
 static double since(clk::time_point t0)
 {
     return std::chrono::duration_cast<std::chrono::duration<double>>(clk::now() - t0).count();
@@ -90,10 +92,9 @@ F direct_relay(const layered_circuit &C, int depth, const F *r_g, const F *r_u)
 }
 }  // namespace
 
-// Gate storage of a circuit shared by forked sessions.
+// A device circuit and its layer widths, shared by forked sessions.
 struct CircuitData {
-    layered_circuit C;
-    std::vector<std::vector<gate> > storage;
+    layered_circuit C;   // widths only (gates stay on the device)
     vg_circuit *dev = nullptr;
     ~CircuitData()
     {
@@ -111,93 +112,8 @@ struct vg_session {
     zk_prover *p = nullptr;
     void *pub = nullptr;   // device buffer for the public eq table
     size_t pub_bytes = 0;
+    bool loaded = false;   // false after a failed load: no valid circuit
 };
-
-// ----------------------------------------------------------- circuit build
-// The file-level layers (input layer first) turned into the prover's circuit
-// the way zk_verifier::read_circuit does (zk_verifier.cpp:24-191): the input
-// layer becomes layer 0 (values) plus a relay layer 1, padded to 2^17 gates
-// when there are more than three file layers and to 2^15 otherwise.
-static int build_circuit(CircuitData *s, int d, const long *n, const uint8_t *const *ty, const int64_t *const *u,
-                         const int64_t *const *v, std::string &err)
-{
-    if (d < 1) {
-        err = "circuit needs at least one layer";
-        return VG_ERR_ARG;
-    }
-    layered_circuit &C = s->C;
-    C.total_depth = d + 1;
-    C.circuit = new layer[d + 1];
-    s->storage.assign(d + 1, std::vector<gate>());
-    const int pad_log = d > 3 ? 17 : 15;
-    for (int i = 1; i <= d; ++i) {
-        long cnt = n[i - 1];
-        if (cnt < 1) {
-            err = "empty layer";
-            return VG_ERR_ARG;
-        }
-        long padded = cnt;
-        if (i == 1 && cnt < (1L << pad_log)) padded = 1L << pad_log;
-        int bl = 0;
-        while ((1L << bl) < padded) ++bl;
-        if (padded == 1) bl = 1;   // a single gate gets a dummy partner
-        const long full = 1L << bl;
-        const int prev_bl = i == 1 ? 0 : C.circuit[i - 1].bit_length;
-        for (long g = 0; g < cnt; ++g) {
-            const int t = ty[i - 1][g];
-            const long long a = u[i - 1][g], b = v[i - 1][g];
-            if (i == 1) {
-                if (t != 2 && t != 3) {
-                    err = "input layer gates must have type 2 or 3";
-                    return VG_ERR_ARG;
-                }
-                continue;
-            }
-            const long long np = 1LL << prev_bl;
-            bool ok;
-            if (t == 3 || t == 2) ok = true;
-            else if (t == 5) ok = a >= 0 && a < np && b > a && b <= np;
-            else if (t == 12) ok = a >= 0 && a <= b && b < np && b - a + 1 <= 60;
-            else if (t == 6 || t == 10) ok = a >= 0 && a < np;
-            else if (t > 13 || t == 11) ok = false;
-            else ok = a >= 0 && a < np && b >= 0 && b < np && (t != 13 || a == b) && (t != 4 || a < (1LL << bl));
-            if (!ok) {
-                char buf[200];
-                snprintf(buf, sizeof buf, "layer %d gate %ld: type %d u %lld v %lld invalid", i, g, t, a, b);
-                err = buf;
-                return VG_ERR_ARG;
-            }
-        }
-        if (i == 1) {
-            auto &in = s->storage[0];
-            auto &relay = s->storage[1];
-            in.assign(full, gate(2, 0, 0));
-            relay.assign(full, gate(2, 0, 0));
-            for (long g = 0; g < cnt; ++g) {
-                in[g] = gate(ty[0][g], u[0][g], v[0][g]);
-                relay[g] = gate(4, g, 0);
-            }
-            for (long g = cnt; g < padded; ++g) {
-                in[g] = gate(3, 0, 0);
-                relay[g] = gate(4, g, 0);
-            }
-            if (padded == 1) relay[1] = gate(4, 1, 0);
-            C.circuit[0].gates = in.data();
-            C.circuit[1].gates = relay.data();
-            C.circuit[0].bit_length = C.circuit[1].bit_length = bl;
-        } else {
-            auto &L = s->storage[i];
-            L.assign(full, gate(2, 0, 0));
-            for (long g = 0; g < cnt; ++g) {
-                const int t = ty[i - 1][g];
-                L[g] = gate(t, u[i - 1][g], (t == 6 || t == 10) ? 0 : v[i - 1][g]);
-            }
-            C.circuit[i].gates = L.data();
-            C.circuit[i].bit_length = bl;
-        }
-    }
-    return VG_OK;
-}
 
 static int session_device(vg_ctx **ctx)
 {
@@ -212,53 +128,64 @@ static int session_attach(vg_session *s)
     int rc = s->ctx ? VG_OK : session_device(&s->ctx);
     if (rc != VG_OK) return rc;
     rc = vg_ctx_set_hash(s->ctx, virgo_hash_kind());
-    if (rc == VG_OK) rc = vg_pc_create(s->ctx, &s->pc);
+    if (rc == VG_OK && !s->pc) rc = vg_pc_create(s->ctx, &s->pc);
     if (rc != VG_OK) return rc;
-    s->p = new zk_prover();
-    s->p->quiet = true;
+    if (!s->p) {
+        s->p = new zk_prover();
+        s->p->quiet = true;
+    }
     s->p->attach_circuit(s->circuit->C, s->circuit->dev, s->ctx);
     return VG_OK;
 }
 
-static int circuit_upload(CircuitData *cd, vg_ctx *ctx)
+static bool same_shape(const layered_circuit &a, const int *bl, int depth)
 {
-    const int depth = cd->C.total_depth;
-    std::vector<int> bl(depth);
-    std::vector<std::vector<uint8_t> > ty(depth);
-    std::vector<std::vector<int64_t> > u(depth), v(depth);
-    std::vector<const uint8_t *> pty(depth);
-    std::vector<const int64_t *> pu(depth), pv(depth);
-    for (int i = 0; i < depth; ++i) {
-        bl[i] = cd->C.circuit[i].bit_length;
-        const long nn = 1L << bl[i];
-        ty[i].resize(nn);
-        u[i].resize(nn);
-        v[i].resize(nn);
-        for (long k = 0; k < nn; ++k) {
-            ty[i][k] = (uint8_t)cd->C.circuit[i].gates[k].ty;
-            u[i][k] = cd->C.circuit[i].gates[k].u;
-            v[i][k] = cd->C.circuit[i].gates[k].v;
-        }
-        pty[i] = ty[i].data();
-        pu[i] = u[i].data();
-        pv[i] = v[i].data();
+    if (!a.circuit || a.total_depth != depth) return false;
+    for (int i = 0; i < depth; ++i)
+        if (a.circuit[i].bit_length != bl[i]) return false;
+    return true;
+}
+
+// Builds (or rebuilds in place) the session's device circuit from file-level
+// layers; the reader's padding and relay layer are applied on the device.
+extern "C" int vg_session_load(vg_session *s, int d, const long *n, const uint8_t *const *ty, const void *const *u,
+                               const void *const *v, int index_bytes)
+{
+    if (!s || !s->ctx || d < 1 || !n || !ty || !u || !v) return vg_fail(VG_ERR_ARG, "vg_session_load: bad argument");
+    int dev = 0;
+    vg_ctx_device(s->ctx, &dev);
+    cudaSetDevice(dev);
+    if (!s->circuit || s->circuit.use_count() > 1) s->circuit = std::make_shared<CircuitData>();
+    CircuitData *cd = s->circuit.get();
+    std::vector<int> bl(d + 1);
+    s->loaded = false;
+    int rc = vg_circuit_build(s->ctx, d, n, ty, u, v, index_bytes, &cd->dev, bl.data());
+    if (rc != VG_OK) return rc;
+    const bool keep = s->p && s->p->dev_circuit == cd->dev && same_shape(cd->C, bl.data(), d + 1);
+    if (!same_shape(cd->C, bl.data(), d + 1)) {
+        delete[] cd->C.circuit;
+        cd->C.circuit = new layer[d + 1];
+        cd->C.total_depth = d + 1;
+        for (int i = 0; i <= d; ++i) cd->C.circuit[i].bit_length = bl[i];
     }
-    return vg_circuit_upload(ctx, depth, bl.data(), pty.data(), pu.data(), pv.data(), &cd->dev);
+    if (keep) {
+        s->p->C = cd->C;   // same widths: the prover's device tables still fit
+        s->loaded = true;
+        return VG_OK;
+    }
+    rc = session_attach(s);
+    s->loaded = rc == VG_OK;
+    return rc;
 }
 
 extern "C" int vg_session_create(int d, const long *n, const uint8_t *const *ty, const int64_t *const *u,
                                  const int64_t *const *v, vg_session **out)
 {
-    if (!n || !ty || !u || !v || !out) return VG_ERR_ARG;
+    if (!n || !ty || !u || !v || !out) return vg_fail(VG_ERR_ARG, "vg_session_create: bad argument");
     vg_session *s = new vg_session();
-    s->circuit = std::make_shared<CircuitData>();
-    std::string err;
-    int rc = build_circuit(s->circuit.get(), d, n, ty, u, v, err);
-    if (rc == VG_OK) rc = session_device(&s->ctx);
-    if (rc == VG_OK) rc = circuit_upload(s->circuit.get(), s->ctx);
-    if (rc == VG_OK) rc = session_attach(s);
+    int rc = session_device(&s->ctx);
+    if (rc == VG_OK) rc = vg_session_load(s, d, n, ty, (const void *const *)u, (const void *const *)v, 8);
     if (rc != VG_OK) {
-        if (!err.empty()) fprintf(stderr, "vg_session_create: %s\n", err.c_str());
         vg_session_destroy(s);
         return rc;
     }
@@ -268,10 +195,12 @@ extern "C" int vg_session_create(int d, const long *n, const uint8_t *const *ty,
 
 extern "C" int vg_session_fork(vg_session *base, vg_session **out)
 {
-    if (!base || !out) return VG_ERR_ARG;
+    if (!base || !out) return vg_fail(VG_ERR_ARG, "vg_session_fork: null argument");
+    if (!base->loaded) return vg_fail(VG_ERR_STATE, "vg_session_fork: the base session holds no circuit");
     vg_session *s = new vg_session();
     s->circuit = base->circuit;
     int rc = session_attach(s);
+    s->loaded = rc == VG_OK;
     if (rc != VG_OK) {
         vg_session_destroy(s);
         return rc;
@@ -285,7 +214,7 @@ extern "C" int vg_session_fork(vg_session *base, vg_session **out)
 extern "C" int vg_session_from_file(const char *circuit_path, vg_session **out)
 {
     FILE *f = fopen(circuit_path, "rb");
-    if (!f) return VG_ERR_ARG;
+    if (!f) return vg_fail(VG_ERR_ARG, "cannot open circuit file");
     fseek(f, 0, SEEK_END);
     long sz = ftell(f);
     fseek(f, 0, SEEK_SET);
@@ -308,23 +237,23 @@ extern "C" int vg_session_from_file(const char *circuit_path, vg_session **out)
         return true;
     };
     long long d;
-    if (!next(d) || d < 1 || d > 100000) return VG_ERR_ARG;
+    if (!next(d) || d < 1 || d > 100000) return vg_fail(VG_ERR_ARG, "circuit file: bad depth");
     std::vector<long> n(d);
     std::vector<std::vector<uint8_t> > ty(d);
     std::vector<std::vector<int64_t> > u(d), v(d);
     for (long long i = 0; i < d; ++i) {
         long long cnt;
-        if (!next(cnt) || cnt < 1) return VG_ERR_ARG;
+        if (!next(cnt) || cnt < 1) return vg_fail(VG_ERR_ARG, "circuit file: bad gate count");
         n[i] = (long)cnt;
         ty[i].resize(cnt);
         u[i].resize(cnt);
         v[i].resize(cnt);
         for (long long j = 0; j < cnt; ++j) {
             long long t, g, a, b;
-            if (!next(t) || !next(g) || !next(a) || !next(b)) return VG_ERR_ARG;
+            if (!next(t) || !next(g) || !next(a) || !next(b)) return vg_fail(VG_ERR_ARG, "circuit file: truncated gate");
             if (g != j) {
                 fprintf(stderr, "Error, gates must be in sorted order, and full [0, 2^n - 1]. %lld %lld %lld\n", i + 1, j, g);
-                return VG_ERR_ARG;
+                return vg_fail(VG_ERR_ARG, "circuit file: bad gate");
             }
             ty[i][j] = (uint8_t)t;
             u[i][j] = a;
@@ -358,7 +287,7 @@ extern "C" int vg_session_destroy(vg_session *s)
 
 extern "C" int vg_session_depth(vg_session *s, int *depth, int *input_log)
 {
-    if (!s) return VG_ERR_ARG;
+    if (!s) return vg_fail(VG_ERR_ARG, "vg_session_depth: null session");
     if (depth) *depth = s->circuit->C.total_depth;
     if (input_log) *input_log = s->circuit->C.circuit[0].bit_length;
     return VG_OK;
@@ -368,14 +297,14 @@ extern "C" void vg_free(void *p) { free(p); }
 
 extern "C" int vg_session_ctx(vg_session *s, vg_ctx **out)
 {
-    if (!s || !out) return VG_ERR_ARG;
+    if (!s || !out) return vg_fail(VG_ERR_ARG, "null argument");
     *out = s->ctx;
     return VG_OK;
 }
 
 extern "C" int vg_default_ctx(vg_ctx **out)
 {
-    if (!out) return VG_ERR_ARG;
+    if (!out) return vg_fail(VG_ERR_ARG, "null argument");
     *out = virgo::ctx();
     return VG_OK;
 }
@@ -398,9 +327,9 @@ static char *put_int(char *p, long long x)
 extern "C" int vg_circuit_write_text(int d, const long *n, const uint8_t *const *ty, const int64_t *const *u,
                                      const int64_t *const *v, const char *circuit_path, const char *meta_path)
 {
-    if (d < 1 || !n || !ty || !u || !v || !circuit_path) return VG_ERR_ARG;
+    if (d < 1 || !n || !ty || !u || !v || !circuit_path) return vg_fail(VG_ERR_ARG, "vg_circuit_write_text: bad argument");
     FILE *f = fopen(circuit_path, "wb");
-    if (!f) return VG_ERR_ARG;
+    if (!f) return vg_fail(VG_ERR_ARG, "vg_circuit_write_text: cannot open output");
     std::vector<char> buf(1 << 22);
     char *p = buf.data();
     char *end = buf.data() + buf.size() - 128;
@@ -430,7 +359,7 @@ extern "C" int vg_circuit_write_text(int d, const long *n, const uint8_t *const 
     fclose(f);
     if (meta_path) {
         FILE *m = fopen(meta_path, "wb");
-        if (!m) return VG_ERR_ARG;
+        if (!m) return vg_fail(VG_ERR_ARG, "out of host memory");
         for (int i = 0; i < d; ++i) fputs("0 0 1 0 0\n", m);
         fclose(m);
     }
@@ -440,7 +369,8 @@ extern "C" int vg_circuit_write_text(int d, const long *n, const uint8_t *const 
 extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcript, vg_proof_stats *stats,
                                 uint8_t **transcript, size_t *transcript_len)
 {
-    if (!s || !s->p) return VG_ERR_ARG;
+    if (!s || !s->p) return vg_fail(VG_ERR_ARG, "vg_session_prove: null session");
+    if (!s->loaded) return vg_fail(VG_ERR_STATE, "vg_session_prove: no circuit loaded (the last load failed)");
     {
         int dev = 0;
         vg_ctx_device(s->ctx, &dev);
@@ -643,7 +573,7 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
     SESSION_TRY(vg_eq_table(s->ctx, (const vg_fe *)r_0.data(), L, (vg_fe *)s->pub));
     if ((long)all_pub_mask.size() > M) {
         prime_field::set_thread_random_state(nullptr);
-        return VG_ERR_STATE;
+        return vg_fail(VG_ERR_STATE, "vg_session_prove: public mask longer than the slice");
     }
     while ((long)all_pub_mask.size() < M) all_pub_mask.push_back(F(0));   // poly_commit.h:138-139
     F all_sum[slice_number + 1], inner;
@@ -652,9 +582,8 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
     // the claimed inner product the reference asserts (poly_commit.h:193)
     const F target = alpha_beta_sum - p.Zu * p.sumRc.eval(p.preu1) + all_mask_sum;
     if (inner != target) {
-        fprintf(stderr, "vg_session_prove: committed inner product differs from the sumcheck claim\n");
         prime_field::set_thread_random_state(nullptr);
-        return VG_ERR_STATE;
+        return vg_fail(VG_ERR_STATE, "vg_session_prove: committed inner product differs from the sumcheck claim");
     }
     SESSION_TRY(vg_pc_init_commit(s->pc, 1, (vg_digest *)&root_h));
     tr.put('C', &root_h, 2);
@@ -797,16 +726,18 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
 extern "C" int vg_session_prove_batch(vg_session *const *ss, int n, const unsigned *seeds, int want_transcript,
                                       vg_proof_stats *stats, uint8_t **transcripts, size_t *transcript_lens)
 {
-    if (!ss || !seeds || n < 0) return VG_ERR_ARG;
+    if (!ss || !seeds || n < 0) return vg_fail(VG_ERR_ARG, "vg_session_prove_batch: bad argument");
     std::vector<int> rcs(n, VG_OK);
+    std::vector<std::string> msgs(n);   // the error text is per thread: carry it back
     std::vector<std::thread> th;
     for (int i = 0; i < n; ++i)
         th.emplace_back([&, i]() {
             rcs[i] = vg_session_prove(ss[i], seeds[i], want_transcript, stats ? &stats[i] : nullptr,
                                       transcripts ? &transcripts[i] : nullptr, transcript_lens ? &transcript_lens[i] : nullptr);
+            if (rcs[i] != VG_OK) msgs[i] = vg_last_error();
         });
     for (auto &t : th) t.join();
     for (int i = 0; i < n; ++i)
-        if (rcs[i] != VG_OK) return rcs[i];
+        if (rcs[i] != VG_OK) return vg_fail(rcs[i], "session %d: %s", i, msgs[i].c_str());
     return VG_OK;
 }
