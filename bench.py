@@ -244,7 +244,7 @@ def ours(args, layers, rank, world):
     barrier(world)
     timer = ctypes.c_void_p()
     ctx0 = ctx_of(base)
-    stages = {"evaluate_s": 0.0, "gkr_s": 0.0, "commit_s": 0.0, "fri_s": 0.0, "query_s": 0.0}
+    stages = {"launch_s": 0.0, "wait_s": 0.0, "replay_s": 0.0}
     vb.check(L.vg_timer_start(ctx0, ctypes.byref(timer)))
     for k in range(args.steps):
         st, _ = base.prove(seed0 + 100 + k, transcript=True)

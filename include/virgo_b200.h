@@ -248,9 +248,16 @@ int vg_pc_info(vg_pc *pc, int *log_len, long *slice_size, int *levels);
  * answers equal those of the reference prover run by the reference verifier
  * with that seed (the fft_gkr side proof is not part of it). */
 typedef struct vg_session vg_session;
+/* A proof runs the protocol twice from the same rand() state: the launch pass
+ * enqueues every device step of the proof on the session's stream without
+ * reading anything back, one synchronisation follows, and the replay pass
+ * forms the messages, checks and transcript from the device results. */
 typedef struct {
-    double evaluate_s, gkr_s, commit_s, fri_s, query_s, total_s;   /* wall time per stage */
-    double prove_time;      /* zk_prover::total_time + poly_commit_prover::total_time */
+    double launch_s;        /* host time of the launch pass */
+    double wait_s;          /* then the wait for the device */
+    double replay_s;        /* host time of the replay pass */
+    double total_s;         /* wall time of the call */
+    double prove_time;      /* launch_s + wait_s: every prover message is on the host */
     long long proof_size;   /* bytes by the reference's accounting, without fft_gkr */
     long long launches;     /* kernels launched for this proof */
 } vg_proof_stats;

@@ -34,9 +34,8 @@ class vg_fe(ctypes.Structure):
 
 class vg_proof_stats(ctypes.Structure):
     _fields_ = [
-        ("evaluate_s", ctypes.c_double), ("gkr_s", ctypes.c_double), ("commit_s", ctypes.c_double),
-        ("fri_s", ctypes.c_double), ("query_s", ctypes.c_double), ("total_s", ctypes.c_double),
-        ("prove_time", ctypes.c_double), ("proof_size", ctypes.c_longlong), ("launches", ctypes.c_longlong),
+        ("launch_s", ctypes.c_double), ("wait_s", ctypes.c_double), ("replay_s", ctypes.c_double),
+        ("total_s", ctypes.c_double), ("prove_time", ctypes.c_double), ("proof_size", ctypes.c_longlong), ("launches", ctypes.c_longlong),
     ]
 
 

@@ -14,6 +14,7 @@
 #include "common.cuh"
 #include "merkle.cuh"
 #include "hash.cuh"
+#include "internal.h"
 #include <algorithm>
 #include <cstring>
 
@@ -123,6 +124,20 @@ __global__ void __launch_bounds__(128) k_fri_fold_leaf(const fe *__restrict__ c,
     o[1] = make_ulonglong2(h[2], h[3]);
 }
 
+// One FRI fold without hashing (the leaf chains of all levels are batched):
+// out[s][i] = ((a + b) + r w^-(i 2^t) (a - b)) / 2, a = c[s][i], b = c[s][i + n/2].
+__global__ void k_fri_fold(const fe *__restrict__ c, long n, int t, fe r, const fe *__restrict__ twi_lo,
+                           const fe *__restrict__ twi_hi, fe *__restrict__ out)
+{
+    const long h = n >> 1, total = 65 * h;
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < total; i += (long)gridDim.x * blockDim.x) {
+        const long s = i / h, k = i - s * h;
+        const fe a = c[s * n + k], b = c[s * n + k + h];
+        const fe w = r * tw_pow(twi_lo, twi_hi, (uint64_t)k << t);
+        out[i] = half_fe((a + b) + w * (a - b));
+    }
+}
+
 // Query answers for a batch: block q answers query q from codeword set
 // desc[which[q]] at position pos[q] (taken modulo n/2): 65 value pairs and the
 // authentication path (siblings bottom-up, then the leaf).
@@ -201,6 +216,9 @@ struct vg_pc {
     int log_len = 0;
     long S = 0, R = 0, gap = 0, M = 0;
     DevBuf l_eval, h_eval, q_eval, vo, lq, lqc, mask, staging, tree_l, tree_h, qdesc, qio;
+    DevBuf mask2, res, roots;   // deferred proof: public mask, <l,q> + all_sum, roots
+    fe *hpin = nullptr;         // deferred proof: pinned staging and results
+    size_t hpin_cap = 0;        // in elements
     std::vector<PcLevel> levels;
     int nlevels = 0;
     bool have_private = false, have_public = false;
@@ -211,7 +229,7 @@ struct vg_pc {
 static void pc_free(vg_pc *pc)
 {
     DevBuf *all[] = {&pc->l_eval, &pc->h_eval, &pc->q_eval, &pc->vo, &pc->lq, &pc->lqc, &pc->mask, &pc->staging,
-                     &pc->tree_l, &pc->tree_h, &pc->qdesc, &pc->qio};
+                     &pc->tree_l, &pc->tree_h, &pc->qdesc, &pc->qio, &pc->mask2, &pc->res, &pc->roots};
     for (DevBuf *b : all) {
         cudaFree(b->p);
         b->p = nullptr;
@@ -224,6 +242,9 @@ static void pc_free(vg_pc *pc)
     pc->levels.clear();
     pc->nlevels = 0;
     pc->have_private = pc->have_public = false;
+    if (pc->hpin) cudaFreeHost(pc->hpin);
+    pc->hpin = nullptr;
+    pc->hpin_cap = 0;
 }
 
 static fe root_of(int log_order) { return vg::fe_root_of_unity(log_order); }
@@ -294,21 +315,23 @@ static int device_input(vg_pc *pc, const vg_fe *x, long N, const fe **out)
     return VG_OK;
 }
 
-// zero-padded mask of M entries on the device (poly_commit.h:66-70, 138-139)
-static int device_mask(vg_pc *pc, const vg_fe *mask, long n_mask, long M)
+// zero-padded mask of M entries on the device (poly_commit.h:66-70, 138-139);
+// with staging == nullptr through the context's pinned buffer (synchronised,
+// it is reused), else through the caller's pinned staging (not synchronised)
+static int device_mask(vg_pc *pc, DevBuf &dst, const vg_fe *mask, long n_mask, long M, fe *staging = nullptr)
 {
     vg_ctx *c = pc->ctx;
-    VG_TRY(ensure(c, pc->mask, M * sizeof(fe)));
-    fe *host;
-    VG_TRY(vg_pinned(c, M, &host));
+    VG_TRY(ensure(c, dst, M * sizeof(fe)));
+    fe *host = staging;
+    if (!host) VG_TRY(vg_pinned(c, M, &host));
     for (long i = 0; i < M; ++i) host[i] = i < n_mask ? vg::fe_make(mask[i].real, mask[i].img) : vg::fe_zero();
-    VG_CHECK_CUDA(cudaMemcpyAsync(pc->mask.p, host, M * sizeof(fe), cudaMemcpyHostToDevice, c->stream));
-    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));   // the pinned staging is reused
+    VG_CHECK_CUDA(cudaMemcpyAsync(dst.p, host, M * sizeof(fe), cudaMemcpyHostToDevice, c->stream));
+    if (!staging) VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
     return VG_OK;
 }
 
-extern "C" int vg_pc_encode_private(vg_pc *pc, const vg_fe *priv, int log_len, const vg_fe *mask, long n_mask,
-                                    long *mask_len)
+static int encode_private(vg_pc *pc, const vg_fe *priv, int log_len, const vg_fe *mask, long n_mask, long *mask_len,
+                          fe *staging)
 {
     if (!pc || !priv || !mask || n_mask < 1 || log_len < 7 || log_len > 28)
         return vg_fail(VG_ERR_ARG, "vg_pc_encode_private: bad argument (log_len=%d n_mask=%ld)", log_len, n_mask);
@@ -328,17 +351,29 @@ extern "C" int vg_pc_encode_private(vg_pc *pc, const vg_fe *priv, int log_len, c
     fe *coef;
     VG_TRY(vg_scratch2(c, 64 * R * sizeof(fe), (void **)&coef));
     VG_TRY(rs_encode(c, priv_d, R, 64, pc->F(pc->l_eval), S, coef));
-    VG_TRY(device_mask(pc, mask, n_mask, M));
+    VG_TRY(device_mask(pc, pc->mask, mask, n_mask, M, staging));
     VG_TRY(rs_encode(c, pc->F(pc->mask), M, 1, pc->F(pc->l_eval) + 64 * S, S, coef));
     if (mask_len) *mask_len = M;
     pc->have_private = true;
     return VG_OK;
 }
 
-extern "C" int vg_pc_encode_public(vg_pc *pc, const vg_fe *pub, const vg_fe *pub_mask, long n_mask, vg_fe *all_sum,
-                                   vg_fe *inner_product)
+extern "C" int vg_pc_encode_private(vg_pc *pc, const vg_fe *priv, int log_len, const vg_fe *mask, long n_mask,
+                                    long *mask_len)
 {
-    if (!pc || !pub || !pub_mask || !all_sum) return vg_fail(VG_ERR_ARG, "vg_pc_encode_public: null argument");
+    return encode_private(pc, priv, log_len, mask, n_mask, mask_len, nullptr);
+}
+
+long vg_pc_mask_len(int log_len, long n_pri_mask)
+{
+    const long S = 1L << (log_len - 1);
+    return S / mask_gap(S, n_pri_mask);
+}
+
+// <l, q> to res_dev[0] and all_sum to res_dev[1 .. 65]
+static int encode_public(vg_pc *pc, const vg_fe *pub, const vg_fe *pub_mask, long n_mask, fe *res_dev, fe *staging)
+{
+    if (!pc || !pub || !pub_mask) return vg_fail(VG_ERR_ARG, "vg_pc_encode_public: null argument");
     if (!pc->have_private) return vg_fail(VG_ERR_STATE, "commit_public before commit_private");
     if (n_mask > pc->M) return vg_fail(VG_ERR_ARG, "public mask longer than the padded private mask (%ld > %ld)", n_mask, pc->M);
     if (pc->gap == 1) return vg_fail(VG_ERR_ARG, "mask fills the whole slice (mask_position_gap == 1)");
@@ -359,16 +394,17 @@ extern "C" int vg_pc_encode_public(vg_pc *pc, const vg_fe *pub, const vg_fe *pub
     fe *coef;
     VG_TRY(vg_scratch2(c, 64 * R * sizeof(fe), (void **)&coef));
     VG_TRY(rs_encode(c, pub_d, R, 64, q_eval, S, coef));
-    VG_TRY(device_mask(pc, pub_mask, n_mask, M));
-    VG_TRY(rs_encode(c, pc->F(pc->mask), M, 1, q_eval + 64 * S, S, coef));
+    DevBuf &mbuf = staging ? pc->mask2 : pc->mask;   // the deferred proof keeps the private mask
+    VG_TRY(device_mask(pc, mbuf, pub_mask, n_mask, M, staging));
+    VG_TRY(rs_encode(c, pc->F(mbuf), M, 1, q_eval + 64 * S, S, coef));
 
     // inner product check value
     fe *parts;
     const int nb = 148 * 4;
-    VG_TRY(vg_partials(c, nb + 1 + 65, &parts));   // block partials, <l,q>, all_sum[65]
+    VG_TRY(vg_partials(c, nb, &parts));
     k_inner_product<<<nb, 256, 0, c->stream>>>(l_eval, q_eval, S, pc->gap, parts);
     VG_LAUNCHED(c);
-    VG_TRY(vg_reduce_partials(c, parts, nb, 1, parts + nb));
+    VG_TRY(vg_reduce_partials(c, parts, nb, 1, res_dev));
 
     // lq samples, their interpolation and the quotient h
     fe *lq_m = lq + 64 * 2 * R, *lqc_m = lqc + 64 * 2 * R;
@@ -395,19 +431,28 @@ extern "C" int vg_pc_encode_public(vg_pc *pc, const vg_fe *pub, const vg_fe *pub
     k_virtual_oracle<<<grid_for(S, 256), 256, 0, c->stream>>>(l_eval, q_eval, h_eval, lqc_m, S, M, logS, 64, 1,
                                                              tf_lo, tf_hi, ti_lo, ti_hi, pc->F(pc->vo));
     VG_LAUNCHED(c);
-    fe *sums_d = parts + nb + 1;
+    fe *sums_d = res_dev + 1;
     k_all_sum<<<1, 64, 0, c->stream>>>(lqc, R, 0, 64, sums_d);
     VG_LAUNCHED(c);
     k_all_sum<<<1, 1, 0, c->stream>>>(lqc_m, M, 64, 1, sums_d);
     VG_LAUNCHED(c);
+    pc->have_public = true;
+    return VG_OK;
+}
 
+extern "C" int vg_pc_encode_public(vg_pc *pc, const vg_fe *pub, const vg_fe *pub_mask, long n_mask, vg_fe *all_sum,
+                                   vg_fe *inner_product)
+{
+    if (!pc || !all_sum) return vg_fail(VG_ERR_ARG, "vg_pc_encode_public: null argument");
+    vg_ctx *c = pc->ctx;
+    VG_TRY(ensure(c, pc->res, 66 * sizeof(fe)));
+    VG_TRY(encode_public(pc, pub, pub_mask, n_mask, pc->F(pc->res), nullptr));
     fe *host;
     VG_TRY(vg_pinned(c, 66, &host));
-    VG_CHECK_CUDA(cudaMemcpyAsync(host, parts + nb, 66 * sizeof(fe), cudaMemcpyDeviceToHost, c->stream));
+    VG_CHECK_CUDA(cudaMemcpyAsync(host, pc->res.p, 66 * sizeof(fe), cudaMemcpyDeviceToHost, c->stream));
     VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
     for (int i = 0; i < 65; ++i) all_sum[i] = to_vg(host[1 + i]);
     if (inner_product) *inner_product = to_vg(host[0]);
-    pc->have_public = true;
     return VG_OK;
 }
 
@@ -569,5 +614,139 @@ extern "C" int vg_pc_query_step(vg_pc *pc, int lvl, long pow, vg_fe *values, vg_
     VG_TRY(vg_pc_query_batch(pc, 1, &which, &pow, values, p.data(), &plen));
     memcpy(path, p.data(), plen * sizeof(vg_digest));
     if (path_len) *path_len = plen;
+    return VG_OK;
+}
+
+// ------------------------------------------------ one-sync proof commitment
+static int ensure_pinned(vg_pc *pc, size_t elems)
+{
+    if (elems <= pc->hpin_cap) return VG_OK;
+    VG_CHECK_CUDA(cudaStreamSynchronize(pc->ctx->stream));
+    if (pc->hpin) cudaFreeHost(pc->hpin);
+    pc->hpin = nullptr;
+    pc->hpin_cap = 0;
+    VG_CHECK_CUDA(cudaMallocHost((void **)&pc->hpin, elems * sizeof(fe)));
+    pc->hpin_cap = elems;
+    return VG_OK;
+}
+
+int vg_pc_prove_deferred(vg_pc *pc, const vg_fe *priv, int log_len, const vg_fe *pri_mask, long n_pri_mask,
+                         const vg_fe *pub, const vg_fe *pub_mask, long n_pub_mask, const vg_fe *fri_r, int nlevels,
+                         int nq, const int *which, const long *pos, vg_pc_results *out)
+{
+    if (!pc || !priv || !pri_mask || !pub || !pub_mask || (nlevels && !fri_r) || nq < 0 || (nq && (!which || !pos)) || !out)
+        return vg_fail(VG_ERR_ARG, "vg_pc_prove_deferred: bad argument");
+    if (log_len < 7 || log_len > 28 || n_pri_mask < 1) return vg_fail(VG_ERR_ARG, "vg_pc_prove_deferred: log_len %d", log_len);
+    vg_ctx *c = pc->ctx;
+    const long S = 1L << (log_len - 1);
+    if (nlevels < 0 || (S >> nlevels) < 8) return vg_fail(VG_ERR_ARG, "%d FRI levels fold below 8 elements", nlevels);
+    const long M = vg_pc_mask_len(log_len, n_pri_mask);
+    const long n_final = nlevels ? (S >> nlevels) : S;
+
+    // pinned layout (16-byte elements): masks | query upload | results
+    const size_t ndesc = 2 + nlevels;
+    auto up16 = [](size_t x) { return (x + 15) / 16 * 16; };
+    const size_t desc_b = ndesc * sizeof(QueryDesc), pos_b = (size_t)nq * sizeof(long), which_b = (size_t)nq * sizeof(int);
+    const size_t off_pos = up16(desc_b), off_which = off_pos + up16(pos_b), in_b = off_which + up16(which_b);
+    const size_t e_masks = 2 * (size_t)M, e_in = in_b / 16;
+    const size_t e_res = 66, e_roots = 2 * ndesc, e_final = 65 * (size_t)n_final, e_qv = (size_t)nq * 130,
+                 e_qp = (size_t)nq * 32 * 2;
+    VG_TRY(ensure_pinned(pc, e_masks + e_in + e_res + e_roots + e_final + e_qv + e_qp));
+    fe *h_mask = pc->hpin, *h_in = h_mask + e_masks, *h_res = h_in + e_in, *h_roots = h_res + e_res,
+       *h_final = h_roots + e_roots, *h_qv = h_final + e_final, *h_qp = h_qv + e_qv;
+
+    // commitment of the private and public inputs, virtual oracle
+    long Mp = 0;
+    VG_TRY(encode_private(pc, priv, log_len, pri_mask, n_pri_mask, &Mp, h_mask));
+    if (Mp != M) return vg_fail(VG_ERR_STATE, "mask length %ld != %ld", Mp, M);
+    if (n_pub_mask > M) return vg_fail(VG_ERR_ARG, "public mask longer than the padded private mask (%ld > %ld)", n_pub_mask, M);
+    VG_TRY(ensure(c, pc->res, 66 * sizeof(fe)));
+    VG_TRY(encode_public(pc, pub, pub_mask, n_pub_mask, pc->F(pc->res), h_mask + M));
+
+    // FRI folds, level by level (fri.cpp:321-340, 367-379)
+    const int logS = ilog2l(S);
+    const fe *ti_lo, *ti_hi;
+    VG_TRY(vg_twiddles(c, vg::fe_inv(root_of(logS)), logS, &ti_lo, &ti_hi));
+    if ((int)pc->levels.size() < nlevels) pc->levels.resize(nlevels);
+    for (int t = 0; t < nlevels; ++t) {
+        const long n = S >> t;
+        PcLevel &L = pc->levels[t];
+        L.n = n >> 1;
+        VG_TRY(ensure(c, L.cw, 65 * L.n * sizeof(fe)));
+        VG_TRY(ensure(c, L.tree, L.n * 32));
+        const fe *in = t == 0 ? pc->F(pc->vo) : pc->F(pc->levels[t - 1].cw);
+        const long total = 65 * L.n;
+        {
+            ProfScope ps(c, KF_FRI_FOLD, 16.0 * 65.0 * (double)n * 1.5);
+            k_fri_fold<<<std::min<unsigned>(grid_for(total, 256), 148u * 16u), 256, 0, c->stream>>>(
+                in, n, t, vg::fe_make(fri_r[t].real, fri_r[t].img), ti_lo, ti_hi, pc->F(L.cw));
+        }
+        VG_LAUNCHED(c);
+    }
+    pc->nlevels = nlevels;
+
+    // every leaf chain, then every Merkle tree, batched (fri.cpp:394-420, merkle_tree.cpp)
+    VG_TRY(ensure(c, pc->tree_l, (size_t)S * 32));
+    VG_TRY(ensure(c, pc->tree_h, (size_t)S * 32));
+    VG_TRY(ensure(c, pc->roots, ndesc * 32));
+    struct Set { const fe *cw; long n; uint64_t *tree; };
+    std::vector<Set> sets;
+    sets.push_back({pc->F(pc->l_eval), S, pc->U(pc->tree_l)});
+    sets.push_back({pc->F(pc->h_eval), S, pc->U(pc->tree_h)});
+    for (int t = 0; t < nlevels; ++t) sets.push_back({pc->F(pc->levels[t].cw), pc->levels[t].n, pc->U(pc->levels[t].tree)});
+    for (size_t b = 0; b < sets.size(); b += MAX_HASH_JOBS) {
+        ChainJobs cj{};
+        long total = 0;
+        for (size_t k = b; k < sets.size() && k < b + MAX_HASH_JOBS; ++k) {
+            const long nleaves = sets[k].n >> 1;
+            cj.j[cj.count++] = {sets[k].cw, sets[k].n, sets[k].tree + 4 * nleaves, total};
+            total += nleaves;
+        }
+        cj.total = total;
+        VG_TRY(vg_leaf_chains(c, cj));
+    }
+    for (size_t b = 0; b < sets.size(); b += MAX_HASH_JOBS) {
+        TreeJobs tj{};
+        for (size_t k = b; k < sets.size() && k < b + MAX_HASH_JOBS; ++k) tj.t[tj.count++] = {sets[k].tree, sets[k].n >> 1};
+        VG_TRY(vg_merkle_trees(c, tj, pc->U(pc->roots) + 4 * b));
+    }
+
+    // query answers (fri.cpp:148-289), positions checked as in vg_pc_query_batch
+    std::vector<QueryDesc> dsc;
+    query_descs(pc, dsc);
+    for (int q = 0; q < nq; ++q) {
+        if (which[q] < 0 || which[q] >= (int)dsc.size()) return vg_fail(VG_ERR_ARG, "query %d: no codeword set %d", q, which[q]);
+        if (pos[q] < 0) return vg_fail(VG_ERR_ARG, "query %d: negative position", q);
+        if (which[q] < 2 && pos[q] >= S / 2) return vg_fail(VG_ERR_ARG, "query %d: position out of range", q);
+    }
+    const size_t vals_b = (size_t)nq * 130 * sizeof(fe), paths_b = (size_t)nq * 32 * 32;
+    if (nq) {
+        VG_TRY(ensure(c, pc->qdesc, in_b));
+        VG_TRY(ensure(c, pc->qio, vals_b + paths_b));
+        char *hb = (char *)h_in;
+        memcpy(hb, dsc.data(), desc_b);
+        memcpy(hb + off_pos, pos, pos_b);
+        memcpy(hb + off_which, which, which_b);
+        char *db = (char *)pc->qdesc.p;
+        VG_CHECK_CUDA(cudaMemcpyAsync(db, hb, in_b, cudaMemcpyHostToDevice, c->stream));
+        k_gather_batch<<<nq, 96, 0, c->stream>>>((const QueryDesc *)db, (const int *)(db + off_which),
+                                                 (const long *)(db + off_pos), (fe *)pc->qio.p,
+                                                 (uint64_t *)((char *)pc->qio.p + vals_b));
+        VG_LAUNCHED(c);
+    }
+
+    // results to pinned memory
+    VG_CHECK_CUDA(cudaMemcpyAsync(h_res, pc->res.p, 66 * sizeof(fe), cudaMemcpyDeviceToHost, c->stream));
+    VG_CHECK_CUDA(cudaMemcpyAsync(h_roots, pc->roots.p, ndesc * 32, cudaMemcpyDeviceToHost, c->stream));
+    const fe *fin = nlevels ? pc->F(pc->levels[nlevels - 1].cw) : pc->F(pc->vo);
+    VG_CHECK_CUDA(cudaMemcpyAsync(h_final, fin, e_final * sizeof(fe), cudaMemcpyDeviceToHost, c->stream));
+    if (nq) VG_CHECK_CUDA(cudaMemcpyAsync(h_qv, pc->qio.p, vals_b + paths_b, cudaMemcpyDeviceToHost, c->stream));
+    out->inner = (const vg_fe *)h_res;
+    out->all_sum = (const vg_fe *)(h_res + 1);
+    out->roots = (const vg_digest *)h_roots;
+    out->final_cw = (const vg_fe *)h_final;
+    out->n_final = n_final;
+    out->qvals = (const vg_fe *)h_qv;
+    out->qpaths = (const vg_digest *)h_qp;
     return VG_OK;
 }

@@ -23,6 +23,7 @@
 // contributions per entry keeps both below 2^64), and a finalise pass folds
 // lo + hi * 2^32 back into a canonical element.
 #include "common.cuh"
+#include "internal.h"
 #include <algorithm>
 #include <cstring>
 
@@ -227,9 +228,11 @@ __global__ void __launch_bounds__(GKR_THREADS) k_phase1_scatter(const uint8_t *_
 // first and added with one set of atomics per block.
 __global__ void __launch_bounds__(GKR_THREADS) k_phase2_scatter(const uint8_t *__restrict__ ty, const uint32_t *__restrict__ uu,
                                                                 const uint32_t *__restrict__ vv, long ng, BetaG bg, BetaU bu,
-                                                                fe vu, unsigned long long *am, unsigned long long *av)
+                                                                const fe *__restrict__ vu_ptr, unsigned long long *am,
+                                                                unsigned long long *av)
 {
     __shared__ fe sm[32];
+    const fe vu = *vu_ptr;
     fe zero_acc = vg::fe_zero();
     const long stride = (long)gridDim.x * blockDim.x;
     const long start = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -289,6 +292,14 @@ __global__ void __launch_bounds__(GKR_THREADS) k_phase2_scatter(const uint8_t *_
     block_acc_add(av, 0, zero_acc, sm);
 }
 
+// v_u = V(r_u) + mask term: the folded V pair of the last phase-1 round at r
+// (zk_prover.cpp:796-797), computed where the pair is, so phase 2 can start
+// without the host reading it first
+__global__ void k_vu(const fe *__restrict__ last6, fe r, fe addend, fe *__restrict__ vu)
+{
+    *vu = (last6[0] + r * (last6[1] - last6[0])) + addend;
+}
+
 // ------------------------------------------------------------ round kernel
 __device__ __forceinline__ fe fold(fe x0, fe x1, fe r) { return x0 + r * (x1 - x0); }
 
@@ -299,7 +310,7 @@ __global__ void __launch_bounds__(GKR_THREADS) k_round(const fe *__restrict__ xV
                                                        const fe *__restrict__ xAM, long npairs, fe r,
                                                        fe *__restrict__ yV, fe *__restrict__ yAV, fe *__restrict__ yAM,
                                                        fe *__restrict__ parts, unsigned *__restrict__ counter,
-                                                       fe *__restrict__ out3)
+                                                       fe *__restrict__ out3, fe *__restrict__ last6)
 {
     __shared__ fe sm[3 * 32];
     __shared__ bool last;
@@ -321,6 +332,9 @@ __global__ void __launch_bounds__(GKR_THREADS) k_round(const fe *__restrict__ xV
             v0 = xV[2 * i]; v1 = xV[2 * i + 1];
             a0 = xAV[2 * i]; a1 = xAV[2 * i + 1];
             m0 = xAM[2 * i]; m1 = xAM[2 * i + 1];
+        }
+        if (last6 && npairs == 1) {   // the folded pairs the last round of a phase needs
+            last6[0] = v0; last6[1] = v1; last6[2] = a0; last6[3] = a1; last6[4] = m0; last6[5] = m1;
         }
         const fe va = v1 - v0, aa = a1 - a0, ma = m1 - m0;
         acc[0] = acc[0] + ma * va;
@@ -456,6 +470,15 @@ struct vg_gkr {
     int next_buf = 1;
     bool round0_pending = false;
     BetaG bg{};
+    fe *vu = nullptr;                    // v_u of phase 2 (device scalar)
+    // deferred mode: results stay on the device as records of 9 values
+    // (round: 3 sums + the 6 folded values when one pair remained;
+    // v_res: the value), read back once with vg_gkr_records
+    bool deferred = false;
+    fe *rec = nullptr;
+    int rec_cap = 0, rec_n = 0;
+    fe *rec_host = nullptr;              // pinned
+    int rec_host_cap = 0;
 };
 
 // ------------------------------------------------------------------ circuit
@@ -712,6 +735,7 @@ extern "C" int vg_gkr_create(vg_ctx *ctx, const vg_circuit *c, vg_gkr **out)
     if (cudaMalloc(&g->round_parts, 3 * 148 * 8 * sizeof(fe)) != cudaSuccess) return fail("round partials");
     if (cudaMalloc(&g->round_out, 16 * sizeof(fe)) != cudaSuccess) return fail("round sums");
     if (cudaMalloc(&g->round_counter, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
+    if (cudaMalloc(&g->vu, sizeof(fe)) != cudaSuccess) return fail("v_u");
     if (cudaMemset(g->round_counter, 0, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
     *out = g;
     return VG_OK;
@@ -730,6 +754,9 @@ extern "C" int vg_gkr_destroy(vg_gkr *g)
     cudaFree(g->round_parts);
     cudaFree(g->round_out);
     cudaFree(g->round_counter);
+    cudaFree(g->vu);
+    cudaFree(g->rec);
+    if (g->rec_host) cudaFreeHost(g->rec_host);
     delete g;
     return VG_OK;
 }
@@ -747,7 +774,7 @@ extern "C" int vg_gkr_evaluate(vg_gkr *g)
         }
         VG_LAUNCHED(c);
     }
-    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    if (!g->deferred) VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
     return VG_OK;
 }
 
@@ -795,6 +822,11 @@ extern "C" int vg_gkr_v_res(vg_gkr *g, const vg_fe *r, int r_len, vg_fe *out)
     const long n = 1L << r_len;
     k_eq_dot<<<nb, 256, 0, c->stream>>>(g->vals[last], lo, hi, fh, n, parts);
     VG_LAUNCHED(c);
+    if (g->deferred) {
+        if (g->rec_n >= g->rec_cap) return vg_fail(VG_ERR_STATE, "deferred record buffer full");
+        VG_TRY(vg_reduce_partials(c, parts, nb, 1, g->rec + 9 * g->rec_n++));
+        return VG_OK;
+    }
     VG_TRY(vg_reduce_partials(c, parts, nb, 1, parts + nb));
     VG_CHECK_CUDA(cudaMemcpyAsync(out, parts + nb, sizeof(fe), cudaMemcpyDeviceToHost, c->stream));
     VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
@@ -840,14 +872,14 @@ extern "C" int vg_mle_eval(vg_ctx *c, const vg_fe *vals, long n, const vg_fe *r,
     return rc;
 }
 
-extern "C" int vg_eq_table(vg_ctx *c, const vg_fe *r, int log_len, vg_fe *pub)
+static int eq_table(vg_ctx *c, const vg_fe *r, int log_len, vg_fe *pub)
 {
     if (!c || !r || !pub || log_len < 1 || log_len > 30) return vg_fail(VG_ERR_ARG, "vg_eq_table: bad argument");
     fe *tmp;
     int f = log_len >> 1, s = log_len - f;
     VG_TRY(vg_scratch2(c, ((1L << f) + (1L << s) + 64) * sizeof(fe), (void **)&tmp));
     fe *lo = tmp, *hi = tmp + (1L << f), *rd = hi + (1L << s);
-    cudaMemcpyAsync(rd, r, log_len * sizeof(fe), cudaMemcpyHostToDevice, c->stream);
+    VG_CHECK_CUDA(cudaMemcpyAsync(rd, r, log_len * sizeof(fe), cudaMemcpyHostToDevice, c->stream));   // staged copy
     k_eq_half<<<grid_for(1L << f, 256), 256, 0, c->stream>>>(rd, f, vg::fe_one(), lo);
     c->launches++;
     k_eq_half<<<grid_for(1L << s, 256), 256, 0, c->stream>>>(rd + f, s, vg::fe_one(), hi);
@@ -855,9 +887,17 @@ extern "C" int vg_eq_table(vg_ctx *c, const vg_fe *r, int log_len, vg_fe *pub)
     long n = 1L << log_len;
     k_eq_combine<<<std::min<unsigned>(grid_for(n, 256), 148u * 32u), 256, 0, c->stream>>>(lo, hi, f, n, (fe *)pub);
     VG_LAUNCHED(c);
+    return VG_OK;
+}
+
+extern "C" int vg_eq_table(vg_ctx *c, const vg_fe *r, int log_len, vg_fe *pub)
+{
+    VG_TRY(eq_table(c, r, log_len, pub));
     VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
     return VG_OK;
 }
+
+int vg_eq_table_async(vg_ctx *c, const vg_fe *r, int log_len, vg_fe *pub) { return eq_table(c, r, log_len, pub); }
 
 static int finalize_tables(vg_gkr *g, long N)
 {
@@ -920,12 +960,10 @@ extern "C" int vg_gkr_phase1_init(vg_gkr *g, int layer, const vg_fe *r0, const v
     return finalize_tables(g, N);
 }
 
-extern "C" int vg_gkr_phase2_init(vg_gkr *g, const vg_fe *r_u, int length_u, vg_fe v_u)
+// phase-2 tables for the current layer once g->vu holds v_u
+static int phase2_tables(vg_gkr *g, const vg_fe *r_u, int length_u)
 {
-    if (!g || !r_u) return vg_fail(VG_ERR_ARG, "vg_gkr_phase2_init: null argument");
-    if (g->layer < 1) return vg_fail(VG_ERR_STATE, "phase2_init before phase1_init");
     const int layer = g->layer;
-    if (length_u != g->C->L[layer - 1].bl) return vg_fail(VG_ERR_ARG, "length_u %d != previous layer bit length %d", length_u, g->C->L[layer - 1].bl);
     vg_ctx *c = g->ctx;
     const DevLayer &D = g->C->L[layer];
     const long N = g->C->L[layer - 1].n, maxN = 1L << g->C->max_bl;
@@ -943,7 +981,7 @@ extern "C" int vg_gkr_phase2_init(vg_gkr *g, const vg_fe *r_u, int length_u, vg_
     unsigned grid = std::min<unsigned>(grid_for(D.n, GKR_THREADS), 148u * 32u);
     {
         ProfScope ps(c, KF_SCATTER2, 73.0 * (double)D.n);   // gate record, two accumulator updates
-        k_phase2_scatter<<<grid, GKR_THREADS, 0, c->stream>>>(D.ty, D.u, D.v, D.n, g->bg, bu, tofe(v_u), g->acc,
+        k_phase2_scatter<<<grid, GKR_THREADS, 0, c->stream>>>(D.ty, D.u, D.v, D.n, g->bg, bu, g->vu, g->acc,
                                                              g->acc + 4 * maxN);
     }
     VG_LAUNCHED(c);
@@ -951,9 +989,78 @@ extern "C" int vg_gkr_phase2_init(vg_gkr *g, const vg_fe *r_u, int length_u, vg_
     return finalize_tables(g, N);
 }
 
+static int phase2_check(vg_gkr *g, const vg_fe *r_u, int length_u)
+{
+    if (!g || !r_u) return vg_fail(VG_ERR_ARG, "vg_gkr_phase2_init: null argument");
+    if (g->layer < 1) return vg_fail(VG_ERR_STATE, "phase2_init before phase1_init");
+    if (length_u != g->C->L[g->layer - 1].bl)
+        return vg_fail(VG_ERR_ARG, "length_u %d != previous layer bit length %d", length_u, g->C->L[g->layer - 1].bl);
+    return VG_OK;
+}
+
+extern "C" int vg_gkr_phase2_init(vg_gkr *g, const vg_fe *r_u, int length_u, vg_fe v_u)
+{
+    VG_TRY(phase2_check(g, r_u, length_u));
+    fe vu = tofe(v_u);
+    VG_CHECK_CUDA(cudaMemcpyAsync(g->vu, &vu, sizeof(fe), cudaMemcpyHostToDevice, g->ctx->stream));   // staged copy
+    return phase2_tables(g, r_u, length_u);
+}
+
+int vg_gkr_phase2_init_deferred(vg_gkr *g, const vg_fe *r_u, int length_u, vg_fe r_last, vg_fe addend)
+{
+    VG_TRY(phase2_check(g, r_u, length_u));
+    if (!g->deferred || g->rec_n < 1 || g->n != 2)
+        return vg_fail(VG_ERR_STATE, "deferred phase2_init must follow the last deferred phase-1 round");
+    k_vu<<<1, 1, 0, g->ctx->stream>>>(g->rec + 9 * (g->rec_n - 1) + 3, tofe(r_last), tofe(addend), g->vu);
+    VG_LAUNCHED(g->ctx);
+    return phase2_tables(g, r_u, length_u);
+}
+
+int vg_gkr_defer(vg_gkr *g, int on)
+{
+    if (!g) return vg_fail(VG_ERR_ARG, "null gkr");
+    g->deferred = on != 0;
+    g->rec_n = 0;
+    if (!on) return VG_OK;
+    // one record per round (at most 2 x 32 per layer) plus v_res
+    const int need = 64 * g->C->depth + 16;
+    if (need > g->rec_cap) {
+        VG_CHECK_CUDA(cudaStreamSynchronize(g->ctx->stream));
+        cudaFree(g->rec);
+        g->rec = nullptr;
+        g->rec_cap = 0;
+        if (cudaMalloc(&g->rec, (size_t)need * 9 * sizeof(fe)) != cudaSuccess) {
+            cudaGetLastError();
+            return vg_fail(VG_ERR_OOM, "deferred records");
+        }
+        g->rec_cap = need;
+    }
+    return VG_OK;
+}
+
+int vg_gkr_records(vg_gkr *g, const vg_fe **host, int *n)
+{
+    if (!g || !host || !n) return vg_fail(VG_ERR_ARG, "vg_gkr_records: null argument");
+    if (g->rec_n > g->rec_host_cap) {
+        VG_CHECK_CUDA(cudaStreamSynchronize(g->ctx->stream));
+        if (g->rec_host) cudaFreeHost(g->rec_host);
+        g->rec_host = nullptr;
+        g->rec_host_cap = 0;
+        VG_CHECK_CUDA(cudaMallocHost((void **)&g->rec_host, (size_t)g->rec_cap * 9 * sizeof(fe)));
+        g->rec_host_cap = g->rec_cap;
+    }
+    if (g->rec_n)
+        VG_CHECK_CUDA(cudaMemcpyAsync(g->rec_host, g->rec, (size_t)g->rec_n * 9 * sizeof(fe), cudaMemcpyDeviceToHost,
+                                      g->ctx->stream));
+    *host = (const vg_fe *)g->rec_host;
+    *n = g->rec_n;
+    return VG_OK;
+}
+
 extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, vg_fe *out3, vg_fe *last6)
 {
-    if (!g || !out3) return vg_fail(VG_ERR_ARG, "vg_gkr_round: null argument");
+    if (!g || (!out3 && !(g && g->deferred))) return vg_fail(VG_ERR_ARG, "vg_gkr_round: null argument");
+    if (g->deferred && g->rec_n >= g->rec_cap) return vg_fail(VG_ERR_STATE, "deferred record buffer full");
     if (g->layer < 1 || g->n < 2) return vg_fail(VG_ERR_STATE, "sumcheck round without tables (n=%ld)", g->n);
     const bool fold = current_bit != 0;
     if (!fold && !g->round0_pending) return vg_fail(VG_ERR_STATE, "current_bit 0 only directly after an init");
@@ -965,15 +1072,17 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
     unsigned grid = std::min<unsigned>(grid_for(npairs, GKR_THREADS), 148u * 8u);
     fe *y[3] = {g->buf[g->next_buf][0], g->buf[g->next_buf][1], g->buf[g->next_buf][2]};
     fe r = tofe(previous_random);
+    fe *o3 = g->deferred ? g->rec + 9 * g->rec_n : g->round_out;
+    fe *o6 = g->deferred ? o3 + 3 : nullptr;
     {
         // fold: read 3 tables x 4 entries, write 3 x 2 per pair; else read 3 x 2
         ProfScope ps(c, KF_ROUND, (fold ? 288.0 : 96.0) * (double)npairs);
         if (fold)
             k_round<true><<<grid, GKR_THREADS, 0, c->stream>>>(g->cur[0], g->cur[1], g->cur[2], npairs, r, y[0], y[1], y[2],
-                                                               g->round_parts, g->round_counter, g->round_out);
+                                                               g->round_parts, g->round_counter, o3, o6);
         else
             k_round<false><<<grid, GKR_THREADS, 0, c->stream>>>(g->cur[0], g->cur[1], g->cur[2], npairs, r, nullptr, nullptr,
-                                                                nullptr, g->round_parts, g->round_counter, g->round_out);
+                                                                nullptr, g->round_parts, g->round_counter, o3, o6);
     }
     VG_LAUNCHED(c);
     if (fold) {
@@ -984,6 +1093,10 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
         g->n = n_out;
     }
     g->round0_pending = false;
+    if (g->deferred) {
+        ++g->rec_n;
+        return VG_OK;
+    }
     fe *host;
     VG_TRY(vg_pinned(c, 9, &host));
     VG_CHECK_CUDA(cudaMemcpyAsync(host, g->round_out, 3 * sizeof(fe), cudaMemcpyDeviceToHost, c->stream));

@@ -99,6 +99,118 @@ __global__ void __launch_bounds__(HASH_THREADS) k_leaf_chain(const fe *__restric
     store_digest(leaves + 4 * k, h);
 }
 
+// ---- batched forms: every leaf chain and every Merkle tree of a proof ----
+// Leaf chains of several codeword sets in one launch: thread t serves leaf
+// t - begin of the job whose range holds t.  The next slice's pair is loaded
+// before the current hash so the loads overlap the permutation.
+template <int KIND>
+__global__ void __launch_bounds__(HASH_THREADS) k_leaf_chains(ChainJobs jobs)
+{
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t >= jobs.total) return;
+    int q = 0;
+    while (q + 1 < jobs.count && t >= jobs.j[q + 1].begin) ++q;
+    const fe *__restrict__ c = jobs.j[q].cw;
+    const long n = jobs.j[q].n, half = n >> 1, k = t - jobs.j[q].begin;
+    uint64_t h[4] = {0, 0, 0, 0};
+    fe a = c[k], b = c[k + half];
+    for (int s = 0; s < 65; ++s) {
+        fe na = a, nb = b;
+        if (s + 1 < 65) {
+            na = c[(long)(s + 1) * n + k];
+            nb = c[(long)(s + 1) * n + k + half];
+        }
+        uint64_t w[8] = {a.img, a.real, b.img, b.real, h[0], h[1], h[2], h[3]};
+        vg::hash64<KIND>(w, h);
+        a = na;
+        b = nb;
+    }
+    store_digest(jobs.j[q].leaves + 4 * k, h);
+}
+
+// One Merkle level (parents of height `height`) of every tree that still has
+// more than MERKLE_TOP parents there.
+template <int KIND>
+__global__ void __launch_bounds__(HASH_THREADS) k_merkle_levels(TreeJobs jobs, int height, long total)
+{
+    long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t >= total) return;
+    int q = 0;
+    for (; q < jobs.count; ++q) {
+        const long cnt = jobs.t[q].nleaves >> height;
+        if (cnt <= MERKLE_TOP) continue;
+        if (t < cnt) break;
+        t -= cnt;
+    }
+    if (q >= jobs.count) return;
+    const long p = (jobs.t[q].nleaves >> height) + t;
+    uint64_t w[8], d[4];
+    load_digest2(jobs.t[q].tree + 8 * p, w);
+    vg::hash64<KIND>(w, d);
+    store_digest(jobs.t[q].tree + 4 * p, d);
+}
+
+// The top MERKLE_TOP parents and above of every tree, one CTA per tree; the
+// root is also copied to roots[tree].
+template <int KIND>
+__global__ void __launch_bounds__(MERKLE_TOP) k_merkle_tops(TreeJobs jobs, uint64_t *__restrict__ roots)
+{
+    const TreeJob J = jobs.t[blockIdx.x];
+    uint64_t *tree = J.tree;
+    for (long cnt = J.nleaves >> 1 < MERKLE_TOP ? J.nleaves >> 1 : MERKLE_TOP; cnt >= 1; cnt >>= 1) {
+        for (long j = threadIdx.x; j < cnt; j += blockDim.x) {
+            const long p = cnt + j;
+            uint64_t w[8], d[4];
+            load_digest2(tree + 8 * p, w);
+            vg::hash64<KIND>(w, d);
+            store_digest(tree + 4 * p, d);
+        }
+        __threadfence_block();
+        __syncthreads();
+    }
+    if (threadIdx.x < 4) roots[4 * blockIdx.x + threadIdx.x] = tree[4 + threadIdx.x];
+}
+
+int vg_leaf_chains(vg_ctx *c, const ChainJobs &jobs)
+{
+    if (jobs.total < 1) return VG_OK;
+    double bytes = 0;
+    for (int q = 0; q < jobs.count; ++q) bytes += 16.0 * 65.0 * (double)jobs.j[q].n + 32.0 * (double)(jobs.j[q].n >> 1);
+    ProfScope ps(c, KF_LEAF_CHAIN, bytes);
+    if (c->hash_kind == VG_HASH_SHA256)
+        k_leaf_chains<VG_HASH_SHA256><<<grid_for(jobs.total, HASH_THREADS), HASH_THREADS, 0, c->stream>>>(jobs);
+    else
+        k_leaf_chains<VG_HASH_SHA3_256><<<grid_for(jobs.total, HASH_THREADS), HASH_THREADS, 0, c->stream>>>(jobs);
+    VG_LAUNCHED(c);
+    return VG_OK;
+}
+
+int vg_merkle_trees(vg_ctx *c, const TreeJobs &jobs, uint64_t *roots_dev)
+{
+    if (jobs.count < 1) return VG_OK;
+    for (int height = 1;; ++height) {
+        long total = 0;
+        for (int q = 0; q < jobs.count; ++q) {
+            const long cnt = jobs.t[q].nleaves >> height;
+            if (cnt > MERKLE_TOP) total += cnt;
+        }
+        if (total == 0) break;
+        ProfScope ps(c, KF_MERKLE, 96.0 * (double)total);
+        if (c->hash_kind == VG_HASH_SHA256)
+            k_merkle_levels<VG_HASH_SHA256><<<grid_for(total, HASH_THREADS), HASH_THREADS, 0, c->stream>>>(jobs, height, total);
+        else
+            k_merkle_levels<VG_HASH_SHA3_256><<<grid_for(total, HASH_THREADS), HASH_THREADS, 0, c->stream>>>(jobs, height, total);
+        VG_LAUNCHED(c);
+    }
+    ProfScope ps(c, KF_MERKLE, 96.0 * 2.0 * MERKLE_TOP * jobs.count);
+    if (c->hash_kind == VG_HASH_SHA256)
+        k_merkle_tops<VG_HASH_SHA256><<<jobs.count, MERKLE_TOP, 0, c->stream>>>(jobs, roots_dev);
+    else
+        k_merkle_tops<VG_HASH_SHA3_256><<<jobs.count, MERKLE_TOP, 0, c->stream>>>(jobs, roots_dev);
+    VG_LAUNCHED(c);
+    return VG_OK;
+}
+
 // ------------------------------------------------------------------ host
 int vg_merkle_build(vg_ctx *c, uint64_t *tree, long n_leaves_padded)
 {

@@ -1,0 +1,43 @@
+// Entry points of the one-sync proof pipeline used by vg_session_prove.
+// They are internal to the library (the public C ABI is include/virgo_b200.h):
+// every call only enqueues work on the context stream; results stay on the
+// device or land in pinned host memory that is valid after the stream is
+// synchronised.
+#pragma once
+#include "virgo_b200.h"
+
+// ---- GKR (gkr.cu) ----
+// Deferred mode on: rounds and v_res write records of 9 values on the device
+// (round: the 3 sums, then the 6 folded values when one pair remained;
+// v_res: the value) instead of returning them; records are numbered in call
+// order from 0.
+int vg_gkr_defer(vg_gkr *g, int on);
+// phase2_init whose v_u = fold of the previous record's V pair at r_last,
+// plus addend, is formed on the device.
+int vg_gkr_phase2_init_deferred(vg_gkr *g, const vg_fe *r_u, int length_u, vg_fe r_last, vg_fe addend);
+// Enqueues the copy of all records to pinned host memory (*host, 9 * *n values).
+int vg_gkr_records(vg_gkr *g, const vg_fe **host, int *n);
+
+// vg_eq_table without the final synchronisation.
+int vg_eq_table_async(vg_ctx *c, const vg_fe *r, int log_len, vg_fe *pub);
+
+// ---- commitment + FRI + queries (commit.cu) ----
+struct vg_pc_results {
+    const vg_fe *inner;          // sampled <l, q>, compared with the sumcheck claim
+    const vg_fe *all_sum;        // 65
+    const vg_digest *roots;      // 2 + nlevels: l, h, then every FRI level
+    const vg_fe *final_cw;       // last FRI level, 65 slices of n_final, slice-major
+    long n_final;
+    const vg_fe *qvals;          // nq x 130: the 65 value pairs of each query
+    const vg_digest *qpaths;     // nq x 32: siblings bottom-up, then the leaf
+};
+// Mask length M the private mask is padded to (poly_commit.h:66-70).
+long vg_pc_mask_len(int log_len, long n_pri_mask);
+// The whole commitment of one proof: RS encodings of the private input and of
+// the public eq table, the virtual oracle, every FRI fold (challenges fri_r),
+// all leaf chains and Merkle trees batched, the query answers for
+// (which, pos) as in vg_pc_query_batch, and the copies of every result into
+// pinned memory (out points there).
+int vg_pc_prove_deferred(vg_pc *pc, const vg_fe *priv, int log_len, const vg_fe *pri_mask, long n_pri_mask,
+                         const vg_fe *pub, const vg_fe *pub_mask, long n_pub_mask, const vg_fe *fri_r, int nlevels,
+                         int nq, const int *which, const long *pos, vg_pc_results *out);

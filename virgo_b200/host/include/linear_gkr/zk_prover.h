@@ -98,6 +98,15 @@ public:
     void attach_circuit(const layered_circuit &c, vg_circuit *dev, struct vg_ctx *ctx = nullptr);
     // Clears the per-proof state so the same object can prove again.
     void reset_proof();
+    // One-sync proofs (vg_session_prove) run the protocol twice from the same
+    // rand() state: DEFER_LAUNCH only enqueues the device work (round sums and
+    // the other device results stay on the device as records), DEFER_REPLAY
+    // does no device work and takes the device results from `replay`, in call
+    // order.  DEFER_OFF (default) is the reference's synchronous behaviour.
+    enum { DEFER_OFF = 0, DEFER_LAUNCH = 1, DEFER_REPLAY = 2 };
+    int defer_mode;
+    const prime_field::field_element *replay;   // 9 values per record
+    int replay_n, replay_i;
 };
 
 #endif

@@ -27,6 +27,7 @@
 #include <string>
 #include <vector>
 #include "device.h"
+#include "internal.h"
 #include "linear_gkr/zk_prover.h"
 #include "poly_commitment/poly_commit.h"
 
@@ -366,47 +367,46 @@ extern "C" int vg_circuit_write_text(int d, const long *n, const uint8_t *const 
     return VG_OK;
 }
 
-extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcript, vg_proof_stats *stats,
-                                uint8_t **transcript, size_t *transcript_len)
-{
-    if (!s || !s->p) return vg_fail(VG_ERR_ARG, "vg_session_prove: null session");
-    if (!s->loaded) return vg_fail(VG_ERR_STATE, "vg_session_prove: no circuit loaded (the last load failed)");
-    {
-        int dev = 0;
-        vg_ctx_device(s->ctx, &dev);
-        cudaSetDevice(dev);   // this thread may not have used the session's device yet
-    }
-    auto t_all = clk::now();
-    vg_proof_stats st;
-    memset(&st, 0, sizeof st);
-    long long launches0 = 0;
-    vg_ctx_launch_count(s->ctx, &launches0);
+// Device results of the launch pass, read by the replay pass.
+struct PassResults {
+    const F *rec = nullptr;   // GKR records (9 values each)
+    int nrec = 0;
+    vg_pc_results pc{};
+    int levels = 0;
+};
 
-    // the reference's rand() stream after srand(seed), private to this thread
+// One run of the protocol from srand(seed).  launch: every device step is
+// enqueued and nothing is read back (the transcript is off); replay: no
+// device work, every device result comes from `res`, and the transcript,
+// the claim check and the proof-size bookkeeping are produced.  Both runs
+// draw the same rand() values in the same order.
+static int prove_pass(vg_session *s, unsigned seed, bool launch, PassResults &res, Transcript &tr, int &proof_size_out)
+{
     struct random_data rd;
     int32_t statebuf[32];   // 128 bytes: glibc's default TYPE_3 state, as srand() uses
     memset(&rd, 0, sizeof rd);
     memset(statebuf, 0, sizeof statebuf);
     initstate_r(seed, (char *)statebuf, sizeof statebuf, &rd);
     prime_field::set_thread_random_state(&rd);
+    struct Restore {
+        ~Restore() { prime_field::set_thread_random_state(nullptr); }
+    } restore;
     auto rand_int = [&]() {
         int32_t r;
         random_r(&rd, &r);
         return (int)r;
     };
-
-    Transcript tr;
-    tr.on = want_transcript != 0;
     zk_prover &p = *s->p;
     layered_circuit &C = s->circuit->C;
     p.reset_proof();
+    p.defer_mode = launch ? zk_prover::DEFER_LAUNCH : zk_prover::DEFER_REPLAY;
+    p.replay = res.rec;
+    p.replay_n = res.nrec;
+    p.replay_i = 0;
     int proof_size = 0;
 
     // ---------------- GKR (zk_verifier.cpp:919-1207) ----------------
-    auto t0 = clk::now();
     F *result = p.evaluate();
-    st.evaluate_s = since(t0);
-    t0 = clk::now();
     F alpha(1), beta(0);
     const int out_bl = C.circuit[C.total_depth - 1].bit_length;
     std::vector<F> r_0 = draws(out_bl), r_1 = draws(out_bl);
@@ -543,86 +543,20 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
     p.all_pri_mask.push_back(p.maskr[0]);
     p.all_pri_mask.push_back(p.maskr[1]);
     all_mask_sum = all_mask_sum + p.Zu * p.sumRc.eval(p.preu1);
-    st.gkr_s = since(t0);
 
     // ---------------- commitments (zk_verifier.cpp:1210-1219; poly_commit.h:42-351) ----------------
-    t0 = clk::now();
     const int L = C.circuit[0].bit_length;
-    int rc;
-#define SESSION_TRY(x)                 \
-    do {                               \
-        rc = (x);                      \
-        if (rc != VG_OK) {             \
-            prime_field::set_thread_random_state(nullptr); \
-            return rc;                 \
-        }                              \
-    } while (0)
-    long M = 0;
-    SESSION_TRY(vg_pc_encode_private(s->pc, (const vg_fe *)p.circuit_value[0], L, (const vg_fe *)p.all_pri_mask.data(),
-                                     (long)p.all_pri_mask.size(), &M));
-    __hhash_digest root_l, root_h;
-    SESSION_TRY(vg_pc_init_commit(s->pc, 0, (vg_digest *)&root_l));
-    tr.put('C', &root_l, 2);
-    const size_t pub_bytes = ((size_t)1 << L) * sizeof(F);
-    if (s->pub_bytes < pub_bytes) {
-        if (s->pub) vg_dev_free(s->ctx, s->pub);
-        s->pub = nullptr;
-        SESSION_TRY(vg_dev_alloc(s->ctx, pub_bytes, &s->pub));
-        s->pub_bytes = pub_bytes;
-    }
-    SESSION_TRY(vg_eq_table(s->ctx, (const vg_fe *)r_0.data(), L, (vg_fe *)s->pub));
-    if ((long)all_pub_mask.size() > M) {
-        prime_field::set_thread_random_state(nullptr);
-        return vg_fail(VG_ERR_STATE, "vg_session_prove: public mask longer than the slice");
-    }
+    const long M = vg_pc_mask_len(L, (long)p.all_pri_mask.size());
+    if ((long)all_pub_mask.size() > M) return vg_fail(VG_ERR_STATE, "vg_session_prove: public mask longer than the slice");
     while ((long)all_pub_mask.size() < M) all_pub_mask.push_back(F(0));   // poly_commit.h:138-139
-    F all_sum[slice_number + 1], inner;
-    SESSION_TRY(vg_pc_encode_public(s->pc, (const vg_fe *)s->pub, (const vg_fe *)all_pub_mask.data(), M,
-                                    (vg_fe *)all_sum, (vg_fe *)&inner));
-    // the claimed inner product the reference asserts (poly_commit.h:193)
-    const F target = alpha_beta_sum - p.Zu * p.sumRc.eval(p.preu1) + all_mask_sum;
-    if (inner != target) {
-        prime_field::set_thread_random_state(nullptr);
-        return vg_fail(VG_ERR_STATE, "vg_session_prove: committed inner product differs from the sumcheck claim");
-    }
-    SESSION_TRY(vg_pc_init_commit(s->pc, 1, (vg_digest *)&root_h));
-    tr.put('C', &root_h, 2);
-    proof_size += 2 * sizeof(__hhash_digest);
-    tr.put('A', all_sum, slice_number + 1);
-    __hhash_digest lh[2] = {root_l, root_h};
-    tr.put('B', lh, 4);
-    st.commit_s = since(t0);
 
-    // ---------------- FRI commit phase (vpd_verifier.cpp:46-78, 101) ----------------
-    t0 = clk::now();
-    int codeword_size = 1 << (L + rs_code_rate - log_slice_number);
-    int levels = 0;
-    while (codeword_size > (1 << rs_code_rate)) {
-        F r = prime_field::random();
-        __hhash_digest h;
-        vg_fe rv;
-        rv.real = r.real;
-        rv.img = r.img;
-        SESSION_TRY(vg_pc_fri_step(s->pc, rv, (vg_digest *)&h));
-        tr.put('T', &h, 2);
-        codeword_size /= 2;
-        ++levels;
-    }
-    {
-        long nfin = 0;
-        SESSION_TRY(vg_pc_fri_final(s->pc, nullptr, nullptr, &nfin));
-        std::vector<F> data(nfin * (slice_number + 1)), msk(nfin);
-        SESSION_TRY(vg_pc_fri_final(s->pc, (vg_fe *)data.data(), (vg_fe *)msk.data(), &nfin));
-        tr.put('X', data.data(), (uint32_t)(nfin * slice_number));
-        tr.put('x', msk.data(), (uint32_t)nfin);
-    }
-    st.fri_s = since(t0);
+    // FRI challenges (vpd_verifier.cpp:46-78): one per fold
+    std::vector<F> fri_r;
+    for (int cw = 1 << (L + rs_code_rate - log_slice_number); cw > (1 << rs_code_rate); cw /= 2)
+        fri_r.push_back(prime_field::random());
+    const int levels = (int)fri_r.size();
 
-    // ---------------- query answers (vpd_verifier.cpp:105-312) ----------------
-    // All positions come from the rand() stream alone, so they are drawn
-    // first and every answer is gathered in one batch; the answers and the
-    // proof-size bookkeeping (fri.cpp:148-289) are then assembled in order.
-    t0 = clk::now();
+    // query positions (vpd_verifier.cpp:105-312): from the rand() stream alone
     std::vector<int> which;
     std::vector<long> pos;
     for (int rep = 0; rep < ldt_repeat_num; ++rep) {
@@ -645,11 +579,60 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
         }
     }
     const int nq = (int)which.size();
-    std::vector<F> qvals((size_t)nq * 130);
-    std::vector<__hhash_digest> qpaths((size_t)nq * 32);
-    std::vector<int> qlen(nq);
-    SESSION_TRY(vg_pc_query_batch(s->pc, nq, which.data(), pos.data(), (vg_fe *)qvals.data(), (vg_digest *)qpaths.data(),
-                                  qlen.data()));
+
+    if (launch) {
+        const size_t pub_bytes = ((size_t)1 << L) * sizeof(F);
+        if (s->pub_bytes < pub_bytes) {
+            if (s->pub) vg_dev_free(s->ctx, s->pub);
+            s->pub = nullptr;
+            int rc = vg_dev_alloc(s->ctx, pub_bytes, &s->pub);
+            if (rc != VG_OK) return rc;
+            s->pub_bytes = pub_bytes;
+        }
+        int rc = vg_eq_table_async(s->ctx, (const vg_fe *)r_0.data(), L, (vg_fe *)s->pub);
+        if (rc == VG_OK)
+            rc = vg_pc_prove_deferred(s->pc, (const vg_fe *)p.circuit_value[0], L, (const vg_fe *)p.all_pri_mask.data(),
+                                      (long)p.all_pri_mask.size(), (const vg_fe *)s->pub,
+                                      (const vg_fe *)all_pub_mask.data(), M, (const vg_fe *)fri_r.data(), levels, nq,
+                                      which.data(), pos.data(), &res.pc);
+        res.levels = levels;
+        return rc;
+    }
+
+    // ---- replay: commitment messages ----
+    const vg_pc_results &pr = res.pc;
+    // the claimed inner product the reference asserts (poly_commit.h:193)
+    const F target = alpha_beta_sum - p.Zu * p.sumRc.eval(p.preu1) + all_mask_sum;
+    const F inner = *(const F *)pr.inner;
+    if (inner != target)
+        return vg_fail(VG_ERR_STATE, "vg_session_prove: committed inner product differs from the sumcheck claim");
+    const __hhash_digest *roots = (const __hhash_digest *)pr.roots;
+    tr.put('C', &roots[0], 2);
+    tr.put('C', &roots[1], 2);
+    proof_size += 2 * sizeof(__hhash_digest);
+    tr.put('A', pr.all_sum, slice_number + 1);
+    tr.put('B', roots, 4);
+    for (int t = 0; t < levels; ++t) tr.put('T', &roots[2 + t], 2);
+    {
+        // the final level in the interleaved layout of fri.cpp:348-363 and 382-388
+        const long n = pr.n_final, h = n >> 1;
+        const F *b = (const F *)pr.final_cw;
+        std::vector<F> data((size_t)n * slice_number), msk(n);
+        for (long j = 0; j < h; ++j) {
+            for (int sl = 0; sl < slice_number; ++sl) {
+                data[(j << 7) | (sl << 1) | 0] = b[sl * n + j];
+                data[(j << 7) | (sl << 1) | 1] = b[sl * n + j + h];
+            }
+            msk[2 * j] = b[64 * n + j];
+            msk[2 * j + 1] = b[64 * n + j + h];
+        }
+        tr.put('X', data.data(), (uint32_t)(n * slice_number));
+        tr.put('x', msk.data(), (uint32_t)n);
+    }
+
+    // ---- replay: query answers and the proof-size bookkeeping (fri.cpp:148-289) ----
+    const F *qvals = (const F *)pr.qvals;
+    const __hhash_digest *qpaths = (const __hhash_digest *)pr.qpaths;
     std::unordered_set<long long> seen_elem[2], seen_node[2];
     std::vector<std::unordered_set<long long> > seen_level(levels);
     const long long half_S = 1LL << (L - 2);
@@ -658,7 +641,7 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
         const F *v = &qvals[(size_t)q * 130];
         for (int k = 0; k <= slice_number; ++k) a.first.push_back(std::make_pair(v[2 * k], v[2 * k + 1]));
         const __hhash_digest *pth = &qpaths[(size_t)q * 32];
-        const int depth = qlen[q] - 1;
+        const int depth = which[q] < 2 ? L - 2 : L - (which[q] - 2) - 3;   // log2 of the set's leaf count
         int new_size = 0;
         if (which[q] < 2) {   // fri::request_init_value_with_merkle
             const int o = which[q];
@@ -702,11 +685,60 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
             proof_size += new_size;
         }
     }
-    st.query_s = since(t0);
-    prime_field::set_thread_random_state(nullptr);
-#undef SESSION_TRY
+    if (p.replay_i != res.nrec) return vg_fail(VG_ERR_STATE, "replay used %d of %d device records", p.replay_i, res.nrec);
+    proof_size_out = proof_size;
+    return VG_OK;
+}
 
-    st.prove_time = p.total_time + st.commit_s + st.fri_s;   // GKR methods + commitments + FRI
+extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcript, vg_proof_stats *stats,
+                                uint8_t **transcript, size_t *transcript_len)
+{
+    if (!s || !s->p) return vg_fail(VG_ERR_ARG, "vg_session_prove: null session");
+    if (!s->loaded) return vg_fail(VG_ERR_STATE, "vg_session_prove: no circuit loaded (the last load failed)");
+    {
+        int dev = 0;
+        vg_ctx_device(s->ctx, &dev);
+        cudaSetDevice(dev);   // this thread may not have used the session's device yet
+    }
+    auto t_all = clk::now();
+    vg_proof_stats st;
+    memset(&st, 0, sizeof st);
+    long long launches0 = 0;
+    vg_ctx_launch_count(s->ctx, &launches0);
+    zk_prover &p = *s->p;
+
+    // launch pass: the whole proof enqueued on the session's stream
+    PassResults res;
+    Transcript tr;
+    tr.on = false;
+    int proof_size = 0;
+    int rc = vg_gkr_defer(p.dev_gkr, 1);
+    if (rc == VG_OK) rc = prove_pass(s, seed, true, res, tr, proof_size);
+    const vg_fe *recs = nullptr;
+    if (rc == VG_OK) rc = vg_gkr_records(p.dev_gkr, &recs, &res.nrec);
+    vg_gkr_defer(p.dev_gkr, 0);
+    p.defer_mode = zk_prover::DEFER_OFF;
+    if (rc != VG_OK) {
+        vg_ctx_sync(s->ctx);   // drain what was enqueued before the error
+        return rc;
+    }
+    st.launch_s = since(t_all);
+    auto t0 = clk::now();
+    rc = vg_ctx_sync(s->ctx);
+    if (rc != VG_OK) return rc;
+    st.wait_s = since(t0);
+    st.prove_time = since(t_all);
+
+    // replay pass: messages, checks and the transcript from the device results
+    t0 = clk::now();
+    res.rec = (const F *)recs;
+    tr.on = want_transcript != 0;
+    rc = prove_pass(s, seed, false, res, tr, proof_size);
+    p.defer_mode = zk_prover::DEFER_OFF;
+    p.replay = nullptr;
+    if (rc != VG_OK) return rc;
+    st.replay_s = since(t0);
+
     st.total_s = since(t_all);
     st.proof_size = proof_size;
     long long launches1 = 0;

@@ -9,6 +9,7 @@
 #include <cstdlib>
 #include <iostream>
 #include "device.h"
+#include "internal.h"
 #include "infrastructure/utility.h"
 
 typedef prime_field::field_element F;
@@ -54,6 +55,9 @@ zk_prover::zk_prover()
     total_time = 0;
     r_0 = r_1 = nullptr;
     one_minus_r_0 = one_minus_r_1 = nullptr;
+    defer_mode = DEFER_OFF;
+    replay = nullptr;
+    replay_n = replay_i = 0;
 }
 
 zk_prover::~zk_prover() {}
@@ -135,7 +139,7 @@ void zk_prover::proof_init() {}
 F *zk_prover::evaluate()
 {
     auto t0 = clk::now();
-    virgo::check(vg_gkr_evaluate(dev_gkr), "vg_gkr_evaluate");
+    if (defer_mode != DEFER_REPLAY) virgo::check(vg_gkr_evaluate(dev_gkr), "vg_gkr_evaluate");
     for (int i = 0; i < C.total_depth; ++i) {
         const vg_fe *p;
         virgo::check(vg_gkr_layer_values(dev_gkr, i, &p), "vg_gkr_layer_values");
@@ -153,7 +157,13 @@ F zk_prover::V_res(const F *one_minus_r_0, const F *r_0, const F *output_raw, in
     F res;
     std::vector<vg_fe> r(r_0_size);
     for (int i = 0; i < r_0_size; ++i) r[i] = to_vg(r_0[i]);
-    vg_fe out;
+    vg_fe out{0, 0};
+    if (defer_mode == DEFER_REPLAY) {
+        if (replay_i >= replay_n) virgo::check(VG_ERR_STATE, "V_res: no recorded result");
+        res = replay[9 * replay_i++];
+        total_time += since(t0);
+        return res;
+    }
     if (output_raw == circuit_value[C.total_depth - 1] && output_size == (1 << C.circuit[C.total_depth - 1].bit_length)) {
         virgo::check(vg_gkr_v_res(dev_gkr, r.data(), r_0_size, &out), "vg_gkr_v_res");
     } else {
@@ -283,6 +293,7 @@ void zk_prover::sumcheck_phase1_init()
 {
     auto t0 = clk::now();
     total_uv = 1 << C.circuit[sumcheck_layer_id - 1].bit_length;
+    if (defer_mode == DEFER_REPLAY) return;
     std::vector<vg_fe> a(length_g), b(length_g);
     for (int i = 0; i < length_g; ++i) {
         a[i] = to_vg(r_0[i]);
@@ -294,9 +305,23 @@ void zk_prover::sumcheck_phase1_init()
 }
 
 // one device round: the three sums of the array loop, and the folded tables
-// when two entries remain
-static quadratic_poly device_round(vg_gkr *g, const F &r, int bit, F *last6)
+// when two entries remain (deferred modes: enqueue only, or the recorded result)
+static quadratic_poly device_round(zk_prover *p, const F &r, int bit, F *last6)
 {
+    if (p->defer_mode == zk_prover::DEFER_LAUNCH) {
+        virgo::check(vg_gkr_round(p->dev_gkr, to_vg(r), bit, nullptr, nullptr), "vg_gkr_round");
+        if (last6)
+            for (int k = 0; k < 6; ++k) last6[k] = F(0);
+        return quadratic_poly(F(0), F(0), F(0));
+    }
+    if (p->defer_mode == zk_prover::DEFER_REPLAY) {
+        if (p->replay_i >= p->replay_n) virgo::check(VG_ERR_STATE, "sumcheck round: no recorded result");
+        const F *rec = p->replay + 9 * p->replay_i++;
+        if (last6)
+            for (int k = 0; k < 6; ++k) last6[k] = rec[3 + k];
+        return quadratic_poly(rec[0], rec[1], rec[2]);
+    }
+    vg_gkr *g = p->dev_gkr;
     vg_fe s[3], l6[6];
     virgo::check(vg_gkr_round(g, to_vg(r), bit, s, last6 ? l6 : nullptr), "vg_gkr_round");
     if (last6)
@@ -308,7 +333,7 @@ static quadratic_poly device_round(vg_gkr *g, const F &r, int bit, F *last6)
 quadratic_poly zk_prover::sumcheck_phase1_update(F previous_random, int current_bit)
 {
     auto t0 = clk::now();
-    quadratic_poly ret = device_round(dev_gkr, previous_random, current_bit, nullptr);
+    quadratic_poly ret = device_round(this, previous_random, current_bit, nullptr);
     total_uv >>= 1;
     const F one(1), omr = one - previous_random;
     Iuv = Iuv * omr;
@@ -355,7 +380,7 @@ static void last_bit_terms(quadratic_poly &ret, F &rd, F &re, F &rf, const quadr
 quintuple_poly zk_prover::sumcheck_phase1_updatelastbit(F previous_random, int current_bit)
 {
     auto t0 = clk::now();
-    quadratic_poly ret = device_round(dev_gkr, previous_random, current_bit, tables_last);
+    quadratic_poly ret = device_round(this, previous_random, current_bit, tables_last);
     total_uv >>= 1;
     const F one(1), omr = one - previous_random;
     Iuv = Iuv * omr;
@@ -404,13 +429,17 @@ void zk_prover::sumcheck_phase2_init(F previous_random, const F *r_u, const F *o
     maskR_sumcv = maskR_sumcv * omr;
     Iuv = Iuv * omr;
     // V_mult_add[0].eval(r): the folded pair of the last phase-1 round
-    v_u = tables_last[0] + previous_random * (tables_last[1] - tables_last[0]);
     Zu = Zu * omr * previous_random;
-    v_u = v_u + Zu * sumRc.eval(previous_random);
+    const F addend = Zu * sumRc.eval(previous_random);
+    v_u = tables_last[0] + previous_random * (tables_last[1] - tables_last[0]) + addend;
 
     std::vector<vg_fe> ru(length_u);
     for (int i = 0; i < length_u; ++i) ru[i] = to_vg(r_u[i]);
-    virgo::check(vg_gkr_phase2_init(dev_gkr, ru.data(), length_u, to_vg(v_u)), "vg_gkr_phase2_init");
+    if (defer_mode == DEFER_LAUNCH)   // v_u is formed on the device from the recorded pair
+        virgo::check(vg_gkr_phase2_init_deferred(dev_gkr, ru.data(), length_u, to_vg(previous_random), to_vg(addend)),
+                     "vg_gkr_phase2_init");
+    else if (defer_mode == DEFER_OFF)
+        virgo::check(vg_gkr_phase2_init(dev_gkr, ru.data(), length_u, to_vg(v_u)), "vg_gkr_phase2_init");
     total_uv = 1 << C.circuit[sumcheck_layer_id - 1].bit_length;
 
     const int m = (length_u + length_v + 1) * 2;
@@ -426,7 +455,7 @@ void zk_prover::sumcheck_phase2_init(F previous_random, const F *r_u, const F *o
 quadratic_poly zk_prover::sumcheck_phase2_update(F previous_random, int current_bit)
 {
     auto t0 = clk::now();
-    quadratic_poly ret = device_round(dev_gkr, previous_random, current_bit, nullptr);
+    quadratic_poly ret = device_round(this, previous_random, current_bit, nullptr);
     total_uv >>= 1;
     const F one(1), omr = one - previous_random;
     if (current_bit > 0) {
@@ -457,7 +486,7 @@ quadratic_poly zk_prover::sumcheck_phase2_update(F previous_random, int current_
 quintuple_poly zk_prover::sumcheck_phase2_updatelastbit(F previous_random, int current_bit)
 {
     auto t0 = clk::now();
-    quadratic_poly ret = device_round(dev_gkr, previous_random, current_bit, tables_last);
+    quadratic_poly ret = device_round(this, previous_random, current_bit, tables_last);
     total_uv >>= 1;
     const F one(1), omr = one - previous_random;
     Iuv = Iuv * omr;
