@@ -187,3 +187,29 @@ def test_session_load_reuses_buffers_and_matches():
         assert s.prove(c["seed"])[1] == t32
     finally:
         s.close()
+
+
+def test_atomic_phase_tables_match_golden():
+    """The phase inits have two table constructions: gathers over the wiring
+    grouped per table entry (default) and the atomic scatter kept for layers
+    whose edge sets cannot be built.  VIRGO_PHASE_TABLES=atomic forces the
+    scatter everywhere; both must give the golden transcripts."""
+    code = r'''
+import json, sys
+import virgo_b200 as vb
+from virgo_b200 import circuits, transcript
+out = {}
+for c in json.load(open(sys.argv[1])):
+    if c["name"] not in ("mixed_gates", "random_5layer", "matmul8_32bit"):
+        continue
+    s = vb.Session(getattr(circuits, c["generator"])(**c["params"]))
+    out[c["name"]] = transcript.digest(transcript.parse(s.prove(c["seed"])[1]))
+    s.close()
+print(json.dumps(out))
+'''
+    env = dict(os.environ, VIRGO_PHASE_TABLES="atomic", PYTHONPATH=ROOT)
+    r = subprocess.run(["python", "-c", code, GOLD], capture_output=True, text=True, timeout=600, env=env, cwd=ROOT)
+    assert r.returncode == 0, r.stderr[-2000:]
+    got = json.loads(r.stdout.strip().splitlines()[-1])
+    want = {c["name"]: c["digest"] for c in _golden()}
+    assert got and all(got[k] == want[k] for k in got), (got, want)

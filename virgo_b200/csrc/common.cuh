@@ -148,3 +148,8 @@ __device__ __forceinline__ void block_sum(fe (&v)[K], fe *sm)
 
 // sum of `nparts` groups of K partials (layout [part][K]) into out[K]
 int vg_reduce_partials(vg_ctx *ctx, const fe *parts, int nparts, int K, fe *out_dev);
+
+// Exclusive prefix sum of d[0 .. n) in place, d[n] (zero on entry) receives
+// the total; tmp holds vg_scan_tmp_words(n) words.
+long vg_scan_tmp_words(long n);
+int vg_scan_u32(vg_ctx *c, uint32_t *d, long n, uint32_t *tmp);

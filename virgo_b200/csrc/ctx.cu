@@ -371,3 +371,76 @@ int vg_reduce_partials(vg_ctx *c, const fe *parts, int nparts, int K, fe *out_de
     VG_LAUNCHED(c);
     return VG_OK;
 }
+
+// ------------------------------------------------------------ prefix sums
+namespace {
+constexpr int SCAN_THREADS = 1024, SCAN_TILE = 2 * SCAN_THREADS;
+
+// exclusive scan of each tile of SCAN_TILE entries in place; tile totals to sums
+__global__ void __launch_bounds__(SCAN_THREADS) k_scan_tiles(uint32_t *__restrict__ d, long n, uint32_t *__restrict__ sums)
+{
+    __shared__ uint32_t s[SCAN_TILE];
+    const long base = (long)blockIdx.x * SCAN_TILE;
+    const int t = threadIdx.x;
+    s[2 * t] = base + 2 * t < n ? d[base + 2 * t] : 0;
+    s[2 * t + 1] = base + 2 * t + 1 < n ? d[base + 2 * t + 1] : 0;
+    // work-efficient (up-sweep / down-sweep) scan
+    int off = 1;
+    for (int w = SCAN_TILE >> 1; w > 0; w >>= 1) {
+        __syncthreads();
+        if (t < w) {
+            const int a = off * (2 * t + 1) - 1, b = off * (2 * t + 2) - 1;
+            s[b] += s[a];
+        }
+        off <<= 1;
+    }
+    if (t == 0) {
+        sums[blockIdx.x] = s[SCAN_TILE - 1];
+        s[SCAN_TILE - 1] = 0;
+    }
+    for (int w = 1; w < SCAN_TILE; w <<= 1) {
+        off >>= 1;
+        __syncthreads();
+        if (t < w) {
+            const int a = off * (2 * t + 1) - 1, b = off * (2 * t + 2) - 1;
+            const uint32_t x = s[a];
+            s[a] = s[b];
+            s[b] += x;
+        }
+    }
+    __syncthreads();
+    if (base + 2 * t < n) d[base + 2 * t] = s[2 * t];
+    if (base + 2 * t + 1 < n) d[base + 2 * t + 1] = s[2 * t + 1];
+}
+
+__global__ void k_scan_add(uint32_t *__restrict__ d, long n, const uint32_t *__restrict__ offs)
+{
+    const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i < n) d[i] += offs[i / SCAN_TILE];
+}
+}  // namespace
+
+// Exclusive prefix sum of d[0 .. n) in place; d[n] receives the total.  tmp
+// needs vg_scan_tmp_words(n) words.
+long vg_scan_tmp_words(long n)
+{
+    long w = 0;
+    for (long m = n + 1; m > 1; m = (m + SCAN_TILE - 1) / SCAN_TILE) w += (m + SCAN_TILE - 1) / SCAN_TILE + 1;
+    return w + 1;
+}
+
+int vg_scan_u32(vg_ctx *c, uint32_t *d, long n, uint32_t *tmp)
+{
+    // scan n + 1 entries (d[n] = 0 on entry after the caller's counts) so the
+    // last entry becomes the total
+    const long m = n + 1;
+    const long tiles = (m + SCAN_TILE - 1) / SCAN_TILE;
+    k_scan_tiles<<<(unsigned)tiles, SCAN_THREADS, 0, c->stream>>>(d, m, tmp);
+    VG_LAUNCHED(c);
+    if (tiles > 1) {
+        VG_TRY(vg_scan_u32(c, tmp, tiles - 1, tmp + tiles + 1));   // tmp[0 .. tiles) exclusive
+        k_scan_add<<<grid_for(m, 256), 256, 0, c->stream>>>(d, m, tmp);
+        VG_LAUNCHED(c);
+    }
+    return VG_OK;
+}

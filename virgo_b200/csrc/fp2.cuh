@@ -89,6 +89,11 @@ VG_HD fe operator*(fe a, fe b)
 
 VG_HD fe fe_double(fe a) { return a + a; }
 
+// a * 2^k for canonical a and 0 <= k <= 60: since 2^61 = 1 (mod p), this is a
+// left rotation of each 61-bit component
+VG_HD uint64_t rotp(uint64_t x, int k) { return ((x << k) | (x >> (61 - k))) & P; }
+VG_HD fe fe_mul_pow2(fe a, int k) { return fe_make(rotp(a.real, k), rotp(a.img, k)); }
+
 // multiplication by an element of F_p (img = 0)
 VG_HD fe fe_scale(fe a, uint64_t s) { return fe_make(mulp(a.real, s), mulp(a.img, s)); }
 

@@ -31,12 +31,34 @@ namespace {
 
 constexpr int GKR_THREADS = 256;
 
+// The wiring of one layer grouped by the table entry each gate feeds in one
+// sumcheck phase (phase 1: u, phase 2: v; summation gates expanded to one
+// edge per summed wire).  Built once per circuit, it turns the phase inits
+// into gathers: every table entry is summed by one thread (or one warp for
+// long lists) and written once, without atomics.
+struct EdgeSet {
+    bool launched = false;        // offsets and edges enqueued by launch_edges
+    bool ok = false;
+    long N = 0;                   // table entries (keys)
+    long E = 0;                   // edges
+    uint32_t *off = nullptr;      // N + 1 offsets
+    uint32_t *g = nullptr;        // gate index (the relay's u in phase 1)
+    uint32_t *o = nullptr;        // the other wire (phase 1: v, phase 2: u or the summed wire)
+    uint16_t *tk = nullptr;       // gate type | doubling count << 8
+    uint32_t *medium = nullptr;   // keys with more than LIGHT_MAX edges
+    long n_medium = 0;
+    long cap_N = 0, cap_E = 0, cap_M = 0;
+};
+
 struct DevLayer {
     int bl = 0;
     long n = 0;
     uint8_t *ty = nullptr;
     uint32_t *u = nullptr, *v = nullptr;
+    EdgeSet ph[2];
 };
+
+constexpr int LIGHT_MAX = 64;   // edges a single thread sums; longer lists get a warp
 
 __device__ __forceinline__ fe from_int32(int32_t x)
 {
@@ -292,6 +314,185 @@ __global__ void __launch_bounds__(GKR_THREADS) k_phase2_scatter(const uint8_t *_
     block_acc_add(av, 0, zero_acc, sm);
 }
 
+// ------------------------------------------------------- wiring transpose
+// Calls emit(key, gate, other, type | doublings << 8) for every edge of gate
+// g in phase PH (0: keyed by u as in k_phase1_scatter, 1: keyed by v as in
+// k_phase2_scatter, summation gates at key 0).
+template <int PH, typename Emit>
+__device__ __forceinline__ void gate_edges(int t, uint32_t g, uint32_t u, uint32_t v, Emit emit)
+{
+    if (t == 2 || t == 3 || t == 11 || t > 13) return;
+    if (PH == 0) {
+        if (t == 4) emit(u, u, 0u, (uint16_t)4);
+        else if (t == 5)
+            for (uint32_t j = u; j < v; ++j) emit(j, g, 0u, (uint16_t)5);
+        else if (t == 12)
+            for (uint32_t j = u; j <= v; ++j) emit(j, g, 0u, (uint16_t)(12 | ((j - u) << 8)));
+        else emit(u, g, v, (uint16_t)t);
+    } else {
+        if (t == 4) return;
+        if (t == 5)
+            for (uint32_t j = u; j < v; ++j) emit(0u, g, j, (uint16_t)5);
+        else if (t == 12)
+            for (uint32_t j = u; j <= v; ++j) emit(0u, g, j, (uint16_t)(12 | ((j - u) << 8)));
+        else emit(v, g, u, (uint16_t)t);
+    }
+}
+
+// FILL == false: count edges per key; FILL == true: place them (cursor holds
+// the offsets on entry) unless the total exceeds cap, which sets stats[2].
+// The order inside a key is not fixed, which does not matter: the gathers sum
+// exactly in F_p2.
+template <int PH, bool FILL>
+__global__ void k_edges(const uint8_t *__restrict__ ty, const uint32_t *__restrict__ uu, const uint32_t *__restrict__ vv,
+                        long ng, uint32_t *__restrict__ cnt, uint32_t *__restrict__ eg, uint32_t *__restrict__ eo,
+                        uint16_t *__restrict__ etk, const uint32_t *__restrict__ total, long cap,
+                        unsigned long long *__restrict__ stats)
+{
+    if (FILL && (long)*total > cap) {
+        if (blockIdx.x == 0 && threadIdx.x == 0) stats[2] = 1;
+        return;
+    }
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < ng; i += (long)gridDim.x * blockDim.x) {
+        gate_edges<PH>(ty[i], (uint32_t)i, uu[i], vv[i], [&](uint32_t key, uint32_t gv, uint32_t o, uint16_t tk) {
+            const uint32_t p = atomicAdd(&cnt[key], 1u);
+            if (FILL) {
+                eg[p] = gv;
+                eo[p] = o;
+                etk[p] = tk;
+            }
+        });
+    }
+}
+
+// keys with more than LIGHT_MAX edges into list (room for cap_list);
+// stats[0] = edge total, stats[1] = listed keys
+__global__ void k_medium_keys(const uint32_t *__restrict__ off, long N, uint32_t *__restrict__ list, long cap_list,
+                              unsigned long long *__restrict__ stats)
+{
+    if (blockIdx.x == 0 && threadIdx.x == 0) stats[0] = off[N];
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < N; k += (long)gridDim.x * blockDim.x)
+        if (off[k + 1] - off[k] > (uint32_t)LIGHT_MAX) {
+            const unsigned long long i = atomicAdd(&stats[1], 1ull);
+            if ((long)i < cap_list) list[i] = (uint32_t)k;
+        }
+}
+
+// contribution of one edge to the phase-1 tables (k_phase1_scatter's cases)
+__device__ __forceinline__ void edge1(int tk, uint32_t gv, uint32_t o, const BetaG &bg, const fe *__restrict__ prev, fe &am,
+                                      fe &av)
+{
+    const int t = tk & 255;
+    const fe b = bg.at(gv);
+    switch (t) {
+    case 0: av = av + prev[o] * b; am = am + b; break;
+    case 1: am = am + prev[o] * b; break;
+    case 4:
+    case 5:
+    case 10: am = am + b; break;
+    case 12: am = am + vg::fe_mul_pow2(b, tk >> 8); break;
+    case 6: am = am - b; av = av + b; break;
+    case 7: av = av - prev[o] * b; am = am + b; break;
+    case 8: {
+        const fe x = b * prev[o];
+        av = av + x;
+        am = am + (b - (x + x));
+    } break;
+    case 13: am = am + (b - b * prev[o]); break;
+    case 9: {
+        const fe x = b * prev[o];
+        av = av + x;
+        am = am - x;
+    } break;
+    default: break;
+    }
+}
+
+// contribution to the phase-2 tables, split into the parts with and without
+// the factor v_u (applied once per key): am = am1 + amv v_u, av = av1 + avv v_u
+__device__ __forceinline__ void edge2(int tk, uint32_t gv, uint32_t o, const BetaG &bg, const BetaU &bu, fe (&a)[4])
+{
+    const int t = tk & 255;
+    const fe x = bg.at(gv) * bu.at(o);
+    switch (t) {
+    case 1: a[1] = a[1] + x; break;
+    case 0: a[0] = a[0] + x; a[3] = a[3] + x; break;
+    case 5:
+    case 10: a[3] = a[3] + x; break;
+    case 12: a[3] = a[3] + vg::fe_mul_pow2(x, tk >> 8); break;
+    case 6: a[2] = a[2] + x; a[3] = a[3] - x; break;
+    case 7: a[0] = a[0] - x; a[3] = a[3] + x; break;
+    case 8: a[0] = a[0] + x; a[1] = a[1] - (x + x); a[3] = a[3] + x; break;
+    case 13: a[1] = a[1] - x; a[3] = a[3] + x; break;
+    case 9: a[0] = a[0] + x; a[1] = a[1] - x; break;
+    default: break;
+    }
+}
+
+struct EdgeView {
+    const uint32_t *off, *g, *o;
+    const uint16_t *tk;
+};
+
+// One thread per key with at most LIGHT_MAX edges; out_m / out_v are the
+// add_mult_sum and addV_array tables.
+template <int PH>
+__global__ void __launch_bounds__(GKR_THREADS) k_gather_keys(EdgeView e, long N, BetaG bg, BetaU bu,
+                                                             const fe *__restrict__ prev, const fe *__restrict__ vu_ptr,
+                                                             fe *__restrict__ out_m, fe *__restrict__ out_v)
+{
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < N; k += (long)gridDim.x * blockDim.x) {
+        const uint32_t s = e.off[k], t = e.off[k + 1];
+        if (t - s > (uint32_t)LIGHT_MAX) continue;
+        if (PH == 0) {
+            fe am = vg::fe_zero(), av = vg::fe_zero();
+            for (uint32_t p = s; p < t; ++p) edge1(e.tk[p], e.g[p], e.o[p], bg, prev, am, av);
+            out_m[k] = am;
+            out_v[k] = av;
+        } else {
+            fe a[4] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+            for (uint32_t p = s; p < t; ++p) edge2(e.tk[p], e.g[p], e.o[p], bg, bu, a);
+            const fe vu = *vu_ptr;
+            out_m[k] = a[0] + a[1] * vu;
+            out_v[k] = a[2] + a[3] * vu;
+        }
+    }
+}
+
+// One warp per listed key (more than LIGHT_MAX edges)
+template <int PH>
+__global__ void __launch_bounds__(GKR_THREADS) k_gather_long(EdgeView e, const uint32_t *__restrict__ keys, long nkeys,
+                                                             BetaG bg, BetaU bu, const fe *__restrict__ prev,
+                                                             const fe *__restrict__ vu_ptr, fe *__restrict__ out_m,
+                                                             fe *__restrict__ out_v)
+{
+    const int lane = threadIdx.x & 31;
+    const long nwarps = (long)gridDim.x * (blockDim.x >> 5);
+    for (long w = (blockIdx.x * (long)blockDim.x + threadIdx.x) >> 5; w < nkeys; w += nwarps) {
+        const uint32_t k = keys[w], s = e.off[k], t = e.off[k + 1];
+        if (PH == 0) {
+            fe am = vg::fe_zero(), av = vg::fe_zero();
+            for (uint32_t p = s + lane; p < t; p += 32) edge1(e.tk[p], e.g[p], e.o[p], bg, prev, am, av);
+            am = warp_sum(am);
+            av = warp_sum(av);
+            if (lane == 0) {
+                out_m[k] = am;
+                out_v[k] = av;
+            }
+        } else {
+            fe a[4] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+            for (uint32_t p = s + lane; p < t; p += 32) edge2(e.tk[p], e.g[p], e.o[p], bg, bu, a);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) a[q] = warp_sum(a[q]);
+            if (lane == 0) {
+                const fe vu = *vu_ptr;
+                out_m[k] = a[0] + a[1] * vu;
+                out_v[k] = a[2] + a[3] * vu;
+            }
+        }
+    }
+}
+
 // v_u = V(r_u) + mask term: the folded V pair of the last phase-1 round at r
 // (zk_prover.cpp:796-797), computed where the pair is, so phase 2 can start
 // without the host reading it first
@@ -336,10 +537,13 @@ __global__ void __launch_bounds__(GKR_THREADS) k_round(const fe *__restrict__ xV
         if (last6 && npairs == 1) {   // the folded pairs the last round of a phase needs
             last6[0] = v0; last6[1] = v1; last6[2] = a0; last6[3] = a1; last6[4] = m0; last6[5] = m1;
         }
-        const fe va = v1 - v0, aa = a1 - a0, ma = m1 - m0;
-        acc[0] = acc[0] + ma * va;
-        acc[1] = acc[1] + (ma * v0 + m0 * va) + aa;
-        acc[2] = acc[2] + m0 * v0 + a0;
+        // (m0 + ma x)(v0 + va x) + a0 + aa x: x^2 term ma va, x term
+        // ma v0 + m0 va = m1 v1 - m0 v0 - ma va (three products, not four)
+        const fe va = v1 - v0, ma = m1 - m0;
+        const fe p2 = ma * va, p0 = m0 * v0, p1 = m1 * v1;
+        acc[0] = acc[0] + p2;
+        acc[1] = acc[1] + ((p1 - p0 - p2) + (a1 - a0));
+        acc[2] = acc[2] + p0 + a0;
     }
     block_sum<3>(acc, sm);
     if (threadIdx.x == 0) {
@@ -450,6 +654,11 @@ struct vg_circuit {
     void *staging = nullptr;   // upload staging for one layer
     size_t staging_cap = 0;
     unsigned long long *err = nullptr;
+    uint32_t *work = nullptr;   // edge build: cursors and scan temporaries
+    size_t work_cap = 0;        // words
+    unsigned long long *edge_stats = nullptr;   // 3 per edge set: total, long keys, overflow
+    int edge_stats_cap = 0;
+    std::vector<unsigned long long> edge_stats_host;
 };
 
 struct vg_gkr {
@@ -470,6 +679,7 @@ struct vg_gkr {
     int next_buf = 1;
     bool round0_pending = false;
     BetaG bg{};
+    BetaU bu{};                          // eq(r_u) halves of phase 2
     fe *vu = nullptr;                    // v_u of phase 2 (device scalar)
     // deferred mode: results stay on the device as records of 9 values
     // (round: 3 sums + the 6 folded values when one pair remained;
@@ -482,6 +692,172 @@ struct vg_gkr {
 };
 
 // ------------------------------------------------------------------ circuit
+static int grow_u32(uint32_t **p, long *cap, long n)
+{
+    if (n <= *cap) return VG_OK;
+    cudaFree(*p);
+    *p = nullptr;
+    *cap = 0;
+    if (cudaMalloc(p, (size_t)std::max(n, 1L) * 4) != cudaSuccess) {
+        cudaGetLastError();
+        *p = nullptr;
+        return vg_fail(VG_ERR_OOM, "edge arrays (%ld words)", n);
+    }
+    *cap = n;
+    return VG_OK;
+}
+
+static int alloc_edges(EdgeSet &E, long n)
+{
+    cudaFree(E.g);
+    cudaFree(E.o);
+    cudaFree(E.tk);
+    E.g = E.o = nullptr;
+    E.tk = nullptr;
+    E.cap_E = 0;
+    n = std::max(n, 1L);
+    if (cudaMalloc(&E.g, (size_t)n * 4) != cudaSuccess || cudaMalloc(&E.o, (size_t)n * 4) != cudaSuccess ||
+        cudaMalloc(&E.tk, (size_t)n * 2) != cudaSuccess) {
+        cudaGetLastError();
+        return vg_fail(VG_ERR_OOM, "edge arrays (%ld edges)", n);
+    }
+    E.cap_E = n;
+    return VG_OK;
+}
+
+// Enqueues the fill of edge set ph of layer li (offsets already scanned) and
+// the list of its long keys.
+static int fill_edges(vg_circuit *c, int li, int ph)
+{
+    vg_ctx *ctx = c->ctx;
+    DevLayer &D = c->L[li];
+    EdgeSet &E = D.ph[ph];
+    const long N = E.N;
+    unsigned long long *st = c->edge_stats + 3 * (2 * li + ph);
+    const unsigned grid = std::min<unsigned>(grid_for(D.n, 256), 148u * 32u);
+    VG_CHECK_CUDA(cudaMemsetAsync(st, 0, 3 * 8, ctx->stream));
+    VG_CHECK_CUDA(cudaMemcpyAsync(c->work, E.off, N * 4, cudaMemcpyDeviceToDevice, ctx->stream));
+    if (ph == 0)
+        k_edges<0, true><<<grid, 256, 0, ctx->stream>>>(D.ty, D.u, D.v, D.n, c->work, E.g, E.o, E.tk, E.off + N, E.cap_E, st);
+    else
+        k_edges<1, true><<<grid, 256, 0, ctx->stream>>>(D.ty, D.u, D.v, D.n, c->work, E.g, E.o, E.tk, E.off + N, E.cap_E, st);
+    VG_LAUNCHED(ctx);
+    // a key with more than LIGHT_MAX edges: at most cap_E / (LIGHT_MAX + 1) of them
+    VG_TRY(grow_u32(&E.medium, &E.cap_M, E.cap_E / (LIGHT_MAX + 1) + 1));
+    k_medium_keys<<<std::min<unsigned>(grid_for(N, 256), 148u * 32u), 256, 0, ctx->stream>>>(E.off, N, E.medium, E.cap_M, st);
+    VG_LAUNCHED(ctx);
+    return VG_OK;
+}
+
+// Enqueues the phase-1 and phase-2 edge sets of prover layer li (see
+// EdgeSet), without synchronising: the edge arrays are sized for one edge per
+// gate, and a set that needs more is rebuilt by finish_edges.
+static int launch_edges(vg_circuit *c, int li)
+{
+    vg_ctx *ctx = c->ctx;
+    DevLayer &D = c->L[li];
+    D.ph[0].ok = D.ph[1].ok = false;
+    D.ph[0].launched = D.ph[1].launched = false;
+    const char *mode = getenv("VIRGO_PHASE_TABLES");   // "atomic": keep the scatter path (tests compare both)
+    if (mode && !strcmp(mode, "atomic")) return VG_OK;
+    const long N = c->L[li - 1].n;
+    const unsigned grid = std::min<unsigned>(grid_for(D.n, 256), 148u * 32u);
+    const size_t work = (size_t)N + (size_t)vg_scan_tmp_words(N);
+    if (work > c->work_cap) {
+        VG_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+        cudaFree(c->work);
+        c->work = nullptr;
+        c->work_cap = 0;
+        if (cudaMalloc(&c->work, work * 4) != cudaSuccess) {
+            cudaGetLastError();
+            return vg_fail(VG_ERR_OOM, "edge build scratch");
+        }
+        c->work_cap = work;
+    }
+    for (int ph = 0; ph < 2; ++ph) {
+        EdgeSet &E = D.ph[ph];
+        E.N = N;
+        VG_TRY(grow_u32(&E.off, &E.cap_N, N + 1));
+        if (E.cap_E < D.n) VG_TRY(alloc_edges(E, D.n));
+        VG_CHECK_CUDA(cudaMemsetAsync(E.off, 0, (N + 1) * 4, ctx->stream));
+        if (ph == 0)
+            k_edges<0, false><<<grid, 256, 0, ctx->stream>>>(D.ty, D.u, D.v, D.n, E.off, nullptr, nullptr, nullptr, nullptr, 0,
+                                                            nullptr);
+        else
+            k_edges<1, false><<<grid, 256, 0, ctx->stream>>>(D.ty, D.u, D.v, D.n, E.off, nullptr, nullptr, nullptr, nullptr, 0,
+                                                            nullptr);
+        VG_LAUNCHED(ctx);
+        VG_TRY(vg_scan_u32(ctx, E.off, N, c->work + N));
+        VG_TRY(fill_edges(c, li, ph));
+        E.launched = true;
+    }
+    return VG_OK;
+}
+
+// Enqueues the edge sets of every layer and the copy of their counts to
+// c->edge_stats_host (valid after the stream is synchronised).
+static int launch_all_edges(vg_circuit *c)
+{
+    const int need = 3 * 2 * c->depth;
+    if (need > c->edge_stats_cap) {
+        cudaFree(c->edge_stats);
+        c->edge_stats = nullptr;
+        c->edge_stats_cap = 0;
+        if (cudaMalloc(&c->edge_stats, need * 8) != cudaSuccess) {
+            cudaGetLastError();
+            return vg_fail(VG_ERR_OOM, "edge statistics");
+        }
+        c->edge_stats_cap = need;
+    }
+    c->edge_stats_host.assign(need, 0);
+    VG_CHECK_CUDA(cudaMemsetAsync(c->edge_stats, 0, need * 8, c->ctx->stream));
+    for (int li = 1; li < c->depth; ++li) VG_TRY(launch_edges(c, li));
+    VG_CHECK_CUDA(cudaMemcpyAsync(c->edge_stats_host.data(), c->edge_stats, need * 8, cudaMemcpyDeviceToHost, c->ctx->stream));
+    return VG_OK;
+}
+
+// Reads the edge counts of every layer (the caller synchronised the stream
+// after stats_host was copied) and rebuilds the sets whose edges did not fit.
+static int finish_edges(vg_circuit *c, const unsigned long long *stats_host)
+{
+    bool refill = false;
+    for (int li = 1; li < c->depth; ++li)
+        for (int ph = 0; ph < 2; ++ph) {
+            EdgeSet &E = c->L[li].ph[ph];
+            const unsigned long long *st = stats_host + 3 * (2 * li + ph);
+            if (!E.launched) continue;
+            if (st[0] >= (1ull << 31)) {   // too many edges: atomic path
+                E.launched = false;
+                continue;
+            }
+            E.E = (long)st[0];
+            if (st[2]) {   // overflowed: exact size now known (rare: summation gates)
+                VG_TRY(alloc_edges(E, E.E));
+                refill = true;
+                E.ok = false;
+                continue;
+            }
+            E.n_medium = (long)st[1];
+            E.ok = true;
+        }
+    if (!refill) return VG_OK;
+    // the offsets are intact (the fill works on a copy): fill again with room
+    vg_ctx *ctx = c->ctx;
+    for (int li = 1; li < c->depth; ++li)
+        for (int ph = 0; ph < 2; ++ph) {
+            EdgeSet &E = c->L[li].ph[ph];
+            if (!E.launched || E.ok || E.cap_E < E.E || E.E >= (1L << 31)) continue;
+            VG_TRY(fill_edges(c, li, ph));
+            unsigned long long st[3];
+            VG_CHECK_CUDA(cudaMemcpyAsync(st, c->edge_stats + 3 * (2 * li + ph), 3 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            VG_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
+            if (st[2]) continue;   // still does not fit: atomic path
+            E.n_medium = (long)st[1];
+            E.ok = true;
+        }
+    return VG_OK;
+}
+
 extern "C" int vg_circuit_upload(vg_ctx *ctx, int depth, const int *bit_length, const uint8_t *const *ty,
                                  const int64_t *const *u, const int64_t *const *v, vg_circuit **out)
 {
@@ -547,6 +923,13 @@ extern "C" int vg_circuit_upload(vg_ctx *ctx, int depth, const int *bit_length, 
         cudaError_t e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) return fail(vg_fail(VG_ERR_CUDA, "circuit upload: %s", cudaGetErrorString(e)));
     }
+    int rc = launch_all_edges(c);
+    if (rc == VG_OK) {
+        cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) return fail(vg_fail(VG_ERR_CUDA, "circuit upload: %s", cudaGetErrorString(e)));
+        rc = finish_edges(c, c->edge_stats_host.data());
+    }
+    if (rc != VG_OK) return fail(rc);
     *out = c;
     return VG_OK;
 }
@@ -559,10 +942,19 @@ extern "C" int vg_circuit_destroy(vg_circuit *c)
         cudaFree(D.ty);
         cudaFree(D.u);
         cudaFree(D.v);
+        for (auto &E : D.ph) {
+            cudaFree(E.off);
+            cudaFree(E.g);
+            cudaFree(E.o);
+            cudaFree(E.tk);
+            cudaFree(E.medium);
+        }
     }
     cudaFree(c->input);
     cudaFree(c->staging);
     cudaFree(c->err);
+    cudaFree(c->work);
+    cudaFree(c->edge_stats);
     delete c;
     return VG_OK;
 }
@@ -687,6 +1079,10 @@ extern "C" int vg_circuit_build(vg_ctx *ctx, int d, const long *n, const uint8_t
             VG_LAUNCHED(ctx);
         }
     }
+    // edge sets from the checked wires (invalid gates became dummies), then one
+    // synchronisation for the error flag and the edge counts
+    rc = launch_all_edges(c);
+    if (rc != VG_OK) return fail(rc);
     unsigned long long e = 0;
     VG_CHECK_CUDA(cudaMemcpyAsync(&e, c->err, sizeof e, cudaMemcpyDeviceToHost, ctx->stream));
     VG_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -695,6 +1091,8 @@ extern "C" int vg_circuit_build(vg_ctx *ctx, int d, const long *n, const uint8_t
         const long gi = (long)(e & ((1ull << 40) - 1));
         return fail(vg_fail(VG_ERR_ARG, "file layer %d gate %ld: invalid type or wire", li == 0 ? 0 : li - 1, gi));
     }
+    rc = finish_edges(c, c->edge_stats_host.data());
+    if (rc != VG_OK) return fail(rc);
     if (bit_lengths)
         for (int i = 0; i < depth; ++i) bit_lengths[i] = bl[i];
     *inout = c;
@@ -899,6 +1297,40 @@ extern "C" int vg_eq_table(vg_ctx *c, const vg_fe *r, int log_len, vg_fe *pub)
 
 int vg_eq_table_async(vg_ctx *c, const vg_fe *r, int log_len, vg_fe *pub) { return eq_table(c, r, log_len, pub); }
 
+// the phase's tables (add_mult_sum in buf[0][2], addV_array in buf[0][1]) are
+// in place: the rounds start from them
+static int tables_ready(vg_gkr *g, long N)
+{
+    g->n = N;
+    g->cur[1] = g->buf[0][1];
+    g->cur[2] = g->buf[0][2];
+    g->next_buf = 1;
+    g->round0_pending = true;
+    return VG_OK;
+}
+
+// phase tables by gathering over the layer's edge set (no atomics, no finalize)
+template <int PH>
+static int gather_tables(vg_gkr *g, const EdgeSet &E, long N, const fe *prev)
+{
+    vg_ctx *c = g->ctx;
+    const EdgeView ev{E.off, E.g, E.o, E.tk};
+    fe *out_m = g->buf[0][2], *out_v = g->buf[0][1];
+    {
+        ProfScope ps(c, PH == 0 ? KF_SCATTER1 : KF_SCATTER2, 10.0 * (double)E.E + 4.0 * (double)N + 32.0 * (double)N);
+        k_gather_keys<PH><<<std::min<unsigned>(grid_for(N, GKR_THREADS), 148u * 64u), GKR_THREADS, 0, c->stream>>>(
+            ev, N, g->bg, g->bu, prev, g->vu, out_m, out_v);
+    }
+    VG_LAUNCHED(c);
+    if (E.n_medium) {
+        ProfScope ps(c, PH == 0 ? KF_SCATTER1 : KF_SCATTER2, 0.0);
+        k_gather_long<PH><<<std::min<unsigned>(grid_for(E.n_medium * 32, GKR_THREADS), 148u * 64u), GKR_THREADS, 0,
+                            c->stream>>>(ev, E.medium, E.n_medium, g->bg, g->bu, prev, g->vu, out_m, out_v);
+        VG_LAUNCHED(c);
+    }
+    return VG_OK;
+}
+
 static int finalize_tables(vg_gkr *g, long N)
 {
     vg_ctx *c = g->ctx;
@@ -914,12 +1346,7 @@ static int finalize_tables(vg_gkr *g, long N)
         k_acc_finalize<<<grid, 256, 0, c->stream>>>(g->acc + 4 * maxN, N, g->buf[0][1]);   // addV_array
     }
     VG_LAUNCHED(c);
-    g->n = N;
-    g->cur[1] = g->buf[0][1];
-    g->cur[2] = g->buf[0][2];
-    g->next_buf = 1;
-    g->round0_pending = true;
-    return VG_OK;
+    return tables_ready(g, N);
 }
 
 extern "C" int vg_gkr_phase1_init(vg_gkr *g, int layer, const vg_fe *r0, const vg_fe *r1, int length_g, vg_fe alpha,
@@ -946,6 +1373,11 @@ extern "C" int vg_gkr_phase1_init(vg_gkr *g, int layer, const vg_fe *r0, const v
     g->bg.s1 = e + 3 * H;
     g->bg.fh = fh;
     g->bg.mask = (1L << fh) - 1;
+    if (D.ph[0].ok) {
+        VG_TRY(gather_tables<0>(g, D.ph[0], N, g->vals[layer - 1]));
+        g->cur[0] = g->vals[layer - 1];
+        return tables_ready(g, N);
+    }
     VG_CHECK_CUDA(cudaMemsetAsync(g->acc, 0, N * 4 * sizeof(unsigned long long), c->stream));
     VG_CHECK_CUDA(cudaMemsetAsync(g->acc + 4 * maxN, 0, N * 4 * sizeof(unsigned long long), c->stream));
     unsigned grid = std::min<unsigned>(grid_for(D.n, GKR_THREADS), 148u * 32u);
@@ -976,6 +1408,12 @@ static int phase2_tables(vg_gkr *g, const vg_fe *r_u, int length_u)
     bu.s = e + g->eq_half;
     bu.fh = fh;
     bu.mask = (1L << fh) - 1;
+    g->bu = bu;
+    if (D.ph[1].ok) {
+        VG_TRY(gather_tables<1>(g, D.ph[1], N, nullptr));
+        g->cur[0] = g->vals[layer - 1];
+        return tables_ready(g, N);
+    }
     VG_CHECK_CUDA(cudaMemsetAsync(g->acc, 0, N * 4 * sizeof(unsigned long long), c->stream));
     VG_CHECK_CUDA(cudaMemsetAsync(g->acc + 4 * maxN, 0, N * 4 * sizeof(unsigned long long), c->stream));
     unsigned grid = std::min<unsigned>(grid_for(D.n, GKR_THREADS), 148u * 32u);
