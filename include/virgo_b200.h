@@ -71,6 +71,9 @@ int vg_ctx_launch_count(vg_ctx *ctx, long long *count);
  * 11 other.  Enabling resets the counters. */
 int vg_ctx_profile(vg_ctx *ctx, int enable);
 int vg_ctx_profile_read(vg_ctx *ctx, int family, long long *launches, double *ms, double *bytes);
+/* The profiled launches in launch order (family, device ms, algorithmic
+ * bytes), at most max of them; *n receives how many were recorded. */
+int vg_ctx_profile_trace(vg_ctx *ctx, int *family, double *ms, double *bytes, long max, long *n);
 /* Device time between two points of the context's stream. */
 int vg_timer_start(vg_ctx *ctx, void **timer);
 int vg_timer_stop(vg_ctx *ctx, void *timer, double *ms);

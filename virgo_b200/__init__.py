@@ -96,6 +96,7 @@ def lib():
             "vg_session_ctx": (c_i, [c_p, ctypes.POINTER(c_p)]),
             "vg_pc_query_batch": (c_i, [c_p, c_i, c_p, c_p, c_p, c_p, c_p]),
             "vg_ctx_profile": (c_i, [c_p, c_i]),
+            "vg_ctx_profile_trace": (c_i, [c_p, c_p, c_p, c_p, c_l, ctypes.POINTER(c_l)]),
             "vg_ctx_profile_read": (c_i, [c_p, c_i, ctypes.POINTER(ctypes.c_longlong), ctypes.POINTER(ctypes.c_double),
                                           ctypes.POINTER(ctypes.c_double)]),
             "vg_timer_start": (c_i, [c_p, ctypes.POINTER(c_p)]),

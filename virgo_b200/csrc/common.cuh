@@ -28,6 +28,10 @@ struct ProfRec {
     cudaEvent_t a, b;
     double bytes;
 };
+struct TraceRec {
+    int fam;
+    double ms, bytes;
+};
 
 struct vg_ctx {
     int device = 0;
@@ -48,6 +52,7 @@ struct vg_ctx {
     bool profiling = false;
     std::vector<ProfRec> prof;
     std::vector<cudaEvent_t> event_pool;
+    std::vector<TraceRec> trace;   // every profiled launch in order
     long long prof_launches[KF_COUNT] = {0};
     double prof_ms[KF_COUNT] = {0}, prof_bytes[KF_COUNT] = {0};
 };

@@ -1,3 +1,4 @@
+#include <algorithm>
 // Context, device memory, error reporting, elementwise field ops and the
 // generic partial-sum reduction.
 #include "common.cuh"
@@ -68,6 +69,7 @@ void vg_prof_end(vg_ctx *c, ProfRec *r, double bytes)
         for (auto &p : c->prof) {
             float ms = 0;
             cudaEventElapsedTime(&ms, p.a, p.b);
+            if (c->trace.size() < 1000000) c->trace.push_back({p.fam, ms, p.bytes});
             c->prof_launches[p.fam]++;
             c->prof_ms[p.fam] += ms;
             c->prof_bytes[p.fam] += p.bytes;
@@ -88,6 +90,7 @@ extern "C" int vg_ctx_profile(vg_ctx *c, int enable)
         c->event_pool.push_back(p.b);
     }
     c->prof.clear();
+    c->trace.clear();
     for (int k = 0; k < KF_COUNT; ++k) {
         c->prof_launches[k] = 0;
         c->prof_ms[k] = c->prof_bytes[k] = 0;
@@ -102,6 +105,7 @@ extern "C" int vg_ctx_profile_read(vg_ctx *c, int family, long long *launches, d
     for (auto &p : c->prof) {
         float t = 0;
         cudaEventElapsedTime(&t, p.a, p.b);
+        if (c->trace.size() < 1000000) c->trace.push_back({p.fam, t, p.bytes});
         c->prof_launches[p.fam]++;
         c->prof_ms[p.fam] += t;
         c->prof_bytes[p.fam] += p.bytes;
@@ -112,6 +116,20 @@ extern "C" int vg_ctx_profile_read(vg_ctx *c, int family, long long *launches, d
     if (launches) *launches = c->prof_launches[family];
     if (ms) *ms = c->prof_ms[family];
     if (bytes) *bytes = c->prof_bytes[family];
+    return VG_OK;
+}
+
+extern "C" int vg_ctx_profile_trace(vg_ctx *c, int *family, double *ms, double *bytes, long max, long *n)
+{
+    if (!c || !n) return vg_fail(VG_ERR_ARG, "vg_ctx_profile_trace: null argument");
+    VG_TRY(vg_ctx_profile_read(c, 0, nullptr, nullptr, nullptr));   // resolves pending events
+    const long k = std::min<long>(max, (long)c->trace.size());
+    for (long i = 0; i < k; ++i) {
+        if (family) family[i] = c->trace[i].fam;
+        if (ms) ms[i] = c->trace[i].ms;
+        if (bytes) bytes[i] = c->trace[i].bytes;
+    }
+    *n = (long)c->trace.size();
     return VG_OK;
 }
 

@@ -25,6 +25,7 @@
 #include "common.cuh"
 #include "internal.h"
 #include <algorithm>
+#include <mutex>
 #include <cstring>
 
 namespace {
@@ -493,6 +494,171 @@ __global__ void __launch_bounds__(GKR_THREADS) k_gather_long(EdgeView e, const u
     }
 }
 
+// --------------------------------------------------- chunked round groups
+// Round folds only combine neighbouring entries, so a CTA that owns a
+// contiguous chunk of the three tables can run several consecutive rounds on
+// it without any other CTA: a chunk of 2 RG_CHUNK entries folds into shared
+// memory (RG_CHUNK entries) and keeps folding there until two entries are
+// left, i.e. up to 11 rounds per launch.  The challenges of all those rounds
+// are known in advance (they come from the verifier's rand() stream), so one
+// launch replaces up to 11 round launches and each table is read from HBM
+// once per group instead of once per round.  Per-round partial sums are
+// reduced by the last CTA to finish; every round's sums go to its record.
+constexpr int RG_LOG = 10, RG_CHUNK = 1 << RG_LOG, RG_THREADS = 256, RG_MAX = 12;
+// shared-memory index of table entry i: one pad entry per 8 keeps the
+// stride-4 reads (entries 4k .. 4k+3 of a pair) and the stride-2 writes free
+// of bank conflicts
+__device__ __forceinline__ int rg_ix(long i) { return (int)(i + (i >> 3)); }
+constexpr int RG_TABLE = RG_CHUNK + RG_CHUNK / 8;
+struct RoundGroup {
+    int nsteps;         // rounds in this launch
+    int first_nofold;   // the first round has no fold (the round right after a phase init)
+    int slot0;          // record of the first round; the others follow
+    int last6;          // write the final pair (the table ends at 2 entries) into the last record
+    fe r[RG_MAX];       // fold challenge of each round
+};
+
+__device__ __forceinline__ fe rg_fold(fe x0, fe x1, fe r) { return x0 + r * (x1 - x0); }
+
+__device__ __forceinline__ void rg_sums(fe v0, fe v1, fe a0, fe a1, fe m0, fe m1, fe (&acc)[3])
+{
+    const fe va = v1 - v0, ma = m1 - m0;
+    const fe p2 = ma * va, p0 = m0 * v0, p1 = m1 * v1;
+    acc[0] = acc[0] + p2;
+    acc[1] = acc[1] + ((p1 - p0 - p2) + (a1 - a0));
+    acc[2] = acc[2] + p0 + a0;
+}
+
+// warp sums of acc into sm[step][warp][3]; warps without an active lane
+// (first thread >= active) only store zeros
+__device__ __forceinline__ void rg_warp_store(fe (&acc)[3], fe *sm, int step, long active)
+{
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if ((long)(threadIdx.x & ~31) < active) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) acc[k] = warp_sum(acc[k]);
+    }
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < 3; ++k) sm[(step * (RG_THREADS / 32) + wid) * 3 + k] = acc[k];
+    }
+}
+
+__global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict__ xV, const fe *__restrict__ xA,
+                                                            const fe *__restrict__ xM, long n_in, RoundGroup G,
+                                                            fe *__restrict__ yV, fe *__restrict__ yA, fe *__restrict__ yM,
+                                                            fe *__restrict__ parts, unsigned *__restrict__ counter,
+                                                            fe *__restrict__ rec)
+{
+    extern __shared__ fe smem[];
+    fe *sV = smem, *sA = smem + RG_TABLE, *sM = smem + 2 * RG_TABLE;
+    fe *wsum = smem + 3 * RG_TABLE;   // [RG_MAX][warps][3]
+    __shared__ bool last;
+    const int t = threadIdx.x;
+    // first step: from global into shared
+    const long cin = G.first_nofold ? min(n_in, (long)RG_CHUNK) : min(n_in, 2L * RG_CHUNK);
+    const long base = (long)blockIdx.x * cin;
+    long m = G.first_nofold ? cin : cin / 2;   // entries in shared after the first step
+    {
+        fe acc[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+        const fe r = G.r[0];
+        for (long k = t; k < m / 2; k += RG_THREADS) {
+            fe v0, v1, a0, a1, m0, m1;
+            if (G.first_nofold) {
+                const long b = base + 2 * k;
+                v0 = xV[b]; v1 = xV[b + 1];
+                a0 = xA[b]; a1 = xA[b + 1];
+                m0 = xM[b]; m1 = xM[b + 1];
+            } else {
+                const long b = base + 4 * k;
+                v0 = rg_fold(xV[b], xV[b + 1], r); v1 = rg_fold(xV[b + 2], xV[b + 3], r);
+                a0 = rg_fold(xA[b], xA[b + 1], r); a1 = rg_fold(xA[b + 2], xA[b + 3], r);
+                m0 = rg_fold(xM[b], xM[b + 1], r); m1 = rg_fold(xM[b + 2], xM[b + 3], r);
+            }
+            const int i0 = rg_ix(2 * k), i1 = rg_ix(2 * k + 1);
+            sV[i0] = v0; sV[i1] = v1;
+            sA[i0] = a0; sA[i1] = a1;
+            sM[i0] = m0; sM[i1] = m1;
+            rg_sums(v0, v1, a0, a1, m0, m1, acc);
+        }
+        rg_warp_store(acc, wsum, 0, m / 2);
+    }
+    // further steps in shared memory: fold m -> m/2, sums over m/4 pairs
+    for (int st = 1; st < G.nsteps; ++st) {
+        const fe r = G.r[st];
+        fe acc[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+        fe v0, v1, a0, a1, m0, m1;
+        const long npairs = m / 4;
+        __syncthreads();
+        const bool act = t < npairs;   // m / 4 <= RG_CHUNK / 4 = RG_THREADS: at most one pair per thread
+        if (act) {
+            const int b0 = rg_ix(4 * t), b1 = rg_ix(4 * t + 1), b2 = rg_ix(4 * t + 2), b3 = rg_ix(4 * t + 3);
+            v0 = rg_fold(sV[b0], sV[b1], r); v1 = rg_fold(sV[b2], sV[b3], r);
+            a0 = rg_fold(sA[b0], sA[b1], r); a1 = rg_fold(sA[b2], sA[b3], r);
+            m0 = rg_fold(sM[b0], sM[b1], r); m1 = rg_fold(sM[b2], sM[b3], r);
+            rg_sums(v0, v1, a0, a1, m0, m1, acc);
+        }
+        __syncthreads();
+        if (act) {
+            const int i0 = rg_ix(2 * t), i1 = rg_ix(2 * t + 1);
+            sV[i0] = v0; sV[i1] = v1;
+            sA[i0] = a0; sA[i1] = a1;
+            sM[i0] = m0; sM[i1] = m1;
+        }
+        m >>= 1;
+        rg_warp_store(acc, wsum, st, npairs);
+    }
+    __syncthreads();
+    // the chunk's remaining m entries (none when the group folded nothing)
+    for (long k = t; yV && k < m; k += RG_THREADS) {
+        yV[(long)blockIdx.x * m + k] = sV[rg_ix(k)];
+        yA[(long)blockIdx.x * m + k] = sA[rg_ix(k)];
+        yM[(long)blockIdx.x * m + k] = sM[rg_ix(k)];
+    }
+    // CTA partials per round
+    constexpr int NW = RG_THREADS / 32;
+    if ((t & 31) < 3) {
+        const int k = t & 31;
+        for (int st = t >> 5; st < G.nsteps; st += NW) {
+            fe x = vg::fe_zero();
+            for (int w = 0; w < NW; ++w) x = x + wsum[(st * NW + w) * 3 + k];
+            parts[((long)st * gridDim.x + blockIdx.x) * 3 + k] = x;
+        }
+    }
+    if (G.last6 && gridDim.x == 1 && m == 2 && t == 0) {
+        fe *l6 = rec + 9 * (G.slot0 + G.nsteps - 1) + 3;
+        l6[0] = sV[0]; l6[1] = sV[1]; l6[2] = sA[0]; l6[3] = sA[1]; l6[4] = sM[0]; l6[5] = sM[1];   // rg_ix(0, 1) = 0, 1
+    }
+    __threadfence();
+    __syncthreads();
+    if (t == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    // warp st sums round st over all CTAs
+    const int wid = t >> 5, lane = t & 31;
+    for (int st = wid; st < G.nsteps; st += NW) {
+        fe tot[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+        for (long b = lane; b < gridDim.x; b += 32) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                const fe *p = &parts[((long)st * gridDim.x + b) * 3 + k];
+                fe x;
+                x.img = __ldcg(&p->img);
+                x.real = __ldcg(&p->real);
+                tot[k] = tot[k] + x;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k) tot[k] = warp_sum(tot[k]);
+        if (lane == 0) {
+            fe *o = rec + 9 * (G.slot0 + st);
+            o[0] = tot[0]; o[1] = tot[1]; o[2] = tot[2];
+        }
+    }
+    if (t == 0) *counter = 0;
+}
+
 // v_u = V(r_u) + mask term: the folded V pair of the last phase-1 round at r
 // (zk_prover.cpp:796-797), computed where the pair is, so phase 2 can start
 // without the host reading it first
@@ -689,7 +855,15 @@ struct vg_gkr {
     int rec_cap = 0, rec_n = 0;
     fe *rec_host = nullptr;              // pinned
     int rec_host_cap = 0;
+    // deferred rounds not yet launched: they run as one k_round_group
+    std::vector<fe> pend_r;
+    int pend_slot0 = 0;
+    long pend_n0 = 0;                    // table length before the group's first round
+    bool pend_nofold = false;
+    fe *rg_parts = nullptr;              // per-CTA, per-round partial sums of a group
 };
+
+static int flush_rounds(vg_gkr *g);
 
 // ------------------------------------------------------------------ circuit
 static int grow_u32(uint32_t **p, long *cap, long n)
@@ -1134,6 +1308,7 @@ extern "C" int vg_gkr_create(vg_ctx *ctx, const vg_circuit *c, vg_gkr **out)
     if (cudaMalloc(&g->round_out, 16 * sizeof(fe)) != cudaSuccess) return fail("round sums");
     if (cudaMalloc(&g->round_counter, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
     if (cudaMalloc(&g->vu, sizeof(fe)) != cudaSuccess) return fail("v_u");
+    if (cudaMalloc(&g->rg_parts, (N / RG_CHUNK + 1) * RG_MAX * 3 * sizeof(fe)) != cudaSuccess) return fail("group partials");
     if (cudaMemset(g->round_counter, 0, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
     *out = g;
     return VG_OK;
@@ -1153,6 +1328,7 @@ extern "C" int vg_gkr_destroy(vg_gkr *g)
     cudaFree(g->round_out);
     cudaFree(g->round_counter);
     cudaFree(g->vu);
+    cudaFree(g->rg_parts);
     cudaFree(g->rec);
     if (g->rec_host) cudaFreeHost(g->rec_host);
     delete g;
@@ -1210,6 +1386,7 @@ extern "C" int vg_gkr_v_res(vg_gkr *g, const vg_fe *r, int r_len, vg_fe *out)
     const int last = g->C->depth - 1;
     if (r_len != g->C->L[last].bl) return vg_fail(VG_ERR_ARG, "r_len %d != output bit length %d", r_len, g->C->L[last].bl);
     vg_ctx *c = g->ctx;
+    VG_TRY(flush_rounds(g));
     VG_TRY(upload_r(g, 0, r, r_len));
     fe *lo = g->eq, *hi = g->eq + g->eq_half;
     int fh;
@@ -1353,6 +1530,7 @@ extern "C" int vg_gkr_phase1_init(vg_gkr *g, int layer, const vg_fe *r0, const v
                                   vg_fe beta)
 {
     if (!g || !r0 || !r1) return vg_fail(VG_ERR_ARG, "vg_gkr_phase1_init: null argument");
+    VG_TRY(flush_rounds(g));
     if (layer < 1 || layer >= g->C->depth) return vg_fail(VG_ERR_ARG, "layer %d out of range", layer);
     if (length_g != g->C->L[layer].bl) return vg_fail(VG_ERR_ARG, "length_g %d != layer bit length %d", length_g, g->C->L[layer].bl);
     vg_ctx *c = g->ctx;
@@ -1390,6 +1568,68 @@ extern "C" int vg_gkr_phase1_init(vg_gkr *g, int layer, const vg_fe *r0, const v
     VG_LAUNCHED(c);
     g->cur[0] = g->vals[layer - 1];
     return finalize_tables(g, N);
+}
+
+// Rounds a group starting at table length n0 can hold (see k_round_group).
+static int group_capacity(long n0, bool nofold)
+{
+    const long m0 = nofold ? std::min(n0, (long)RG_CHUNK) : std::min(n0, 2L * RG_CHUNK) / 2;
+    int k = 0;
+    while ((1L << (k + 1)) <= m0) ++k;
+    return std::min(k, RG_MAX);
+}
+
+static int rg_smem_attribute(int dev)
+{
+    static std::mutex mu;
+    static std::vector<bool> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= (int)done.size()) done.resize(dev + 1, false);
+    if (!done[dev]) {
+        VG_CHECK_CUDA(cudaFuncSetAttribute(k_round_group, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)((3 * RG_TABLE + RG_MAX * (RG_THREADS / 32) * 3) * sizeof(fe))));
+        done[dev] = true;
+    }
+    return VG_OK;
+}
+
+// Launches the pending deferred rounds as one group (a single CTA: the
+// group starts when the table fits one chunk).
+static int flush_rounds(vg_gkr *g)
+{
+    if (g->pend_r.empty()) return VG_OK;
+    vg_ctx *c = g->ctx;
+    RoundGroup G{};
+    G.nsteps = (int)g->pend_r.size();
+    G.first_nofold = g->pend_nofold ? 1 : 0;
+    G.slot0 = g->pend_slot0;
+    for (int i = 0; i < G.nsteps; ++i) G.r[i] = g->pend_r[i];
+    const long n_in = g->pend_n0;
+    const long cin = G.first_nofold ? std::min(n_in, (long)RG_CHUNK) : std::min(n_in, 2L * RG_CHUNK);
+    const long grid = n_in / cin;
+    const long m_final = (G.first_nofold ? cin : cin / 2) >> (G.nsteps - 1);
+    G.last6 = (grid == 1 && m_final == 2) ? 1 : 0;
+    const bool folds = !(G.first_nofold && G.nsteps == 1);
+    fe *y[3] = {g->buf[g->next_buf][0], g->buf[g->next_buf][1], g->buf[g->next_buf][2]};
+    const size_t smem = (3 * RG_TABLE + RG_MAX * (RG_THREADS / 32) * 3) * sizeof(fe);
+    VG_TRY(rg_smem_attribute(c->device));
+    {
+        // every round of the group: the first reads 3 tables of n_in, writes nothing more than the chunk tails
+        ProfScope ps(c, KF_ROUND, 48.0 * (double)n_in + (folds ? 48.0 * (double)(grid * m_final) : 0.0));
+        k_round_group<<<(unsigned)grid, RG_THREADS, smem, c->stream>>>(g->cur[0], g->cur[1], g->cur[2], n_in, G,
+                                                                      folds ? y[0] : nullptr, folds ? y[1] : nullptr,
+                                                                      folds ? y[2] : nullptr, g->rg_parts,
+                                                                      g->round_counter, g->rec);
+    }
+    VG_LAUNCHED(c);
+    if (folds) {
+        g->cur[0] = y[0];
+        g->cur[1] = y[1];
+        g->cur[2] = y[2];
+        g->next_buf ^= 1;
+    }
+    g->pend_r.clear();
+    return VG_OK;
 }
 
 // phase-2 tables for the current layer once g->vu holds v_u
@@ -1430,6 +1670,7 @@ static int phase2_tables(vg_gkr *g, const vg_fe *r_u, int length_u)
 static int phase2_check(vg_gkr *g, const vg_fe *r_u, int length_u)
 {
     if (!g || !r_u) return vg_fail(VG_ERR_ARG, "vg_gkr_phase2_init: null argument");
+    VG_TRY(flush_rounds(g));
     if (g->layer < 1) return vg_fail(VG_ERR_STATE, "phase2_init before phase1_init");
     if (length_u != g->C->L[g->layer - 1].bl)
         return vg_fail(VG_ERR_ARG, "length_u %d != previous layer bit length %d", length_u, g->C->L[g->layer - 1].bl);
@@ -1457,6 +1698,8 @@ int vg_gkr_phase2_init_deferred(vg_gkr *g, const vg_fe *r_u, int length_u, vg_fe
 int vg_gkr_defer(vg_gkr *g, int on)
 {
     if (!g) return vg_fail(VG_ERR_ARG, "null gkr");
+    VG_TRY(flush_rounds(g));
+    g->pend_r.clear();
     g->deferred = on != 0;
     g->rec_n = 0;
     if (!on) return VG_OK;
@@ -1479,6 +1722,7 @@ int vg_gkr_defer(vg_gkr *g, int on)
 int vg_gkr_records(vg_gkr *g, const vg_fe **host, int *n)
 {
     if (!g || !host || !n) return vg_fail(VG_ERR_ARG, "vg_gkr_records: null argument");
+    VG_TRY(flush_rounds(g));
     if (g->rec_n > g->rec_host_cap) {
         VG_CHECK_CUDA(cudaStreamSynchronize(g->ctx->stream));
         if (g->rec_host) cudaFreeHost(g->rec_host);
@@ -1504,6 +1748,24 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
     if (!fold && !g->round0_pending) return vg_fail(VG_ERR_STATE, "current_bit 0 only directly after an init");
     if (fold && g->round0_pending) return vg_fail(VG_ERR_STATE, "first round after an init must have current_bit 0");
     if (fold && g->n < 4) return vg_fail(VG_ERR_STATE, "no variables left to fold");
+    // deferred: once the table fits one CTA's chunk, the remaining rounds of
+    // the phase are queued and run as one single-CTA group; larger tables run
+    // one round per launch (their rounds are throughput bound, the group
+    // kernel's serial in-CTA steps are not)
+    const long lim = fold ? 2L * RG_CHUNK : (long)RG_CHUNK;
+    if (g->deferred && (!g->pend_r.empty() || g->n <= lim)) {
+        if (g->pend_r.empty()) {
+            g->pend_n0 = g->n;
+            g->pend_nofold = !fold;
+            g->pend_slot0 = g->rec_n;
+        }
+        g->pend_r.push_back(tofe(previous_random));
+        ++g->rec_n;
+        if (fold) g->n /= 2;
+        g->round0_pending = false;
+        if ((int)g->pend_r.size() >= group_capacity(g->pend_n0, g->pend_nofold)) VG_TRY(flush_rounds(g));
+        return VG_OK;
+    }
     vg_ctx *c = g->ctx;
     const long n_out = fold ? g->n / 2 : g->n;   // table length the sums are taken over
     const long npairs = n_out / 2;
