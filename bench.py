@@ -317,6 +317,118 @@ def ours(args, layers, rank, world):
             "launches": n_launch, "stages": {k: v / args.steps for k, v in stages.items()}, "h2d": h2d, "d2h": d2h}
 
 
+# ------------------------------------------------- batched and served forms
+def _pctl(xs, q):
+    xs = sorted(xs)
+    if not xs:
+        return None
+    k = min(len(xs) - 1, max(0, int(round(q * (len(xs) - 1)))))
+    return xs[k]
+
+
+def batched_random(count, seed, slots):
+    """Random layered circuits (per circuit a depth in 8..32, per layer a width
+    2^12..2^20, add/mult p = 0.5) proved through the server all at once, and
+    the same circuits proved one after another on one session (the plain
+    form).  Both are wall clock and include the circuit upload."""
+    import virgo_b200 as vb
+    from virgo_b200 import circuits
+    batch = circuits.random_batch(count, seed)
+    gates = int(sum(circuits.total_gates(c) for c in batch))
+    # pin the wire arrays as uint32 once, as a client would hold them
+    prepared = [[(t, u, v) if i == 0 else (t, u.astype(np.uint32), v.astype(np.uint32)) for i, (t, u, v) in enumerate(c)]
+                for c in batch]
+    s = vb.Session(batch[0])
+    try:
+        s.load(prepared[0], index_bytes=4)
+        s.prove(1, transcript=False)   # warm-up
+        t0 = time.perf_counter()
+        for k, c in enumerate(prepared):
+            s.load(c, index_bytes=4)
+            s.prove(100 + k, transcript=True)
+        t_plain = time.perf_counter() - t0
+    finally:
+        s.close()
+    srv = vb.Server(slots=slots)
+    try:
+        warm = [srv.submit(c, 1, transcript=False) for c in prepared[:slots]]
+        for j in warm:
+            srv.wait(j)
+        t0 = time.perf_counter()
+        jobs = [srv.submit(c, 100 + k) for k, c in enumerate(prepared)]
+        for j in jobs:
+            srv.wait(j)
+        t_batch = time.perf_counter() - t0
+    finally:
+        srv.close()
+    return {"value": count / t_batch, "unit": "proofs/s", "plain_value": count / t_plain,
+            "speedup_vs_plain": round(t_plain / t_batch, 3), "circuits": count, "total_gates": gates,
+            "slots": slots, "workload": "random layered circuits, depth U(8,32), widths 2^U(12,20), seed %d" % seed,
+            "timing": "wall clock, circuit upload + proof + transcript download per job"}
+
+
+def served(n_jobs, seed, slots, rate_factor=3.0):
+    """Poisson arrivals of jobs mixing 2^14-, 2^18- and 2^22-gate random
+    layered circuits (depth 16).  The arrival rate is rate_factor x the
+    plain form's throughput on the same mix; the server (continuous
+    batching) and a one-slot server (the plain form with a queue) see the
+    same arrival times.  Latency = submit to transcript on the host."""
+    import threading as th
+    import virgo_b200 as vb
+    from virgo_b200 import circuits
+    rng = np.random.default_rng(seed)
+    pool = {g: [circuits.random_by_gates(g, 16, seed=1000 * g + i) for i in range(3)] for g in (14, 18, 22)}
+    pool = {g: [[(t, u, v) if i == 0 else (t, u.astype(np.uint32), v.astype(np.uint32)) for i, (t, u, v) in enumerate(c)]
+                for c in cs] for g, cs in pool.items()}
+    kinds = rng.choice([14, 18, 22], size=n_jobs)
+    picks = [pool[int(g)][int(rng.integers(3))] for g in kinds]
+
+    def run(nslots, times):
+        srv = vb.Server(slots=nslots)
+        lat, done_at = [], []
+        try:
+            for c in list(pool[22]) + list(pool[18]):   # warm every slot on the largest shapes
+                srv.wait(srv.submit(c, 1, transcript=False))
+            ids = [None] * n_jobs
+            t0 = time.perf_counter()
+
+            def feeder():
+                for k in range(n_jobs):
+                    dt = t0 + times[k] - time.perf_counter()
+                    if dt > 0:
+                        time.sleep(dt)
+                    ids[k] = srv.submit(picks[k], 500 + k)
+
+            f = th.Thread(target=feeder)
+            f.start()
+            for k in range(n_jobs):
+                while ids[k] is None:
+                    time.sleep(0.0005)
+                info, _ = srv.wait(ids[k])
+                lat.append(info.latency_s)
+                done_at.append(time.perf_counter() - t0)
+            f.join()
+        finally:
+            srv.close()
+        return lat, max(done_at)
+
+    # the plain form's service rate on this mix (one job at a time)
+    lat1, span1 = run(1, np.zeros(n_jobs))
+    plain_rate = n_jobs / span1
+    rate = rate_factor * plain_rate
+    times = np.cumsum(rng.exponential(1.0 / rate, size=n_jobs))
+    lat_s, span_s = run(slots, times)
+    lat_p, span_p = run(1, times)
+    return {"value": n_jobs / span_s, "unit": "proofs/s", "p50_ms": 1000 * _pctl(lat_s, 0.5),
+            "p99_ms": 1000 * _pctl(lat_s, 0.99),
+            "plain": {"value": n_jobs / span_p, "p50_ms": 1000 * _pctl(lat_p, 0.5), "p99_ms": 1000 * _pctl(lat_p, 0.99),
+                      "saturated_value": plain_rate},
+            "arrival_rate": rate, "jobs": n_jobs, "slots": slots,
+            "workload": "Poisson arrivals at %.1fx the plain form's rate; random layered circuits of 2^14, 2^18, "
+                        "2^22 gates, depth 16, equal shares" % rate_factor,
+            "timing": "wall clock, submit to transcript on the host (circuit upload included)"}
+
+
 def barrier(world):
     if world > 1:
         import torch.distributed as dist
@@ -355,6 +467,7 @@ def main():
     ap.add_argument("--workload", choices=["matmul256", "matmul16"], default="matmul256")
     ap.add_argument("--batch", type=int, default=8, help="proofs in flight at once (one stream each)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-served", action="store_true", help="skip the batched-random and served measurements")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -403,6 +516,9 @@ def main():
             "stages_s": r["stages"],
             "kernel_families": fam,
         }
+        if not args.no_served and world == 1:
+            line["batched_random64"] = batched_random(64, seed=4, slots=args.batch)
+            line["served"] = served(48, seed=5, slots=args.batch)
         if not args.no_cpu_baseline and world >= 1 and os.path.exists(REF_BIN):
             tmp = tempfile.mkdtemp(prefix="virgo_circ_")
             c, m = os.path.join(tmp, "c.txt"), os.path.join(tmp, "m.txt")

@@ -148,6 +148,10 @@ int vg_circuit_depth(const vg_circuit *c, int *depth);
  * (zk_prover::init_array, zk_prover.cpp:337-350). */
 int vg_gkr_create(vg_ctx *ctx, const vg_circuit *c, vg_gkr **out);
 int vg_gkr_destroy(vg_gkr *g);
+/* Points an existing GKR state at another circuit on the same context; its
+ * device tables are reused and only grow when the circuit needs more (no
+ * reference counterpart: the reference allocates per zk_prover). */
+int vg_gkr_rebind(vg_gkr *g, const vg_circuit *c);
 /* All layer values (zk_prover::evaluate, zk_prover.cpp:54-157). */
 int vg_gkr_evaluate(vg_gkr *g);
 /* Device pointer to the 2^bit_length values of a layer (after evaluate). */
@@ -301,6 +305,35 @@ int vg_session_prove(vg_session *s, unsigned seed, int want_transcript, vg_proof
  * stats, transcripts and transcript_lens have n entries (or are NULL). */
 int vg_session_prove_batch(vg_session *const *ss, int n, const unsigned *seeds, int want_transcript,
                            vg_proof_stats *stats, uint8_t **transcripts, size_t *transcript_lens);
+/* A session with a context and no circuit yet (vg_session_load gives it one). */
+int vg_session_new(vg_session **out);
+
+/* ---- proof server (no reference counterpart: the reference proves one
+ * circuit per process).  Continuous batching on one GPU: `slots` worker
+ * sessions, each on its own stream, take queued jobs in arrival order as
+ * they become free and as the job's device footprint fits hbm_budget bytes
+ * (0: 90% of the free memory) next to what the other workers hold.  A job is
+ * a circuit in the vg_session_load layout plus a seed; the arrays must stay
+ * valid until vg_server_wait returns for that job.  Its transcript equals
+ * the one vg_session_prove gives for the same circuit and seed. */
+typedef struct vg_server vg_server;
+typedef struct {
+    int status;             /* VG_OK or the job's error code */
+    double queued_s;        /* submit -> a worker took it */
+    double run_s;           /* load + prove */
+    double latency_s;       /* submit -> done */
+    size_t footprint;       /* device bytes the admission reserved */
+    vg_proof_stats stats;
+} vg_job_info;
+/* Device bytes a session needs for a circuit with file-layer widths n. */
+size_t vg_job_footprint(int d, const long *n);
+int vg_server_create(int device, int slots, size_t hbm_budget, vg_server **out);
+int vg_server_submit(vg_server *s, int d, const long *n, const uint8_t *const *ty, const void *const *u,
+                     const void *const *v, int index_bytes, unsigned seed, int want_transcript, long long *job_id);
+/* Blocks until the job is done; *transcript (free with vg_free) as for
+ * vg_session_prove.  Returns the job's status. */
+int vg_server_wait(vg_server *s, long long job_id, vg_job_info *info, uint8_t **transcript, size_t *transcript_len);
+int vg_server_destroy(vg_server *s);
 /* The context (stream) a session runs on. */
 int vg_session_ctx(vg_session *s, vg_ctx **out);
 void vg_free(void *p);

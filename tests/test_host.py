@@ -115,3 +115,25 @@ def test_glibc_random_r_reproduces_rand():
             libc.random_r(buf, ctypes.byref(out))
             b.append(out.value)
         assert a == b
+
+
+def test_job_footprint_is_monotone_and_covers_the_matmul(built):
+    f = vb.job_footprint
+    small, big = f([1 << 14] * 4), f([1 << 17, 1 << 24, 1 << 23])
+    assert 0 < small < big
+    assert f([1 << 17, 1 << 20]) < f([1 << 17, 1 << 21]) < f([1 << 18, 1 << 21])
+    # tables + codewords of the 2^24-gate matmul (measured about 3.4 GB per session)
+    assert 3.4e9 < big < 8e9
+
+
+def test_random_batch_shapes():
+    cs = circuits.random_batch(5, seed=3, log_width_range=(4, 6), depth_range=(2, 4))
+    assert len(cs) == 5
+    for c in cs:
+        assert 2 <= len(c) <= 4
+        prev = len(c[0][0])
+        for t, u, v in c[1:]:
+            assert 16 <= len(t) <= 64 and u.max() < prev and v.max() < prev
+            prev = len(t)
+    c = circuits.random_by_gates(14, 16, seed=1)
+    assert len(c) == 16 and circuits.total_gates(c) == 1 << 14

@@ -39,6 +39,11 @@ class vg_proof_stats(ctypes.Structure):
     ]
 
 
+class vg_job_info(ctypes.Structure):
+    _fields_ = [("status", ctypes.c_int), ("queued_s", ctypes.c_double), ("run_s", ctypes.c_double),
+                ("latency_s", ctypes.c_double), ("footprint", ctypes.c_size_t), ("stats", vg_proof_stats)]
+
+
 def lib():
     """Loads the library (raises VirgoError when it has not been built)."""
     global _lib
@@ -93,6 +98,15 @@ def lib():
                                        ctypes.POINTER(c_p), ctypes.POINTER(c_sz)]),
             "vg_session_fork": (c_i, [c_p, ctypes.POINTER(c_p)]),
             "vg_session_prove_batch": (c_i, [c_p, c_i, c_p, c_i, c_p, c_p, c_p]),
+            "vg_session_new": (c_i, [ctypes.POINTER(c_p)]),
+            "vg_gkr_rebind": (c_i, [c_p, c_p]),
+            "vg_job_footprint": (c_sz, [c_i, c_p]),
+            "vg_server_create": (c_i, [c_i, c_i, c_sz, ctypes.POINTER(c_p)]),
+            "vg_server_submit": (c_i, [c_p, c_i, c_p, c_p, c_p, c_p, c_i, ctypes.c_uint, c_i,
+                                       ctypes.POINTER(ctypes.c_longlong)]),
+            "vg_server_wait": (c_i, [c_p, ctypes.c_longlong, ctypes.POINTER(vg_job_info), ctypes.POINTER(c_p),
+                                     ctypes.POINTER(c_sz)]),
+            "vg_server_destroy": (c_i, [c_p]),
             "vg_session_ctx": (c_i, [c_p, ctypes.POINTER(c_p)]),
             "vg_pc_query_batch": (c_i, [c_p, c_i, c_p, c_p, c_p, c_p, c_p]),
             "vg_ctx_profile": (c_i, [c_p, c_i]),
@@ -240,18 +254,8 @@ class Session:
         """Replaces the circuit (device buffers reused when it fits).  layers
         are (ty, u, v) arrays; with index_bytes=4 the wires of layers >= 1 are
         passed as uint32 (the input layer's u, its values, stay int64)."""
-        d = len(layers)
-        ns = np.array([len(t) for t, _, _ in layers], dtype=np.int64)
-        keep = [ns]
-        tys, us, vs = (ctypes.c_void_p * d)(), (ctypes.c_void_p * d)(), (ctypes.c_void_p * d)()
-        for i, (t, u, v) in enumerate(layers):
-            dt = np.int64 if (i == 0 or index_bytes == 8) else np.uint32
-            t = t if isinstance(t, np.ndarray) and t.dtype == np.uint8 and t.flags.c_contiguous else np.ascontiguousarray(t, np.uint8)
-            u = u if getattr(u, "dtype", None) == dt and u.flags.c_contiguous else np.ascontiguousarray(u, dt)
-            v = v if getattr(v, "dtype", None) == dt and v.flags.c_contiguous else np.ascontiguousarray(v, dt)
-            keep += [t, u, v]
-            tys[i], us[i], vs[i] = t.ctypes.data, u.ctypes.data, v.ctypes.data
-        check(lib().vg_session_load(self.h, d, ptr(ns), tys, us, vs, index_bytes), "vg_session_load")
+        ns, tys, us, vs, keep = _layer_arrays(layers, index_bytes)
+        check(lib().vg_session_load(self.h, len(layers), ptr(ns), tys, us, vs, index_bytes), "vg_session_load")
 
     def fork(self) -> "Session":
         """A session on the same (shared) device circuit with its own stream."""
@@ -287,6 +291,64 @@ def prove_batch(sessions, seeds, transcript: bool = True):
         lib().vg_free(bufs[i])
         out.append((st[i], data))
     return out
+
+
+def _layer_arrays(layers, index_bytes):
+    """(n, ty*, u*, v*, keep) for the vg_session_load layout"""
+    d = len(layers)
+    ns = np.array([len(t) for t, _, _ in layers], dtype=np.int64)
+    keep = [ns]
+    tys, us, vs = (ctypes.c_void_p * d)(), (ctypes.c_void_p * d)(), (ctypes.c_void_p * d)()
+    for i, (t, u, v) in enumerate(layers):
+        dt = np.int64 if (i == 0 or index_bytes == 8) else np.uint32
+        t = t if isinstance(t, np.ndarray) and t.dtype == np.uint8 and t.flags.c_contiguous else np.ascontiguousarray(t, np.uint8)
+        u = u if getattr(u, "dtype", None) == dt and u.flags.c_contiguous else np.ascontiguousarray(u, dt)
+        v = v if getattr(v, "dtype", None) == dt and v.flags.c_contiguous else np.ascontiguousarray(v, dt)
+        keep += [t, u, v]
+        tys[i], us[i], vs[i] = t.ctypes.data, u.ctypes.data, v.ctypes.data
+    keep += [tys, us, vs]
+    return ns, tys, us, vs, keep
+
+
+def job_footprint(widths) -> int:
+    """Device bytes a proof of a circuit with these file-layer widths needs."""
+    ns = np.ascontiguousarray(widths, dtype=np.int64)
+    return int(lib().vg_job_footprint(len(ns), ns.ctypes.data))
+
+
+class Server:
+    """Continuous-batching proof server on one GPU (vg_server_*): jobs are
+    taken in arrival order by `slots` worker sessions as they free up and as
+    their device footprint fits the HBM budget."""
+
+    def __init__(self, slots: int = 8, device: int = 0, hbm_budget: int = 0):
+        self.h = ctypes.c_void_p()
+        check(lib().vg_server_create(device, slots, hbm_budget, ctypes.byref(self.h)), "vg_server_create")
+        self._keep = {}
+
+    def submit(self, layers, seed: int, transcript: bool = True, index_bytes: int = 4) -> int:
+        ns, tys, us, vs, keep = _layer_arrays(layers, index_bytes)
+        jid = ctypes.c_longlong()
+        check(lib().vg_server_submit(self.h, len(layers), ns.ctypes.data, tys, us, vs, index_bytes, seed,
+                                     1 if transcript else 0, ctypes.byref(jid)), "vg_server_submit")
+        self._keep[jid.value] = keep   # the arrays must live until the job is done
+        return jid.value
+
+    def wait(self, job: int):
+        info = vg_job_info()
+        buf, n = ctypes.c_void_p(), ctypes.c_size_t()
+        rc = lib().vg_server_wait(self.h, job, ctypes.byref(info), ctypes.byref(buf), ctypes.byref(n))
+        data = ctypes.string_at(buf, n.value) if n.value else b""
+        lib().vg_free(buf)
+        self._keep.pop(job, None)
+        check(rc, "vg_server_wait")
+        return info, data
+
+    def close(self):
+        if self.h:
+            lib().vg_server_destroy(self.h)
+            self.h = None
+            self._keep.clear()
 
 
 def header_functions(path: str = HEADER) -> list:

@@ -62,6 +62,27 @@ def random_layered(log_widths: list, seed: int, p_mult: float = 0.5, input_bits:
     return layers
 
 
+def random_batch(count: int, seed: int, log_width_range=(12, 20), depth_range=(8, 32), p_mult: float = 0.5) -> list:
+    """Independent random layered circuits: per circuit a depth uniform in
+    depth_range, per layer a width 2^k with k uniform in log_width_range,
+    gates add/mult with probability p_mult, wires uniform over the previous
+    layer, 31-bit inputs."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for c in range(count):
+        depth = int(rng.integers(depth_range[0], depth_range[1] + 1))
+        lw = [int(x) for x in rng.integers(log_width_range[0], log_width_range[1] + 1, size=depth)]
+        out.append(random_layered(lw, seed=int(rng.integers(1 << 31)), p_mult=p_mult))
+    return out
+
+
+def random_by_gates(total_log: int, depth: int, seed: int, p_mult: float = 0.5) -> list:
+    """A random layered circuit of 2^total_log gates spread evenly over
+    `depth` layers (the input layer included)."""
+    lw = max(1, total_log - int(np.log2(depth)))
+    return random_layered([lw] * depth, seed=seed, p_mult=p_mult)
+
+
 def mixed_gates(seed: int, log_width: int = 6) -> list:
     """Every gate type the reference proves in interior layers (0-2, 5-10,
     12, 13; type 3 constants are only evaluated, zk_prover.cpp:581-584 has no

@@ -190,18 +190,10 @@ struct DevBuf {
 static int ensure(vg_ctx *c, DevBuf &b, size_t bytes)
 {
     if (bytes <= b.cap) return VG_OK;
-    if (b.p) {
-        cudaStreamSynchronize(c->stream);
-        cudaFree(b.p);
-    }
+    vg_release(c, b.p);   // stream ordered: no device-wide synchronisation
     b.p = nullptr;
     b.cap = 0;
-    cudaError_t e = cudaMalloc(&b.p, bytes);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        b.p = nullptr;
-        return vg_fail(VG_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
-    }
+    VG_TRY(vg_alloc(c, &b.p, bytes));
     b.cap = bytes;
     return VG_OK;
 }

@@ -48,6 +48,9 @@ struct vg_ctx {
     size_t partials_cap = 0;
     fe *pinned = nullptr;    // pinned host staging for small results
     size_t pinned_cap = 0;
+    // pinned ring for uploads from pageable host memory (vg_h2d_staged)
+    char *ring[2] = {nullptr, nullptr};
+    cudaEvent_t ring_ev[2] = {nullptr, nullptr};
     // per-launch profiler: event pairs around launches of each kernel family
     bool profiling = false;
     std::vector<ProfRec> prof;
@@ -99,6 +102,18 @@ int vg_fail(int code, const char *fmt, ...);
             return vg_fail(VG_ERR_CUDA, "%s:%d launch: %s", __FILE__, __LINE__,             \
                            cudaGetErrorString(e_));                                        \
     } while (0)
+
+// Host-to-device copy on the context stream.  Pageable sources go through the
+// context's two pinned chunks (host memcpy of one chunk overlaps the DMA of
+// the other), so concurrent sessions do not serialise on the driver's
+// staging.  A pageable source may be reused on return; a pinned or device
+// source is copied directly and must stay valid until the stream reaches the
+// copy.
+int vg_h2d_staged(vg_ctx *c, void *dst, const void *src, size_t bytes);
+
+// stream-ordered device memory from the device pool (see ctx.cu)
+int vg_alloc(vg_ctx *c, void **p, size_t bytes);
+void vg_release(vg_ctx *c, void *p);
 
 // scratch buffers owned by the context; contents do not survive other calls
 int vg_scratch(vg_ctx *ctx, size_t bytes, void **p);

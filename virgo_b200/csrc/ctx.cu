@@ -1,3 +1,4 @@
+#include <cstring>
 #include <algorithm>
 // Context, device memory, error reporting, elementwise field ops and the
 // generic partial-sum reduction.
@@ -199,6 +200,10 @@ extern "C" int vg_ctx_destroy(vg_ctx *c)
     if (c->scratch2) cudaFree(c->scratch2);
     if (c->partials) cudaFree(c->partials);
     if (c->pinned) cudaFreeHost(c->pinned);
+    for (int k = 0; k < 2; ++k) {
+        if (c->ring[k]) cudaFreeHost(c->ring[k]);
+        if (c->ring_ev[k]) cudaEventDestroy(c->ring_ev[k]);
+    }
     cudaStreamDestroy(c->stream);
     delete c;
     return VG_OK;
@@ -239,41 +244,98 @@ extern "C" int vg_ctx_launch_count(vg_ctx *c, long long *count)
     return VG_OK;
 }
 
-static int grow(void **p, size_t *cap, size_t bytes)
+// Stream-ordered allocations from the device's default memory pool.  The
+// pool keeps freed blocks (its release threshold is raised once per device),
+// so growing a buffer neither synchronises the device, as cudaFree does, nor
+// returns memory to the driver between proofs.
+static int pool_setup(int dev)
 {
-    if (bytes <= *cap) return VG_OK;
-    if (*p) cudaFree(*p);
-    *p = nullptr;
-    *cap = 0;
-    cudaError_t e = cudaMalloc(p, bytes);
+    static std::mutex mu;
+    static std::vector<bool> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= (int)done.size()) done.resize(dev + 1, false);
+    if (done[dev]) return VG_OK;
+    cudaMemPool_t pool;
+    VG_CHECK_CUDA(cudaDeviceGetDefaultMemPool(&pool, dev));
+    uint64_t thr = ~0ull;
+    VG_CHECK_CUDA(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr));
+    done[dev] = true;
+    return VG_OK;
+}
+
+int vg_alloc(vg_ctx *c, void **p, size_t bytes)
+{
+    VG_TRY(pool_setup(c->device));
+    cudaError_t e = cudaMallocAsync(p, bytes ? bytes : 16, c->stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         *p = nullptr;
-        return vg_fail(VG_ERR_OOM, "cudaMalloc(%zu): %s", bytes, cudaGetErrorString(e));
+        return vg_fail(VG_ERR_OOM, "device allocation of %zu bytes: %s", bytes, cudaGetErrorString(e));
     }
+    return VG_OK;
+}
+
+void vg_release(vg_ctx *c, void *p)
+{
+    if (p) cudaFreeAsync(p, c->stream);
+}
+
+constexpr size_t RING_CHUNK = 8u << 20;
+
+int vg_h2d_staged(vg_ctx *c, void *dst, const void *src, size_t bytes)
+{
+    if (!bytes) return VG_OK;
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, src) == cudaSuccess && a.type != cudaMemoryTypeUnregistered) {
+        VG_CHECK_CUDA(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, c->stream));
+        return VG_OK;   // pinned or device source: in flight until the stream gets there
+    }
+    cudaGetLastError();
+    if (!c->ring[0]) {
+        for (int k = 0; k < 2; ++k) {
+            VG_CHECK_CUDA(cudaMallocHost((void **)&c->ring[k], RING_CHUNK));
+            VG_CHECK_CUDA(cudaEventCreateWithFlags(&c->ring_ev[k], cudaEventDisableTiming));
+            VG_CHECK_CUDA(cudaEventRecord(c->ring_ev[k], c->stream));
+        }
+    }
+    int k = 0;
+    for (size_t off = 0; off < bytes; off += RING_CHUNK, k ^= 1) {
+        const size_t len = std::min(RING_CHUNK, bytes - off);
+        VG_CHECK_CUDA(cudaEventSynchronize(c->ring_ev[k]));   // the chunk's previous copy is done
+        memcpy(c->ring[k], (const char *)src + off, len);
+        VG_CHECK_CUDA(cudaMemcpyAsync((char *)dst + off, c->ring[k], len, cudaMemcpyHostToDevice, c->stream));
+        VG_CHECK_CUDA(cudaEventRecord(c->ring_ev[k], c->stream));
+    }
+    return VG_OK;
+}
+
+static int grow(vg_ctx *c, void **p, size_t *cap, size_t bytes)
+{
+    if (bytes <= *cap) return VG_OK;
+    vg_release(c, *p);
+    *p = nullptr;
+    *cap = 0;
+    VG_TRY(vg_alloc(c, p, bytes));
     *cap = bytes;
     return VG_OK;
 }
 
 int vg_scratch(vg_ctx *c, size_t bytes, void **p)
 {
-    if (bytes > c->scratch_cap) VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
-    VG_TRY(grow(&c->scratch, &c->scratch_cap, bytes));
+    VG_TRY(grow(c, &c->scratch, &c->scratch_cap, bytes));
     *p = c->scratch;
     return VG_OK;
 }
 int vg_scratch2(vg_ctx *c, size_t bytes, void **p)
 {
-    if (bytes > c->scratch2_cap) VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
-    VG_TRY(grow(&c->scratch2, &c->scratch2_cap, bytes));
+    VG_TRY(grow(c, &c->scratch2, &c->scratch2_cap, bytes));
     *p = c->scratch2;
     return VG_OK;
 }
 int vg_partials(vg_ctx *c, size_t n, fe **p)
 {
-    if (n * sizeof(fe) > c->partials_cap) VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
     void *q = c->partials;
-    VG_TRY(grow(&q, &c->partials_cap, n * sizeof(fe)));
+    VG_TRY(grow(c, &q, &c->partials_cap, n * sizeof(fe)));
     c->partials = (fe *)q;
     *p = c->partials;
     return VG_OK;

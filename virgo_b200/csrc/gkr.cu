@@ -809,7 +809,8 @@ __global__ void k_build_layer(const uint8_t *__restrict__ ty_in, const IDX *__re
 }  // namespace
 
 struct vg_circuit {
-    vg_ctx *ctx = nullptr;
+    vg_ctx *ctx = nullptr;     // the context it was built on (may be gone when forks outlive it)
+    int device = 0;
     int depth = 0;
     int max_bl = 0;
     std::vector<DevLayer> L;
@@ -830,7 +831,9 @@ struct vg_circuit {
 struct vg_gkr {
     vg_ctx *ctx = nullptr;
     const vg_circuit *C = nullptr;
-    std::vector<fe *> vals;
+    std::vector<fe *> vals;              // per layer, into vals_slab (layer 0: the circuit's input)
+    fe *vals_slab = nullptr;
+    long vals_cap = 0, N_cap = 0, acc_cap = 0;
     fe *buf[2][3] = {{nullptr, nullptr, nullptr}, {nullptr, nullptr, nullptr}};   // ping-pong V, AV, AM
     unsigned long long *acc = nullptr;   // 2 tables x 4 words x 2^max_bl
     fe *eq = nullptr;                    // half tables
@@ -866,35 +869,29 @@ struct vg_gkr {
 static int flush_rounds(vg_gkr *g);
 
 // ------------------------------------------------------------------ circuit
-static int grow_u32(uint32_t **p, long *cap, long n)
+static int grow_u32(vg_ctx *c, uint32_t **p, long *cap, long n)
 {
     if (n <= *cap) return VG_OK;
-    cudaFree(*p);
+    vg_release(c, *p);
     *p = nullptr;
     *cap = 0;
-    if (cudaMalloc(p, (size_t)std::max(n, 1L) * 4) != cudaSuccess) {
-        cudaGetLastError();
-        *p = nullptr;
-        return vg_fail(VG_ERR_OOM, "edge arrays (%ld words)", n);
-    }
+    VG_TRY(vg_alloc(c, (void **)p, (size_t)std::max(n, 1L) * 4));
     *cap = n;
     return VG_OK;
 }
 
-static int alloc_edges(EdgeSet &E, long n)
+static int alloc_edges(vg_ctx *c, EdgeSet &E, long n)
 {
-    cudaFree(E.g);
-    cudaFree(E.o);
-    cudaFree(E.tk);
+    vg_release(c, E.g);
+    vg_release(c, E.o);
+    vg_release(c, E.tk);
     E.g = E.o = nullptr;
     E.tk = nullptr;
     E.cap_E = 0;
     n = std::max(n, 1L);
-    if (cudaMalloc(&E.g, (size_t)n * 4) != cudaSuccess || cudaMalloc(&E.o, (size_t)n * 4) != cudaSuccess ||
-        cudaMalloc(&E.tk, (size_t)n * 2) != cudaSuccess) {
-        cudaGetLastError();
-        return vg_fail(VG_ERR_OOM, "edge arrays (%ld edges)", n);
-    }
+    VG_TRY(vg_alloc(c, (void **)&E.g, (size_t)n * 4));
+    VG_TRY(vg_alloc(c, (void **)&E.o, (size_t)n * 4));
+    VG_TRY(vg_alloc(c, (void **)&E.tk, (size_t)n * 2));
     E.cap_E = n;
     return VG_OK;
 }
@@ -917,7 +914,7 @@ static int fill_edges(vg_circuit *c, int li, int ph)
         k_edges<1, true><<<grid, 256, 0, ctx->stream>>>(D.ty, D.u, D.v, D.n, c->work, E.g, E.o, E.tk, E.off + N, E.cap_E, st);
     VG_LAUNCHED(ctx);
     // a key with more than LIGHT_MAX edges: at most cap_E / (LIGHT_MAX + 1) of them
-    VG_TRY(grow_u32(&E.medium, &E.cap_M, E.cap_E / (LIGHT_MAX + 1) + 1));
+    VG_TRY(grow_u32(ctx, &E.medium, &E.cap_M, E.cap_E / (LIGHT_MAX + 1) + 1));
     k_medium_keys<<<std::min<unsigned>(grid_for(N, 256), 148u * 32u), 256, 0, ctx->stream>>>(E.off, N, E.medium, E.cap_M, st);
     VG_LAUNCHED(ctx);
     return VG_OK;
@@ -938,21 +935,17 @@ static int launch_edges(vg_circuit *c, int li)
     const unsigned grid = std::min<unsigned>(grid_for(D.n, 256), 148u * 32u);
     const size_t work = (size_t)N + (size_t)vg_scan_tmp_words(N);
     if (work > c->work_cap) {
-        VG_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
-        cudaFree(c->work);
+        vg_release(ctx, c->work);
         c->work = nullptr;
         c->work_cap = 0;
-        if (cudaMalloc(&c->work, work * 4) != cudaSuccess) {
-            cudaGetLastError();
-            return vg_fail(VG_ERR_OOM, "edge build scratch");
-        }
+        VG_TRY(vg_alloc(ctx, (void **)&c->work, work * 4));
         c->work_cap = work;
     }
     for (int ph = 0; ph < 2; ++ph) {
         EdgeSet &E = D.ph[ph];
         E.N = N;
-        VG_TRY(grow_u32(&E.off, &E.cap_N, N + 1));
-        if (E.cap_E < D.n) VG_TRY(alloc_edges(E, D.n));
+        VG_TRY(grow_u32(ctx, &E.off, &E.cap_N, N + 1));
+        if (E.cap_E < D.n) VG_TRY(alloc_edges(ctx, E, D.n));
         VG_CHECK_CUDA(cudaMemsetAsync(E.off, 0, (N + 1) * 4, ctx->stream));
         if (ph == 0)
             k_edges<0, false><<<grid, 256, 0, ctx->stream>>>(D.ty, D.u, D.v, D.n, E.off, nullptr, nullptr, nullptr, nullptr, 0,
@@ -974,13 +967,10 @@ static int launch_all_edges(vg_circuit *c)
 {
     const int need = 3 * 2 * c->depth;
     if (need > c->edge_stats_cap) {
-        cudaFree(c->edge_stats);
+        vg_release(c->ctx, c->edge_stats);
         c->edge_stats = nullptr;
         c->edge_stats_cap = 0;
-        if (cudaMalloc(&c->edge_stats, need * 8) != cudaSuccess) {
-            cudaGetLastError();
-            return vg_fail(VG_ERR_OOM, "edge statistics");
-        }
+        VG_TRY(vg_alloc(c->ctx, (void **)&c->edge_stats, need * 8));
         c->edge_stats_cap = need;
     }
     c->edge_stats_host.assign(need, 0);
@@ -1006,7 +996,7 @@ static int finish_edges(vg_circuit *c, const unsigned long long *stats_host)
             }
             E.E = (long)st[0];
             if (st[2]) {   // overflowed: exact size now known (rare: summation gates)
-                VG_TRY(alloc_edges(E, E.E));
+                VG_TRY(alloc_edges(c->ctx, E, E.E));
                 refill = true;
                 E.ok = false;
                 continue;
@@ -1060,6 +1050,7 @@ extern "C" int vg_circuit_upload(vg_ctx *ctx, int depth, const int *bit_length, 
     }
     vg_circuit *c = new vg_circuit();
     c->ctx = ctx;
+    c->device = ctx->device;
     c->depth = depth;
     c->L.resize(depth);
     auto fail = [&](int rc) { vg_circuit_destroy(c); return rc; };
@@ -1111,7 +1102,12 @@ extern "C" int vg_circuit_upload(vg_ctx *ctx, int depth, const int *bit_length, 
 extern "C" int vg_circuit_destroy(vg_circuit *c)
 {
     if (!c) return VG_OK;
-    cudaStreamSynchronize(c->ctx->stream);
+    // not through c->ctx: forked sessions may release the circuit after the
+    // context that built it is gone
+    int cur = 0;
+    cudaGetDevice(&cur);
+    cudaSetDevice(c->device);
+    cudaDeviceSynchronize();
     for (auto &D : c->L) {
         cudaFree(D.ty);
         cudaFree(D.u);
@@ -1129,21 +1125,18 @@ extern "C" int vg_circuit_destroy(vg_circuit *c)
     cudaFree(c->err);
     cudaFree(c->work);
     cudaFree(c->edge_stats);
+    cudaSetDevice(cur);
     delete c;
     return VG_OK;
 }
 
-static int grow_dev(void **p, size_t *cap, size_t bytes)
+static int grow_dev(vg_ctx *c, void **p, size_t *cap, size_t bytes)
 {
     if (bytes <= *cap) return VG_OK;
-    cudaFree(*p);
+    vg_release(c, *p);
     *p = nullptr;
     *cap = 0;
-    if (cudaMalloc(p, bytes) != cudaSuccess) {
-        cudaGetLastError();
-        *p = nullptr;
-        return vg_fail(VG_ERR_OOM, "cudaMalloc(%zu) failed", bytes);
-    }
+    VG_TRY(vg_alloc(c, p, bytes));
     *cap = bytes;
     return VG_OK;
 }
@@ -1175,6 +1168,7 @@ extern "C" int vg_circuit_build(vg_ctx *ctx, int d, const long *n, const uint8_t
         c->ctx = ctx;
     }
     c->ctx = ctx;
+    c->device = ctx->device;
     c->depth = depth;
     c->max_bl = 0;
     c->L.resize(depth);
@@ -1195,22 +1189,22 @@ extern "C" int vg_circuit_build(vg_ctx *ctx, int d, const long *n, const uint8_t
         c->max_bl = std::max(c->max_bl, D.bl);
         if (i == 0) {
             size_t capb = c->input_cap * sizeof(fe);
-            int rc = grow_dev((void **)&c->input, &capb, D.n * sizeof(fe));
+            int rc = grow_dev(ctx, (void **)&c->input, &capb, D.n * sizeof(fe));
             if (rc != VG_OK) return fail(rc);
             c->input_cap = (long)(capb / sizeof(fe));
             continue;
         }
         if (c->cap[i] < D.n) {
-            cudaFree(D.ty);
-            cudaFree(D.u);
-            cudaFree(D.v);
+            vg_release(ctx, D.ty);
+            vg_release(ctx, D.u);
+            vg_release(ctx, D.v);
             D.ty = nullptr;
             D.u = D.v = nullptr;
-            if (cudaMalloc(&D.ty, D.n) != cudaSuccess || cudaMalloc(&D.u, D.n * 4) != cudaSuccess ||
-                cudaMalloc(&D.v, D.n * 4) != cudaSuccess) {
-                cudaGetLastError();
-                return fail(vg_fail(VG_ERR_OOM, "circuit layer %d allocation", i));
-            }
+            c->cap[i] = 0;
+            int rc = vg_alloc(ctx, (void **)&D.ty, D.n);
+            if (rc == VG_OK) rc = vg_alloc(ctx, (void **)&D.u, D.n * 4);
+            if (rc == VG_OK) rc = vg_alloc(ctx, (void **)&D.v, D.n * 4);
+            if (rc != VG_OK) return fail(rc);
             c->cap[i] = D.n;
         }
     }
@@ -1218,7 +1212,7 @@ extern "C" int vg_circuit_build(vg_ctx *ctx, int d, const long *n, const uint8_t
     long nmax = 0;
     for (int i = 0; i < d; ++i) nmax = std::max(nmax, n[i]);
     const size_t stage_b = ((size_t)nmax + 255) / 256 * 256 + 2 * (size_t)nmax * 8;
-    int rc = grow_dev(&c->staging, &c->staging_cap, stage_b);
+    int rc = grow_dev(ctx, &c->staging, &c->staging_cap, stage_b);
     if (rc != VG_OK) return fail(rc);
     const unsigned grid_cap = 148u * 32u;
     for (int fi = 0; fi < d; ++fi) {
@@ -1227,9 +1221,9 @@ extern "C" int vg_circuit_build(vg_ctx *ctx, int d, const long *n, const uint8_t
         uint8_t *sty = (uint8_t *)c->staging;
         char *su = (char *)c->staging + ((size_t)nmax + 255) / 256 * 256;
         char *sv = su + (size_t)nmax * 8;
-        VG_CHECK_CUDA(cudaMemcpyAsync(sty, ty[fi], cnt, cudaMemcpyHostToDevice, ctx->stream));
-        VG_CHECK_CUDA(cudaMemcpyAsync(su, u[fi], cnt * wb, cudaMemcpyHostToDevice, ctx->stream));
-        if (fi > 0) VG_CHECK_CUDA(cudaMemcpyAsync(sv, v[fi], cnt * wb, cudaMemcpyHostToDevice, ctx->stream));
+        VG_TRY(vg_h2d_staged(ctx, sty, ty[fi], cnt));
+        VG_TRY(vg_h2d_staged(ctx, su, u[fi], cnt * wb));
+        if (fi > 0) VG_TRY(vg_h2d_staged(ctx, sv, v[fi], cnt * wb));
         if (fi == 0) {
             const long width = c->L[0].n;
             k_build_input<<<std::min<unsigned>(grid_for(width, 256), grid_cap), 256, 0, ctx->stream>>>(
@@ -1281,44 +1275,109 @@ extern "C" int vg_circuit_depth(const vg_circuit *c, int *depth)
 }
 
 // ---------------------------------------------------------------------- GKR
+// Points g at circuit c, reusing every buffer that is large enough (a server
+// proving circuits of changing shapes then allocates only when one grows,
+// and cudaFree's device-wide synchronisation stays out of the proofs).
+static int gkr_bind(vg_gkr *g, const vg_circuit *c)
+{
+    auto oom = [&](const char *what) {
+        cudaGetLastError();
+        return vg_fail(VG_ERR_OOM, "vg_gkr: %s allocation failed", what);
+    };
+    long total = 0;
+    for (int i = 1; i < c->depth; ++i) total += c->L[i].n;
+    vg_ctx *x = g->ctx;
+    if (total > g->vals_cap) {
+        vg_release(x, g->vals_slab);
+        g->vals_slab = nullptr;
+        g->vals_cap = 0;
+        if (vg_alloc(x, (void **)&g->vals_slab, total * sizeof(fe)) != VG_OK) return oom("layer values");
+        g->vals_cap = total;
+    }
+    g->vals.assign(c->depth, nullptr);
+    g->vals[0] = c->input;
+    long off = 0;
+    for (int i = 1; i < c->depth; ++i) {
+        g->vals[i] = g->vals_slab + off;
+        off += c->L[i].n;
+    }
+    const long N = 1L << c->max_bl;
+    if (N > g->N_cap) {
+        for (int b = 0; b < 2; ++b)
+            for (int k = 0; k < 3; ++k) {
+                vg_release(x, g->buf[b][k]);
+                g->buf[b][k] = nullptr;
+            }
+        vg_release(x, g->eq);
+        vg_release(x, g->rg_parts);
+        g->eq = g->rg_parts = nullptr;
+        g->N_cap = 0;
+        for (int b = 0; b < 2; ++b)
+            for (int k = 0; k < 3; ++k)
+                if (vg_alloc(x, (void **)&g->buf[b][k], (b == 0 ? N : N / 2 + 1) * sizeof(fe)) != VG_OK) return oom("tables");
+        if (vg_alloc(x, (void **)&g->eq, 6 * (1L << (c->max_bl / 2 + 1)) * sizeof(fe)) != VG_OK) return oom("eq tables");
+        if (vg_alloc(x, (void **)&g->rg_parts, (N / RG_CHUNK + 1) * RG_MAX * 3 * sizeof(fe)) != VG_OK)
+            return oom("group partials");
+        g->N_cap = N;
+    }
+    g->C = c;
+    g->eq_half = 1L << (c->max_bl / 2 + 1);
+    g->layer = -1;
+    g->n = 0;
+    g->round0_pending = false;
+    g->pend_r.clear();
+    return VG_OK;
+}
+
+// the 2 x 4 x N accumulators of the atomic scatter path, on first use
+static int ensure_acc(vg_gkr *g, long N)
+{
+    if (N <= g->acc_cap) return VG_OK;
+    vg_release(g->ctx, g->acc);
+    g->acc = nullptr;
+    g->acc_cap = 0;
+    VG_TRY(vg_alloc(g->ctx, (void **)&g->acc, 2 * 4 * N * sizeof(unsigned long long)));
+    g->acc_cap = N;
+    return VG_OK;
+}
+
 extern "C" int vg_gkr_create(vg_ctx *ctx, const vg_circuit *c, vg_gkr **out)
 {
     if (!ctx || !c || !out) return vg_fail(VG_ERR_ARG, "vg_gkr_create: null argument");
     vg_gkr *g = new vg_gkr();
     g->ctx = ctx;
-    g->C = c;
-    g->vals.assign(c->depth, nullptr);
-    const long N = 1L << c->max_bl;
     auto fail = [&](const char *what) {
         cudaGetLastError();
         vg_gkr_destroy(g);
         return vg_fail(VG_ERR_OOM, "vg_gkr_create: %s allocation failed", what);
     };
-    for (int i = 1; i < c->depth; ++i)
-        if (cudaMalloc(&g->vals[i], c->L[i].n * sizeof(fe)) != cudaSuccess) return fail("layer values");
-    g->vals[0] = c->input;
-    for (int b = 0; b < 2; ++b)
-        for (int k = 0; k < 3; ++k)
-            if (cudaMalloc(&g->buf[b][k], (b == 0 ? N : N / 2 + 1) * sizeof(fe)) != cudaSuccess) return fail("tables");
-    if (cudaMalloc(&g->acc, 2 * 4 * N * sizeof(unsigned long long)) != cudaSuccess) return fail("accumulators");
-    g->eq_half = 1L << (c->max_bl / 2 + 1);
-    if (cudaMalloc(&g->eq, 6 * g->eq_half * sizeof(fe)) != cudaSuccess) return fail("eq tables");
     if (cudaMalloc(&g->rbuf, 3 * 64 * sizeof(fe)) != cudaSuccess) return fail("challenges");
     if (cudaMalloc(&g->round_parts, 3 * 148 * 8 * sizeof(fe)) != cudaSuccess) return fail("round partials");
     if (cudaMalloc(&g->round_out, 16 * sizeof(fe)) != cudaSuccess) return fail("round sums");
     if (cudaMalloc(&g->round_counter, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
     if (cudaMalloc(&g->vu, sizeof(fe)) != cudaSuccess) return fail("v_u");
-    if (cudaMalloc(&g->rg_parts, (N / RG_CHUNK + 1) * RG_MAX * 3 * sizeof(fe)) != cudaSuccess) return fail("group partials");
     if (cudaMemset(g->round_counter, 0, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
+    int rc = gkr_bind(g, c);
+    if (rc != VG_OK) {
+        vg_gkr_destroy(g);
+        return rc;
+    }
     *out = g;
     return VG_OK;
+}
+
+extern "C" int vg_gkr_rebind(vg_gkr *g, const vg_circuit *c)
+{
+    if (!g || !c) return vg_fail(VG_ERR_ARG, "vg_gkr_rebind: null argument");
+    VG_TRY(flush_rounds(g));
+    return gkr_bind(g, c);
 }
 
 extern "C" int vg_gkr_destroy(vg_gkr *g)
 {
     if (!g) return VG_OK;
     cudaStreamSynchronize(g->ctx->stream);
-    for (size_t i = 1; i < g->vals.size(); ++i) cudaFree(g->vals[i]);
+    cudaFree(g->vals_slab);
     for (int b = 0; b < 2; ++b)
         for (int k = 0; k < 3; ++k) cudaFree(g->buf[b][k]);
     cudaFree(g->acc);
@@ -1556,6 +1615,7 @@ extern "C" int vg_gkr_phase1_init(vg_gkr *g, int layer, const vg_fe *r0, const v
         g->cur[0] = g->vals[layer - 1];
         return tables_ready(g, N);
     }
+    VG_TRY(ensure_acc(g, maxN));
     VG_CHECK_CUDA(cudaMemsetAsync(g->acc, 0, N * 4 * sizeof(unsigned long long), c->stream));
     VG_CHECK_CUDA(cudaMemsetAsync(g->acc + 4 * maxN, 0, N * 4 * sizeof(unsigned long long), c->stream));
     unsigned grid = std::min<unsigned>(grid_for(D.n, GKR_THREADS), 148u * 32u);
@@ -1654,6 +1714,7 @@ static int phase2_tables(vg_gkr *g, const vg_fe *r_u, int length_u)
         g->cur[0] = g->vals[layer - 1];
         return tables_ready(g, N);
     }
+    VG_TRY(ensure_acc(g, maxN));
     VG_CHECK_CUDA(cudaMemsetAsync(g->acc, 0, N * 4 * sizeof(unsigned long long), c->stream));
     VG_CHECK_CUDA(cudaMemsetAsync(g->acc + 4 * maxN, 0, N * 4 * sizeof(unsigned long long), c->stream));
     unsigned grid = std::min<unsigned>(grid_for(D.n, GKR_THREADS), 148u * 32u);
@@ -1706,14 +1767,10 @@ int vg_gkr_defer(vg_gkr *g, int on)
     // one record per round (at most 2 x 32 per layer) plus v_res
     const int need = 64 * g->C->depth + 16;
     if (need > g->rec_cap) {
-        VG_CHECK_CUDA(cudaStreamSynchronize(g->ctx->stream));
-        cudaFree(g->rec);
+        vg_release(g->ctx, g->rec);
         g->rec = nullptr;
         g->rec_cap = 0;
-        if (cudaMalloc(&g->rec, (size_t)need * 9 * sizeof(fe)) != cudaSuccess) {
-            cudaGetLastError();
-            return vg_fail(VG_ERR_OOM, "deferred records");
-        }
+        VG_TRY(vg_alloc(g->ctx, (void **)&g->rec, (size_t)need * 9 * sizeof(fe)));
         g->rec_cap = need;
     }
     return VG_OK;

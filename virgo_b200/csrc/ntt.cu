@@ -120,7 +120,26 @@ __global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(PassArgs a)
     __syncthreads();
 
     // ---- radix-2 DIT stages ----
-    for (int s = 0; s < a.lm; ++s) {
+    // stage 0 multiplies by w^0 = 1 and stage 1 by 1 or w_m^(m/4), the
+    // square root of -1, which is +-i in F_p2 (i^2 = -1): no products there
+    for (int s = 0; s < a.lm && s < 2; ++s) {
+        const int half = 1 << s;
+        for (int b = threadIdx.x; b < (mg >> 1); b += blockDim.x) {
+            const int g = b & (G - 1), q = b >> a.logG;
+            const int pos = q & (half - 1), grp = q >> s;
+            const int i0 = (grp << (s + 1)) + pos, i1 = i0 + half;
+            fe x0 = S[(i0 << a.logG) + g];
+            fe x1 = S[(i1 << a.logG) + g];
+            if (pos) {   // times T[m/4] = +-i: (x.real + i x.img) i = -x.img + i x.real
+                const fe w = T[pos << (a.lm - 1 - s)];
+                x1 = w.img == 1 ? vg::fe_make(vg::negp(x1.img), x1.real) : vg::fe_make(x1.img, vg::negp(x1.real));
+            }
+            S[(i0 << a.logG) + g] = x0 + x1;
+            S[(i1 << a.logG) + g] = x0 - x1;
+        }
+        __syncthreads();
+    }
+    for (int s = 2; s < a.lm; ++s) {
         const int half = 1 << s;
         for (int b = threadIdx.x; b < (mg >> 1); b += blockDim.x) {
             const int g = b & (G - 1), q = b >> a.logG;
@@ -208,15 +227,14 @@ int vg_twiddles(vg_ctx *c, fe root, int logn, const fe **lo, const fe **hi)
     t.key_img = root.img;
     t.logn = logn;
     int nhi = logn > 12 ? (1 << (logn - 12)) : 1;
-    VG_CHECK_CUDA(cudaMalloc(&t.lo, 4096 * sizeof(fe)));
-    VG_CHECK_CUDA(cudaMalloc(&t.hi, nhi * sizeof(fe)));
+    VG_TRY(vg_alloc(c, (void **)&t.lo, 4096 * sizeof(fe)));
+    VG_TRY(vg_alloc(c, (void **)&t.hi, nhi * sizeof(fe)));
     fe w4096 = vg::fe_pow(root, 4096);
     k_tw_build<<<grid_for(std::max(4096, nhi), 256), 256, 0, c->stream>>>(root, w4096, t.lo, t.hi, nhi);
     VG_LAUNCHED(c);
     if (c->tw_cache.size() >= 64) {
-        cudaStreamSynchronize(c->stream);
-        cudaFree(c->tw_cache.front().lo);
-        cudaFree(c->tw_cache.front().hi);
+        vg_release(c, c->tw_cache.front().lo);
+        vg_release(c, c->tw_cache.front().hi);
         c->tw_cache.erase(c->tw_cache.begin());
     }
     c->tw_cache.push_back(t);

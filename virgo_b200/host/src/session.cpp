@@ -179,6 +179,19 @@ extern "C" int vg_session_load(vg_session *s, int d, const long *n, const uint8_
     return rc;
 }
 
+extern "C" int vg_session_new(vg_session **out)
+{
+    if (!out) return vg_fail(VG_ERR_ARG, "vg_session_new: null out");
+    vg_session *s = new vg_session();
+    int rc = session_device(&s->ctx);
+    if (rc != VG_OK) {
+        delete s;
+        return rc;
+    }
+    *out = s;
+    return VG_OK;
+}
+
 extern "C" int vg_session_create(int d, const long *n, const uint8_t *const *ty, const int64_t *const *u,
                                  const int64_t *const *v, vg_session **out)
 {

@@ -111,11 +111,16 @@ void zk_prover::get_circuit(const layered_circuit &from_verifier)
 void zk_prover::attach_circuit(const layered_circuit &c, vg_circuit *dev, vg_ctx *ctx)
 {
     C = c;
+    const bool same_ctx = !ctx || ctx == dev_ctx;
     if (ctx) dev_ctx = ctx;
-    if (dev_gkr) vg_gkr_destroy(dev_gkr);
-    if (dev_circuit && owns_circuit) vg_circuit_destroy(dev_circuit);
+    if (dev_circuit && owns_circuit && dev_circuit != dev) vg_circuit_destroy(dev_circuit);
     dev_circuit = dev;
     owns_circuit = false;
+    if (dev_gkr && same_ctx) {   // keep the device tables, grown if the circuit needs more
+        virgo::check(vg_gkr_rebind(dev_gkr, dev_circuit), "vg_gkr_rebind");
+        return;
+    }
+    if (dev_gkr) vg_gkr_destroy(dev_gkr);
     virgo::check(vg_gkr_create(ctx_of(this), dev_circuit, &dev_gkr), "vg_gkr_create");
 }
 
