@@ -1171,8 +1171,12 @@ extern "C" int vg_circuit_build(vg_ctx *ctx, int d, const long *n, const uint8_t
     c->device = ctx->device;
     c->depth = depth;
     c->max_bl = 0;
-    c->L.resize(depth);
-    c->cap.resize(depth, 0);
+    // layer slots only grow: a shallower circuit leaves the deeper slots'
+    // buffers allocated for the next deep one (dropping them would leak them)
+    if ((int)c->L.size() < depth) {
+        c->L.resize(depth);
+        c->cap.resize(depth, 0);
+    }
     auto fail = [&](int rc) {
         if (!*inout) vg_circuit_destroy(c);
         return rc;

@@ -179,13 +179,28 @@ extern "C" int vg_server_create(int device, int slots, size_t hbm_budget, vg_ser
     }
     vg_server *s = new vg_server();
     s->device = device;
-    if (!hbm_budget) {   // default: 90% of what is free now
+    if (!hbm_budget) {   // default: 90% of what is free now, counting the pool's idle reserve as free
         size_t fr = 0, tot = 0;
         cudaSetDevice(device);
         cudaMemGetInfo(&fr, &tot);
-        hbm_budget = fr / 10 * 9;
+        cudaMemPool_t pool;
+        uint64_t reserved = 0, used = 0;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+            cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+            cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+        }
+        cudaGetLastError();
+        hbm_budget = (fr + (reserved > used ? reserved - used : 0)) / 10 * 9;
     }
     s->budget = hbm_budget;
+    {   // stream-ordered allocations keep their freed blocks (see vg_alloc)
+        cudaSetDevice(device);
+        cudaMemPool_t pool;
+        uint64_t thr = ~0ull;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess)
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        cudaGetLastError();
+    }
     s->held.assign(slots, 0);
     s->busy.assign(slots, 0);
     for (int w = 0; w < slots; ++w) s->workers.emplace_back([s, w]() { s->worker(w); });
@@ -264,6 +279,12 @@ extern "C" int vg_server_destroy(vg_server *s)
     }
     s->cv_work.notify_all();
     for (auto &t : s->workers) t.join();
+    // give the pool's unused reserve back to the device
+    cudaMemPool_t pool;
+    cudaSetDevice(s->device);
+    cudaDeviceSynchronize();
+    if (cudaDeviceGetDefaultMemPool(&pool, s->device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+    cudaGetLastError();
     delete s;
     return VG_OK;
 }
