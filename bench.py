@@ -47,6 +47,10 @@ REF_BIN = os.path.join(ROOT, "oracle", "_ref", "zk_proof_ref")
 FFT_BIN = os.path.join(ROOT, "oracle", "_ref", "fft_gkr")
 FAMILIES = ["ntt_pass", "leaf_chain", "merkle_level", "fri_fold_leaf", "virtual_oracle", "eval_layer",
             "phase1_scatter", "phase2_scatter", "acc_finalize", "sumcheck_round", "reduce", "other"]
+# DRAM bytes / algorithmic bytes measured by ncu on full-size launches
+# (profiles/k_round_matmul256.txt: (805.4 + 376.0) MB read + written for
+# 1208 MB algorithmic on a 2^24-entry folding round)
+TRAFFIC_RATIO = {"sumcheck_round": 0.978}
 HBM_BOUND = {"ntt_pass", "virtual_oracle", "eval_layer", "phase1_scatter", "phase2_scatter", "acc_finalize",
              "sumcheck_round", "reduce"}
 
@@ -223,7 +227,8 @@ def ours(args, layers, rank, world):
     L = vb.lib()
     base = vb.Session(layers)
     sessions = [base] + [base.fork() for _ in range(args.batch - 1)]
-    seed0 = 1000 * rank + 1
+    from virgo_b200 import replicas
+    seed0 = replicas.rank_seed_base(rank)
 
     def ctx_of(s):
         return s.ctx()
@@ -449,19 +454,13 @@ def served(n_jobs, seed, slots, rate_factor=3.0):
 
 
 def barrier(world):
-    if world > 1:
-        import torch.distributed as dist
-        dist.barrier()
+    from virgo_b200 import replicas
+    replicas.barrier()
 
 
 def max_over_ranks(x, world):
-    if world == 1:
-        return x
-    import torch
-    import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
-    dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    return float(t.item())
+    from virgo_b200 import replicas
+    return replicas.max_over_ranks(x)
 
 
 def roofline(fam, hbm_peak, peak_kind):
@@ -471,10 +470,17 @@ def roofline(fam, hbm_peak, peak_kind):
     top = max(mem, key=lambda k: mem[k]["ms"])
     f = mem[top]
     gbs = f["bytes"] / (f["ms"] / 1000.0) / 1e9 if f["ms"] > 0 else 0.0
+    per_launch = f["bytes"] / f["launches"]
+    traffic = TRAFFIC_RATIO.get(top)
     return {"bound": "hbm", "kernel": top, "achieved": round(gbs, 1), "peak": hbm_peak, "unit": "GB/s",
-            "frac": round(gbs / hbm_peak, 4), "traffic": None, "peak_source": peak_kind,
-            "launches_per_proof": f["launches"], "avg_launch_us": round(1000.0 * f["ms"] / f["launches"], 2),
-            "bytes_per_launch": f["bytes"] / f["launches"]}
+            "frac": round(gbs / hbm_peak, 4),
+            "traffic": round(per_launch * traffic) if traffic else None,
+            "traffic_note": ("ncu dram read+write / algorithmic bytes on full-size launches (profiles/), times the "
+                             "average launch's algorithmic bytes") if traffic else None,
+            "peak_source": peak_kind, "launches_per_proof": f["launches"],
+            "avg_launch_us": round(1000.0 * f["ms"] / f["launches"], 2), "bytes_per_launch": per_launch,
+            "note": "per-launch CUDA events add about 10 us to every launch's measured time; the kernel is "
+                    "integer-ALU bound (ncu ALU pipe 80%)"}
 
 
 def main():
