@@ -244,6 +244,21 @@ int vg_pc_query_step(vg_pc *pc, int lvl, long pow, vg_fe *values, vg_digest *pat
  * bottom-up, then the leaf).  All arrays host. */
 int vg_pc_query_batch(vg_pc *pc, int nq, const int *which, const long *pos, vg_fe *values, vg_digest *paths,
                       int *path_len);
+/* The whole commitment of one proof in one call and one synchronisation
+ * (poly_commit.h:42-351 commit_private_array / commit_public_array,
+ * vpd_verifier.cpp:46-78 commit_phase, fri.cpp:36-139 and 291-430 with the
+ * query answers of fri.cpp:148-289): RS encodings of priv and pub with their
+ * masks, the virtual oracle, nlevels FRI folds with challenges fri_r, every
+ * leaf chain and Merkle tree batched, and the nq query answers of
+ * vg_pc_query_batch.  Outputs (host): roots[2 + nlevels] (l, h, FRI level
+ * t), all_sum[65], *inner (the sampled <l, q>), final_cw[65 * n] (the last
+ * level, slice-major, n = 2^(log_len - 1 - nlevels)), qvals[nq * 130],
+ * qpaths[nq * 32].  The private mask is padded to vg_pc_info's mask length;
+ * n_pub_mask may not exceed it. */
+int vg_pc_commit_all(vg_pc *pc, const vg_fe *priv, int log_len, const vg_fe *pri_mask, long n_pri_mask,
+                     const vg_fe *pub, const vg_fe *pub_mask, long n_pub_mask, const vg_fe *fri_r, int nlevels,
+                     int nq, const int *which, const long *pos, vg_digest *roots, vg_fe *all_sum, vg_fe *inner,
+                     vg_fe *final_cw, vg_fe *qvals, vg_digest *qpaths);
 /* Sizes of the current commitment: log_len, slice size S, FRI levels so far. */
 int vg_pc_info(vg_pc *pc, int *log_len, long *slice_size, int *levels);
 

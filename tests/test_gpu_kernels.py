@@ -283,3 +283,79 @@ def test_gkr_layer_pieces(ctx, case):
     finally:
         L.vg_gkr_destroy(g)
         L.vg_circuit_destroy(hc)
+
+
+def _mask_len(log_len, n_mask):
+    S = 1 << (log_len - 1)
+    gap = 1
+    while gap * 2 <= S // n_mask:
+        gap *= 2
+    return S // gap
+
+
+@pytest.mark.parametrize("log_len", [11, 20, 22, 24])
+def test_commit_all_matches_step_api(ctx, log_len):
+    """The kernel-level commit path at its full sizes (2^20, 2^22, 2^24): the
+    one-call pipeline (fold-only FRI kernels, every leaf chain and tree in
+    batched launches, one synchronisation) against the step API (the fused
+    fold + leaf-chain kernel, per-set trees), which test_commitment_and_fri
+    pins to the oracle: every root, all_sum, <l, q>, the final codeword and
+    every query answer bit for bit."""
+    L = vb.lib()
+    n, S = 1 << log_len, 1 << (log_len - 1)
+    nlevels = log_len - 6                      # fold until 32 entries per slice
+    priv, pub = O.fe_random(50 + log_len, n), O.fe_random(60 + log_len, n)
+    mask = O.fe_random(70 + log_len, 300)
+    M = _mask_len(log_len, 300)
+    pub_mask = O.fe_random(80 + log_len, M)
+    fri_r = O.fe_random(90 + log_len, nlevels)
+    rng = np.random.default_rng(log_len)
+    which = np.array([0, 1] + [2 + t for t in range(nlevels)] * 2, np.int32)
+    pos = np.array([rng.integers(0, S // 2) for _ in which], np.int64)
+    nq = len(which)
+
+    roots = np.zeros((2 + nlevels, 32), np.uint8)
+    sums, inner = np.zeros((65, 2), np.uint64), np.zeros(2, np.uint64)
+    fin = np.zeros((65 * 32, 2), np.uint64)
+    qv, qp = np.zeros((nq * 130, 2), np.uint64), np.zeros((nq * 32, 32), np.uint8)
+    pc = _pc(ctx)
+    try:
+        vb.check(L.vg_pc_commit_all(pc, vb.ptr(priv), log_len, vb.ptr(mask), 300, vb.ptr(pub), vb.ptr(pub_mask), M,
+                                    vb.ptr(fri_r), nlevels, nq, vb.ptr(which), vb.ptr(pos), vb.ptr(roots), vb.ptr(sums),
+                                    vb.ptr(inner), vb.ptr(fin), vb.ptr(qv), vb.ptr(qp)), "vg_pc_commit_all")
+    finally:
+        L.vg_pc_destroy(pc)
+
+    pc = _pc(ctx)
+    try:
+        Mc = ctypes.c_long()
+        vb.check(L.vg_pc_encode_private(pc, vb.ptr(priv), log_len, vb.ptr(mask), 300, ctypes.byref(Mc)))
+        assert Mc.value == M
+        r = np.zeros(32, np.uint8)
+        vb.check(L.vg_pc_init_commit(pc, 0, vb.ptr(r)))
+        assert (r == roots[0]).all()
+        s2, i2 = np.zeros((65, 2), np.uint64), np.zeros(2, np.uint64)
+        vb.check(L.vg_pc_encode_public(pc, vb.ptr(pub), vb.ptr(pub_mask), M, vb.ptr(s2), vb.ptr(i2)))
+        assert (s2 == sums).all() and (i2 == inner).all()
+        vb.check(L.vg_pc_init_commit(pc, 1, vb.ptr(r)))
+        assert (r == roots[1]).all()
+        for t in range(nlevels):
+            vb.check(L.vg_pc_fri_step(pc, vb.to_fe(fri_r[t]), vb.ptr(r)))
+            assert (r == roots[2 + t]).all(), ("level", t)
+        data, msk, nn = np.zeros((32 * 65, 2), np.uint64), np.zeros((32, 2), np.uint64), ctypes.c_long()
+        vb.check(L.vg_pc_fri_final(pc, vb.ptr(data), vb.ptr(msk), ctypes.byref(nn)))
+        assert nn.value == 32
+        for j in range(16):
+            for s in range(64):
+                assert (data[(j << 7) | (s << 1)] == fin[s * 32 + j]).all()
+                assert (data[(j << 7) | (s << 1) | 1] == fin[s * 32 + j + 16]).all()
+            assert (msk[2 * j] == fin[64 * 32 + j]).all() and (msk[2 * j + 1] == fin[64 * 32 + j + 16]).all()
+        v2, p2 = np.zeros_like(qv), np.zeros_like(qp)
+        plen = np.zeros(nq, np.int32)
+        vb.check(L.vg_pc_query_batch(pc, nq, vb.ptr(which), vb.ptr(pos), vb.ptr(v2), vb.ptr(p2), vb.ptr(plen)))
+        assert (v2 == qv).all()
+        for q in range(nq):
+            k = plen[q]
+            assert (p2[q * 32:q * 32 + k] == qp[q * 32:q * 32 + k]).all(), ("query", q)
+    finally:
+        L.vg_pc_destroy(pc)

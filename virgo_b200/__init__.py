@@ -99,6 +99,8 @@ def lib():
             "vg_session_fork": (c_i, [c_p, ctypes.POINTER(c_p)]),
             "vg_session_prove_batch": (c_i, [c_p, c_i, c_p, c_i, c_p, c_p, c_p]),
             "vg_session_new": (c_i, [ctypes.POINTER(c_p)]),
+            "vg_pc_commit_all": (c_i, [c_p, c_p, c_i, c_p, c_l, c_p, c_p, c_l, c_p, c_i, c_i, c_p, c_p, c_p, c_p, c_p,
+                                       c_p, c_p, c_p]),
             "vg_gkr_rebind": (c_i, [c_p, c_p]),
             "vg_job_footprint": (c_sz, [c_i, c_p]),
             "vg_server_create": (c_i, [c_i, c_i, c_sz, ctypes.POINTER(c_p)]),

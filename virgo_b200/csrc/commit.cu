@@ -742,3 +742,25 @@ int vg_pc_prove_deferred(vg_pc *pc, const vg_fe *priv, int log_len, const vg_fe 
     out->qpaths = (const vg_digest *)h_qp;
     return VG_OK;
 }
+
+extern "C" int vg_pc_commit_all(vg_pc *pc, const vg_fe *priv, int log_len, const vg_fe *pri_mask, long n_pri_mask,
+                                const vg_fe *pub, const vg_fe *pub_mask, long n_pub_mask, const vg_fe *fri_r,
+                                int nlevels, int nq, const int *which, const long *pos, vg_digest *roots,
+                                vg_fe *all_sum, vg_fe *inner, vg_fe *final_cw, vg_fe *qvals, vg_digest *qpaths)
+{
+    if (!roots || !all_sum || !inner || !final_cw || (nq && (!qvals || !qpaths)))
+        return vg_fail(VG_ERR_ARG, "vg_pc_commit_all: null output");
+    vg_pc_results r{};
+    VG_TRY(vg_pc_prove_deferred(pc, priv, log_len, pri_mask, n_pri_mask, pub, pub_mask, n_pub_mask, fri_r, nlevels, nq,
+                                which, pos, &r));
+    VG_CHECK_CUDA(cudaStreamSynchronize(pc->ctx->stream));
+    memcpy(roots, r.roots, (size_t)(2 + nlevels) * sizeof(vg_digest));
+    memcpy(all_sum, r.all_sum, 65 * sizeof(vg_fe));
+    *inner = *r.inner;
+    memcpy(final_cw, r.final_cw, (size_t)65 * r.n_final * sizeof(vg_fe));
+    if (nq) {
+        memcpy(qvals, r.qvals, (size_t)nq * 130 * sizeof(vg_fe));
+        memcpy(qpaths, r.qpaths, (size_t)nq * 32 * sizeof(vg_digest));
+    }
+    return VG_OK;
+}
