@@ -309,6 +309,21 @@ int vg_default_ctx(vg_ctx **out);
  * format, and a meta file with one "0 0 1 0 0" line per layer.  Host only. */
 int vg_circuit_write_text(int d, const long *n, const uint8_t *const *ty, const int64_t *const *u,
                           const int64_t *const *v, const char *circuit_path, const char *meta_path);
+/* Binary circuit files (no reference counterpart; the reference parses text
+ * with fscanf, zk_verifier.cpp:15-217): the file-level layers in the
+ * vg_session_load layout (8-byte sections: "VGC1", version, d, index_bytes,
+ * n[d], then per layer types, u, v; the input layer's u/v are int64), so a
+ * load maps the file and builds the circuit on the device without parsing.
+ * vg_session_from_file accepts either format. */
+int vg_circuit_write_binary(const char *path, int d, const long *n, const uint8_t *const *ty, const void *const *u,
+                            const void *const *v, int index_bytes);
+/* 1 if path starts with the binary circuit magic, else 0.  Host only. */
+int vg_circuit_is_binary(const char *path);
+/* Header of a binary circuit file (validated against the file size): layer
+ * count, wire width, and up to n_cap layer sizes.  Host only. */
+int vg_circuit_binary_info(const char *path, int *d, int *index_bytes, long *n, int n_cap);
+/* vg_session_load from a binary circuit file. */
+int vg_session_load_file(vg_session *s, const char *path);
 /* depth of the prover's circuit (file layers + 1) and log2 of the padded input */
 int vg_session_depth(vg_session *s, int *depth, int *input_log);
 /* One proof.  With want_transcript, *transcript (free with vg_free) receives

@@ -213,3 +213,19 @@ print(json.dumps(out))
     got = json.loads(r.stdout.strip().splitlines()[-1])
     want = {c["name"]: c["digest"] for c in _golden()}
     assert got and all(got[k] == want[k] for k in got), (got, want)
+
+
+@pytest.mark.parametrize("index_bytes", [4, 8])
+def test_session_from_binary_file(tmp_path, index_bytes):
+    """A binary circuit file (mapped, no parsing) proves the same transcript
+    as the layers it was written from."""
+    c = next(x for x in _golden() if x["name"] == "random_5layer")
+    layers = getattr(circuits, c["generator"])(**c["params"])
+    path = str(tmp_path / "c.vgc")
+    vb.write_circuit_binary(layers, path, index_bytes=index_bytes)
+    s = vb.Session(circuit_path=path)
+    try:
+        blob = s.prove(c["seed"])[1]
+    finally:
+        s.close()
+    assert transcript.digest(transcript.parse(blob)) == c["digest"]

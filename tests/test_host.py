@@ -137,3 +137,45 @@ def test_random_batch_shapes():
             prev = len(t)
     c = circuits.random_by_gates(14, 16, seed=1)
     assert len(c) == 16 and circuits.total_gates(c) == 1 << 14
+
+
+def _read_binary_circuit(path):
+    """independent numpy reader of the binary circuit layout"""
+    raw = open(path, "rb").read()
+    assert raw[:4] == b"VGC1"
+    version, d, ib = np.frombuffer(raw, np.uint32, 3, 4)
+    assert version == 1
+    n = np.frombuffer(raw, np.int64, d, 16)
+    pos = (16 + 8 * int(d) + 7) // 8 * 8
+    out = []
+    for i in range(d):
+        wb = 8 if i == 0 else int(ib)
+        dt = np.int64 if wb == 8 else np.uint32
+        arrs = []
+        for k, (cnt, width, t) in enumerate(((n[i], 1, np.uint8), (n[i], wb, dt), (n[i], wb, dt))):
+            arrs.append(np.frombuffer(raw, t, int(cnt), pos))
+            pos = (pos + int(cnt) * width + 7) // 8 * 8
+        out.append(tuple(arrs))
+    assert pos == len(raw)
+    return out, int(ib)
+
+
+@pytest.mark.parametrize("index_bytes", [4, 8])
+def test_binary_circuit_file_roundtrip(built, tmp_path, index_bytes):
+    layers = circuits.random_layered([9, 11, 10, 7], seed=3)
+    path = str(tmp_path / "c.vgc")
+    vb.write_circuit_binary(layers, path, index_bytes=index_bytes)
+    assert vb.lib().vg_circuit_is_binary(path.encode()) == 1
+    sizes, ib = vb.circuit_binary_info(path)
+    assert sizes == [len(t) for t, _, _ in layers] and ib == index_bytes
+    got, _ = _read_binary_circuit(path)
+    for (t, u, v), (t2, u2, v2) in zip(layers, got):
+        assert (t == t2).all() and (u == u2).all() and (v == v2).all()
+    # a truncated file is rejected before any device work
+    raw = open(path, "rb").read()
+    open(path, "wb").write(raw[:-9])
+    with pytest.raises(vb.VirgoError):
+        vb.circuit_binary_info(path)
+    txt = str(tmp_path / "c.txt")
+    circuits.write_text(layers, txt, str(tmp_path / "m.txt"))
+    assert vb.lib().vg_circuit_is_binary(txt.encode()) == 0

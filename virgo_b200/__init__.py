@@ -99,6 +99,10 @@ def lib():
             "vg_session_fork": (c_i, [c_p, ctypes.POINTER(c_p)]),
             "vg_session_prove_batch": (c_i, [c_p, c_i, c_p, c_i, c_p, c_p, c_p]),
             "vg_session_new": (c_i, [ctypes.POINTER(c_p)]),
+            "vg_circuit_write_binary": (c_i, [ctypes.c_char_p, c_i, c_p, c_p, c_p, c_p, c_i]),
+            "vg_circuit_is_binary": (c_i, [ctypes.c_char_p]),
+            "vg_circuit_binary_info": (c_i, [ctypes.c_char_p, ctypes.POINTER(c_i), ctypes.POINTER(c_i), c_p, c_i]),
+            "vg_session_load_file": (c_i, [c_p, ctypes.c_char_p]),
             "vg_pc_commit_all": (c_i, [c_p, c_p, c_i, c_p, c_l, c_p, c_p, c_l, c_p, c_i, c_i, c_p, c_p, c_p, c_p, c_p,
                                        c_p, c_p, c_p]),
             "vg_gkr_rebind": (c_i, [c_p, c_p]),
@@ -310,6 +314,22 @@ def _layer_arrays(layers, index_bytes):
         tys[i], us[i], vs[i] = t.ctypes.data, u.ctypes.data, v.ctypes.data
     keep += [tys, us, vs]
     return ns, tys, us, vs, keep
+
+
+def write_circuit_binary(layers, path: str, index_bytes: int = 4):
+    """Writes file-level layers (input layer first) as a binary circuit file."""
+    ns, tys, us, vs, keep = _layer_arrays(layers, index_bytes)
+    check(lib().vg_circuit_write_binary(path.encode(), len(layers), ns.ctypes.data, tys, us, vs, index_bytes),
+          "vg_circuit_write_binary")
+
+
+def circuit_binary_info(path: str):
+    """(layer sizes, index_bytes) of a binary circuit file."""
+    d, ib = ctypes.c_int(), ctypes.c_int()
+    check(lib().vg_circuit_binary_info(path.encode(), ctypes.byref(d), ctypes.byref(ib), None, 0))
+    n = np.zeros(d.value, np.int64)
+    check(lib().vg_circuit_binary_info(path.encode(), ctypes.byref(d), ctypes.byref(ib), n.ctypes.data, d.value))
+    return [int(x) for x in n], ib.value
 
 
 def job_footprint(widths) -> int:

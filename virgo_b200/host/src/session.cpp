@@ -225,8 +225,22 @@ extern "C" int vg_session_fork(vg_session *base, vg_session **out)
 
 // text circuit format of src/linear_gkr/README.md (the meta file is only
 // needed by the verifier's predicate evaluation and is not read here)
+extern "C" int vg_circuit_is_binary(const char *path);
+
 extern "C" int vg_session_from_file(const char *circuit_path, vg_session **out)
 {
+    if (!circuit_path || !out) return vg_fail(VG_ERR_ARG, "vg_session_from_file: null argument");
+    if (vg_circuit_is_binary(circuit_path)) {   // binary circuit file: mapped, no parsing
+        vg_session *s = nullptr;
+        int rc = vg_session_new(&s);
+        if (rc == VG_OK) rc = vg_session_load_file(s, circuit_path);
+        if (rc != VG_OK) {
+            vg_session_destroy(s);
+            return rc;
+        }
+        *out = s;
+        return VG_OK;
+    }
     FILE *f = fopen(circuit_path, "rb");
     if (!f) return vg_fail(VG_ERR_ARG, "cannot open circuit file");
     fseek(f, 0, SEEK_END);
