@@ -123,6 +123,29 @@ __global__ void k_eq_half(const fe *__restrict__ r, int nbits, fe scale, fe *__r
     out[i] = x;
 }
 
+// Several half tables in one launch (the tables of a phase init are built
+// together): table q covers threads [begin[q], begin[q + 1]).
+struct EqJobs {
+    const fe *r[4];
+    fe *out[4];
+    fe scale[4];
+    int nbits[4];
+    long begin[5];
+    int count;
+};
+__global__ void k_eq_halves(EqJobs J)
+{
+    const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (t >= J.begin[J.count]) return;
+    int q = 0;
+    while (t >= J.begin[q + 1]) ++q;
+    const long i = t - J.begin[q];
+    const fe *r = J.r[q];
+    fe x = J.scale[q];
+    for (int b = 0; b < J.nbits[q]; ++b) x = x * (((i >> b) & 1) ? r[b] : vg::fe_one() - r[b]);
+    J.out[q][i] = x;
+}
+
 // out[x] = lo[x & mask] * hi[x >> fh]
 __global__ void k_eq_combine(const fe *__restrict__ lo, const fe *__restrict__ hi, int fh, long n, fe *__restrict__ out)
 {
@@ -1423,16 +1446,37 @@ extern "C" int vg_gkr_layer_values(vg_gkr *g, int layer, const vg_fe **dev_value
 }
 
 // eq half tables for bits r[0..len): low half (len >> 1 bits, scaled) and high half
+// Adds the low half (len >> 1 bits, scaled) and the high half of the eq table
+// of r to J; *fh = the low half's bit count.
+static void add_halves(EqJobs &J, const fe *r_dev, int len, fe scale, fe *lo, fe *hi, int *fh)
+{
+    const int f = len >> 1, s = len - f;
+    const int bits[2] = {f, s};
+    const fe *rs[2] = {r_dev, r_dev + f};
+    fe *outs[2] = {lo, hi};
+    for (int k = 0; k < 2; ++k) {
+        const int q = J.count++;
+        J.r[q] = rs[k];
+        J.out[q] = outs[k];
+        J.scale[q] = k == 0 ? scale : vg::fe_one();
+        J.nbits[q] = bits[k];
+        J.begin[q + 1] = J.begin[q] + (1L << bits[k]);
+    }
+    *fh = f;
+}
+
+static int launch_halves(vg_gkr *g, const EqJobs &J)
+{
+    k_eq_halves<<<grid_for(J.begin[J.count], 256), 256, 0, g->ctx->stream>>>(J);
+    VG_LAUNCHED(g->ctx);
+    return VG_OK;
+}
+
 static int build_halves(vg_gkr *g, const fe *r_dev, int len, fe scale, fe *lo, fe *hi, int *fh)
 {
-    vg_ctx *c = g->ctx;
-    int f = len >> 1, s = len - f;
-    k_eq_half<<<grid_for(1L << f, 256), 256, 0, c->stream>>>(r_dev, f, scale, lo);
-    VG_LAUNCHED(c);
-    k_eq_half<<<grid_for(1L << s, 256), 256, 0, c->stream>>>(r_dev + f, s, vg::fe_one(), hi);
-    VG_LAUNCHED(c);
-    *fh = f;
-    return VG_OK;
+    EqJobs J{};
+    add_halves(J, r_dev, len, scale, lo, hi, fh);
+    return launch_halves(g, J);
 }
 
 static int upload_r(vg_gkr *g, int slot, const vg_fe *r, int len)
@@ -1606,8 +1650,12 @@ extern "C" int vg_gkr_phase1_init(vg_gkr *g, int layer, const vg_fe *r0, const v
     fe *e = g->eq;
     const long H = g->eq_half;
     int fh;
-    VG_TRY(build_halves(g, g->rbuf, length_g, tofe(alpha), e, e + H, &fh));
-    VG_TRY(build_halves(g, g->rbuf + 64, length_g, tofe(beta), e + 2 * H, e + 3 * H, &fh));
+    {   // the alpha- and beta-weighted tables of r0 and r1 in one launch
+        EqJobs J{};
+        add_halves(J, g->rbuf, length_g, tofe(alpha), e, e + H, &fh);
+        add_halves(J, g->rbuf + 64, length_g, tofe(beta), e + 2 * H, e + 3 * H, &fh);
+        VG_TRY(launch_halves(g, J));
+    }
     g->bg.f0 = e;
     g->bg.s0 = e + H;
     g->bg.f1 = e + 2 * H;
