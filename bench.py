@@ -402,11 +402,16 @@ def served(n_jobs, seed, slots, rate_factor=3.0):
     import threading as th
     import virgo_b200 as vb
     from virgo_b200 import circuits
+    from virgo_b200 import sha256_circuit
     rng = np.random.default_rng(seed)
     pool = {g: [circuits.random_by_gates(g, 16, seed=1000 * g + i) for i in range(3)] for g in (14, 18, 22)}
+    # SHA-256 compression circuits over 2^4 and 2^6 blocks (2.1 M and 8.4 M gates)
+    pool["sha4"] = [sha256_circuit.sha256_blocks(16, seed=41 + i) for i in range(2)]
+    pool["sha6"] = [sha256_circuit.sha256_blocks(64, seed=61)]
     pool = {g: [_pinned_layers(c) for c in cs] for g, cs in pool.items()}
-    kinds = rng.choice([14, 18, 22], size=n_jobs)
-    picks = [pool[int(g)][int(rng.integers(3))] for g in kinds]
+    classes = [14, 18, 22, "sha4", "sha6"]
+    kinds = [classes[int(k)] for k in rng.integers(0, len(classes), size=n_jobs)]
+    picks = [pool[g][int(rng.integers(len(pool[g])))] for g in kinds]
 
     def run(nslots, times):
         srv = vb.Server(slots=nslots)
@@ -414,7 +419,8 @@ def served(n_jobs, seed, slots, rate_factor=3.0):
         try:
             # warm every slot on the largest shape, all at once so each worker
             # grows its buffers before the timed arrivals
-            warm = [srv.submit(pool[22][k % 3], 1, transcript=False) for k in range(2 * nslots)]
+            big = pool[22] + pool["sha6"]
+            warm = [srv.submit(big[k % len(big)], 1, transcript=False) for k in range(2 * nslots)]
             for j in warm:
                 srv.wait(j)
             ids = [None] * n_jobs
@@ -452,8 +458,9 @@ def served(n_jobs, seed, slots, rate_factor=3.0):
             "plain": {"value": n_jobs / span_p, "p50_ms": 1000 * _pctl(lat_p, 0.5), "p99_ms": 1000 * _pctl(lat_p, 0.99),
                       "saturated_value": plain_rate},
             "arrival_rate": rate, "jobs": n_jobs, "slots": slots,
-            "workload": "Poisson arrivals at %.1fx the plain form's rate; random layered circuits of 2^14, 2^18, "
-                        "2^22 gates, depth 16, equal shares" % rate_factor,
+            "workload": "Poisson arrivals at %.1fx the plain form's rate; equal shares of random layered circuits "
+                        "of 2^14, 2^18, 2^22 gates (depth 16) and SHA-256 compression circuits over 2^4 and 2^6 "
+                        "blocks" % rate_factor,
             "timing": "wall clock, submit to transcript on the host (circuit upload included)"}
 
 

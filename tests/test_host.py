@@ -179,3 +179,25 @@ def test_binary_circuit_file_roundtrip(built, tmp_path, index_bytes):
     txt = str(tmp_path / "c.txt")
     circuits.write_text(layers, txt, str(tmp_path / "m.txt"))
     assert vb.lib().vg_circuit_is_binary(txt.encode()) == 0
+
+
+def test_sha256_compression_and_circuit():
+    """The generator's compression equals hashlib's SHA-256 on padded single
+    blocks, and its circuit, evaluated by the oracle, outputs only zeros
+    (every addition and bit test holds for the witness)."""
+    import hashlib
+    import struct
+    import sys
+    from virgo_b200 import sha256_circuit as S
+    sys.path.insert(0, os.path.dirname(os.path.abspath(__file__)))
+    import _oracle as O
+    for m in (b"", b"abc", bytes(range(55))):
+        blk = m + b"\x80" + b"\x00" * (55 - len(m)) + struct.pack(">Q", 8 * len(m))
+        out = S.compress(S.H0, list(struct.unpack(">16I", blk)))["out"]
+        assert b"".join(struct.pack(">I", x) for x in out) == hashlib.sha256(m).digest()
+    L = S.sha256_blocks(1, seed=2)
+    assert all(len(t) & (len(t) - 1) == 0 for t, _, _ in L)
+    vals = O.eval_input(L[0][1])
+    for t, u, v in L[1:]:
+        vals = O.eval_layer(t, u, v, vals)
+    assert not vals.any()
