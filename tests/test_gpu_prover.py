@@ -233,11 +233,13 @@ def test_session_from_binary_file(tmp_path, index_bytes):
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(REF, "zk_proof_ref")), reason="reference not compiled here")
 def test_sha256_circuit_matches_reference(tmp_path):
-    """A SHA-256 compression circuit (two blocks; xor, not-a-and-b, exp-sum,
-    bit-test, range-sum and relay gates): the reference verifier accepts the
-    reference prover's proof, and the GPU transcript equals it."""
+    """A SHA-256 compression circuit (four blocks; xor, not-a-and-b, exp-sum,
+    bit-test, range-sum and relay gates; in phase 2 table entry 0 collects
+    55 000 summation edges, so the split heavy-entry path runs): the
+    reference verifier accepts the reference prover's proof, and the GPU
+    transcript equals it."""
     from virgo_b200 import sha256_circuit
-    layers = sha256_circuit.sha256_blocks(2, seed=7)
+    layers = sha256_circuit.sha256_blocks(4, seed=7)
     out, ref = _run_binary(os.path.join(REF, "zk_proof_ref"), layers, 77, tmp_path)
     assert out.returncode == 0 and "Pass" in out.stdout, out.stdout[-2000:]
     s = vb.Session(layers)

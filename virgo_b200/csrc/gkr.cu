@@ -46,8 +46,11 @@ struct EdgeSet {
     uint32_t *g = nullptr;        // gate index (the relay's u in phase 1)
     uint32_t *o = nullptr;        // the other wire (phase 1: v, phase 2: u or the summed wire)
     uint16_t *tk = nullptr;       // gate type | doubling count << 8
-    uint32_t *medium = nullptr;   // keys with more than LIGHT_MAX edges
+    uint32_t *medium = nullptr;   // keys with LIGHT_MAX < edges <= HEAVY_MIN
     long n_medium = 0;
+    uint32_t *heavy = nullptr;    // (key, first edge, end edge) of keys with more than HEAVY_MIN edges
+    long cap_H = 0;
+    std::vector<uint32_t> heavy_host;   // the same triples on the host
     long cap_N = 0, cap_E = 0, cap_M = 0;
 };
 
@@ -60,6 +63,10 @@ struct DevLayer {
 };
 
 constexpr int LIGHT_MAX = 64;   // edges a single thread sums; longer lists get a warp
+constexpr long HEAVY_MIN = 32768;   // longer lists are split over many CTAs
+constexpr int EDGE_STATS = 4;       // per edge set: total, long keys, overflow, heavy keys
+constexpr int MAX_HEAVY = 16;       // heavy keys per launch
+constexpr int HEAVY_PARTS = 296;    // CTAs per heavy key
 
 __device__ __forceinline__ fe from_int32(int32_t x)
 {
@@ -389,17 +396,27 @@ __global__ void k_edges(const uint8_t *__restrict__ ty, const uint32_t *__restri
     }
 }
 
-// keys with more than LIGHT_MAX edges into list (room for cap_list);
-// stats[0] = edge total, stats[1] = listed keys
+// keys with more than LIGHT_MAX edges into list (room for cap_list), those
+// with more than HEAVY_MIN as (key, first, end) triples into heavy;
+// stats[0] = edge total, stats[1] = listed keys, stats[3] = heavy keys
 __global__ void k_medium_keys(const uint32_t *__restrict__ off, long N, uint32_t *__restrict__ list, long cap_list,
-                              unsigned long long *__restrict__ stats)
+                              uint32_t *__restrict__ heavy, long cap_heavy, unsigned long long *__restrict__ stats)
 {
     if (blockIdx.x == 0 && threadIdx.x == 0) stats[0] = off[N];
-    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < N; k += (long)gridDim.x * blockDim.x)
-        if (off[k + 1] - off[k] > (uint32_t)LIGHT_MAX) {
+    for (long k = blockIdx.x * (long)blockDim.x + threadIdx.x; k < N; k += (long)gridDim.x * blockDim.x) {
+        const uint32_t len = off[k + 1] - off[k];
+        if (len > (uint32_t)HEAVY_MIN) {
+            const unsigned long long i = atomicAdd(&stats[3], 1ull);
+            if ((long)i < cap_heavy) {
+                heavy[3 * i] = (uint32_t)k;
+                heavy[3 * i + 1] = off[k];
+                heavy[3 * i + 2] = off[k + 1];
+            }
+        } else if (len > (uint32_t)LIGHT_MAX) {
             const unsigned long long i = atomicAdd(&stats[1], 1ull);
             if ((long)i < cap_list) list[i] = (uint32_t)k;
         }
+    }
 }
 
 // contribution of one edge to the phase-1 tables (k_phase1_scatter's cases)
@@ -513,6 +530,55 @@ __global__ void __launch_bounds__(GKR_THREADS) k_gather_long(EdgeView e, const u
                 out_m[k] = a[0] + a[1] * vu;
                 out_v[k] = a[2] + a[3] * vu;
             }
+        }
+    }
+}
+
+// Keys with more than HEAVY_MIN edges (in phase 2 every summation gate's
+// edges land on entry 0): CTA (x, q) sums a strided share of heavy key q's
+// edges into parts[q][x], then k_heavy_finish adds the shares of each key.
+struct HeavyKeys {
+    uint32_t key[MAX_HEAVY], s[MAX_HEAVY], e[MAX_HEAVY];
+    int count;
+};
+
+template <int PH>
+__global__ void __launch_bounds__(GKR_THREADS) k_gather_heavy(EdgeView e, HeavyKeys H, BetaG bg, BetaU bu,
+                                                              const fe *__restrict__ prev, fe *__restrict__ parts)
+{
+    __shared__ fe sm[4 * 32];
+    const int q = blockIdx.y;
+    fe a[4] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+    for (long p = H.s[q] + blockIdx.x * (long)blockDim.x + threadIdx.x; p < (long)H.e[q];
+         p += (long)gridDim.x * blockDim.x) {
+        if (PH == 0) edge1(e.tk[p], e.g[p], e.o[p], bg, prev, a[0], a[1]);
+        else edge2(e.tk[p], e.g[p], e.o[p], bg, bu, a);
+    }
+    block_sum<4>(a, sm);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 4; ++k) parts[((long)q * gridDim.x + blockIdx.x) * 4 + k] = a[k];
+}
+
+template <int PH>
+__global__ void __launch_bounds__(GKR_THREADS) k_heavy_finish(HeavyKeys H, const fe *__restrict__ parts, int nparts,
+                                                              const fe *__restrict__ vu_ptr, fe *__restrict__ out_m,
+                                                              fe *__restrict__ out_v)
+{
+    __shared__ fe sm[4 * 32];
+    const int q = blockIdx.x;
+    fe a[4] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+    for (int b = threadIdx.x; b < nparts; b += blockDim.x)
+        for (int k = 0; k < 4; ++k) a[k] = a[k] + parts[((long)q * nparts + b) * 4 + k];
+    block_sum<4>(a, sm);
+    if (threadIdx.x == 0) {
+        const uint32_t k = H.key[q];
+        if (PH == 0) {
+            out_m[k] = a[0];
+            out_v[k] = a[1];
+        } else {
+            const fe vu = *vu_ptr;
+            out_m[k] = a[0] + a[1] * vu;
+            out_v[k] = a[2] + a[3] * vu;
         }
     }
 }
@@ -887,6 +953,7 @@ struct vg_gkr {
     long pend_n0 = 0;                    // table length before the group's first round
     bool pend_nofold = false;
     fe *rg_parts = nullptr;              // per-CTA, per-round partial sums of a group
+    fe *heavy_parts = nullptr;           // per-CTA partial sums of heavy keys
 };
 
 static int flush_rounds(vg_gkr *g);
@@ -927,9 +994,9 @@ static int fill_edges(vg_circuit *c, int li, int ph)
     DevLayer &D = c->L[li];
     EdgeSet &E = D.ph[ph];
     const long N = E.N;
-    unsigned long long *st = c->edge_stats + 3 * (2 * li + ph);
+    unsigned long long *st = c->edge_stats + EDGE_STATS * (2 * li + ph);
     const unsigned grid = std::min<unsigned>(grid_for(D.n, 256), 148u * 32u);
-    VG_CHECK_CUDA(cudaMemsetAsync(st, 0, 3 * 8, ctx->stream));
+    VG_CHECK_CUDA(cudaMemsetAsync(st, 0, EDGE_STATS * 8, ctx->stream));
     VG_CHECK_CUDA(cudaMemcpyAsync(c->work, E.off, N * 4, cudaMemcpyDeviceToDevice, ctx->stream));
     if (ph == 0)
         k_edges<0, true><<<grid, 256, 0, ctx->stream>>>(D.ty, D.u, D.v, D.n, c->work, E.g, E.o, E.tk, E.off + N, E.cap_E, st);
@@ -938,7 +1005,9 @@ static int fill_edges(vg_circuit *c, int li, int ph)
     VG_LAUNCHED(ctx);
     // a key with more than LIGHT_MAX edges: at most cap_E / (LIGHT_MAX + 1) of them
     VG_TRY(grow_u32(ctx, &E.medium, &E.cap_M, E.cap_E / (LIGHT_MAX + 1) + 1));
-    k_medium_keys<<<std::min<unsigned>(grid_for(N, 256), 148u * 32u), 256, 0, ctx->stream>>>(E.off, N, E.medium, E.cap_M, st);
+    VG_TRY(grow_u32(ctx, &E.heavy, &E.cap_H, 3 * (E.cap_E / HEAVY_MIN + 1)));
+    k_medium_keys<<<std::min<unsigned>(grid_for(N, 256), 148u * 32u), 256, 0, ctx->stream>>>(
+        E.off, N, E.medium, E.cap_M, E.heavy, E.cap_H / 3, st);
     VG_LAUNCHED(ctx);
     return VG_OK;
 }
@@ -988,7 +1057,7 @@ static int launch_edges(vg_circuit *c, int li)
 // c->edge_stats_host (valid after the stream is synchronised).
 static int launch_all_edges(vg_circuit *c)
 {
-    const int need = 3 * 2 * c->depth;
+    const int need = EDGE_STATS * 2 * c->depth;
     if (need > c->edge_stats_cap) {
         vg_release(c->ctx, c->edge_stats);
         c->edge_stats = nullptr;
@@ -1003,6 +1072,18 @@ static int launch_all_edges(vg_circuit *c)
     return VG_OK;
 }
 
+// The heavy keys' (key, first, end) triples to the host (circuits that have
+// any: one more synchronisation at build time).
+static int read_heavy(vg_circuit *c, EdgeSet &E, long n_heavy)
+{
+    E.heavy_host.assign(3 * (size_t)n_heavy, 0);
+    if (!n_heavy) return VG_OK;
+    if (3 * n_heavy > E.cap_H) return vg_fail(VG_ERR_STATE, "heavy key list overflow");
+    VG_CHECK_CUDA(cudaMemcpyAsync(E.heavy_host.data(), E.heavy, 3 * n_heavy * 4, cudaMemcpyDeviceToHost, c->ctx->stream));
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->ctx->stream));
+    return VG_OK;
+}
+
 // Reads the edge counts of every layer (the caller synchronised the stream
 // after stats_host was copied) and rebuilds the sets whose edges did not fit.
 static int finish_edges(vg_circuit *c, const unsigned long long *stats_host)
@@ -1011,7 +1092,7 @@ static int finish_edges(vg_circuit *c, const unsigned long long *stats_host)
     for (int li = 1; li < c->depth; ++li)
         for (int ph = 0; ph < 2; ++ph) {
             EdgeSet &E = c->L[li].ph[ph];
-            const unsigned long long *st = stats_host + 3 * (2 * li + ph);
+            const unsigned long long *st = stats_host + EDGE_STATS * (2 * li + ph);
             if (!E.launched) continue;
             if (st[0] >= (1ull << 31)) {   // too many edges: atomic path
                 E.launched = false;
@@ -1025,6 +1106,7 @@ static int finish_edges(vg_circuit *c, const unsigned long long *stats_host)
                 continue;
             }
             E.n_medium = (long)st[1];
+            VG_TRY(read_heavy(c, E, (long)st[3]));
             E.ok = true;
         }
     if (!refill) return VG_OK;
@@ -1035,11 +1117,13 @@ static int finish_edges(vg_circuit *c, const unsigned long long *stats_host)
             EdgeSet &E = c->L[li].ph[ph];
             if (!E.launched || E.ok || E.cap_E < E.E || E.E >= (1L << 31)) continue;
             VG_TRY(fill_edges(c, li, ph));
-            unsigned long long st[3];
-            VG_CHECK_CUDA(cudaMemcpyAsync(st, c->edge_stats + 3 * (2 * li + ph), 3 * 8, cudaMemcpyDeviceToHost, ctx->stream));
+            unsigned long long st[EDGE_STATS];
+            VG_CHECK_CUDA(cudaMemcpyAsync(st, c->edge_stats + EDGE_STATS * (2 * li + ph), EDGE_STATS * 8,
+                                          cudaMemcpyDeviceToHost, ctx->stream));
             VG_CHECK_CUDA(cudaStreamSynchronize(ctx->stream));
             if (st[2]) continue;   // still does not fit: atomic path
             E.n_medium = (long)st[1];
+            VG_TRY(read_heavy(c, E, (long)st[3]));
             E.ok = true;
         }
     return VG_OK;
@@ -1141,6 +1225,7 @@ extern "C" int vg_circuit_destroy(vg_circuit *c)
             cudaFree(E.o);
             cudaFree(E.tk);
             cudaFree(E.medium);
+            cudaFree(E.heavy);
         }
     }
     cudaFree(c->input);
@@ -1383,6 +1468,8 @@ extern "C" int vg_gkr_create(vg_ctx *ctx, const vg_circuit *c, vg_gkr **out)
     if (cudaMalloc(&g->round_out, 16 * sizeof(fe)) != cudaSuccess) return fail("round sums");
     if (cudaMalloc(&g->round_counter, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
     if (cudaMalloc(&g->vu, sizeof(fe)) != cudaSuccess) return fail("v_u");
+    if (cudaMalloc(&g->heavy_parts, (size_t)MAX_HEAVY * HEAVY_PARTS * 4 * sizeof(fe)) != cudaSuccess)
+        return fail("heavy partials");
     if (cudaMemset(g->round_counter, 0, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
     int rc = gkr_bind(g, c);
     if (rc != VG_OK) {
@@ -1414,6 +1501,7 @@ extern "C" int vg_gkr_destroy(vg_gkr *g)
     cudaFree(g->round_out);
     cudaFree(g->round_counter);
     cudaFree(g->vu);
+    cudaFree(g->heavy_parts);
     cudaFree(g->rg_parts);
     cudaFree(g->rec);
     if (g->rec_host) cudaFreeHost(g->rec_host);
@@ -1606,6 +1694,22 @@ static int gather_tables(vg_gkr *g, const EdgeSet &E, long N, const fe *prev)
             ev, N, g->bg, g->bu, prev, g->vu, out_m, out_v);
     }
     VG_LAUNCHED(c);
+    const int nheavy = (int)(E.heavy_host.size() / 3);
+    for (int h0 = 0; h0 < nheavy; h0 += MAX_HEAVY) {   // heavy keys, split over many CTAs
+        HeavyKeys H{};
+        for (int q = h0; q < nheavy && H.count < MAX_HEAVY; ++q) {
+            H.key[H.count] = E.heavy_host[3 * q];
+            H.s[H.count] = E.heavy_host[3 * q + 1];
+            H.e[H.count] = E.heavy_host[3 * q + 2];
+            ++H.count;
+        }
+        const int nparts = HEAVY_PARTS;
+        ProfScope ps(c, PH == 0 ? KF_SCATTER1 : KF_SCATTER2, 0.0);
+        k_gather_heavy<PH><<<dim3(nparts, H.count), GKR_THREADS, 0, c->stream>>>(ev, H, g->bg, g->bu, prev, g->heavy_parts);
+        VG_LAUNCHED(c);
+        k_heavy_finish<PH><<<H.count, GKR_THREADS, 0, c->stream>>>(H, g->heavy_parts, nparts, g->vu, out_m, out_v);
+        VG_LAUNCHED(c);
+    }
     if (E.n_medium) {
         ProfScope ps(c, PH == 0 ? KF_SCATTER1 : KF_SCATTER2, 0.0);
         k_gather_long<PH><<<std::min<unsigned>(grid_for(E.n_medium * 32, GKR_THREADS), 148u * 64u), GKR_THREADS, 0,
