@@ -236,9 +236,10 @@ def ours(args, layers, rank, world):
     def launches(ss):
         tot = 0
         for s in ss:
-            c = ctypes.c_longlong()
-            L.vg_ctx_launch_count(ctx_of(s), ctypes.byref(c))
-            tot += c.value
+            for cx in (s.ctx(), s.commit_ctx()):
+                c = ctypes.c_longlong()
+                L.vg_ctx_launch_count(cx, ctypes.byref(c))
+                tot += c.value
         return tot
 
     # warm-up: every session proves once per warm-up step
@@ -277,16 +278,22 @@ def ours(args, layers, rank, world):
     t_batch = max_over_ranks(t_batch, world)
 
     # ---- per-kernel profile (separate pass, one stream, events around every launch) ----
-    vb.check(L.vg_ctx_profile(ctx0, 1))
+    pctxs = (ctx0, base.commit_ctx())   # sumcheck stream and commitment stream
+    for cx in pctxs:
+        vb.check(L.vg_ctx_profile(cx, 1))
     for k in range(args.steps):
         base.prove(seed0 + 500 + k, transcript=False)
     fam = {}
     for i, name in enumerate(FAMILIES):
-        n, t, b = ctypes.c_longlong(), ctypes.c_double(), ctypes.c_double()
-        vb.check(L.vg_ctx_profile_read(ctx0, i, ctypes.byref(n), ctypes.byref(t), ctypes.byref(b)))
-        if n.value:
-            fam[name] = {"launches": n.value / args.steps, "ms": t.value / args.steps, "bytes": b.value / args.steps}
-    vb.check(L.vg_ctx_profile(ctx0, 0))
+        tot_n, tot_t, tot_b = 0, 0.0, 0.0
+        for cx in pctxs:
+            n, t, b = ctypes.c_longlong(), ctypes.c_double(), ctypes.c_double()
+            vb.check(L.vg_ctx_profile_read(cx, i, ctypes.byref(n), ctypes.byref(t), ctypes.byref(b)))
+            tot_n, tot_t, tot_b = tot_n + n.value, tot_t + t.value, tot_b + b.value
+        if tot_n:
+            fam[name] = {"launches": tot_n / args.steps, "ms": tot_t / args.steps, "bytes": tot_b / args.steps}
+    for cx in pctxs:
+        vb.check(L.vg_ctx_profile(cx, 0))
     for s in sessions[1:]:
         s.close()
 

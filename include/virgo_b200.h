@@ -366,6 +366,10 @@ int vg_server_wait(vg_server *s, long long job_id, vg_job_info *info, uint8_t **
 int vg_server_destroy(vg_server *s);
 /* The context (stream) a session runs on. */
 int vg_session_ctx(vg_session *s, vg_ctx **out);
+/* The context of the session's commitment work (its second stream; the
+ * commitment overlaps the sumcheck rounds).  Profile both contexts to see a
+ * whole proof. */
+int vg_session_commit_ctx(vg_session *s, vg_ctx **out);
 void vg_free(void *p);
 
 #ifdef __cplusplus

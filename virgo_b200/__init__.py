@@ -99,6 +99,7 @@ def lib():
             "vg_session_fork": (c_i, [c_p, ctypes.POINTER(c_p)]),
             "vg_session_prove_batch": (c_i, [c_p, c_i, c_p, c_i, c_p, c_p, c_p]),
             "vg_session_new": (c_i, [ctypes.POINTER(c_p)]),
+            "vg_session_commit_ctx": (c_i, [c_p, ctypes.POINTER(c_p)]),
             "vg_circuit_write_binary": (c_i, [ctypes.c_char_p, c_i, c_p, c_p, c_p, c_p, c_i]),
             "vg_circuit_is_binary": (c_i, [ctypes.c_char_p]),
             "vg_circuit_binary_info": (c_i, [ctypes.c_char_p, ctypes.POINTER(c_i), ctypes.POINTER(c_i), c_p, c_i]),
@@ -274,6 +275,12 @@ class Session:
     def ctx(self):
         c = ctypes.c_void_p()
         check(lib().vg_session_ctx(self.h, ctypes.byref(c)), "vg_session_ctx")
+        return c
+
+    def commit_ctx(self):
+        """the context (second stream) of the commitment work"""
+        c = ctypes.c_void_p()
+        check(lib().vg_session_commit_ctx(self.h, ctypes.byref(c)), "vg_session_commit_ctx")
         return c
 
     def close(self):

@@ -613,12 +613,11 @@ extern "C" int vg_pc_query_step(vg_pc *pc, int lvl, long pow, vg_fe *values, vg_
 static int ensure_pinned(vg_pc *pc, size_t elems)
 {
     if (elems <= pc->hpin_cap) return VG_OK;
-    VG_CHECK_CUDA(cudaStreamSynchronize(pc->ctx->stream));
-    if (pc->hpin) cudaFreeHost(pc->hpin);
-    pc->hpin = nullptr;
-    pc->hpin_cap = 0;
-    VG_CHECK_CUDA(cudaMallocHost((void **)&pc->hpin, elems * sizeof(fe)));
-    pc->hpin_cap = elems;
+    void *p = pc->hpin;
+    size_t cap = pc->hpin_cap * sizeof(fe);
+    VG_TRY(vg_pinned_grow(pc->ctx, &p, &cap, elems * sizeof(fe)));
+    pc->hpin = (fe *)p;
+    pc->hpin_cap = cap / sizeof(fe);
     return VG_OK;
 }
 

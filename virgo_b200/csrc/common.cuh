@@ -50,6 +50,7 @@ struct vg_ctx {
     size_t pinned_cap = 0;
     // pinned ring for uploads from pageable host memory (vg_h2d_staged)
     char *ring[2] = {nullptr, nullptr};
+    std::vector<void *> retired_pinned;   // outgrown pinned blocks, freed with the context
     cudaEvent_t ring_ev[2] = {nullptr, nullptr};
     // per-launch profiler: event pairs around launches of each kernel family
     bool profiling = false;
@@ -110,6 +111,11 @@ int vg_fail(int code, const char *fmt, ...);
 // source is copied directly and must stay valid until the stream reaches the
 // copy.
 int vg_h2d_staged(vg_ctx *c, void *dst, const void *src, size_t bytes);
+
+// Grows a pinned host buffer geometrically without synchronising: the
+// outgrown block is retired (freed when the context is destroyed), since
+// cudaFreeHost would wait for the whole device.
+int vg_pinned_grow(vg_ctx *c, void **p, size_t *cap, size_t bytes);
 
 // stream-ordered device memory from the device pool (see ctx.cu)
 int vg_alloc(vg_ctx *c, void **p, size_t bytes);

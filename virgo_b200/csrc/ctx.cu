@@ -200,6 +200,7 @@ extern "C" int vg_ctx_destroy(vg_ctx *c)
     if (c->scratch2) cudaFree(c->scratch2);
     if (c->partials) cudaFree(c->partials);
     if (c->pinned) cudaFreeHost(c->pinned);
+    for (void *q : c->retired_pinned) cudaFreeHost(q);
     for (int k = 0; k < 2; ++k) {
         if (c->ring[k]) cudaFreeHost(c->ring[k]);
         if (c->ring_ev[k]) cudaEventDestroy(c->ring_ev[k]);
@@ -340,21 +341,28 @@ int vg_partials(vg_ctx *c, size_t n, fe **p)
     *p = c->partials;
     return VG_OK;
 }
+int vg_pinned_grow(vg_ctx *c, void **p, size_t *cap, size_t bytes)
+{
+    if (bytes <= *cap) return VG_OK;
+    size_t ncap = std::max(bytes, std::max(2 * *cap, (size_t)1 << 20));
+    void *q = nullptr;
+    VG_CHECK_CUDA(cudaMallocHost(&q, ncap));
+    if (*p) c->retired_pinned.push_back(*p);
+    *p = q;
+    *cap = ncap;
+    return VG_OK;
+}
+
 int vg_pinned(vg_ctx *c, size_t n, fe **p)
 {
-    size_t bytes = n * sizeof(fe);
-    if (bytes > c->pinned_cap) {
-        VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
-        if (c->pinned) cudaFreeHost(c->pinned);
-        c->pinned = nullptr;
-        c->pinned_cap = 0;
-        size_t cap = bytes < 65536 ? 65536 : bytes;
-        VG_CHECK_CUDA(cudaMallocHost((void **)&c->pinned, cap));
-        c->pinned_cap = cap;
-    }
+    void *q = c->pinned;
+    VG_TRY(vg_pinned_grow(c, &q, &c->pinned_cap, n * sizeof(fe)));
+    c->pinned = (fe *)q;
     *p = c->pinned;
     return VG_OK;
 }
+
+int vg_ctx_grow_dev(vg_ctx *c, void **p, size_t *cap, size_t bytes) { return grow(c, p, cap, bytes); }
 
 bool vg_is_device_ptr(const void *p)
 {

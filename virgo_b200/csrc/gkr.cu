@@ -1937,12 +1937,11 @@ int vg_gkr_records(vg_gkr *g, const vg_fe **host, int *n)
     if (!g || !host || !n) return vg_fail(VG_ERR_ARG, "vg_gkr_records: null argument");
     VG_TRY(flush_rounds(g));
     if (g->rec_n > g->rec_host_cap) {
-        VG_CHECK_CUDA(cudaStreamSynchronize(g->ctx->stream));
-        if (g->rec_host) cudaFreeHost(g->rec_host);
-        g->rec_host = nullptr;
-        g->rec_host_cap = 0;
-        VG_CHECK_CUDA(cudaMallocHost((void **)&g->rec_host, (size_t)g->rec_cap * 9 * sizeof(fe)));
-        g->rec_host_cap = g->rec_cap;
+        void *p = g->rec_host;
+        size_t cap = (size_t)g->rec_host_cap * 9 * sizeof(fe);
+        VG_TRY(vg_pinned_grow(g->ctx, &p, &cap, (size_t)g->rec_cap * 9 * sizeof(fe)));
+        g->rec_host = (fe *)p;
+        g->rec_host_cap = (int)(cap / (9 * sizeof(fe)));
     }
     if (g->rec_n)
         VG_CHECK_CUDA(cudaMemcpyAsync(g->rec_host, g->rec, (size_t)g->rec_n * 9 * sizeof(fe), cudaMemcpyDeviceToHost,

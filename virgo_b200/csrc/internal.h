@@ -18,6 +18,9 @@ int vg_gkr_phase2_init_deferred(vg_gkr *g, const vg_fe *r_u, int length_u, vg_fe
 // Enqueues the copy of all records to pinned host memory (*host, 9 * *n values).
 int vg_gkr_records(vg_gkr *g, const vg_fe **host, int *n);
 
+// Grows a device buffer from the stream-ordered pool on c's stream.
+int vg_ctx_grow_dev(vg_ctx *c, void **p, size_t *cap, size_t bytes);
+
 // vg_eq_table without the final synchronisation.
 int vg_eq_table_async(vg_ctx *c, const vg_fe *r, int log_len, vg_fe *pub);
 

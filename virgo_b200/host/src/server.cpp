@@ -193,12 +193,23 @@ extern "C" int vg_server_create(int device, int slots, size_t hbm_budget, vg_ser
         hbm_budget = (fr + (reserved > used ? reserved - used : 0)) / 10 * 9;
     }
     s->budget = hbm_budget;
-    {   // stream-ordered allocations keep their freed blocks (see vg_alloc)
+    {   // stream-ordered allocations keep their freed blocks (see vg_alloc); the
+        // budget is reserved in the pool up front, so sessions growing their
+        // buffers for a larger circuit draw reserved memory instead of mapping
+        // new memory through the driver while the other slots prove
         cudaSetDevice(device);
         cudaMemPool_t pool;
-        uint64_t thr = ~0ull;
-        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess)
-            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+        uint64_t thr = ~0ull, reserved = 0;
+        cudaStream_t st;
+        if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess &&
+            cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr) == cudaSuccess &&
+            cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved) == cudaSuccess &&
+            reserved < hbm_budget && cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) == cudaSuccess) {
+            void *p = nullptr;
+            if (cudaMallocAsync(&p, hbm_budget - reserved, st) == cudaSuccess) cudaFreeAsync(p, st);
+            cudaStreamSynchronize(st);
+            cudaStreamDestroy(st);
+        }
         cudaGetLastError();
     }
     s->held.assign(slots, 0);

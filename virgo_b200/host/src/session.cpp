@@ -111,6 +111,8 @@ struct vg_session {
     vg_ctx *ctx = nullptr;
     vg_pc *pc = nullptr;
     zk_prover *p = nullptr;
+    vg_ctx *cctx = nullptr;   // the commitment's context: its own stream, so the
+                              // commitment overlaps the sumcheck rounds
     void *pub = nullptr;   // device buffer for the public eq table
     size_t pub_bytes = 0;
     bool loaded = false;   // false after a failed load: no valid circuit
@@ -129,7 +131,13 @@ static int session_attach(vg_session *s)
     int rc = s->ctx ? VG_OK : session_device(&s->ctx);
     if (rc != VG_OK) return rc;
     rc = vg_ctx_set_hash(s->ctx, virgo_hash_kind());
-    if (rc == VG_OK && !s->pc) rc = vg_pc_create(s->ctx, &s->pc);
+    if (rc == VG_OK && !s->cctx) {
+        int dev = 0;
+        vg_ctx_device(s->ctx, &dev);
+        rc = vg_ctx_create(dev, &s->cctx);
+    }
+    if (rc == VG_OK) rc = vg_ctx_set_hash(s->cctx, virgo_hash_kind());
+    if (rc == VG_OK && !s->pc) rc = vg_pc_create(s->cctx, &s->pc);
     if (rc != VG_OK) return rc;
     if (!s->p) {
         s->p = new zk_prover();
@@ -305,8 +313,9 @@ extern "C" int vg_session_destroy(vg_session *s)
         s->p->delete_self();
         delete s->p;
     }
-    if (s->pub) vg_dev_free(s->ctx, s->pub);
+    if (s->pub) vg_dev_free(s->cctx, s->pub);
     if (s->pc) vg_pc_destroy(s->pc);
+    if (s->cctx) vg_ctx_destroy(s->cctx);
     s->circuit.reset();
     if (s->ctx) vg_ctx_destroy(s->ctx);
     delete s;
@@ -322,6 +331,13 @@ extern "C" int vg_session_depth(vg_session *s, int *depth, int *input_log)
 }
 
 extern "C" void vg_free(void *p) { free(p); }
+
+extern "C" int vg_session_commit_ctx(vg_session *s, vg_ctx **out)
+{
+    if (!s || !out) return vg_fail(VG_ERR_ARG, "vg_session_commit_ctx: null argument");
+    *out = s->cctx;
+    return VG_OK;
+}
 
 extern "C" int vg_session_ctx(vg_session *s, vg_ctx **out)
 {
@@ -609,14 +625,13 @@ static int prove_pass(vg_session *s, unsigned seed, bool launch, PassResults &re
 
     if (launch) {
         const size_t pub_bytes = ((size_t)1 << L) * sizeof(F);
-        if (s->pub_bytes < pub_bytes) {
-            if (s->pub) vg_dev_free(s->ctx, s->pub);
-            s->pub = nullptr;
-            int rc = vg_dev_alloc(s->ctx, pub_bytes, &s->pub);
+        if (s->pub_bytes < pub_bytes) {   // stream ordered on the commitment stream: no device-wide wait
+            int rc = vg_ctx_grow_dev(s->cctx, &s->pub, &s->pub_bytes, pub_bytes);
             if (rc != VG_OK) return rc;
-            s->pub_bytes = pub_bytes;
         }
-        int rc = vg_eq_table_async(s->ctx, (const vg_fe *)r_0.data(), L, (vg_fe *)s->pub);
+        // the commitment depends on no GKR device result: it runs on its own
+        // stream, concurrently with the sumcheck work enqueued above
+        int rc = vg_eq_table_async(s->cctx, (const vg_fe *)r_0.data(), L, (vg_fe *)s->pub);
         if (rc == VG_OK)
             rc = vg_pc_prove_deferred(s->pc, (const vg_fe *)p.circuit_value[0], L, (const vg_fe *)p.all_pri_mask.data(),
                                       (long)p.all_pri_mask.size(), (const vg_fe *)s->pub,
@@ -732,6 +747,11 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
     memset(&st, 0, sizeof st);
     long long launches0 = 0;
     vg_ctx_launch_count(s->ctx, &launches0);
+    if (s->cctx) {
+        long long l2 = 0;
+        vg_ctx_launch_count(s->cctx, &l2);
+        launches0 += l2;
+    }
     zk_prover &p = *s->p;
 
     // launch pass: the whole proof enqueued on the session's stream
@@ -747,11 +767,13 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
     p.defer_mode = zk_prover::DEFER_OFF;
     if (rc != VG_OK) {
         vg_ctx_sync(s->ctx);   // drain what was enqueued before the error
+        vg_ctx_sync(s->cctx);
         return rc;
     }
     st.launch_s = since(t_all);
     auto t0 = clk::now();
     rc = vg_ctx_sync(s->ctx);
+    if (rc == VG_OK) rc = vg_ctx_sync(s->cctx);
     if (rc != VG_OK) return rc;
     st.wait_s = since(t0);
     st.prove_time = since(t_all);
@@ -770,6 +792,11 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
     st.proof_size = proof_size;
     long long launches1 = 0;
     vg_ctx_launch_count(s->ctx, &launches1);
+    {
+        long long l2 = 0;
+        vg_ctx_launch_count(s->cctx, &l2);
+        launches1 += l2;
+    }
     st.launches = launches1 - launches0;
     if (stats) *stats = st;
     if (transcript && transcript_len) {
