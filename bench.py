@@ -38,6 +38,12 @@ import time
 
 import numpy as np
 
+# load every kernel when the CUDA context is created: with lazy loading (the
+# CUDA 12 default) the first launch of a kernel in the timed region (e.g. a
+# gate type or table shape seen for the first time by the server) loads its
+# module mid-measurement
+os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
