@@ -142,6 +142,15 @@ int vg_circuit_build(vg_ctx *ctx, int d, const long *n, const uint8_t *const *ty
                      const void *const *v, int index_bytes, vg_circuit **inout, int *bit_lengths);
 int vg_circuit_destroy(vg_circuit *c);
 int vg_circuit_depth(const vg_circuit *c, int *depth);
+/* The verifier's wiring predicates of prover layer `layer` (>= 1) at
+ * (r_0, r_1; r_u, r_v): zk_verifier::predicates, zk_verifier.cpp:219-606,
+ * with the beta tables of zk_verifier::beta_init (alpha- and beta-weighted
+ * eq(r_0, g), eq(r_1, g); eq(r_u, .), eq(r_v, .)).  out[t], t < 14, is the
+ * sum over the layer's gates of type t; layer 1 (the reader's relay layer)
+ * gives zeros as in the reference.  r_0/r_1 have bl(layer) entries, r_u/r_v
+ * bl(layer - 1); all host.  Layers are taken as not data-parallel. */
+int vg_circuit_predicates(vg_ctx *ctx, const vg_circuit *c, int layer, const vg_fe *r_0, const vg_fe *r_1,
+                          const vg_fe *r_u, const vg_fe *r_v, vg_fe alpha, vg_fe beta, vg_fe *out);
 
 /* ------------------------------------------------------------------- GKR */
 /* State for proving one circuit; buffers are sized for its widest layer

@@ -478,6 +478,45 @@ void vo_phase2_init(const uint8_t *ty, const int64_t *u64, const int64_t *v64, l
     }
 }
 
+void vo_predicates(const uint8_t *ty, const int64_t *u64, const int64_t *v64, int bl_g, int bl_uv, const vo_fe *r0,
+                   const vo_fe *r1, const vo_fe *ru, const vo_fe *rv, const vo_fe *alpha, const vo_fe *beta,
+                   vo_fe out[14])
+{
+    const long n_g = 1L << bl_g, n_uv = 1L << bl_uv;
+    vo_fe *bg = malloc(n_g * sizeof(vo_fe)), *bu = malloc(n_uv * sizeof(vo_fe)), *bv = malloc(n_uv * sizeof(vo_fe));
+    vo_beta_g(bl_g, r0, r1, alpha, beta, bg);
+    for (long i = 0; i < n_uv; ++i) {
+        bu[i] = eq_at(ru, bl_uv, i);
+        bv[i] = eq_at(rv, bl_uv, i);
+    }
+    for (int t = 0; t < 14; ++t) out[t] = fe(0, 0);
+    for (long g = 0; g < n_g; ++g) {
+        const long u = u64[g], v = v64[g];
+        const int t = ty[g];
+        switch (t) {
+        case 0: case 1: case 6: case 7: case 8: case 9: case 13:
+            out[t] = fadd(out[t], fmul(fmul(bg[g], bu[u]), bv[v]));
+            break;
+        case 5:
+            for (long j = u; j < v; ++j) out[5] = fadd(out[5], fmul(fmul(bg[g], bv[0]), bu[j]));
+            break;
+        case 12: {
+            vo_fe w = fmul(bg[g], bv[0]);
+            for (long j = u; j <= v; ++j) {
+                out[12] = fadd(out[12], fmul(w, bu[j]));
+                w = fadd(w, w);
+            }
+        } break;
+        case 10: out[10] = fadd(out[10], fmul(bg[g], bu[u])); break;
+        default: break;
+        }
+    }
+    out[10] = fmul(out[10], bv[0]);
+    free(bg);
+    free(bu);
+    free(bv);
+}
+
 void vo_sumcheck_round(vo_lp *V, vo_lp *addv, vo_lp *am, long total_uv, const vo_fe *r, int current_bit, vo_fe out3[3])
 {
     vo_fe ra = fe(0, 0), rb = fe(0, 0), rc = fe(0, 0);

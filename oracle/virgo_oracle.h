@@ -79,6 +79,16 @@ void vo_phase1_init(const uint8_t *ty, const int64_t *u, const int64_t *v, long 
                     const vo_fe *prev, long n_uv, vo_fe *add_mult_b, vo_fe *addv_b);  /* :375-592 */
 void vo_phase2_init(const uint8_t *ty, const int64_t *u, const int64_t *v, long n_g, const vo_fe *beta_g,
                     const vo_fe *beta_u, const vo_fe *v_u, long n_uv, vo_fe *add_mult_b, vo_fe *addv_b); /* :789-972 */
+/* The verifier's wiring predicates of one layer (src/linear_gkr/zk_verifier.cpp
+ * :219-606, the layer not data-parallel): out[t] sums, over the layer's gates
+ * of type t, beta_g(g) beta_u(u) beta_v(v) with beta_g as vo_beta_g,
+ * beta_u = eq(r_u, .), beta_v = eq(r_v, .) over bl_uv bits; summation (5,
+ * u <= j < v) and exp-sum (12, u <= j <= v, weight 2^(j-u)) sum beta_u over
+ * the range times beta_v(0); relays (10) take beta_u(u), the total times
+ * beta_v(0).  Types 2, 3, 4 contribute nothing. */
+void vo_predicates(const uint8_t *ty, const int64_t *u, const int64_t *v, int bl_g, int bl_uv, const vo_fe *r0,
+                   const vo_fe *r1, const vo_fe *ru, const vo_fe *rv, const vo_fe *alpha, const vo_fe *beta,
+                   vo_fe out[14]);
 /* One round of sumcheck_phase{1,2}_update (:596-633, :988-1025) on the
  * linear-polynomial tables V_mult_add, addV_array, add_mult_sum ({a, b} pairs,
  * total_uv entries), in place exactly as the reference loop; returns the

@@ -23,7 +23,7 @@ def oracle():
         _o = ctypes.CDLL(LIB)
         for name in ["vo_fft", "vo_ifft", "vo_merkle_tree", "vo_leaf_chain", "vo_fri_fold", "vo_rs_encode",
                      "vo_commit_private", "vo_commit_public", "vo_eval_input", "vo_eval_layer", "vo_v_res",
-                     "vo_beta_g", "vo_phase1_init", "vo_phase2_init", "vo_hash64_batch"]:
+                     "vo_beta_g", "vo_phase1_init", "vo_phase2_init", "vo_hash64_batch", "vo_predicates"]:
             getattr(_o, name).restype = ctypes.c_long if name == "vo_commit_private" else None
     return _o
 
@@ -168,6 +168,36 @@ def phase2_init(ty, u, v, bg, bu, vu, n_uv):
                             vp(np.ascontiguousarray(v, dtype=np.int64)), L(len(ty)), vp(bg), vp(bu),
                             vp(np.ascontiguousarray(vu)), L(n_uv), vp(am), vp(av))
     return am, av
+
+
+def predicates(layers, which, r0, r1, ru, rv, alpha, beta):
+    """the wiring predicates of layer `which` (>= 2) of prover-level layers"""
+    t, u, v = layers[which]
+    bl_g = len(t).bit_length() - 1
+    bl_uv = len(layers[which - 1][0]).bit_length() - 1
+    out = np.zeros((14, 2), np.uint64)
+    oracle().vo_predicates(vp(np.ascontiguousarray(t, dtype=np.uint8)), vp(np.ascontiguousarray(u, dtype=np.int64)),
+                           vp(np.ascontiguousarray(v, dtype=np.int64)), bl_g, bl_uv,
+                           *[vp(np.ascontiguousarray(x)) for x in (r0, r1, ru, rv, alpha, beta)], vp(out))
+    return out
+
+
+def ref_predicates(layers, which, r0, r1, ru, rv, alpha, beta):
+    """the same through the reference's own zk_verifier::predicates (the C
+    shim oracle/_ref/libvirgo_refverifier.so); None when it is not built"""
+    path = os.path.join(REF_DIR, "libvirgo_refverifier.so")
+    if not os.path.exists(path):
+        return None
+    lib = ctypes.CDLL(path)
+    d = len(layers)
+    bl = np.array([len(t).bit_length() - 1 for t, _, _ in layers], np.int32)
+    keep = [[np.ascontiguousarray(t, np.uint8), np.ascontiguousarray(u, np.int64), np.ascontiguousarray(v, np.int64)]
+            for t, u, v in layers]
+    ptrs = [(ctypes.c_void_p * d)(*[k[j].ctypes.data for k in keep]) for j in range(3)]
+    out = np.zeros((14, 2), np.uint64)
+    lib.ref_predicates(d, vp(bl), *ptrs, which, *[vp(np.ascontiguousarray(x)) for x in (r0, r1, ru, rv, alpha, beta)],
+                       vp(out))
+    return out
 
 
 class RoundTables:

@@ -119,12 +119,57 @@ def kernels():
         d = np.zeros(32, np.uint8)
         L.ref_hash64(vp(m), vp(d))
         out["hash"].append({"seed": 4000 + k, "sha3_256": d.tobytes().hex()})
+    out["predicates"] = predicates()
+    return out
+
+
+PRED_CASES = [
+    # name, generator, params
+    ("mixed_gates", "mixed_gates", {"seed": 3}),
+    ("random_5layer", "random_layered", {"log_widths": [10, 12, 11, 12, 9], "seed": 4}),
+    ("sha256_1block", "sha256_blocks", {"blocks": 1, "seed": 7}),
+]
+
+
+def pred_inputs(case_idx, layers, which):
+    """r_0, r_1 (bit length of layer `which`), r_u, r_v (of the layer below),
+    alpha, beta: seeded as fe_random(6000 + 100 * case + layer + k)."""
+    lg = len(layers[which][0]).bit_length() - 1
+    luv = len(layers[which - 1][0]).bit_length() - 1
+    base = 6000 + 100 * case_idx + 10 * which
+    return [fe_random(base + k, n) for k, n in enumerate([lg, lg, luv, luv, 1, 1])]
+
+
+def predicates():
+    """zk_verifier::predicates of every layer >= 1, through the shim
+    oracle/_ref/libvirgo_refverifier.so over the reference's own objects."""
+    import hashlib
+    from virgo_b200 import sha256_circuit
+    L = ctypes.CDLL(os.path.join(REF, "libvirgo_refverifier.so"))
+    vp = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    out = []
+    for ci, (name, gen, params) in enumerate(PRED_CASES):
+        layers = (sha256_circuit.sha256_blocks(**params) if gen == "sha256_blocks"
+                  else getattr(circuits, gen)(**params))
+        d = len(layers)
+        bl = np.array([len(t).bit_length() - 1 for t, _, _ in layers], np.int32)
+        keep = [[np.ascontiguousarray(t, np.uint8), np.ascontiguousarray(u, np.int64),
+                 np.ascontiguousarray(v, np.int64)] for t, u, v in layers]
+        ptrs = [(ctypes.c_void_p * d)(*[k[j].ctypes.data for k in keep]) for j in range(3)]
+        res = []
+        for which in range(1, d):
+            ins = pred_inputs(ci, layers, which)
+            o = np.zeros((14, 2), np.uint64)
+            L.ref_predicates(d, vp(bl), *ptrs, which, *[vp(x) for x in ins], vp(o))
+            res.append(o.tobytes().hex())
+        out.append({"name": name, "generator": gen, "params": params,
+                    "layers": [hashlib.sha256(bytes.fromhex(h)).hexdigest() for h in res] if d > 12 else res})
     return out
 
 
 if __name__ == "__main__":
     here = os.path.dirname(os.path.abspath(__file__))
     with open(os.path.join(here, "kernels.json"), "w") as f:
-        json.dump(kernels(), f)
+        json.dump(kernels(), f, indent=0)
     with open(os.path.join(here, "transcripts.json"), "w") as f:
         json.dump(transcripts(), f, indent=0)

@@ -359,3 +359,36 @@ def test_commit_all_matches_step_api(ctx, log_len):
             assert (p2[q * 32:q * 32 + k] == qp[q * 32:q * 32 + k]).all(), ("query", q)
     finally:
         L.vg_pc_destroy(pc)
+
+
+def _pred_inputs(seed, layers, which):
+    lg = len(layers[which][0]).bit_length() - 1
+    luv = len(layers[which - 1][0]).bit_length() - 1
+    return [O.fe_random(seed + k, n) for k, n in enumerate([lg, lg, luv, luv, 1, 1])]
+
+
+@pytest.mark.parametrize("case", ["mixed", "random", "sha4"])
+def test_circuit_predicates(ctx, case):
+    """vg_circuit_predicates (the verifier's wiring predicates as a reduction
+    over the device circuit) on every layer against the restatement, and
+    against the reference function itself where its shim was built; the
+    4-block SHA-256 circuit has summation gates over wide ranges."""
+    from virgo_b200 import circuits, sha256_circuit
+    layers = {"mixed": circuits_small, "random": lambda: circuits.random_layered([9, 11, 10, 12, 8], seed=5),
+              "sha4": lambda: sha256_circuit.sha256_blocks(4, seed=7)}[case]()
+    hc = _upload(ctx, layers)
+    try:
+        for which in range(1, len(layers)):
+            r0, r1, ru, rv, a, b = _pred_inputs(700 + 10 * which, layers, which)
+            got = np.zeros((14, 2), np.uint64)
+            vb.check(vb.lib().vg_circuit_predicates(ctx.h, hc, which, vb.ptr(r0), vb.ptr(r1), vb.ptr(ru), vb.ptr(rv),
+                                                    vb.to_fe(a[0]), vb.to_fe(b[0]), vb.ptr(got)))
+            if which == 1:
+                assert not got.any()
+                continue
+            exp = O.predicates(layers, which, r0, r1, ru, rv, a, b)
+            assert (got == exp).all(), (case, which)
+            ref = O.ref_predicates(layers, which, r0, r1, ru, rv, a, b) if case != "sha4" else None
+            assert ref is None or (got == ref).all(), (case, which)
+    finally:
+        vb.lib().vg_circuit_destroy(hc)

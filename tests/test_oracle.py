@@ -155,3 +155,47 @@ def test_commit_restatement_consistency():
         return acc[0]
     ip = total(np.concatenate([mul(np.ascontiguousarray(priv), np.ascontiguousarray(pub)), mul(pm, pub_mask)]))
     assert (total(sums) == ip).all()
+
+
+def _pred_case(case):
+    from virgo_b200 import circuits, sha256_circuit
+    gen = sha256_circuit.sha256_blocks if case["generator"] == "sha256_blocks" else getattr(circuits, case["generator"])
+    return gen(**case["params"])
+
+
+def _pred_inputs(case_idx, layers, which):
+    """the seeding of tests/golden/make_golden.py:pred_inputs"""
+    lg = len(layers[which][0]).bit_length() - 1
+    luv = len(layers[which - 1][0]).bit_length() - 1
+    base = 6000 + 100 * case_idx + 10 * which
+    return [O.fe_random(base + k, n) for k, n in enumerate([lg, lg, luv, luv, 1, 1])]
+
+
+def test_predicates_golden():
+    """The restatement of zk_verifier::predicates against the reference's own
+    outputs (every layer of three circuits; every gate type the builders make,
+    summation and exp-sum ranges, relays)."""
+    cases = _kernels()["predicates"]
+    nonzero = set()
+    for ci, case in enumerate(cases):
+        layers = _pred_case(case)
+        assert len(case["layers"]) == len(layers) - 1
+        for which in range(1, len(layers)):
+            got = (np.zeros((14, 2), np.uint64) if which == 1
+                   else O.predicates(layers, which, *_pred_inputs(ci, layers, which)))
+            nonzero |= {t for t in range(14) if got[t].any()}
+            assert _same(got, case["layers"][which - 1]) or \
+                hashlib.sha256(got.tobytes()).hexdigest() == case["layers"][which - 1], (case["name"], which)
+    assert {0, 1, 5, 6, 7, 8, 9, 10, 12, 13} <= nonzero
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(O.REF_DIR, "libvirgo_refverifier.so")),
+                    reason="reference verifier shim not built")
+def test_predicates_match_reference_live():
+    """Fresh random circuits straight through the reference function."""
+    from virgo_b200 import circuits
+    for seed, layers in enumerate([circuits.random_layered([7, 9, 8, 10, 6], seed=21),
+                                   circuits.mixed_gates(8, log_width=5)]):
+        for which in range(2, len(layers)):
+            ins = _pred_inputs(50 + seed, layers, which)
+            assert (O.predicates(layers, which, *ins) == O.ref_predicates(layers, which, *ins)).all(), (seed, which)

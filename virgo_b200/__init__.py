@@ -70,6 +70,7 @@ def lib():
             "vg_leaf_chain": (c_i, [c_p, c_p, c_i, c_l, c_p]),
             "vg_circuit_upload": (c_i, [c_p, c_i, c_p, c_p, c_p, c_p, ctypes.POINTER(c_p)]),
             "vg_circuit_destroy": (c_i, [c_p]),
+            "vg_circuit_predicates": (c_i, [c_p, c_p, c_i, c_p, c_p, c_p, c_p, vg_fe, vg_fe, c_p]),
             "vg_gkr_create": (c_i, [c_p, c_p, ctypes.POINTER(c_p)]),
             "vg_gkr_destroy": (c_i, [c_p]),
             "vg_gkr_evaluate": (c_i, [c_p]),

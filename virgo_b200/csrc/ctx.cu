@@ -454,6 +454,7 @@ int vg_reduce_partials(vg_ctx *c, const fe *parts, int nparts, int K, fe *out_de
     switch (K) {
     case 1: k_reduce_parts<1><<<1, 1024, 0, c->stream>>>(parts, nparts, out_dev); break;
     case 3: k_reduce_parts<3><<<1, 1024, 0, c->stream>>>(parts, nparts, out_dev); break;
+    case 14: k_reduce_parts<14><<<1, 256, 0, c->stream>>>(parts, nparts, out_dev); break;
     default: return vg_fail(VG_ERR_ARG, "vg_reduce_partials: K=%d unsupported", K);
     }
     VG_LAUNCHED(c);

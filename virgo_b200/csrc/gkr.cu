@@ -748,6 +748,58 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
     if (t == 0) *counter = 0;
 }
 
+// ------------------------------------------------ verifier's wiring predicates
+// zk_verifier::predicates (zk_verifier.cpp:219-606) for a layer that is not
+// data-parallel: per gate type t, the sum over the layer's gates of type t of
+// beta_g(g) * beta_u(u) * beta_v(v), with the reference's special forms for
+// summation (5: over u <= j < v, times beta_v(0)), exp-sum (12: over
+// u <= j <= v, times 2^(j-u) beta_v(0)) and relay (10: times beta_v(0) once at
+// the end); beta_g = alpha eq(r_0, g) + beta eq(r_1, g).  One partial of 14
+// values per CTA.
+constexpr int PRED_THREADS = 256;
+__global__ void __launch_bounds__(PRED_THREADS) k_predicates(const uint8_t *__restrict__ ty, const uint32_t *__restrict__ uu,
+                                                            const uint32_t *__restrict__ vv, long ng, BetaG bg, BetaU bu,
+                                                            BetaU bv, uint32_t vmask, fe *__restrict__ parts)
+{
+    __shared__ fe sm[14 * 32];
+    fe acc[14];
+#pragma unroll
+    for (int k = 0; k < 14; ++k) acc[k] = vg::fe_zero();
+    const fe bv0 = bv.at(0);
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < ng; g += (long)gridDim.x * blockDim.x) {
+        const int t = ty[g];
+        if (t == 2 || t == 3 || t == 4 || t == 11 || t > 13) continue;
+        const uint32_t u = uu[g], v = vv[g];
+        const fe b = bg.at(g);
+        switch (t) {
+        case 5: {
+            fe s = vg::fe_zero();
+            for (uint32_t j = u; j < v; ++j) s = s + bu.at(j);
+            acc[5] = acc[5] + (b * bv0) * s;
+        } break;
+        case 12: {
+            fe s = vg::fe_zero();
+            for (uint32_t j = u; j <= v; ++j) s = s + vg::fe_mul_pow2(bu.at(j), (int)(j - u));
+            acc[12] = acc[12] + (b * bv0) * s;
+        } break;
+        case 10: acc[10] = acc[10] + b * bu.at(u); break;
+        // v of a type-6 gate is not checked at upload (the gate reads u only);
+        // masking keeps the read in bounds and leaves valid wires unchanged
+        default: acc[t] = acc[t] + (b * bu.at(u)) * bv.at(v & vmask); break;
+        }
+    }
+    block_sum<14>(acc, sm);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 14; ++k) parts[(long)blockIdx.x * 14 + k] = acc[k];
+}
+
+// ret[10] *= beta_v(0), the product of the two half tables' first entries
+// (zk_verifier.cpp:600)
+__global__ void k_predicates_relay(fe *__restrict__ out, const fe *__restrict__ bv_lo, const fe *__restrict__ bv_hi)
+{
+    out[10] = out[10] * (bv_lo[0] * bv_hi[0]);
+}
+
 // v_u = V(r_u) + mask term: the folded V pair of the last phase-1 round at r
 // (zk_prover.cpp:796-797), computed where the pair is, so phase 2 can start
 // without the host reading it first
@@ -1668,6 +1720,54 @@ extern "C" int vg_eq_table(vg_ctx *c, const vg_fe *r, int log_len, vg_fe *pub)
 }
 
 int vg_eq_table_async(vg_ctx *c, const vg_fe *r, int log_len, vg_fe *pub) { return eq_table(c, r, log_len, pub); }
+
+extern "C" int vg_circuit_predicates(vg_ctx *c, const vg_circuit *C, int layer, const vg_fe *r_0, const vg_fe *r_1,
+                                     const vg_fe *r_u, const vg_fe *r_v, vg_fe alpha, vg_fe beta, vg_fe *out)
+{
+    if (!c || !C || !r_0 || !r_1 || !r_u || !r_v || !out) return vg_fail(VG_ERR_ARG, "vg_circuit_predicates: null argument");
+    if (layer < 1 || layer >= C->depth) return vg_fail(VG_ERR_ARG, "vg_circuit_predicates: layer %d out of range", layer);
+    if (layer == 1) {   // the reader's relay layer: the reference returns zeros (zk_verifier.cpp:231-234)
+        for (int t = 0; t < 14; ++t) out[t] = vg_fe{0, 0};
+        return VG_OK;
+    }
+    const DevLayer &D = C->L[layer];
+    const int lg = D.bl, luv = C->L[layer - 1].bl;   // at most 30 (checked at upload)
+    const int fg = lg >> 1, sg = lg - fg, fuv = luv >> 1, suv = luv - fuv;
+    const long hg = 1L << std::max(fg, sg), huv = 1L << std::max(fuv, suv);
+    const int nb = 148 * 4;
+    // scratch: r values, 4 g halves, 4 u/v halves, partials, result
+    const size_t n_fe = 4 * 64 + 4 * hg + 4 * huv + (size_t)nb * 14 + 16;
+    fe *w;
+    VG_TRY(vg_scratch(c, n_fe * sizeof(fe), (void **)&w));
+    fe *rr = w, *tg = rr + 4 * 64, *tuv = tg + 4 * hg, *parts = tuv + 4 * huv, *res = parts + (size_t)nb * 14;
+    VG_CHECK_CUDA(cudaMemcpyAsync(rr, r_0, lg * sizeof(fe), cudaMemcpyHostToDevice, c->stream));
+    VG_CHECK_CUDA(cudaMemcpyAsync(rr + 64, r_1, lg * sizeof(fe), cudaMemcpyHostToDevice, c->stream));
+    VG_CHECK_CUDA(cudaMemcpyAsync(rr + 128, r_u, luv * sizeof(fe), cudaMemcpyHostToDevice, c->stream));
+    VG_CHECK_CUDA(cudaMemcpyAsync(rr + 192, r_v, luv * sizeof(fe), cudaMemcpyHostToDevice, c->stream));
+    int fh;
+    EqJobs J1{}, J2{};
+    add_halves(J1, rr, lg, tofe(alpha), tg, tg + hg, &fh);
+    add_halves(J1, rr + 64, lg, tofe(beta), tg + 2 * hg, tg + 3 * hg, &fh);
+    add_halves(J2, rr + 128, luv, vg::fe_one(), tuv, tuv + huv, &fh);
+    add_halves(J2, rr + 192, luv, vg::fe_one(), tuv + 2 * huv, tuv + 3 * huv, &fh);
+    for (const EqJobs *J : {&J1, &J2}) {
+        k_eq_halves<<<grid_for(J->begin[J->count], 256), 256, 0, c->stream>>>(*J);
+        VG_LAUNCHED(c);
+    }
+    BetaG bg{tg, tg + hg, tg + 2 * hg, tg + 3 * hg, fg, (1L << fg) - 1};
+    BetaU bu{tuv, tuv + huv, fuv, (1L << fuv) - 1};
+    BetaU bv{tuv + 2 * huv, tuv + 3 * huv, fuv, (1L << fuv) - 1};
+    k_predicates<<<nb, PRED_THREADS, 0, c->stream>>>(D.ty, D.u, D.v, D.n, bg, bu, bv, (uint32_t)((1L << luv) - 1), parts);
+    VG_LAUNCHED(c);
+    VG_TRY(vg_reduce_partials(c, parts, nb, 14, res));
+    k_predicates_relay<<<1, 1, 0, c->stream>>>(res, tuv + 2 * huv, tuv + 3 * huv);
+    VG_LAUNCHED(c);
+    fe host[14];
+    VG_CHECK_CUDA(cudaMemcpyAsync(host, res, 14 * sizeof(fe), cudaMemcpyDeviceToHost, c->stream));
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    for (int t = 0; t < 14; ++t) out[t] = tovg(host[t]);
+    return VG_OK;
+}
 
 // the phase's tables (add_mult_sum in buf[0][2], addV_array in buf[0][1]) are
 // in place: the rounds start from them
