@@ -2,6 +2,7 @@
  * the checker and the timed CPU baseline, never the product.  See
  * virgo_oracle.h for the contract and the reference line each routine
  * restates.  Plain C11 (with the GCC 128-bit integer extension). */
+#define _GNU_SOURCE   /* random_r: a private rand() stream */
 #include "virgo_oracle.h"
 #include <stdlib.h>
 #include <string.h>
@@ -542,3 +543,251 @@ void vo_sumcheck_round(vo_lp *V, vo_lp *addv, vo_lp *am, long total_uv, const vo
 }
 
 int vo_is_zero(const vo_fe *a) { return fzero(*a); }
+
+/* ------------------------------------------------------------ fft_gkr */
+/* prime_field::random (prime_field.cpp:35-41): real, then img, each rand() */
+typedef struct { struct random_data d; char st[128]; } vo_rng;
+static void rng_init(vo_rng *g, unsigned seed) { memset(g, 0, sizeof *g); initstate_r(seed, g->st, sizeof g->st, &g->d); }
+static vo_fe rng_fe(vo_rng *g)
+{
+    int32_t a, b;
+    random_r(&g->d, &a);
+    random_r(&g->d, &b);
+    return fe((uint64_t)a % P61, (uint64_t)b % P61);
+}
+static void rng_fill(vo_rng *g, vo_fe *r, int n) { for (int i = 0; i < n; ++i) r[i] = rng_fe(g); }
+static vo_fe fone(void) { return fe(1, 0); }
+static int feq(vo_fe a, vo_fe b) { return a.real == b.real && a.img == b.img; }
+static vo_fe fomr(vo_fe r) { return fsub(fone(), r); }
+static vo_fe qeval(const vo_fe m[3], vo_fe x) { return fadd(fmul(fadd(fmul(m[0], x), m[1]), x), m[2]); }
+/* alpha eq(r0, g) + beta eq(r1, g) over len bits */
+static vo_fe bgat(const vo_fe *r0, const vo_fe *r1, int len, vo_fe al, vo_fe be, long g)
+{
+    return fadd(fmul(al, eq_at(r0, len, g)), fmul(be, eq_at(r1, len, g)));
+}
+
+int vo_fft_gkr_rounds(int lg) { return (lg + 6) + lg + 2 * lg * lg; }
+
+/* one phase: rounds over (V, addv, am) of 2^nv entries with challenges r;
+ * checks each message against *claim as fft_circuit_GKR.cpp:323-333 does */
+static int fg_phase(vo_lp *V, vo_lp *addv, vo_lp *am, int nv, const vo_fe *r, vo_fe *claim, vo_fe **msgs, vo_fe *vfinal)
+{
+    int ok = 1;
+    vo_fe prev = fe(0, 0);
+    for (int i = 0; i < nv; ++i) {
+        vo_fe m[3];
+        vo_sumcheck_round(V, addv, am, 1L << (nv - i), &prev, i, m);
+        memcpy(*msgs, m, sizeof m);
+        *msgs += 3;
+        prev = r[i];
+        if (!feq(fadd(qeval(m, fe(0, 0)), qeval(m, fone())), *claim)) ok = 0;
+        *claim = qeval(m, r[i]);
+    }
+    *vfinal = fadd(fmul(V[0].a, prev), V[0].b);
+    return ok;
+}
+
+int vo_fft_gkr(int lg, unsigned seed, vo_fe *msgs, vo_fe *vals, int *proof_size)
+{
+    const long N = 1L << lg, NE = 64L << lg;
+    vo_rng g;
+    rng_init(&g, seed);
+    /* ---- build_circuit (:22-112) ---- */
+    vo_fe *r = malloc(lg * sizeof(vo_fe)), ep[64];
+    rng_fill(&g, r, lg);
+    int nl = 2 * lg + 4;   /* layers 0..lg expansion, lg+1..2lg ifft, scaled, products, sums */
+    vo_fe **L = calloc(nl, sizeof(vo_fe *));
+    L[0] = malloc(sizeof(vo_fe));
+    L[0][0] = fone();
+    for (int i = 0; i < lg; ++i) {
+        L[i + 1] = malloc((2L << i) * sizeof(vo_fe));
+        for (long j = 0; j < (1L << i); ++j) {
+            L[i + 1][j << 1] = fmul(L[i][j], r[i]);
+            L[i + 1][j << 1 | 1] = fmul(L[i][j], fomr(r[i]));
+        }
+    }
+    const vo_fe rou = froot(lg), inv_rou = finv(rou), inv_n = finv(fconst((uint64_t)N));
+    vo_fe rot[62];
+    rot[0] = inv_rou;
+    for (int i = 1; i < 62; ++i) rot[i] = fmul(rot[i - 1], rot[i - 1]);
+    vo_fe *xa = malloc(N * sizeof(vo_fe));
+    for (int dep = lg - 1; dep >= 0; --dep) {
+        const long blk = 1L << (lg - dep), half = blk >> 1;
+        const int cur = lg + (lg - dep), pre = cur - 1;
+        L[cur] = malloc(N * sizeof(vo_fe));
+        xa[0] = fone();
+        for (long j = 1; j < blk; ++j) xa[j] = fmul(xa[j - 1], rot[dep]);
+        for (long k = 0; k < half; ++k)
+            for (long j = 0; j < (1L << dep); ++j) {
+                vo_fe l = L[pre][k << (dep + 1) | j], rr = fmul(xa[k], L[pre][k << (dep + 1) | (1L << dep) | j]);
+                L[cur][k << dep | j] = fadd(l, rr);
+                L[cur][(k + half) << dep | j] = fsub(l, rr);
+            }
+    }
+    const int Ls = 2 * lg + 1, Lp = 2 * lg + 2, Lo = 2 * lg + 3;
+    L[Ls] = malloc(N * sizeof(vo_fe));
+    for (long i = 0; i < N; ++i) L[Ls][i] = fmul(L[Ls - 1][i], inv_n);
+    L[Lp] = malloc(NE * sizeof(vo_fe));
+    for (int i = 0; i < 64; ++i) {
+        ep[i] = rng_fe(&g);
+        vo_fe x = fone();
+        for (long j = 0; j < N; ++j) {
+            L[Lp][j + ((long)i << lg)] = fmul(L[Ls][j], x);
+            x = fmul(x, ep[i]);
+        }
+    }
+    L[Lo] = malloc(64 * sizeof(vo_fe));
+    for (int i = 0; i < 64; ++i) {
+        L[Lo][i] = fe(0, 0);
+        for (long j = 0; j < N; ++j) L[Lo][i] = fadd(L[Lo][i], L[Lp][j + i * N]);
+    }
+    /* ---- engage_gkr (:786-825) ---- */
+    const int R = lg + 10;
+    vo_fe *r0 = malloc(R * sizeof(vo_fe)), *r1 = malloc(R * sizeof(vo_fe));
+    vo_fe *ru = malloc(R * sizeof(vo_fe)), *rv = malloc(R * sizeof(vo_fe));
+    rng_fill(&g, r0, R);
+    rng_fill(&g, r1, R);
+    vo_fe al = fone(), be = fe(0, 0), claim;
+    vo_v_res(L[Lo], 6, r0, &claim);   /* V_output (:134-150) */
+    vo_lp *V = malloc(NE * sizeof(vo_lp)), *AV = malloc(NE * sizeof(vo_lp)), *AM = malloc(NE * sizeof(vo_lp));
+    int ok = 1, nm = 0;
+    vo_fe *mp = msgs, vu, vv;
+    /* addition layer (:238-354): add_mult_sum[j] = beta_g(j / N) over 6 bits */
+    for (long j = 0; j < NE; ++j) {
+        V[j].a = fe(0, 0); V[j].b = L[Lp][j];
+        AV[j].a = AV[j].b = fe(0, 0);
+        AM[j].a = fe(0, 0); AM[j].b = bgat(r0, r1, 6, al, be, j >> lg);
+    }
+    rng_fill(&g, ru, lg + 6);
+    rng_fill(&g, rv, lg + 6);
+    ok &= fg_phase(V, AV, AM, lg + 6, ru, &claim, &mp, &vu);
+    {
+        vo_fe sum = fe(0, 0);
+        for (int i = 0; i < 64; ++i) sum = fadd(sum, fmul(bgat(r0, r1, 6, al, be, i), eq_at(ru + lg, 6, i)));
+        if (!feq(claim, fmul(sum, vu))) ok = 0;
+    }
+    vals[nm++] = vu;
+    memcpy(r0, ru, (lg + 6) * sizeof(vo_fe));
+    memcpy(r1, rv, (lg + 6) * sizeof(vo_fe));
+    claim = fmul(al, vu);
+    /* multiplication layer (:356-489): add_mult_sum[i] = sum_j beta_g(jN + i) ep_j^i */
+    for (long i = 0; i < N; ++i) {
+        V[i].a = fe(0, 0); V[i].b = L[Ls][i];
+        AV[i].a = AV[i].b = fe(0, 0);
+        AM[i].a = AM[i].b = fe(0, 0);
+    }
+    for (int j = 0; j < 64; ++j) {
+        vo_fe x = fone();
+        for (long i = 0; i < N; ++i) {
+            AM[i].b = fadd(AM[i].b, fmul(bgat(r0, r1, lg + 6, al, be, (long)j * N + i), x));
+            x = fmul(x, ep[j]);
+        }
+    }
+    rng_fill(&g, ru, lg);
+    rng_fill(&g, rv, lg);
+    ok &= fg_phase(V, AV, AM, lg, ru, &claim, &mp, &vu);
+    {
+        vo_fe sum = fe(0, 0);
+        for (int i = 0; i < 64; ++i) {
+            vo_fe t0 = al, t1 = be, u0 = fone(), u1 = fone(), x = ep[i];
+            for (int j = 0; j < 6; ++j) {
+                t0 = fmul(t0, ((i >> j) & 1) ? r0[lg + j] : fomr(r0[lg + j]));
+                t1 = fmul(t1, ((i >> j) & 1) ? r1[lg + j] : fomr(r1[lg + j]));
+            }
+            for (int j = 0; j < lg; ++j) {
+                u0 = fmul(u0, fadd(fmul(fmul(r0[j], ru[j]), x), fmul(fomr(r0[j]), fomr(ru[j]))));
+                u1 = fmul(u1, fadd(fmul(fmul(r1[j], ru[j]), x), fmul(fomr(r1[j]), fomr(ru[j]))));
+                x = fmul(x, x);
+            }
+            sum = fadd(sum, fadd(fmul(t0, u0), fmul(t1, u1)));
+        }
+        if (!feq(claim, fmul(sum, vu))) ok = 0;
+    }
+    vals[nm++] = vu;
+    memcpy(r0, ru, lg * sizeof(vo_fe));
+    memcpy(r1, rv, lg * sizeof(vo_fe));
+    claim = fmul(al, vu);
+    /* intermediate layer (:491-496) */
+    claim = fmul(claim, fconst((uint64_t)N));
+    /* inverse FFT levels (:498-768) */
+    for (int dep = 0; dep < lg; ++dep) {
+        const long half = 1L << (lg - dep - 1);
+        const int pre = lg + (lg - dep) - 1;
+        const vo_fe *pv = L[pre];
+        for (long i = 0; i < N; ++i) {
+            V[i].a = fe(0, 0); V[i].b = pv[i];
+            AV[i].a = AV[i].b = AM[i].a = AM[i].b = fe(0, 0);
+        }
+        vo_fe x = fone();
+        for (long k = 0; k < half; ++k) {
+            for (long j = 0; j < (1L << dep); ++j) {
+                const long u = k << (dep + 1) | j, v = u | (1L << dep);
+                const vo_fe b1 = bgat(r0, r1, lg, al, be, k << dep | j), b2 = bgat(r0, r1, lg, al, be, (k + half) << dep | j);
+                AM[u].b = fadd(AM[u].b, fadd(b1, b2));
+                AV[u].b = fadd(AV[u].b, fmul(fmul(x, pv[v]), fsub(b1, b2)));
+            }
+            x = fmul(x, rot[dep]);
+        }
+        rng_fill(&g, ru, lg);
+        rng_fill(&g, rv, lg);
+        ok &= fg_phase(V, AV, AM, lg, ru, &claim, &mp, &vu);
+        for (long i = 0; i < N; ++i) {
+            V[i].a = fe(0, 0); V[i].b = pv[i];
+            AV[i].a = AV[i].b = AM[i].a = AM[i].b = fe(0, 0);
+        }
+        x = fone();
+        for (long k = 0; k < half; ++k) {
+            for (long j = 0; j < (1L << dep); ++j) {
+                const long u = k << (dep + 1) | j, v = u | (1L << dep);
+                const vo_fe bu = eq_at(ru, lg, u);
+                const vo_fe t1 = fmul(bgat(r0, r1, lg, al, be, k << dep | j), bu);
+                const vo_fe t2 = fmul(bgat(r0, r1, lg, al, be, (k + half) << dep | j), bu);
+                AM[v].b = fadd(AM[v].b, fmul(x, fsub(t1, t2)));
+                AV[v].b = fadd(AV[v].b, fmul(vu, fadd(t1, t2)));
+            }
+            x = fmul(x, rot[dep]);
+        }
+        ok &= fg_phase(V, AV, AM, lg, rv, &claim, &mp, &vv);
+        /* the verifier's closed form (:681-750) */
+        {
+            const int lk = lg - dep - 1, lj = dep;
+            vo_fe w = rot[dep];
+            const vo_fe c0 = fmul(fomr(ru[lj]), rv[lj]);
+            vo_fe uA0 = fmul(fmul(fomr(r0[lg - 1]), c0), al), uA1 = fmul(fmul(fomr(r1[lg - 1]), c0), be);
+            vo_fe vA0 = uA0, vA1 = uA1;
+            vo_fe uB0 = fmul(fmul(r0[lg - 1], c0), al), uB1 = fmul(fmul(r1[lg - 1], c0), be);
+            vo_fe vB0 = uB0, vB1 = uB1;
+            for (int i = 0; i < lk; ++i) {
+                const vo_fe su = ru[lj + 1 + i], sv = rv[lj + 1 + i];
+                const vo_fe e0 = fmul(fmul(r0[lj + i], su), sv), n0 = fmul(fmul(fomr(r0[lj + i]), fomr(su)), fomr(sv));
+                const vo_fe e1 = fmul(fmul(r1[lj + i], su), sv), n1 = fmul(fmul(fomr(r1[lj + i]), fomr(su)), fomr(sv));
+                uA0 = fmul(uA0, fadd(e0, n0)); uA1 = fmul(uA1, fadd(e1, n1));
+                vA0 = fmul(vA0, fadd(fmul(e0, w), n0)); vA1 = fmul(vA1, fadd(fmul(e1, w), n1));
+                uB0 = fmul(uB0, fadd(e0, n0)); uB1 = fmul(uB1, fadd(e1, n1));
+                vB0 = fmul(vB0, fadd(n0, fmul(e0, w))); vB1 = fmul(vB1, fadd(n1, fmul(e1, w)));
+                w = fmul(w, w);
+            }
+            for (int i = 0; i < lj; ++i) {
+                const vo_fe t0 = fadd(fmul(fmul(r0[i], ru[i]), rv[i]), fmul(fmul(fomr(r0[i]), fomr(ru[i])), fomr(rv[i])));
+                const vo_fe t1 = fadd(fmul(fmul(r1[i], ru[i]), rv[i]), fmul(fmul(fomr(r1[i]), fomr(ru[i])), fomr(rv[i])));
+                uA0 = fmul(uA0, t0); uA1 = fmul(uA1, t1); vA0 = fmul(vA0, t0); vA1 = fmul(vA1, t1);
+                uB0 = fmul(uB0, t0); uB1 = fmul(uB1, t1); vB0 = fmul(vB0, t0); vB1 = fmul(vB1, t1);
+            }
+            const vo_fe want = fadd(fmul(fadd(fadd(uA0, uA1), fadd(uB0, uB1)), vu),
+                                    fmul(fsub(fadd(vA0, vA1), fadd(vB0, vB1)), vv));
+            if (!feq(claim, want)) ok = 0;
+        }
+        vals[nm++] = vu;
+        vals[nm++] = vv;
+        memcpy(r0, ru, lg * sizeof(vo_fe));
+        memcpy(r1, rv, lg * sizeof(vo_fe));
+        al = rng_fe(&g);
+        be = rng_fe(&g);
+        claim = fadd(fmul(al, vu), fmul(be, vv));
+    }
+    /* proof size (:323-324 per message; extension_gkr :770-779) */
+    *proof_size = 48 * (vo_fft_gkr_rounds(lg) + lg * (lg + 1) / 2);
+    for (int i = 0; i < nl; ++i) free(L[i]);
+    free(L); free(r); free(xa); free(r0); free(r1); free(ru); free(rv); free(V); free(AV); free(AM);
+    return ok;
+}

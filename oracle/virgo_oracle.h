@@ -96,6 +96,19 @@ void vo_predicates(const uint8_t *ty, const int64_t *u, const int64_t *v, int bl
 typedef struct { vo_fe a, b; } vo_lp;
 void vo_sumcheck_round(vo_lp *V, vo_lp *addv, vo_lp *am, long total_uv, const vo_fe *r, int current_bit, vo_fe out3[3]);
 
+/* The fft_gkr side prover (src/VPD/fft_circuit_GKR.cpp, run by the
+ * verifier as its own process, vpd_verifier.cpp:89-99) for lg_size:
+ * build_circuit (:22-112) and engage_gkr (:786-825) with the random stream of
+ * rand() after srand(seed) (the reference process never seeds: seed 1).
+ * msgs receives every sumcheck message (a, b, c) in order: the addition
+ * layer (lg+6 rounds), the multiplication layer (lg), then per inverse-FFT
+ * level phase 1 and phase 2 (lg each); vals the final value of each phase
+ * (addition v_u, multiplication v_u, then v_u, v_v per level).  Returns 1
+ * when every check of the reference's in-process verifier passes;
+ * *proof_size as the reference counts it. */
+int vo_fft_gkr_rounds(int lg_size);
+int vo_fft_gkr(int lg_size, unsigned seed, vo_fe *msgs, vo_fe *vals, int *proof_size);
+
 #ifdef __cplusplus
 }
 #endif

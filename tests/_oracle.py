@@ -200,6 +200,18 @@ def ref_predicates(layers, which, r0, r1, ru, rv, alpha, beta):
     return out
 
 
+def fft_gkr(lg, seed=1):
+    """the fft_gkr side prover restated: (pass, messages (rounds, 3, 2),
+    final value of each phase, proof size)"""
+    o = oracle()
+    n = o.vo_fft_gkr_rounds(lg)
+    msgs = np.zeros((n, 3, 2), np.uint64)
+    vals = np.zeros((2 + 2 * lg, 2), np.uint64)
+    ps = ctypes.c_int()
+    ok = o.vo_fft_gkr(lg, ctypes.c_uint(seed), vp(msgs), vp(vals), ctypes.byref(ps))
+    return bool(ok), msgs, vals, ps.value
+
+
 class RoundTables:
     """The reference's linear-polynomial tables ({a, b} per entry) for the
     round-by-round oracle."""

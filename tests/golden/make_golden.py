@@ -120,6 +120,7 @@ def kernels():
         L.ref_hash64(vp(m), vp(d))
         out["hash"].append({"seed": 4000 + k, "sha3_256": d.tobytes().hex()})
     out["predicates"] = predicates()
+    out["fft_gkr"] = fft_gkr()
     return out
 
 
@@ -164,6 +165,48 @@ def predicates():
             res.append(o.tobytes().hex())
         out.append({"name": name, "generator": gen, "params": params,
                     "layers": [hashlib.sha256(bytes.fromhex(h)).hexdigest() for h in res] if d > 12 else res})
+    return out
+
+
+def _fe_mul_add(a, x, b):
+    """a * x + b in F_p[i]/(i^2 + 1), elements as (img, real)"""
+    ai, ar = int(a[0]), int(a[1])
+    xi, xr = int(x[0]), int(x[1])
+    re = (ar * xr - ai * xi + int(b[1])) % P
+    im = (ar * xi + ai * xr + int(b[0])) % P
+    return np.array([im, re], np.uint64)
+
+
+def fft_gkr_records(lg, workdir):
+    """Runs oracle/_ref/fft_gkr_rec (the reference fft_gkr, its eval calls
+    recorded); returns the sumcheck messages (rounds x 3 x (img, real)), the
+    final value of every phase, and the reference's output line."""
+    rec, out = os.path.join(workdir, "fg.rec"), os.path.join(workdir, "fg.txt")
+    subprocess.run([os.path.join(REF, "fft_gkr_rec"), str(lg), out, rec], check=True, cwd=workdir)
+    b = open(rec, "rb").read()
+    q, lin, i = [], [], 0
+    while i < len(b):
+        k = 4 if b[i:i + 1] == b"Q" else 3
+        a = np.frombuffer(b[i + 1:i + 1 + 16 * k], np.uint64).reshape(k, 2)
+        (q if k == 4 else lin).append(a)
+        i += 1 + 16 * k
+    msgs = np.array([x[:3] for x in q[0::3]], np.uint64)   # eval(0), eval(1), eval(r) per message
+    vals = np.array([_fe_mul_add(x[0], x[2], x[1]) for x in lin], np.uint64)
+    return msgs, vals, open(out).read().split()
+
+
+def fft_gkr():
+    """The fft_gkr side prover's messages for lg 1..12 (the reference process
+    never seeds rand(), so its stream is that of seed 1)."""
+    import hashlib
+    out = []
+    with tempfile.TemporaryDirectory() as d:
+        for lg in range(1, 13):
+            msgs, vals, line = fft_gkr_records(lg, d)
+            out.append({"lg": lg, "seed": 1, "rounds": len(msgs), "proof_size": int(line[1]),
+                        "msgs": msgs.tobytes().hex() if msgs.nbytes <= 4096 else
+                        "sha256:" + hashlib.sha256(msgs.tobytes()).hexdigest(),
+                        "first": msgs[:4].tobytes().hex(), "vals": vals.tobytes().hex()})
     return out
 
 

@@ -199,3 +199,24 @@ def test_predicates_match_reference_live():
         for which in range(2, len(layers)):
             ins = _pred_inputs(50 + seed, layers, which)
             assert (O.predicates(layers, which, *ins) == O.ref_predicates(layers, which, *ins)).all(), (seed, which)
+
+
+def test_fft_gkr_golden():
+    """The fft_gkr restatement against the reference side prover's recorded
+    sumcheck messages and phase values (lg 1..12, the reference's own
+    unseeded rand() stream), and its proof-size count."""
+    for case in _kernels()["fft_gkr"]:
+        ok, msgs, vals, ps = O.fft_gkr(case["lg"], case["seed"])
+        assert ok, case["lg"]
+        assert len(msgs) == case["rounds"] and ps == case["proof_size"]
+        assert _same(msgs, case["msgs"]), case["lg"]
+        assert msgs[:4].tobytes().hex() == case["first"]
+        assert vals.tobytes().hex() == case["vals"], case["lg"]
+
+
+def test_fft_gkr_other_seed():
+    """Another seed of the rand() stream gives another passing run with
+    different messages."""
+    ok1, m1, _, _ = O.fft_gkr(6, 1)
+    ok2, m2, _, _ = O.fft_gkr(6, 12345)
+    assert ok1 and ok2 and not (m1 == m2).all()
