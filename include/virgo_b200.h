@@ -290,7 +290,10 @@ typedef struct {
     double total_s;         /* wall time of the call */
     double prove_time;      /* launch_s + wait_s: every prover message is on the host */
     long long proof_size;   /* bytes by the reference's accounting, without fft_gkr */
-    long long launches;     /* kernels launched for this proof */
+    long long launches;     /* kernels launched for this proof, the side proof's included */
+    double fft_gkr_s;       /* the fft_gkr side proof: launch to checked (0 when not run) */
+    int fft_gkr_lg;         /* its size L - 6, 0 when not run */
+    int fft_gkr_proof_size; /* its bytes as the reference counts them (the verifier adds them) */
 } vg_proof_stats;
 /* From file-level layers as in the circuit text format (src/linear_gkr/README.md):
  * d layers, the input layer first (types 2/3, u = value), layer i has n[i]
@@ -339,6 +342,11 @@ int vg_session_depth(vg_session *s, int *depth, int *input_log);
  * the records: tag byte, uint32 count of 16-byte units, the units. */
 int vg_session_prove(vg_session *s, unsigned seed, int want_transcript, vg_proof_stats *stats,
                      uint8_t **transcript, size_t *transcript_len);
+/* Every proof also runs the fft_gkr side proof for lg = L - 6 (2^L inputs,
+ * L > 6) on the GPU beside it, as the reference verifier runs ./fft_gkr next
+ * to every proof (vpd_verifier.cpp:89-99); on by default, off with on = 0.
+ * A side proof that fails its checks fails the proof. */
+int vg_session_set_fft_gkr(vg_session *s, int on);
 /* n proofs at once, session i with seed i, each on its own host thread and
  * CUDA stream (the sessions must be distinct objects, e.g. forks of one).
  * stats, transcripts and transcript_lens have n entries (or are NULL). */
@@ -380,6 +388,36 @@ int vg_session_ctx(vg_session *s, vg_ctx **out);
  * whole proof. */
 int vg_session_commit_ctx(vg_session *s, vg_ctx **out);
 void vg_free(void *p);
+
+/* ---- the fft_gkr side prover (src/VPD/fft_circuit_GKR.cpp) ----
+ * The reference verifier runs it as a process, `fft_gkr <L-6> <file>`
+ * (vpd_verifier.cpp:89-99), and adds its prover time to Prove Time; main
+ * (fft_circuit_GKR.cpp:827-845) builds the circuit for lg and runs
+ * engage_gkr (:786-825) with the prover's messages checked in process.
+ * vg_fft_gkr_prove does the same on the GPU with the challenge stream of
+ * rand() after srand(seed) (the reference process never seeds: seed 1).
+ * msgs (optional, vg_fft_gkr_rounds(lg) x 3 values) receives every sumcheck
+ * message (a, b, c) in order: addition layer (lg + 6 rounds), multiplication
+ * layer (lg), then per inverse-FFT level phase 1 and phase 2 (lg each); vals
+ * (optional, 2 + 2 lg) the value each phase ends on.  st->pass is 1 when every
+ * check of the reference's in-process verifier holds. */
+typedef struct vg_fft_gkr vg_fft_gkr;
+typedef struct {
+    double p_time;        /* seconds: first launch to the last message checked */
+    double v_time;        /* seconds: the in-process verifier's checks */
+    int proof_size;       /* bytes, counted as fft_circuit_GKR.cpp counts them */
+    int pass;
+    int rounds;           /* sumcheck messages */
+    long long launches;   /* kernels launched */
+} vg_fft_gkr_stats;
+int vg_fft_gkr_rounds(int lg_size);
+int vg_fft_gkr_create(vg_ctx *ctx, int max_lg, vg_fft_gkr **out);   /* max_lg <= 22 */
+int vg_fft_gkr_prove(vg_fft_gkr *f, int lg_size, unsigned seed, vg_fft_gkr_stats *st, vg_fe *msgs, vg_fe *vals);
+int vg_fft_gkr_destroy(vg_fft_gkr *f);
+/* device bytes a vg_fft_gkr object of max_lg holds */
+size_t vg_fft_gkr_footprint(int max_lg);
+/* create + prove + destroy */
+int vg_fft_gkr_run(vg_ctx *ctx, int lg_size, unsigned seed, vg_fft_gkr_stats *st, vg_fe *msgs, vg_fe *vals);
 
 #ifdef __cplusplus
 }

@@ -44,12 +44,16 @@ def test_session_matches_golden_transcript(case):
     assert st.launches > 0
 
 
-def _run_binary(binary, layers, seed, tmp_path):
+GPU_FFT = os.path.join(ROOT, "virgo_b200", "bin", "fft_gkr")
+
+
+def _run_binary(binary, layers, seed, tmp_path, fft_bin=None):
     cpath, mpath = str(tmp_path / "c.txt"), str(tmp_path / "m.txt")
     circuits.write_text(layers, cpath, mpath)
     fft = tmp_path / "fft_gkr"
-    if not fft.exists():
-        os.symlink(os.path.join(REF, "fft_gkr"), fft)
+    if fft.is_symlink() or fft.exists():
+        fft.unlink()
+    os.symlink(fft_bin or os.path.join(REF, "fft_gkr"), fft)
     tr = str(tmp_path / (os.path.basename(binary) + ".bin"))
     out = subprocess.run([binary, cpath, mpath, str(tmp_path / "res.txt"), str(seed), tr], cwd=str(tmp_path),
                          capture_output=True, text=True, timeout=600)
@@ -71,13 +75,17 @@ def test_session_matches_reference_on_fresh_circuit(tmp_path):
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(REF, "zk_proof_accept")), reason="acceptance binary not built")
-def test_reference_verifier_accepts_gpu_proof(tmp_path):
+@pytest.mark.parametrize("fft", ["reference", "gpu"])
+def test_reference_verifier_accepts_gpu_proof(tmp_path, fft):
     """The reference verifier sources, unchanged, drive the GPU prover through
     the drop-in classes and print Pass; the messages equal the reference
-    prover's (golden), including the verifier's proof-size accounting."""
+    prover's (golden), including the verifier's proof-size accounting.  The
+    verifier's ./fft_gkr is the reference binary or the GPU drop-in; the
+    proof size it adds from the side proof is the same."""
     c = _golden()[0]
     layers = getattr(circuits, c["generator"])(**c["params"])
-    out, recs = _run_binary(os.path.join(REF, "zk_proof_accept"), layers, c["seed"], tmp_path)
+    out, recs = _run_binary(os.path.join(REF, "zk_proof_accept"), layers, c["seed"], tmp_path,
+                            fft_bin=GPU_FFT if fft == "gpu" else None)
     assert out.returncode == 0, out.stdout[-2000:] + out.stderr[-2000:]
     assert "Pass" in out.stdout
     # the recorder only sees calls the verifier's object files make, so the
@@ -87,6 +95,44 @@ def test_reference_verifier_accepts_gpu_proof(tmp_path):
     ref = [r for r in c["records"] if r[0] != "C"]
     assert transcript.first_difference(got, ref) is None
     assert recs[-1][0] == "V" and recs[-1][1].hex() == c["verdict"][1]
+    if fft == "gpu":   # the same run with the reference's fft_gkr: same proof size line
+        other = tmp_path / "with_reference_fft"
+        other.mkdir()
+        out2, _ = _run_binary(os.path.join(REF, "zk_proof_accept"), layers, c["seed"], other)
+        assert out2.returncode == 0 and "Pass" in out2.stdout
+        assert open(tmp_path / "res.txt").read().split()[-1] == open(other / "res.txt").read().split()[-1]
+
+
+def test_session_runs_fft_gkr_side_proof():
+    """Every proof runs the fft_gkr side proof for lg = L - 6 beside it (its
+    own stream); turning it off leaves the transcript unchanged."""
+    c = next(x for x in _golden() if x["name"] == "random_5layer")
+    layers = getattr(circuits, c["generator"])(**c["params"])
+    s = vb.Session(layers)
+    try:
+        _, L = s.depth()
+        st, on = s.prove(c["seed"])
+        assert st.fft_gkr_lg == L - 6 and st.fft_gkr_s > 0
+        assert st.fft_gkr_proof_size == 48 * (vb.lib().vg_fft_gkr_rounds(L - 6) + (L - 6) * (L - 5) // 2)
+        s.set_fft_gkr(False)
+        st2, off = s.prove(c["seed"])
+        assert st2.fft_gkr_lg == 0 and st2.fft_gkr_s == 0 and st2.launches < st.launches
+    finally:
+        s.close()
+    assert on == off
+    assert transcript.digest(transcript.parse(on)) == c["digest"]
+
+
+@pytest.mark.skipif(not os.path.exists(GPU_FFT), reason="drop-in fft_gkr not built")
+def test_fft_gkr_dropin_binary(tmp_path):
+    """virgo_b200/bin/fft_gkr writes the line the reference verifier reads:
+    v_time, proof size (equal to the reference binary's) and p_time."""
+    out = tmp_path / "log_fftgkr.txt"
+    r = subprocess.run([GPU_FFT, "11", str(out)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    assert "Error" not in r.stderr
+    v_time, size, p_time = open(out).read().split()
+    assert int(size) == 16128 and float(p_time) > 0 and float(v_time) >= 0
 
 
 def test_session_from_text_file_equals_arrays(tmp_path):

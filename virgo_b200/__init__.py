@@ -36,7 +36,13 @@ class vg_proof_stats(ctypes.Structure):
     _fields_ = [
         ("launch_s", ctypes.c_double), ("wait_s", ctypes.c_double), ("replay_s", ctypes.c_double),
         ("total_s", ctypes.c_double), ("prove_time", ctypes.c_double), ("proof_size", ctypes.c_longlong), ("launches", ctypes.c_longlong),
+        ("fft_gkr_s", ctypes.c_double), ("fft_gkr_lg", ctypes.c_int), ("fft_gkr_proof_size", ctypes.c_int),
     ]
+
+
+class vg_fft_gkr_stats(ctypes.Structure):
+    _fields_ = [("p_time", ctypes.c_double), ("v_time", ctypes.c_double), ("proof_size", ctypes.c_int),
+                ("pass_", ctypes.c_int), ("rounds", ctypes.c_int), ("launches", ctypes.c_longlong)]
 
 
 class vg_job_info(ctypes.Structure):
@@ -71,6 +77,13 @@ def lib():
             "vg_circuit_upload": (c_i, [c_p, c_i, c_p, c_p, c_p, c_p, ctypes.POINTER(c_p)]),
             "vg_circuit_destroy": (c_i, [c_p]),
             "vg_circuit_predicates": (c_i, [c_p, c_p, c_i, c_p, c_p, c_p, c_p, vg_fe, vg_fe, c_p]),
+            "vg_fft_gkr_rounds": (c_i, [c_i]),
+            "vg_fft_gkr_footprint": (c_sz, [c_i]),
+            "vg_session_set_fft_gkr": (c_i, [c_p, c_i]),
+            "vg_fft_gkr_create": (c_i, [c_p, c_i, ctypes.POINTER(c_p)]),
+            "vg_fft_gkr_prove": (c_i, [c_p, c_i, ctypes.c_uint, ctypes.POINTER(vg_fft_gkr_stats), c_p, c_p]),
+            "vg_fft_gkr_destroy": (c_i, [c_p]),
+            "vg_fft_gkr_run": (c_i, [c_p, c_i, ctypes.c_uint, ctypes.POINTER(vg_fft_gkr_stats), c_p, c_p]),
             "vg_gkr_create": (c_i, [c_p, c_p, ctypes.POINTER(c_p)]),
             "vg_gkr_destroy": (c_i, [c_p]),
             "vg_gkr_evaluate": (c_i, [c_p]),
@@ -258,6 +271,10 @@ class Session:
         lib().vg_free(buf)
         return st, data
 
+    def set_fft_gkr(self, on: bool):
+        """Run the fft_gkr side proof beside every proof (default on)."""
+        check(lib().vg_session_set_fft_gkr(self.h, 1 if on else 0), "vg_session_set_fft_gkr")
+
     def load(self, layers, index_bytes: int = 8):
         """Replaces the circuit (device buffers reused when it fits).  layers
         are (ty, u, v) arrays; with index_bytes=4 the wires of layers >= 1 are
@@ -338,6 +355,30 @@ def circuit_binary_info(path: str):
     n = np.zeros(d.value, np.int64)
     check(lib().vg_circuit_binary_info(path.encode(), ctypes.byref(d), ctypes.byref(ib), n.ctypes.data, d.value))
     return [int(x) for x in n], ib.value
+
+
+class FftGkr:
+    """The fft_gkr side prover on the GPU (vg_fft_gkr_*): the reference runs
+    it as `fft_gkr <L-6> <file>` next to every proof of input size 2^L."""
+
+    def __init__(self, ctx: Context, max_lg: int):
+        self.ctx = ctx
+        self.h = ctypes.c_void_p()
+        check(lib().vg_fft_gkr_create(ctx.h, max_lg, ctypes.byref(self.h)), "vg_fft_gkr_create")
+
+    def prove(self, lg: int, seed: int = 1, messages: bool = True):
+        """-> (stats, messages (rounds, 3, 2) or None, phase values (2 + 2 lg, 2))"""
+        st = vg_fft_gkr_stats()
+        msgs = np.zeros((lib().vg_fft_gkr_rounds(lg), 3, 2), np.uint64) if messages else None
+        vals = np.zeros((2 + 2 * lg, 2), np.uint64)
+        check(lib().vg_fft_gkr_prove(self.h, lg, seed, ctypes.byref(st), ptr(msgs) if messages else None, ptr(vals)),
+              "vg_fft_gkr_prove")
+        return st, msgs, vals
+
+    def close(self):
+        if self.h:
+            lib().vg_fft_gkr_destroy(self.h)
+            self.h = None
 
 
 def job_footprint(widths) -> int:

@@ -2123,3 +2123,63 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
         for (int k = 0; k < 6; ++k) last6[k] = tovg(host[3 + k]);
     return VG_OK;
 }
+
+// ------------------------------------------- sumcheck tables without a circuit
+// The rounds of vg_gkr_round (deferred, records on the device) over tables
+// that the caller builds, for provers whose layers are not a gate list (the
+// FFT side prover).  The object owns ping-pong tables for up to max_n entries
+// and max_records records.
+int vg_gkr_tables_create(vg_ctx *ctx, long max_n, int max_records, vg_gkr **out)
+{
+    if (!ctx || !out || max_n < 2 || (max_n & (max_n - 1)) || max_records < 1)
+        return vg_fail(VG_ERR_ARG, "vg_gkr_tables_create: bad argument (max_n %ld, records %d)", max_n, max_records);
+    vg_gkr *g = new vg_gkr();
+    g->ctx = ctx;
+    auto fail = [&](const char *what) {
+        cudaGetLastError();
+        vg_gkr_destroy(g);
+        return vg_fail(VG_ERR_OOM, "vg_gkr_tables_create: %s allocation failed", what);
+    };
+    if (cudaMalloc(&g->round_parts, 3 * 148 * 8 * sizeof(fe)) != cudaSuccess) return fail("round partials");
+    if (cudaMalloc(&g->round_out, 16 * sizeof(fe)) != cudaSuccess) return fail("round sums");
+    if (cudaMalloc(&g->round_counter, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
+    if (cudaMemset(g->round_counter, 0, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
+    for (int b = 0; b < 2; ++b)
+        for (int k = 0; k < 3; ++k)
+            if (cudaMalloc(&g->buf[b][k], (b == 0 ? max_n : max_n / 2 + 1) * sizeof(fe)) != cudaSuccess)
+                return fail("tables");
+    if (cudaMalloc(&g->rg_parts, (max_n / RG_CHUNK + 1) * RG_MAX * 3 * sizeof(fe)) != cudaSuccess)
+        return fail("group partials");
+    if (cudaMalloc(&g->rec, (size_t)max_records * 9 * sizeof(fe)) != cudaSuccess) return fail("records");
+    g->N_cap = max_n;
+    g->rec_cap = max_records;
+    g->deferred = true;
+    *out = g;
+    return VG_OK;
+}
+
+int vg_gkr_tables_rewind(vg_gkr *g)
+{
+    if (!g || g->C) return vg_fail(VG_ERR_ARG, "vg_gkr_tables_rewind: not a tables object");
+    VG_TRY(flush_rounds(g));
+    g->rec_n = 0;
+    g->layer = -1;
+    g->n = 0;
+    g->round0_pending = false;
+    return VG_OK;
+}
+
+int vg_gkr_tables_begin(vg_gkr *g, const vg_fe *V, long n, vg_fe **AV, vg_fe **AM)
+{
+    if (!g || g->C || !V || !AV || !AM) return vg_fail(VG_ERR_ARG, "vg_gkr_tables_begin: bad argument");
+    if (n < 2 || n > g->N_cap || (n & (n - 1))) return vg_fail(VG_ERR_ARG, "vg_gkr_tables_begin: %ld entries", n);
+    VG_TRY(flush_rounds(g));   // pending rounds of the previous phase read the tables handed out now
+    *AV = (vg_fe *)g->buf[0][1];
+    *AM = (vg_fe *)g->buf[0][2];
+    g->cur[0] = (const fe *)V;
+    g->layer = 1;
+    return tables_ready(g, n);
+}
+
+const vg_fe *vg_gkr_records_dev(const vg_gkr *g) { return (const vg_fe *)g->rec; }
+int vg_gkr_record_count(const vg_gkr *g) { return g->rec_n; }

@@ -18,6 +18,23 @@ int vg_gkr_phase2_init_deferred(vg_gkr *g, const vg_fe *r_u, int length_u, vg_fe
 // Enqueues the copy of all records to pinned host memory (*host, 9 * *n values).
 int vg_gkr_records(vg_gkr *g, const vg_fe **host, int *n);
 
+// Sumcheck tables without a circuit: vg_gkr_round (deferred) over tables the
+// caller fills.  vg_gkr_tables_begin flushes the rounds still queued, hands
+// out the AV and AM tables (n entries, to be written before the next round)
+// and takes V (n entries, read in place by the first round).  Records as in
+// deferred mode, numbered from the last rewind; vg_gkr_destroy frees.
+int vg_gkr_tables_create(vg_ctx *ctx, long max_n, int max_records, vg_gkr **out);
+int vg_gkr_tables_rewind(vg_gkr *g);
+int vg_gkr_tables_begin(vg_gkr *g, const vg_fe *V, long n, vg_fe **AV, vg_fe **AM);
+const vg_fe *vg_gkr_records_dev(const vg_gkr *g);
+int vg_gkr_record_count(const vg_gkr *g);
+
+// vg_fft_gkr_prove in two halves: the launch enqueues the whole side proof
+// on the object's context stream; the finish waits for it and checks the
+// messages (so other work can be launched in between).
+int vg_fft_gkr_launch(vg_fft_gkr *f, int lg, unsigned seed);
+int vg_fft_gkr_finish(vg_fft_gkr *f, vg_fft_gkr_stats *st, vg_fe *msgs, vg_fe *vals);
+
 // Grows a device buffer from the stream-ordered pool on c's stream.
 int vg_ctx_grow_dev(vg_ctx *c, void **p, size_t *cap, size_t bytes);
 

@@ -85,6 +85,7 @@ extern "C" size_t vg_job_footprint(int d, const long *n)
     b += 4 * 65 * S * 16;                   // l, h, q and virtual-oracle codewords
     b += 65 * S * 16 + 4 * S * 32;          // FRI levels, Merkle trees
     b += (size_t)64 << 20;                  // staging, scratch, twiddles
+    b += vg_fft_gkr_footprint(L - 6);       // the fft_gkr side proof
     return b + b / 8;
 }
 

@@ -116,7 +116,53 @@ struct vg_session {
     void *pub = nullptr;   // device buffer for the public eq table
     size_t pub_bytes = 0;
     bool loaded = false;   // false after a failed load: no valid circuit
+    // the fft_gkr side proof of every proof (on its own stream), made on first use
+    vg_ctx *fctx = nullptr;
+    vg_fft_gkr *fft = nullptr;
+    int fft_max_lg = 0;
+    bool fft_on = true;
 };
+
+// The verifier runs `./fft_gkr <L - 6>` next to every proof of input size
+// 2^L and counts its prover time (vpd_verifier.cpp:89-99); its random stream
+// is that of a fresh process (seed 1).  Here it is launched on the session's
+// third stream right after the proof's launch pass, so it runs beside the
+// proof.  Returns the size launched, 0 when none (off, or L <= 6).
+static int fft_side_launch(vg_session *s, int *lg_out)
+{
+    *lg_out = 0;
+    const int lg = s->circuit->C.circuit[0].bit_length - 6;
+    if (!s->fft_on || lg < 1) return VG_OK;
+    int rc = VG_OK;
+    if (!s->fctx) {
+        int dev = 0;
+        vg_ctx_device(s->ctx, &dev);
+        rc = vg_ctx_create(dev, &s->fctx);
+        if (rc != VG_OK) return rc;
+    }
+    if (!s->fft || s->fft_max_lg < lg) {
+        if (s->fft) vg_fft_gkr_destroy(s->fft);
+        s->fft = nullptr;
+        s->fft_max_lg = 0;
+        rc = vg_fft_gkr_create(s->fctx, lg, &s->fft);
+        if (rc != VG_OK) return rc;
+        s->fft_max_lg = lg;
+    }
+    rc = vg_fft_gkr_launch(s->fft, lg, 1);
+    if (rc != VG_OK) {
+        vg_ctx_sync(s->fctx);
+        return rc;
+    }
+    *lg_out = lg;
+    return VG_OK;
+}
+
+extern "C" int vg_session_set_fft_gkr(vg_session *s, int on)
+{
+    if (!s) return vg_fail(VG_ERR_ARG, "vg_session_set_fft_gkr: null session");
+    s->fft_on = on != 0;
+    return VG_OK;
+}
 
 static int session_device(vg_ctx **ctx)
 {
@@ -221,6 +267,7 @@ extern "C" int vg_session_fork(vg_session *base, vg_session **out)
     if (!base->loaded) return vg_fail(VG_ERR_STATE, "vg_session_fork: the base session holds no circuit");
     vg_session *s = new vg_session();
     s->circuit = base->circuit;
+    s->fft_on = base->fft_on;
     int rc = session_attach(s);
     s->loaded = rc == VG_OK;
     if (rc != VG_OK) {
@@ -314,6 +361,8 @@ extern "C" int vg_session_destroy(vg_session *s)
         delete s->p;
     }
     if (s->pub) vg_dev_free(s->cctx, s->pub);
+    if (s->fft) vg_fft_gkr_destroy(s->fft);
+    if (s->fctx) vg_ctx_destroy(s->fctx);
     if (s->pc) vg_pc_destroy(s->pc);
     if (s->cctx) vg_ctx_destroy(s->cctx);
     s->circuit.reset();
@@ -747,9 +796,9 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
     memset(&st, 0, sizeof st);
     long long launches0 = 0;
     vg_ctx_launch_count(s->ctx, &launches0);
-    if (s->cctx) {
+    for (vg_ctx *x : {s->cctx, s->fctx}) {
         long long l2 = 0;
-        vg_ctx_launch_count(s->cctx, &l2);
+        if (x) vg_ctx_launch_count(x, &l2);
         launches0 += l2;
     }
     zk_prover &p = *s->p;
@@ -772,9 +821,27 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
     }
     st.launch_s = since(t_all);
     auto t0 = clk::now();
+    int fft_lg = 0;
+    const int rc_fft = fft_side_launch(s, &fft_lg);   // host work hidden behind the proof's device time
     rc = vg_ctx_sync(s->ctx);
     if (rc == VG_OK) rc = vg_ctx_sync(s->cctx);
-    if (rc != VG_OK) return rc;
+    if (rc == VG_OK) rc = rc_fft;
+    if (rc != VG_OK) {
+        if (fft_lg) {   // wait for the side proof and clear its run
+            vg_fft_gkr_stats fs;
+            vg_fft_gkr_finish(s->fft, &fs, nullptr, nullptr);
+        }
+        return rc;
+    }
+    if (fft_lg) {
+        vg_fft_gkr_stats fs;
+        rc = vg_fft_gkr_finish(s->fft, &fs, nullptr, nullptr);
+        if (rc != VG_OK) return rc;
+        if (!fs.pass) return vg_fail(VG_ERR_STATE, "fft_gkr side proof (lg %d) failed its checks", fft_lg);
+        st.fft_gkr_s = fs.p_time;
+        st.fft_gkr_lg = fft_lg;
+        st.fft_gkr_proof_size = fs.proof_size;
+    }
     st.wait_s = since(t0);
     st.prove_time = since(t_all);
 
@@ -792,9 +859,9 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
     st.proof_size = proof_size;
     long long launches1 = 0;
     vg_ctx_launch_count(s->ctx, &launches1);
-    {
+    for (vg_ctx *x : {s->cctx, s->fctx}) {
         long long l2 = 0;
-        vg_ctx_launch_count(s->cctx, &l2);
+        if (x) vg_ctx_launch_count(x, &l2);
         launches1 += l2;
     }
     st.launches = launches1 - launches0;
