@@ -31,12 +31,19 @@ VG_HD bool fe_eq(fe a, fe b) { return a.real == b.real && a.img == b.img; }
 VG_HD bool fe_is_zero(fe a) { return (a.real | a.img) == 0; }
 
 // ---- F_p ----
+// For canonical a, b: a + b - p is negative (as a signed 64-bit value)
+// exactly when a + b < p, and a - b exactly when a < b; the sign picks the
+// result without a 64-bit comparison.
 VG_HD uint64_t addp(uint64_t a, uint64_t b)
 {
-    uint64_t s = a + b;
-    return s >= P ? s - P : s;
+    const uint64_t s = a + b, t = s - P;
+    return (int64_t)t < 0 ? s : t;
 }
-VG_HD uint64_t subp(uint64_t a, uint64_t b) { return a >= b ? a - b : a + P - b; }
+VG_HD uint64_t subp(uint64_t a, uint64_t b)
+{
+    const uint64_t d = a - b;
+    return (int64_t)d < 0 ? d + P : d;
+}
 VG_HD uint64_t negp(uint64_t a) { return a ? P - a : 0; }
 
 VG_HD void mul64wide(uint64_t a, uint64_t b, uint64_t &lo, uint64_t &hi)
@@ -51,26 +58,26 @@ VG_HD void mul64wide(uint64_t a, uint64_t b, uint64_t &lo, uint64_t &hi)
 #endif
 }
 
-// a*b mod p for a, b < 2^61 (canonical).  x = hi*2^64 + lo < 2^122, and
+// x mod p for x < 2^64, partly reduced: the result is below 2^61 + 8.
+VG_HD uint64_t foldp(uint64_t x) { return (x & P) + (x >> 61); }
+// x mod p, canonical, for x < 2p: x + 1 reaches 2^61 exactly when x >= p.
+VG_HD uint64_t canonp(uint64_t x) { return (x + ((x + 1) >> 61)) & P; }
+
+// a*b mod p for a, b < 2^61 (canonical).  x = hi*2^64 + lo <= (p-1)^2, and
 // x = (x >> 61) * 2^61 + (x & p) == (x >> 61) + (x & p) (mod p); both terms are
-// below 2^61, so one conditional subtraction makes the sum canonical.
+// at most p and not both p (x < p 2^61 + p), so the sum is below 2p.
 VG_HD uint64_t mulp(uint64_t a, uint64_t b)
 {
     uint64_t lo, hi;
     mul64wide(a, b, lo, hi);
-    uint64_t r = (lo & P) + ((hi << 3) | (lo >> 61));
-    return r >= P ? r - P : r;
+    return canonp((lo & P) + ((hi << 3) | (lo >> 61)));
 }
-
-// a*b mod p for a, b < 2^62 (sums of two canonical values): x < 2^124 and the
-// first fold leaves a value below 2^64, folded once more.
-VG_HD uint64_t mulp_wide(uint64_t a, uint64_t b)
+// a*b mod p, partly reduced (below 2^61 + 8), for a*b < 2^124.
+VG_HD uint64_t mulp_partial(uint64_t a, uint64_t b)
 {
     uint64_t lo, hi;
     mul64wide(a, b, lo, hi);
-    uint64_t r = (lo & P) + ((hi << 3) | (lo >> 61));
-    r = (r & P) + (r >> 61);
-    return r >= P ? r - P : r;
+    return foldp((lo & P) + ((hi << 3) | (lo >> 61)));
 }
 
 // ---- F_{p^2} ----
@@ -79,12 +86,18 @@ VG_HD fe operator-(fe a, fe b) { return fe_make(subp(a.real, b.real), subp(a.img
 VG_HD fe operator-(fe a) { return fe_make(negp(a.real), negp(a.img)); }
 
 // (ar + i ai)(br + i bi) = (ar br - ai bi) + i((ar + ai)(br + bi) - ar br - ai bi)
+// with the three products partly reduced (below 2^61 + 8; the sums of two
+// canonical values are below 2^62, so every product is below 2^124) and the
+// differences taken as x + 4p - y (positive, below 2^64) before one fold and
+// the final canonical step.
 VG_HD fe operator*(fe a, fe b)
 {
-    uint64_t ac = mulp(a.real, b.real);
-    uint64_t bd = mulp(a.img, b.img);
-    uint64_t t = mulp_wide(a.real + a.img, b.real + b.img);
-    return fe_make(subp(ac, bd), subp(t, addp(ac, bd)));
+    const uint64_t ac = mulp_partial(a.real, b.real);
+    const uint64_t bd = mulp_partial(a.img, b.img);
+    const uint64_t t = mulp_partial(a.real + a.img, b.real + b.img);
+    const uint64_t re = foldp(ac + (4 * P - bd));
+    const uint64_t im = foldp(t + (4 * P - ac - bd));
+    return fe_make(canonp(re), canonp(im));
 }
 
 VG_HD fe fe_double(fe a) { return a + a; }

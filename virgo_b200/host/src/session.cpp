@@ -20,7 +20,6 @@
 #include <algorithm>
 #include <memory>
 #include <thread>
-#include <unordered_set>
 #include <chrono>
 #include <cstdio>
 #include <cstring>
@@ -459,6 +458,39 @@ extern "C" int vg_circuit_write_text(int d, const long *n, const uint8_t *const 
     return VG_OK;
 }
 
+// Open-addressing set of 64-bit keys (linear probing, power-of-two table,
+// grown at half load) for the proof-size bookkeeping of the query answers:
+// a few thousand operations per proof, where node-based sets cost a
+// millisecond.
+class KeySet {
+    std::vector<uint64_t> t_;
+    size_t n_ = 0;
+    static constexpr uint64_t EMPTY = ~0ull;
+    size_t slot(uint64_t k) const
+    {
+        size_t i = (size_t)((k * 0x9E3779B97F4A7C15ull) >> 20) & (t_.size() - 1);
+        while (t_[i] != EMPTY && t_[i] != k) i = (i + 1) & (t_.size() - 1);
+        return i;
+    }
+
+public:
+    KeySet() : t_(1024, EMPTY) {}
+    bool count(uint64_t k) const { return t_[slot(k)] == k; }
+    bool insert(uint64_t k)   // true when k was not there
+    {
+        size_t i = slot(k);
+        if (t_[i] == k) return false;
+        t_[i] = k;
+        if (2 * ++n_ > t_.size()) {
+            std::vector<uint64_t> old(t_.size() * 2, EMPTY);
+            old.swap(t_);
+            for (uint64_t x : old)
+                if (x != EMPTY) t_[slot(x)] = x;
+        }
+        return true;
+    }
+};
+
 // Device results of the launch pass, read by the replay pass.
 struct PassResults {
     const F *rec = nullptr;   // GKR records (9 values each)
@@ -724,8 +756,8 @@ static int prove_pass(vg_session *s, unsigned seed, bool launch, PassResults &re
     // ---- replay: query answers and the proof-size bookkeeping (fri.cpp:148-289) ----
     const F *qvals = (const F *)pr.qvals;
     const __hhash_digest *qpaths = (const __hhash_digest *)pr.qpaths;
-    std::unordered_set<long long> seen_elem[2], seen_node[2];
-    std::vector<std::unordered_set<long long> > seen_level(levels);
+    KeySet seen_elem[2], seen_node[2];
+    std::vector<KeySet> seen_level(levels);
     const long long half_S = 1LL << (L - 2);
     for (int q = 0; q < nq; ++q) {
         std::pair<std::vector<std::pair<F, F> >, std::vector<__hhash_digest> > a;
@@ -737,16 +769,16 @@ static int prove_pass(vg_session *s, unsigned seed, bool launch, PassResults &re
         if (which[q] < 2) {   // fri::request_init_value_with_merkle
             const int o = which[q];
             const long long p0 = pos[q];
-            for (int k = 0; k < slice_number; ++k)
-                for (int b = 0; b < 2; ++b)
-                    if (seen_elem[o].insert((p0 << (log_slice_number + 1)) | (k << 1) | b).second) new_size += sizeof(F);
+            // the reference marks the 2 x 64 elements of position p0 together
+            // (fri.cpp:166-176), so they are new exactly when p0 is
+            if (seen_elem[o].insert((uint64_t)p0)) new_size += 2 * slice_number * (int)sizeof(F);
             a.second.resize(depth + 1);
             a.second[depth] = pth[depth];
             long long node = p0 + half_S;
             for (int k = 0; k < depth; ++k) {
-                if (!seen_node[o].count(node ^ 1)) new_size += sizeof(__hhash_digest);
-                seen_node[o].insert(node);
-                seen_node[o].insert(node ^ 1);
+                if (!seen_node[o].count((uint64_t)(node ^ 1))) new_size += sizeof(__hhash_digest);
+                seen_node[o].insert((uint64_t)node);
+                seen_node[o].insert((uint64_t)(node ^ 1));
                 a.second[k] = pth[k];
                 node /= 2;
             }
@@ -756,17 +788,21 @@ static int prove_pass(vg_session *s, unsigned seed, bool launch, PassResults &re
             const int lvl = which[q] - 2;
             const long long h = 1LL << depth, p0 = pos[q] % h;
             auto &seen = seen_level[lvl];
+            // the reference tests element keys in the array that marks Merkle
+            // nodes (fri.cpp:252-262); the keys 2^(lss+1) p0 + 2k can only
+            // meet a node index below 2h
             bool visited = false;
-            for (int k = 0; k < slice_number; ++k)
-                if (seen.count((p0 << (log_slice_number + 1)) | (k << 1))) visited = true;
+            if ((p0 << (log_slice_number + 1)) < 2 * h)
+                for (int k = 0; k < slice_number && !visited; ++k)
+                    if (seen.count((uint64_t)((p0 << (log_slice_number + 1)) | (k << 1)))) visited = true;
             if (!visited) new_size += sizeof(F);
             long long node = p0 + h;
             int k = 0;
             while (node != 1) {
-                if (!seen.count(node ^ 1)) {
+                if (!seen.count((uint64_t)(node ^ 1))) {
                     new_size += sizeof(__hhash_digest);
-                    seen.insert(node ^ 1);
-                    seen.insert(node);
+                    seen.insert((uint64_t)(node ^ 1));
+                    seen.insert((uint64_t)node);
                 }
                 a.second.push_back(pth[k++]);
                 node /= 2;
