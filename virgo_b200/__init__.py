@@ -41,7 +41,8 @@ class vg_proof_stats(ctypes.Structure):
 
 
 class vg_fft_gkr_stats(ctypes.Structure):
-    _fields_ = [("p_time", ctypes.c_double), ("v_time", ctypes.c_double), ("proof_size", ctypes.c_int),
+    _fields_ = [("p_time", ctypes.c_double), ("v_time", ctypes.c_double), ("gpu_s", ctypes.c_double),
+                ("proof_size", ctypes.c_int),
                 ("pass_", ctypes.c_int), ("rounds", ctypes.c_int), ("launches", ctypes.c_longlong)]
 
 

@@ -27,6 +27,7 @@ struct ProfRec {
     int fam;
     cudaEvent_t a, b;
     double bytes;
+    bool shared_a;   // a is the previous record's b (back-to-back launches)
 };
 struct TraceRec {
     int fam;
@@ -59,6 +60,11 @@ struct vg_ctx {
     std::vector<TraceRec> trace;   // every profiled launch in order
     long long prof_launches[KF_COUNT] = {0};
     double prof_ms[KF_COUNT] = {0}, prof_bytes[KF_COUNT] = {0};
+    // back-to-back profiled launches share one event (the end of one is the
+    // start of the next), so the profiler adds one event per launch
+    bool prof_chain = false;
+    cudaEvent_t prof_prev_end = nullptr;
+    long long prof_prev_launches = -1;
 };
 
 // Profiler hooks around one launch: no-ops unless profiling is on.  Events are

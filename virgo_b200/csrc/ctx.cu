@@ -52,17 +52,28 @@ static cudaEvent_t get_event(vg_ctx *c)
     return e;
 }
 
+// A launch that directly follows the previous profiled one on the stream
+// (exactly one launch since that one began) starts at its end event; an
+// event pair around every launch would add several microseconds to each.
 void vg_prof_begin(vg_ctx *c, int fam, ProfRec *r)
 {
     r->fam = fam;
-    r->a = get_event(c);
+    r->shared_a = c->prof_chain && c->launches == c->prof_prev_launches + 1;
+    if (r->shared_a) {
+        r->a = c->prof_prev_end;
+    } else {
+        r->a = get_event(c);
+        cudaEventRecord(r->a, c->stream);
+    }
     r->b = get_event(c);
-    cudaEventRecord(r->a, c->stream);
+    c->prof_prev_launches = c->launches;
 }
 
 void vg_prof_end(vg_ctx *c, ProfRec *r, double bytes)
 {
     cudaEventRecord(r->b, c->stream);
+    c->prof_prev_end = r->b;
+    c->prof_chain = true;
     r->bytes = bytes;
     c->prof.push_back(*r);
     if (c->prof.size() > 4096) {   // resolve in batches to bound the event count
@@ -74,10 +85,11 @@ void vg_prof_end(vg_ctx *c, ProfRec *r, double bytes)
             c->prof_launches[p.fam]++;
             c->prof_ms[p.fam] += ms;
             c->prof_bytes[p.fam] += p.bytes;
-            c->event_pool.push_back(p.a);
+            if (!p.shared_a) c->event_pool.push_back(p.a);
             c->event_pool.push_back(p.b);
         }
         c->prof.clear();
+        c->prof_chain = false;   // the last end event went back to the pool
     }
 }
 
@@ -86,8 +98,9 @@ extern "C" int vg_ctx_profile(vg_ctx *c, int enable)
     if (!c) return vg_fail(VG_ERR_ARG, "null ctx");
     VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
     c->profiling = enable != 0;
+    c->prof_chain = false;
     for (auto &p : c->prof) {
-        c->event_pool.push_back(p.a);
+        if (!p.shared_a) c->event_pool.push_back(p.a);
         c->event_pool.push_back(p.b);
     }
     c->prof.clear();
@@ -110,10 +123,11 @@ extern "C" int vg_ctx_profile_read(vg_ctx *c, int family, long long *launches, d
         c->prof_launches[p.fam]++;
         c->prof_ms[p.fam] += t;
         c->prof_bytes[p.fam] += p.bytes;
-        c->event_pool.push_back(p.a);
+        if (!p.shared_a) c->event_pool.push_back(p.a);
         c->event_pool.push_back(p.b);
     }
     c->prof.clear();
+    c->prof_chain = false;
     if (launches) *launches = c->prof_launches[family];
     if (ms) *ms = c->prof_ms[family];
     if (bytes) *bytes = c->prof_bytes[family];

@@ -15,7 +15,7 @@
 //   circuit values  k_fg_expand, k_fg_butterfly x lg, k_fg_products (with the
 //                   64 output sums)
 //   phase tables    k_fg_halves (every eq half table of every layer, one
-//                   launch), k_fg_add_tables, k_fg_mult_table,
+//                   launch), k_fg_add_tables, k_fg_mult_part + _reduce,
 //                   k_fg_ifft_p1 / k_fg_ifft_p2 per level (phase 2 reads v_u
 //                   from the device record of phase 1's last round)
 //   rounds          the GKR prover's round kernels (vg_gkr_round over
@@ -45,7 +45,7 @@ vg_fe tovg(fe x)
 constexpr int FG_THREADS = 256;
 constexpr int FG_MAX_LG = 22;
 constexpr int PROD_STEPS = 16;   // products per thread in k_fg_products (stride FG_THREADS)
-constexpr int MULT_STEPS = 8;    // table entries per thread in k_fg_mult_table
+constexpr int MULT_STEPS = 8;    // table entries per thread in k_fg_mult_part (large tables)
 
 __device__ __forceinline__ fe fg_one_minus(fe r) { return vg::fe_one() - r; }
 
@@ -177,35 +177,49 @@ __global__ void k_fg_add_tables(const fe *__restrict__ bg6, int lg, long n, fe *
 }
 
 // multiplication layer (:398-430): add_mult_sum[i] = sum_j beta_g(j 2^lg + i) ep_j^i
-// over lg + 6 bits, addV = 0.  Thread: MULT_STEPS entries i0 + m FG_THREADS.
-__global__ void __launch_bounds__(FG_THREADS) k_fg_mult_table(BetaHalves bg, const fe *__restrict__ ep,
-                                                              const fe *__restrict__ ep_step, int lg,
-                                                              fe *__restrict__ AV, fe *__restrict__ AM)
+// over lg + 6 bits, addV = 0.  Block (bx, q) sums the points q jper ..
+// (q + 1) jper - 1 for the entries i0 + m FG_THREADS (m < STEPS) into
+// parts[q N + i]; k_fg_mult_reduce adds the 64 / jper partials.  Small tables
+// take one point and one entry per thread, so the 64 N terms spread over the
+// whole GPU instead of a few blocks.
+template <int STEPS>
+__global__ void __launch_bounds__(FG_THREADS) k_fg_mult_part(BetaHalves bg, const fe *__restrict__ ep,
+                                                             const fe *__restrict__ ep_step, int lg, int jper,
+                                                             fe *__restrict__ parts)
 {
     const long N = 1L << lg;
-    const long i0 = (long)blockIdx.x * FG_THREADS * MULT_STEPS + threadIdx.x;
+    const long i0 = (long)blockIdx.x * FG_THREADS * STEPS + threadIdx.x;
     if (i0 >= N) return;
-    fe acc[MULT_STEPS];
+    fe acc[STEPS];
 #pragma unroll
-    for (int m = 0; m < MULT_STEPS; ++m) acc[m] = vg::fe_zero();
-    for (int j = 0; j < 64; ++j) {
+    for (int m = 0; m < STEPS; ++m) acc[m] = vg::fe_zero();
+    for (int j = blockIdx.y * jper; j < (int)(blockIdx.y + 1) * jper; ++j) {
         fe x = vg::fe_pow(ep[j], (uint64_t)i0);
         const fe step = ep_step[j];
 #pragma unroll
-        for (int m = 0; m < MULT_STEPS; ++m) {
+        for (int m = 0; m < STEPS; ++m) {
             const long i = i0 + (long)m * FG_THREADS;
             if (i < N) acc[m] = acc[m] + bg.at((long)j * N + i) * x;
             x = x * step;
         }
     }
 #pragma unroll
-    for (int m = 0; m < MULT_STEPS; ++m) {
+    for (int m = 0; m < STEPS; ++m) {
         const long i = i0 + (long)m * FG_THREADS;
-        if (i < N) {
-            AM[i] = acc[m];
-            AV[i] = vg::fe_zero();
-        }
+        if (i < N) parts[(long)blockIdx.y * N + i] = acc[m];
     }
+}
+
+// AM[i] = sum of the partials; AV[i] = 0 (parts may be AV itself: thread i
+// reads its own entry of group 0 before clearing it)
+__global__ void k_fg_mult_reduce(const fe *parts, int groups, long N, fe *AV, fe *__restrict__ AM)
+{
+    const long i = blockIdx.x * (long)blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    fe s = vg::fe_zero();
+    for (int q = 0; q < groups; ++q) s = s + parts[(long)q * N + i];
+    AM[i] = s;
+    AV[i] = vg::fe_zero();
 }
 
 // inverse-FFT level dep, phase 1 (:536-566): for the pair of gates
@@ -334,6 +348,7 @@ struct vg_fft_gkr {
     std::chrono::steady_clock::time_point t0;
     long long launched = 0;
     const vg_fe *recs = nullptr;
+    cudaEvent_t ev[2] = {nullptr, nullptr};   // around the run's device steps
 };
 
 extern "C" int vg_fft_gkr_rounds(int lg) { return (lg + 6) + lg + 2 * lg * lg; }
@@ -357,8 +372,10 @@ extern "C" int vg_fft_gkr_create(vg_ctx *ctx, int max_lg, vg_fft_gkr **out)
     f->ctx = ctx;
     f->max_lg = max_lg;
     int rc = vg_gkr_tables_create(ctx, 64L << max_lg, vg_fft_gkr_rounds(max_lg), &f->tables);
+    if (rc == VG_OK && (cudaEventCreate(&f->ev[0]) != cudaSuccess || cudaEventCreate(&f->ev[1]) != cudaSuccess))
+        rc = vg_fail(VG_ERR_CUDA, "vg_fft_gkr_create: event creation failed");
     if (rc != VG_OK) {
-        delete f;
+        vg_fft_gkr_destroy(f);
         return rc;
     }
     *out = f;
@@ -371,6 +388,8 @@ extern "C" int vg_fft_gkr_destroy(vg_fft_gkr *f)
     cudaStreamSynchronize(f->ctx->stream);
     vg_gkr_destroy(f->tables);
     vg_release(f->ctx, f->dev);
+    for (cudaEvent_t e : f->ev)
+        if (e) cudaEventDestroy(e);
     if (f->host) cudaFreeHost(f->host);
     if (f->parts_host) cudaFreeHost(f->parts_host);
     delete f;
@@ -490,6 +509,7 @@ int vg_fft_gkr_launch(vg_fft_gkr *f, int lg, unsigned seed)
         b.mask = (1L << q.fb) - 1;
         return b;
     };
+    VG_CHECK_CUDA(cudaEventRecord(f->ev[0], c->stream));
     VG_CHECK_CUDA(cudaMemcpyAsync(D, f->host, up_bytes, cudaMemcpyHostToDevice, c->stream));
 
     // ---- circuit values ----
@@ -529,9 +549,22 @@ int vg_fft_gkr_launch(vg_fft_gkr *f, int lg, unsigned seed)
     VG_TRY(rounds(o_au, lg + 6));
     // multiplication layer
     VG_TRY(vg_gkr_tables_begin(g, (const vg_fe *)S, N, &AV, &AM));
-    k_fg_mult_table<<<(unsigned)((N + FG_THREADS * MULT_STEPS - 1) / (FG_THREADS * MULT_STEPS)), FG_THREADS, 0,
-                      c->stream>>>(beta(mult_bg), Rd + o_ep, Rd + o_step, lg, (fe *)AV, (fe *)AM);
-    VG_LAUNCHED(c);
+    {
+        // the partial sums live in AV (64 N entries), cleared by the reduction
+        const bool small = N <= (1L << 14);
+        const int jper = small ? 1 : 4, groups = 64 / jper, per_block = FG_THREADS * (small ? 1 : MULT_STEPS);
+        const dim3 grid((unsigned)((N + per_block - 1) / per_block), (unsigned)groups);
+        if (small)
+            k_fg_mult_part<1><<<grid, FG_THREADS, 0, c->stream>>>(beta(mult_bg), Rd + o_ep, Rd + o_step, lg, jper,
+                                                                (fe *)AV);
+        else
+            k_fg_mult_part<MULT_STEPS><<<grid, FG_THREADS, 0, c->stream>>>(beta(mult_bg), Rd + o_ep, Rd + o_step, lg,
+                                                                         jper, (fe *)AV);
+        VG_LAUNCHED(c);
+        k_fg_mult_reduce<<<grid_for(N, FG_THREADS), FG_THREADS, 0, c->stream>>>((const fe *)AV, groups, N, (fe *)AV,
+                                                                                (fe *)AM);
+        VG_LAUNCHED(c);
+    }
     VG_TRY(rounds(o_mu, lg));
     // inverse-FFT levels
     for (int d = 0; d < lg; ++d) {
@@ -558,6 +591,7 @@ int vg_fft_gkr_launch(vg_fft_gkr *f, int lg, unsigned seed)
     int nrec;
     VG_TRY(vg_gkr_records(g, &f->recs, &nrec));
     if (nrec != nrounds) return vg_fail(VG_ERR_STATE, "fft_gkr: %d records for %d rounds", nrec, nrounds);
+    VG_CHECK_CUDA(cudaEventRecord(f->ev[1], c->stream));
     f->launched = c->launches - launches0;
     f->lg = lg;
     f->pending = true;
@@ -699,6 +733,9 @@ int vg_fft_gkr_finish(vg_fft_gkr *f, vg_fft_gkr_stats *st, vg_fe *msgs, vg_fe *v
     st->proof_size = 48 * (nrounds + lg * (lg + 1) / 2);   // extension_gkr (:770-779) counts messages it never sends
     st->v_time = std::chrono::duration<double>(t1 - tv0).count();
     st->p_time = std::chrono::duration<double>(t1 - f->t0).count();
+    float ms = 0;
+    VG_CHECK_CUDA(cudaEventElapsedTime(&ms, f->ev[0], f->ev[1]));
+    st->gpu_s = ms / 1000.0;
     st->launches = f->launched;
     return VG_OK;
 }

@@ -490,6 +490,9 @@ __global__ void __launch_bounds__(GKR_THREADS) k_gather_keys(EdgeView e, long N,
             for (uint32_t p = s; p < t; ++p) edge1(e.tk[p], e.g[p], e.o[p], bg, prev, am, av);
             out_m[k] = am;
             out_v[k] = av;
+        } else if (t == s) {   // no edges: both entries are zero
+            out_m[k] = vg::fe_zero();
+            out_v[k] = vg::fe_zero();
         } else {
             fe a[4] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
             for (uint32_t p = s; p < t; ++p) edge2(e.tk[p], e.g[p], e.o[p], bg, bu, a);
@@ -594,12 +597,18 @@ __global__ void __launch_bounds__(GKR_THREADS) k_heavy_finish(HeavyKeys H, const
 // once per group instead of once per round.  Per-round partial sums are
 // reduced by the last CTA to finish; every round's sums go to its record.
 constexpr int RG_LOG = 10, RG_CHUNK = 1 << RG_LOG, RG_THREADS = 256, RG_MAX = 12;
+// Per-round partial sums of a group's CTAs ([round][CTA][3]): a group on
+// tables of up to N entries has at most N / RG_CHUNK CTAs, and a group split
+// into small chunks (at most 2 RG_CHUNK entries) at most 2 RG_CHUNK.
+static inline size_t rg_parts_len(long N) { return ((size_t)N / RG_CHUNK + 1 + 2 * RG_CHUNK) * RG_MAX * 3; }
+
 // shared-memory index of table entry i: one pad entry per 8 keeps the
 // stride-4 reads (entries 4k .. 4k+3 of a pair) and the stride-2 writes free
 // of bank conflicts
 __device__ __forceinline__ int rg_ix(long i) { return (int)(i + (i >> 3)); }
 constexpr int RG_TABLE = RG_CHUNK + RG_CHUNK / 8;
 struct RoundGroup {
+    int chunk_log;      // log2 of a CTA's entries after its first step (at most RG_LOG)
     int nsteps;         // rounds in this launch
     int first_nofold;   // the first round has no fold (the round right after a phase init)
     int slot0;          // record of the first round; the others follow
@@ -645,7 +654,8 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
     __shared__ bool last;
     const int t = threadIdx.x;
     // first step: from global into shared
-    const long cin = G.first_nofold ? min(n_in, (long)RG_CHUNK) : min(n_in, 2L * RG_CHUNK);
+    const long chunk = 1L << G.chunk_log;
+    const long cin = G.first_nofold ? min(n_in, chunk) : min(n_in, 2L * chunk);
     const long base = (long)blockIdx.x * cin;
     long m = G.first_nofold ? cin : cin / 2;   // entries in shared after the first step
     {
@@ -1003,6 +1013,7 @@ struct vg_gkr {
     std::vector<fe> pend_r;
     int pend_slot0 = 0;
     long pend_n0 = 0;                    // table length before the group's first round
+    long pend_chunk = 0;                 // a CTA's entries after its first step
     bool pend_nofold = false;
     fe *rg_parts = nullptr;              // per-CTA, per-round partial sums of a group
     fe *heavy_parts = nullptr;           // per-CTA partial sums of heavy keys
@@ -1480,7 +1491,7 @@ static int gkr_bind(vg_gkr *g, const vg_circuit *c)
             for (int k = 0; k < 3; ++k)
                 if (vg_alloc(x, (void **)&g->buf[b][k], (b == 0 ? N : N / 2 + 1) * sizeof(fe)) != VG_OK) return oom("tables");
         if (vg_alloc(x, (void **)&g->eq, 6 * (1L << (c->max_bl / 2 + 1)) * sizeof(fe)) != VG_OK) return oom("eq tables");
-        if (vg_alloc(x, (void **)&g->rg_parts, (N / RG_CHUNK + 1) * RG_MAX * 3 * sizeof(fe)) != VG_OK)
+        if (vg_alloc(x, (void **)&g->rg_parts, rg_parts_len(N) * sizeof(fe)) != VG_OK)
             return oom("group partials");
         g->N_cap = N;
     }
@@ -1886,10 +1897,40 @@ extern "C" int vg_gkr_phase1_init(vg_gkr *g, int layer, const vg_fe *r0, const v
     return finalize_tables(g, N);
 }
 
-// Rounds a group starting at table length n0 can hold (see k_round_group).
-static int group_capacity(long n0, bool nofold)
+// Table length at which a phase's remaining rounds become one single-CTA
+// group (at most one chunk); VIRGO_GROUP_START overrides it (a power of two).
+static long group_start()
 {
-    const long m0 = nofold ? std::min(n0, (long)RG_CHUNK) : std::min(n0, 2L * RG_CHUNK) / 2;
+    static const long v = [] {
+        const char *e = getenv("VIRGO_GROUP_START");
+        long x = e ? atol(e) : 2L * RG_CHUNK;
+        return (x >= 4 && !(x & (x - 1))) ? x : 2L * RG_CHUNK;
+    }();
+    return v;
+}
+
+// With VIRGO_TAIL_CHUNK = c (a power of two below RG_CHUNK), a group starting
+// on more than TAIL_SPLIT chunks' worth of entries uses chunks of c entries,
+// so several CTAs share its first rounds, and the few entries left continue
+// in a single-CTA group.  Off by default: on the matmul and random-circuit
+// proofs measured (c = 32 .. 256) the proof time did not change, since the
+// single-CTA tails overlap the commitment stream.
+constexpr long TAIL_SPLIT = 4;
+static long tail_chunk()
+{
+    static const long v = [] {
+        const char *e = getenv("VIRGO_TAIL_CHUNK");
+        const long x = e ? atol(e) : (long)RG_CHUNK;
+        return (x >= 2 && x <= RG_CHUNK && !(x & (x - 1))) ? x : (long)RG_CHUNK;
+    }();
+    return v;
+}
+
+// Rounds a group starting at table length n0 with chunks of `chunk` can hold
+// (see k_round_group).
+static int group_capacity(long n0, bool nofold, long chunk)
+{
+    const long m0 = nofold ? std::min(n0, chunk) : std::min(n0, 2 * chunk) / 2;
     int k = 0;
     while ((1L << (k + 1)) <= m0) ++k;
     return std::min(k, RG_MAX);
@@ -1916,12 +1957,15 @@ static int flush_rounds(vg_gkr *g)
     if (g->pend_r.empty()) return VG_OK;
     vg_ctx *c = g->ctx;
     RoundGroup G{};
+    int cl = 0;
+    while ((1L << cl) < g->pend_chunk) ++cl;
+    G.chunk_log = cl;
     G.nsteps = (int)g->pend_r.size();
     G.first_nofold = g->pend_nofold ? 1 : 0;
     G.slot0 = g->pend_slot0;
     for (int i = 0; i < G.nsteps; ++i) G.r[i] = g->pend_r[i];
     const long n_in = g->pend_n0;
-    const long cin = G.first_nofold ? std::min(n_in, (long)RG_CHUNK) : std::min(n_in, 2L * RG_CHUNK);
+    const long cin = G.first_nofold ? std::min(n_in, g->pend_chunk) : std::min(n_in, 2 * g->pend_chunk);
     const long grid = n_in / cin;
     const long m_final = (G.first_nofold ? cin : cin / 2) >> (G.nsteps - 1);
     G.last6 = (grid == 1 && m_final == 2) ? 1 : 0;
@@ -2064,18 +2108,20 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
     // the phase are queued and run as one single-CTA group; larger tables run
     // one round per launch (their rounds are throughput bound, the group
     // kernel's serial in-CTA steps are not)
-    const long lim = fold ? 2L * RG_CHUNK : (long)RG_CHUNK;
+    const long lim = std::min(fold ? 2L * RG_CHUNK : (long)RG_CHUNK, group_start());
     if (g->deferred && (!g->pend_r.empty() || g->n <= lim)) {
         if (g->pend_r.empty()) {
             g->pend_n0 = g->n;
             g->pend_nofold = !fold;
             g->pend_slot0 = g->rec_n;
+            const long tc = tail_chunk();
+            g->pend_chunk = (tc < RG_CHUNK && g->n > TAIL_SPLIT * (fold ? 2 * tc : tc)) ? tc : (long)RG_CHUNK;
         }
         g->pend_r.push_back(tofe(previous_random));
         ++g->rec_n;
         if (fold) g->n /= 2;
         g->round0_pending = false;
-        if ((int)g->pend_r.size() >= group_capacity(g->pend_n0, g->pend_nofold)) VG_TRY(flush_rounds(g));
+        if ((int)g->pend_r.size() >= group_capacity(g->pend_n0, g->pend_nofold, g->pend_chunk)) VG_TRY(flush_rounds(g));
         return VG_OK;
     }
     vg_ctx *c = g->ctx;
@@ -2148,7 +2194,7 @@ int vg_gkr_tables_create(vg_ctx *ctx, long max_n, int max_records, vg_gkr **out)
         for (int k = 0; k < 3; ++k)
             if (cudaMalloc(&g->buf[b][k], (b == 0 ? max_n : max_n / 2 + 1) * sizeof(fe)) != cudaSuccess)
                 return fail("tables");
-    if (cudaMalloc(&g->rg_parts, (max_n / RG_CHUNK + 1) * RG_MAX * 3 * sizeof(fe)) != cudaSuccess)
+    if (cudaMalloc(&g->rg_parts, rg_parts_len(max_n) * sizeof(fe)) != cudaSuccess)
         return fail("group partials");
     if (cudaMalloc(&g->rec, (size_t)max_records * 9 * sizeof(fe)) != cudaSuccess) return fail("records");
     g->N_cap = max_n;

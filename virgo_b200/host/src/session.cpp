@@ -874,7 +874,7 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
         rc = vg_fft_gkr_finish(s->fft, &fs, nullptr, nullptr);
         if (rc != VG_OK) return rc;
         if (!fs.pass) return vg_fail(VG_ERR_STATE, "fft_gkr side proof (lg %d) failed its checks", fft_lg);
-        st.fft_gkr_s = fs.p_time;
+        st.fft_gkr_s = fs.gpu_s;
         st.fft_gkr_lg = fft_lg;
         st.fft_gkr_proof_size = fs.proof_size;
     }
