@@ -495,8 +495,9 @@ def roofline(fam, hbm_peak, peak_kind):
                              "average launch's algorithmic bytes") if traffic else None,
             "peak_source": peak_kind, "launches_per_proof": f["launches"],
             "avg_launch_us": round(1000.0 * f["ms"] / f["launches"], 2), "bytes_per_launch": per_launch,
-            "note": "per-launch CUDA events add about 10 us to every launch's measured time; the kernel is "
-                    "integer-ALU bound (ncu ALU pipe 80%)"}
+            "note": "CUDA events on the launching stream; back-to-back launches share one event, so a "
+                    "launch's time runs from the end of the one before it; the kernel is integer-ALU bound "
+                    "(ncu ALU pipe 80%)"}
 
 
 def main():
