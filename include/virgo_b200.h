@@ -291,7 +291,7 @@ typedef struct {
     double prove_time;      /* launch_s + wait_s: every prover message is on the host */
     long long proof_size;   /* bytes by the reference's accounting, without fft_gkr */
     long long launches;     /* kernels launched for this proof, the side proof's included */
-    double fft_gkr_s;       /* the fft_gkr side proof: launch to checked (0 when not run) */
+    double fft_gkr_s;       /* the fft_gkr side proof: device time of its stream (0 when not run) */
     int fft_gkr_lg;         /* its size L - 6, 0 when not run */
     int fft_gkr_proof_size; /* its bytes as the reference counts them (the verifier adds them) */
 } vg_proof_stats;
@@ -347,6 +347,13 @@ int vg_session_prove(vg_session *s, unsigned seed, int want_transcript, vg_proof
  * to every proof (vpd_verifier.cpp:89-99); on by default, off with on = 0.
  * A side proof that fails its checks fails the proof. */
 int vg_session_set_fft_gkr(vg_session *s, int on);
+/* New input values for the loaded circuit: the u of the n input gates of the
+ * file-level input layer (as in vg_session_load: values read through int32,
+ * the rest of the padded layer zero), host memory (pinned or pageable).  The
+ * wiring stays on the device, so a circuit proven for many witnesses uploads
+ * only these values (8 bytes each) per proof.  Forks keep their own values;
+ * loading a circuit returns to that circuit's. */
+int vg_session_set_inputs(vg_session *s, const int64_t *values, long n);
 /* n proofs at once, session i with seed i, each on its own host thread and
  * CUDA stream (the sessions must be distinct objects, e.g. forks of one).
  * stats, transcripts and transcript_lens have n entries (or are NULL). */
@@ -405,6 +412,7 @@ typedef struct vg_fft_gkr vg_fft_gkr;
 typedef struct {
     double p_time;        /* seconds: first launch to the last message checked */
     double v_time;        /* seconds: the in-process verifier's checks */
+    double gpu_s;         /* seconds of its stream: first to last of its device steps */
     int proof_size;       /* bytes, counted as fft_circuit_GKR.cpp counts them */
     int pass;
     int rounds;           /* sumcheck messages */

@@ -6,6 +6,7 @@ import json
 import os
 import subprocess
 
+import numpy as np
 import pytest
 
 import virgo_b200 as vb
@@ -294,3 +295,33 @@ def test_sha256_circuit_matches_reference(tmp_path):
     finally:
         s.close()
     assert transcript.first_difference(transcript.parse(blob), transcript.prover_records(ref)) is None
+
+
+def test_session_set_inputs_equals_fresh_circuit():
+    """A new witness through vg_session_set_inputs (wiring resident) proves
+    the same transcript as a session built from the circuit with those input
+    values; a fork's values leave the base alone; loading a circuit returns to
+    its own values."""
+    a = circuits.matmul_addtree(8, 20, seed=3)
+    b = circuits.matmul_addtree(8, 20, seed=4)
+    for (ta, ua, va), (tb, ub, vb_) in zip(a[1:], b[1:]):   # same wiring, other inputs
+        assert (ta == tb).all() and (ua == ub).all() and (va == vb_).all()
+    assert not (a[0][1] == b[0][1]).all()
+    sa, sb = vb.Session(a), vb.Session(b)
+    fork = sa.fork()
+    try:
+        want_a, want_b = sa.prove(5)[1], sb.prove(5)[1]
+        fork.set_inputs(b[0][1])
+        assert fork.prove(5)[1] == want_b
+        assert sa.prove(5)[1] == want_a
+        sa.set_inputs(b[0][1][:3])   # a prefix: the remaining inputs become zero
+        short = sa.prove(5)[1]
+        assert short != want_a and short != want_b
+        fork.load(a)
+        assert fork.prove(5)[1] == want_a
+        with pytest.raises(vb.VirgoError):
+            sa.set_inputs(np.zeros(1 << 20, np.int64))   # longer than the input layer
+    finally:
+        fork.close()
+        sa.close()
+        sb.close()

@@ -81,6 +81,7 @@ def lib():
             "vg_fft_gkr_rounds": (c_i, [c_i]),
             "vg_fft_gkr_footprint": (c_sz, [c_i]),
             "vg_session_set_fft_gkr": (c_i, [c_p, c_i]),
+            "vg_session_set_inputs": (c_i, [c_p, c_p, c_l]),
             "vg_fft_gkr_create": (c_i, [c_p, c_i, ctypes.POINTER(c_p)]),
             "vg_fft_gkr_prove": (c_i, [c_p, c_i, ctypes.c_uint, ctypes.POINTER(vg_fft_gkr_stats), c_p, c_p]),
             "vg_fft_gkr_destroy": (c_i, [c_p]),
@@ -271,6 +272,15 @@ class Session:
         data = ctypes.string_at(buf, n.value) if (transcript and n.value) else b""
         lib().vg_free(buf)
         return st, data
+
+    def set_inputs(self, values):
+        """New witness for the loaded circuit: the u of its input gates
+        (int64 array, host; pinned memory is copied without staging)."""
+        if isinstance(values, np.ndarray):
+            v = np.ascontiguousarray(values, dtype=np.int64)
+            check(lib().vg_session_set_inputs(self.h, v.ctypes.data, len(v)), "vg_session_set_inputs")
+        else:   # a pinned torch tensor
+            check(lib().vg_session_set_inputs(self.h, values.data_ptr(), values.numel()), "vg_session_set_inputs")
 
     def set_fft_gkr(self, on: bool):
         """Run the fft_gkr side proof beside every proof (default on)."""

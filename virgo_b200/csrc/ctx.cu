@@ -378,6 +378,18 @@ int vg_pinned(vg_ctx *c, size_t n, fe **p)
 
 int vg_ctx_grow_dev(vg_ctx *c, void **p, size_t *cap, size_t bytes) { return grow(c, p, cap, bytes); }
 
+int vg_ctx_wait_for(vg_ctx *waiter, vg_ctx *signaler)
+{
+    if (!waiter || !signaler) return vg_fail(VG_ERR_ARG, "vg_ctx_wait_for: null context");
+    cudaEvent_t e;
+    VG_CHECK_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    cudaError_t rc = cudaEventRecord(e, signaler->stream);
+    if (rc == cudaSuccess) rc = cudaStreamWaitEvent(waiter->stream, e, 0);
+    cudaEventDestroy(e);   // released once the wait is resolved
+    VG_CHECK_CUDA(rc);
+    return VG_OK;
+}
+
 bool vg_is_device_ptr(const void *p)
 {
     cudaPointerAttributes a;

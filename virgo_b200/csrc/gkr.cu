@@ -1589,6 +1589,30 @@ extern "C" int vg_gkr_evaluate(vg_gkr *g)
     return VG_OK;
 }
 
+int vg_gkr_set_input(vg_gkr *g, const vg_fe *input)
+{
+    if (!g || !g->C || g->vals.empty()) return vg_fail(VG_ERR_STATE, "vg_gkr_set_input: no circuit bound");
+    g->vals[0] = input ? (fe *)input : g->C->input;
+    return VG_OK;
+}
+
+// layer-0 values from input-gate u values: read through int32 as the
+// circuit build does (zk_prover.cpp:60-65), zero from n up to width
+__global__ void k_input_values(const int64_t *__restrict__ u, long n, long width, fe *__restrict__ out)
+{
+    for (long g = blockIdx.x * (long)blockDim.x + threadIdx.x; g < width; g += (long)gridDim.x * blockDim.x)
+        out[g] = g < n ? from_int32((int32_t)u[g]) : vg::fe_zero();
+}
+
+int vg_input_values(vg_ctx *c, const int64_t *dev_u, long n, long width, vg_fe *out)
+{
+    if (!c || !dev_u || !out || n < 1 || n > width) return vg_fail(VG_ERR_ARG, "vg_input_values: bad argument");
+    k_input_values<<<std::min<unsigned>(grid_for(width, 256), 148u * 16u), 256, 0, c->stream>>>(dev_u, n, width,
+                                                                                            (fe *)out);
+    VG_LAUNCHED(c);
+    return VG_OK;
+}
+
 extern "C" int vg_gkr_layer_values(vg_gkr *g, int layer, const vg_fe **dev_values)
 {
     if (!g || !dev_values || layer < 0 || layer >= g->C->depth) return vg_fail(VG_ERR_ARG, "vg_gkr_layer_values: bad layer");

@@ -35,6 +35,19 @@ int vg_gkr_record_count(const vg_gkr *g);
 int vg_fft_gkr_launch(vg_fft_gkr *f, int lg, unsigned seed);
 int vg_fft_gkr_finish(vg_fft_gkr *f, vg_fft_gkr_stats *st, vg_fe *msgs, vg_fe *vals);
 
+// The evaluation's input layer read from `input` (device, layer-0 width)
+// instead of the circuit's own values; null goes back to the circuit's.
+int vg_gkr_set_input(vg_gkr *g, const vg_fe *input);
+// Layer-0 values from n input-gate u values on the device (read through int32
+// as the circuit build does), zero up to width; enqueued on c's stream.
+int vg_input_values(vg_ctx *c, const int64_t *dev_u, long n, long width, vg_fe *out);
+// Host-to-device copy on c's stream (pageable sources through the context's
+// pinned ring; a pageable source may be reused on return).
+int vg_h2d_staged(vg_ctx *c, void *dst, const void *src, size_t bytes);
+// Work enqueued on waiter's stream from now on waits for the work enqueued so
+// far on signaler's.
+int vg_ctx_wait_for(vg_ctx *waiter, vg_ctx *signaler);
+
 // Grows a device buffer from the stream-ordered pool on c's stream.
 int vg_ctx_grow_dev(vg_ctx *c, void **p, size_t *cap, size_t bytes);
 

@@ -115,6 +115,10 @@ struct vg_session {
     void *pub = nullptr;   // device buffer for the public eq table
     size_t pub_bytes = 0;
     bool loaded = false;   // false after a failed load: no valid circuit
+    // input values set by vg_session_set_inputs (device; null: the circuit's own)
+    void *inputs = nullptr, *inputs_raw = nullptr;
+    size_t inputs_bytes = 0, inputs_raw_bytes = 0;
+    bool inputs_on = false;
     // the fft_gkr side proof of every proof (on its own stream), made on first use
     vg_ctx *fctx = nullptr;
     vg_fft_gkr *fft = nullptr;
@@ -153,6 +157,37 @@ static int fft_side_launch(vg_session *s, int *lg_out)
         return rc;
     }
     *lg_out = lg;
+    return VG_OK;
+}
+
+// Back to the circuit's own input values (a new circuit was loaded).
+static void drop_inputs(vg_session *s)
+{
+    if (s->inputs_on && s->p && s->p->dev_gkr) vg_gkr_set_input(s->p->dev_gkr, nullptr);
+    s->inputs_on = false;
+}
+
+extern "C" int vg_session_set_inputs(vg_session *s, const int64_t *values, long n)
+{
+    if (!s || !s->p || !values) return vg_fail(VG_ERR_ARG, "vg_session_set_inputs: null argument");
+    if (!s->loaded) return vg_fail(VG_ERR_STATE, "vg_session_set_inputs: no circuit loaded");
+    const long width = 1L << s->circuit->C.circuit[0].bit_length;
+    if (n < 1 || n > width) return vg_fail(VG_ERR_ARG, "vg_session_set_inputs: %ld values for an input layer of %ld", n, width);
+    int dev = 0;
+    vg_ctx_device(s->ctx, &dev);
+    cudaSetDevice(dev);
+    int rc = vg_ctx_grow_dev(s->ctx, &s->inputs_raw, &s->inputs_raw_bytes, (size_t)n * 8);
+    if (rc == VG_OK) rc = vg_ctx_grow_dev(s->ctx, &s->inputs, &s->inputs_bytes, (size_t)width * sizeof(F));
+    if (rc == VG_OK) rc = vg_h2d_staged(s->ctx, s->inputs_raw, values, (size_t)n * 8);
+    if (rc == VG_OK) rc = vg_input_values(s->ctx, (const int64_t *)s->inputs_raw, n, width, (vg_fe *)s->inputs);
+    if (rc == VG_OK) rc = vg_gkr_set_input(s->p->dev_gkr, (const vg_fe *)s->inputs);
+    // the commitment's stream reads the input layer too
+    if (rc == VG_OK) rc = vg_ctx_wait_for(s->cctx, s->ctx);
+    if (rc != VG_OK) {
+        drop_inputs(s);
+        return rc;
+    }
+    s->inputs_on = true;
     return VG_OK;
 }
 
@@ -212,6 +247,7 @@ extern "C" int vg_session_load(vg_session *s, int d, const long *n, const uint8_
     if (!s->circuit || s->circuit.use_count() > 1) s->circuit = std::make_shared<CircuitData>();
     CircuitData *cd = s->circuit.get();
     std::vector<int> bl(d + 1);
+    drop_inputs(s);
     s->loaded = false;
     int rc = vg_circuit_build(s->ctx, d, n, ty, u, v, index_bytes, &cd->dev, bl.data());
     if (rc != VG_OK) return rc;
@@ -360,6 +396,11 @@ extern "C" int vg_session_destroy(vg_session *s)
         delete s->p;
     }
     if (s->pub) vg_dev_free(s->cctx, s->pub);
+    if (s->ctx) {
+        vg_ctx_sync(s->ctx);
+        if (s->inputs) vg_dev_free(s->ctx, s->inputs);
+        if (s->inputs_raw) vg_dev_free(s->ctx, s->inputs_raw);
+    }
     if (s->fft) vg_fft_gkr_destroy(s->fft);
     if (s->fctx) vg_ctx_destroy(s->fctx);
     if (s->pc) vg_pc_destroy(s->pc);
