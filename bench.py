@@ -415,12 +415,15 @@ def batched_random(count, seed, slots):
             "timing": "wall clock, circuit upload + proof + transcript download per job"}
 
 
-def served(n_jobs, seed, slots, rate_factor=3.0):
+def served(n_jobs, seed, slots, rate_factor=3.0, budget_ms=500.0, slo_factors=(0.5, 0.8, 1.0, 1.2, 1.5, 2.0, 3.0)):
     """Poisson arrivals of jobs mixing 2^14-, 2^18- and 2^22-gate random
-    layered circuits (depth 16).  The arrival rate is rate_factor x the
-    plain form's throughput on the same mix; the server (continuous
-    batching) and a one-slot server (the plain form with a queue) see the
-    same arrival times.  Latency = submit to transcript on the host."""
+    layered circuits (depth 16) and SHA-256 compression circuits.  The
+    arrival rate is rate_factor x the plain form's throughput on the same
+    mix; the server (continuous batching) and a one-slot server (the plain
+    form with a queue) see the same arrival times.  Latency = submit to
+    transcript on the host.  slo: both forms at arrival rates slo_factors x
+    the plain form's saturated rate; each form's best throughput among the
+    rates whose p99 stays within budget_ms."""
     import threading as th
     import virgo_b200 as vb
     from virgo_b200 import circuits
@@ -475,15 +478,84 @@ def served(n_jobs, seed, slots, rate_factor=3.0):
     times = np.cumsum(rng.exponential(1.0 / rate, size=n_jobs))
     lat_s, span_s = run(slots, times)
     lat_p, span_p = run(1, times)
+    sweep = []
+    best = {"served": 0.0, "plain": 0.0}
+    base = rng.exponential(1.0, size=n_jobs)   # one arrival pattern, scaled per rate
+    for fct in slo_factors:
+        ts = np.cumsum(base / (fct * plain_rate))
+        row = {"arrival_factor": fct}
+        for form, ns in (("served", slots), ("plain", 1)):
+            lat, span = run(ns, ts)
+            p99 = 1000 * _pctl(lat, 0.99)
+            row[form] = {"proofs_s": round(n_jobs / span, 1), "p99_ms": round(p99, 1)}
+            if p99 <= budget_ms:
+                best[form] = max(best[form], n_jobs / span)
+        sweep.append(row)
     return {"value": n_jobs / span_s, "unit": "proofs/s", "p50_ms": 1000 * _pctl(lat_s, 0.5),
             "p99_ms": 1000 * _pctl(lat_s, 0.99),
             "plain": {"value": n_jobs / span_p, "p50_ms": 1000 * _pctl(lat_p, 0.5), "p99_ms": 1000 * _pctl(lat_p, 0.99),
                       "saturated_value": plain_rate},
             "arrival_rate": rate, "jobs": n_jobs, "slots": slots,
+            "slo": {"p99_budget_ms": budget_ms, "served_proofs_s": round(best["served"], 1),
+                    "plain_proofs_s": round(best["plain"], 1),
+                    "ratio": round(best["served"] / best["plain"], 3) if best["plain"] else None, "sweep": sweep},
             "workload": "Poisson arrivals at %.1fx the plain form's rate; equal shares of random layered circuits "
                         "of 2^14, 2^18, 2^22 gates (depth 16) and SHA-256 compression circuits over 2^4 and 2^6 "
                         "blocks" % rate_factor,
             "timing": "wall clock, submit to transcript on the host (circuit upload included)"}
+
+
+def commit_path(sizes=(20, 22, 24), reps=3):
+    """Config 2: the kernel-level commit path alone (vg_pc_commit_all: RS
+    encodings of a private and a public vector of 2^L seeded F_p2 values,
+    the virtual oracle, every FRI fold to 32 entries per slice, every leaf
+    chain and Merkle tree, 2 + 2 (L - 6) query answers), host arrays in and
+    out, wall clock per call after one warm-up call; Keccak-f count
+    65 (2^(L-2) + 2^(L-2) + sum of the FRI levels' leaves)."""
+    import virgo_b200 as vb
+    L = vb.lib()
+    P = (1 << 61) - 1
+    ctx = vb.Context(0)
+    out = []
+    try:
+        for log_len in sizes:
+            n, S = 1 << log_len, 1 << (log_len - 1)
+            rng = np.random.default_rng(log_len)
+            fe = lambda k: rng.integers(0, P, (k, 2), dtype=np.uint64)  # noqa: E731
+            nlevels = log_len - 6
+            gap = 1
+            while gap * 2 <= S // 300:
+                gap *= 2
+            M = S // gap
+            priv, pub, mask, pub_mask, fri_r = fe(n), fe(n), fe(300), fe(M), fe(nlevels)
+            which = np.array([0, 1] + [2 + t for t in range(nlevels)], np.int32)
+            pos = rng.integers(0, S // 2, len(which)).astype(np.int64)
+            nq = len(which)
+            roots = np.zeros((2 + nlevels, 32), np.uint8)
+            sums, inner = np.zeros((65, 2), np.uint64), np.zeros(2, np.uint64)
+            fin = np.zeros((65 * 32, 2), np.uint64)
+            qv, qp = np.zeros((nq * 130, 2), np.uint64), np.zeros((nq * 32, 32), np.uint8)
+            pc = ctypes.c_void_p()
+            vb.check(L.vg_pc_create(ctx.h, ctypes.byref(pc)))
+            try:
+                ts = []
+                for k in range(reps + 1):
+                    t0 = time.perf_counter()
+                    vb.check(L.vg_pc_commit_all(pc, vb.ptr(priv), log_len, vb.ptr(mask), 300, vb.ptr(pub),
+                                                vb.ptr(pub_mask), M, vb.ptr(fri_r), nlevels, nq, vb.ptr(which),
+                                                vb.ptr(pos), vb.ptr(roots), vb.ptr(sums), vb.ptr(inner), vb.ptr(fin),
+                                                vb.ptr(qv), vb.ptr(qp)), "vg_pc_commit_all")
+                    ts.append(time.perf_counter() - t0)
+            finally:
+                L.vg_pc_destroy(pc)
+            t = min(ts[1:])
+            leaves = 2 * (n >> 2) + sum(n >> (3 + i) for i in range(nlevels))
+            out.append({"log_len": log_len, "ms": round(1000 * t, 2), "keccak_f": 65 * leaves,
+                        "keccak_f_per_s": round(65 * leaves / t / 1e9, 3), "unit": "G Keccak-f/s",
+                        "h2d_bytes": int(priv.nbytes + pub.nbytes + mask.nbytes + pub_mask.nbytes)})
+    finally:
+        ctx.close()
+    return out
 
 
 def barrier(world):
@@ -581,8 +653,10 @@ def main():
             "kernel_families": fam,
         }
         if not args.no_served and world == 1:
+            line["commit_path"] = {"note": "config 2, best of 3 calls, wall clock incl. host<->device copies",
+                                   "sizes": commit_path()}
             line["batched_random64"] = batched_random(64, seed=4, slots=args.batch)
-            line["served"] = served(48, seed=5, slots=args.batch)
+            line["served"] = served(96, seed=5, slots=args.batch)
         if not args.no_cpu_baseline and world >= 1 and os.path.exists(REF_BIN):
             tmp = tempfile.mkdtemp(prefix="virgo_circ_")
             c, m = os.path.join(tmp, "c.txt"), os.path.join(tmp, "m.txt")
