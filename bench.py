@@ -442,12 +442,14 @@ def served(n_jobs, seed, slots, rate_factor=3.0, budget_ms=500.0, slo_factors=(0
         srv = vb.Server(slots=nslots)
         lat, done_at = [], []
         try:
-            # warm every slot on the largest shape, all at once so each worker
-            # grows its buffers before the timed arrivals
-            big = pool[22] + pool["sha6"]
-            warm = [srv.submit(big[k % len(big)], 1, transcript=False) for k in range(2 * nslots)]
-            for j in warm:
-                srv.wait(j)
+            # warm every slot on the largest shapes (the largest input and the
+            # widest layers), one wave per shape submitted at once, so each
+            # idle worker takes one and grows its buffers before the timed
+            # arrivals
+            for big in (pool["sha6"][0], pool[22][0]):
+                warm = [srv.submit(big, 1, transcript=False) for _ in range(nslots)]
+                for j in warm:
+                    srv.wait(j)
             ids = [None] * n_jobs
             t0 = time.perf_counter()
 

@@ -325,3 +325,24 @@ def test_session_set_inputs_equals_fresh_circuit():
         fork.close()
         sa.close()
         sb.close()
+
+
+def test_side_proof_grows_with_the_input():
+    """A session whose next circuit has a larger input grows its fft_gkr side
+    proof in place (lg 9 -> 12) and proves what a fresh session proves."""
+    small = circuits.random_layered([10, 11, 10], seed=8)            # input padded to 2^15
+    large = circuits.random_layered([18, 12, 11, 12, 10], seed=9)    # input 2^18
+    s = vb.Session(small)
+    try:
+        st, _ = s.prove(3)
+        assert st.fft_gkr_lg == 9
+        s.load(large)
+        st, blob = s.prove(3)
+        assert st.fft_gkr_lg == 12
+    finally:
+        s.close()
+    fresh = vb.Session(large)
+    try:
+        assert fresh.prove(3)[1] == blob
+    finally:
+        fresh.close()

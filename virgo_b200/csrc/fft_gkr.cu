@@ -382,6 +382,17 @@ extern "C" int vg_fft_gkr_create(vg_ctx *ctx, int max_lg, vg_fft_gkr **out)
     return VG_OK;
 }
 
+int vg_fft_gkr_reserve(vg_fft_gkr *f, int max_lg)
+{
+    if (!f || max_lg < 1 || max_lg > FG_MAX_LG)
+        return vg_fail(VG_ERR_ARG, "vg_fft_gkr_reserve: max_lg %d outside 1..%d", max_lg, FG_MAX_LG);
+    if (max_lg <= f->max_lg) return VG_OK;
+    if (f->pending) return vg_fail(VG_ERR_STATE, "vg_fft_gkr_reserve: a run is in flight");
+    VG_TRY(vg_gkr_tables_reserve(f->tables, 64L << max_lg, vg_fft_gkr_rounds(max_lg)));
+    f->max_lg = max_lg;
+    return VG_OK;
+}
+
 extern "C" int vg_fft_gkr_destroy(vg_fft_gkr *f)
 {
     if (!f) return VG_OK;

@@ -2214,17 +2214,47 @@ int vg_gkr_tables_create(vg_ctx *ctx, long max_n, int max_records, vg_gkr **out)
     if (cudaMalloc(&g->round_out, 16 * sizeof(fe)) != cudaSuccess) return fail("round sums");
     if (cudaMalloc(&g->round_counter, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
     if (cudaMemset(g->round_counter, 0, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
-    for (int b = 0; b < 2; ++b)
-        for (int k = 0; k < 3; ++k)
-            if (cudaMalloc(&g->buf[b][k], (b == 0 ? max_n : max_n / 2 + 1) * sizeof(fe)) != cudaSuccess)
-                return fail("tables");
-    if (cudaMalloc(&g->rg_parts, rg_parts_len(max_n) * sizeof(fe)) != cudaSuccess)
-        return fail("group partials");
-    if (cudaMalloc(&g->rec, (size_t)max_records * 9 * sizeof(fe)) != cudaSuccess) return fail("records");
-    g->N_cap = max_n;
-    g->rec_cap = max_records;
     g->deferred = true;
+    const int rc = vg_gkr_tables_reserve(g, max_n, max_records);
+    if (rc != VG_OK) {
+        vg_gkr_destroy(g);
+        return rc;
+    }
     *out = g;
+    return VG_OK;
+}
+
+// Grows the tables, group partials and records from the stream-ordered pool
+// (no device-wide synchronisation, so a server slot can grow while the
+// others prove); never shrinks.
+int vg_gkr_tables_reserve(vg_gkr *g, long max_n, int max_records)
+{
+    if (!g || g->C || max_n < 2 || (max_n & (max_n - 1)) || max_records < 1)
+        return vg_fail(VG_ERR_ARG, "vg_gkr_tables_reserve: bad argument (max_n %ld, records %d)", max_n, max_records);
+    vg_ctx *x = g->ctx;
+    VG_TRY(flush_rounds(g));
+    if (max_n > g->N_cap) {
+        for (int b = 0; b < 2; ++b)
+            for (int k = 0; k < 3; ++k) {
+                vg_release(x, g->buf[b][k]);
+                g->buf[b][k] = nullptr;
+            }
+        vg_release(x, g->rg_parts);
+        g->rg_parts = nullptr;
+        g->N_cap = 0;
+        for (int b = 0; b < 2; ++b)
+            for (int k = 0; k < 3; ++k)
+                VG_TRY(vg_alloc(x, (void **)&g->buf[b][k], (b == 0 ? max_n : max_n / 2 + 1) * sizeof(fe)));
+        VG_TRY(vg_alloc(x, (void **)&g->rg_parts, rg_parts_len(max_n) * sizeof(fe)));
+        g->N_cap = max_n;
+    }
+    if (max_records > g->rec_cap) {
+        vg_release(x, g->rec);
+        g->rec = nullptr;
+        g->rec_cap = 0;
+        VG_TRY(vg_alloc(x, (void **)&g->rec, (size_t)max_records * 9 * sizeof(fe)));
+        g->rec_cap = max_records;
+    }
     return VG_OK;
 }
 

@@ -24,6 +24,7 @@ int vg_gkr_records(vg_gkr *g, const vg_fe **host, int *n);
 // and takes V (n entries, read in place by the first round).  Records as in
 // deferred mode, numbered from the last rewind; vg_gkr_destroy frees.
 int vg_gkr_tables_create(vg_ctx *ctx, long max_n, int max_records, vg_gkr **out);
+int vg_gkr_tables_reserve(vg_gkr *g, long max_n, int max_records);
 int vg_gkr_tables_rewind(vg_gkr *g);
 int vg_gkr_tables_begin(vg_gkr *g, const vg_fe *V, long n, vg_fe **AV, vg_fe **AM);
 const vg_fe *vg_gkr_records_dev(const vg_gkr *g);
@@ -34,6 +35,9 @@ int vg_gkr_record_count(const vg_gkr *g);
 // messages (so other work can be launched in between).
 int vg_fft_gkr_launch(vg_fft_gkr *f, int lg, unsigned seed);
 int vg_fft_gkr_finish(vg_fft_gkr *f, vg_fft_gkr_stats *st, vg_fe *msgs, vg_fe *vals);
+// Raises the largest size the object proves to max_lg (buffers from the
+// stream-ordered pool, no device-wide synchronisation).
+int vg_fft_gkr_reserve(vg_fft_gkr *f, int max_lg);
 
 // The evaluation's input layer read from `input` (device, layer-0 width)
 // instead of the circuit's own values; null goes back to the circuit's.

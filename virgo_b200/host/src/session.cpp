@@ -143,11 +143,12 @@ static int fft_side_launch(vg_session *s, int *lg_out)
         rc = vg_ctx_create(dev, &s->fctx);
         if (rc != VG_OK) return rc;
     }
-    if (!s->fft || s->fft_max_lg < lg) {
-        if (s->fft) vg_fft_gkr_destroy(s->fft);
-        s->fft = nullptr;
-        s->fft_max_lg = 0;
+    if (!s->fft) {
         rc = vg_fft_gkr_create(s->fctx, lg, &s->fft);
+        if (rc != VG_OK) return rc;
+        s->fft_max_lg = lg;
+    } else if (s->fft_max_lg < lg) {   // grown in place: no device-wide synchronisation
+        rc = vg_fft_gkr_reserve(s->fft, lg);
         if (rc != VG_OK) return rc;
         s->fft_max_lg = lg;
     }
