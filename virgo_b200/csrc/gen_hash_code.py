@@ -1,5 +1,5 @@
-"""Generates hash_code.inc: the unrolled Keccak-f[1600] permutation and the
-SHA-256 constants used by the device hash kernels.
+"""Generates hash_code.inc: the unrolled Keccak-f[1600] round on 64-bit lanes
+(host) and on 32-bit lane halves (device), and the SHA-256 constants.
 
 All constants are derived from their FIPS definitions rather than typed in:
 Keccak round constants from the rc(t) LFSR and rotation offsets from the
@@ -57,7 +57,7 @@ def main():
     rot = keccak_rotations()
     L = []
     L.append("// Generated by gen_hash_code.py from the FIPS 202 / FIPS 180-4 definitions. Do not edit.")
-    L.append("// Lanes are a[x + 5*y] held in 64-bit registers a0..a24.")
+    # 64-bit lanes a0..a24 (the host implementation)
     L.append("#define VG_KECCAK_ROUND_CONSTANTS { \\")
     L.append("    " + ", ".join("0x%016xull" % v for v in rc) + " }")
     L.append("")
@@ -86,6 +86,51 @@ def main():
             body.append("      a%d = b%d ^ (~b%d & b%d); \\" % (i, i, (x + 1) % 5 + 5 * y, (x + 2) % 5 + 5 * y))
     body.append("      a0 ^= (RC); }")
     L.append("#define VG_KECCAK_ROUND(RC) \\")
+    L.extend(body)
+    L.append("")
+    # Lanes are held as 32-bit halves aL<i> (bits 0..31) and aH<i> (bits
+    # 32..63) of a[x + 5y]: a 64-bit rotation is two funnel shifts, the
+    # 3-input xors of theta and the chi step are one lop3 each (vg_xor3,
+    # vg_chi in hash.cuh), and theta's D[x] is folded into the lane update.
+    L.append("// Lanes a[x + 5*y] are held as 32-bit halves aL<i>, aH<i>.")
+    L.append("#define VG_KECCAK_RC_LO { " + ", ".join("0x%08xu" % (v & 0xFFFFFFFF) for v in rc) + " }")
+    L.append("#define VG_KECCAK_RC_HI { " + ", ".join("0x%08xu" % (v >> 32) for v in rc) + " }")
+    L.append("")
+    body = []
+    for h in "LH":
+        for x in range(5):
+            body.append("    uint32_t c%s%d = vg_xor3(vg_xor3(a%s%d, a%s%d, a%s%d), a%s%d, a%s%d); \\"
+                        % (h, x, h, x, h, x + 5, h, x + 10, h, x + 15, h, x + 20))
+    for x in range(5):   # rot1 of each column parity
+        body.append("    uint32_t rL%d = __funnelshift_l(cH%d, cL%d, 1), rH%d = __funnelshift_l(cL%d, cH%d, 1); \\"
+                    % (x, x, x, x, x, x))
+    for i in range(25):
+        x = i % 5
+        for h in "LH":
+            body.append("    a%s%d = vg_xor3(a%s%d, c%s%d, r%s%d); \\" % (h, i, h, i, h, (x + 4) % 5, h, (x + 1) % 5))
+    # rho + pi: b[y, 2x+3y] = rot(a[x, y], r[x][y])
+    for x in range(5):
+        for y in range(5):
+            dst = y + 5 * ((2 * x + 3 * y) % 5)
+            src = x + 5 * y
+            n = rot[x][y]
+            if n == 0:
+                body.append("    uint32_t bL%d = aL%d, bH%d = aH%d; \\" % (dst, src, dst, src))
+            elif n < 32:
+                body.append("    uint32_t bL%d = __funnelshift_l(aH%d, aL%d, %d), bH%d = __funnelshift_l(aL%d, aH%d, %d); \\"
+                            % (dst, src, src, n, dst, src, src, n))
+            else:   # rotation by 32 swaps the halves
+                body.append("    uint32_t bL%d = __funnelshift_l(aL%d, aH%d, %d), bH%d = __funnelshift_l(aH%d, aL%d, %d); \\"
+                            % (dst, src, src, n - 32, dst, src, src, n - 32))
+    # chi
+    for y in range(5):
+        for x in range(5):
+            i = x + 5 * y
+            j, k = (x + 1) % 5 + 5 * y, (x + 2) % 5 + 5 * y
+            for h in "LH":
+                body.append("    a%s%d = vg_chi(b%s%d, b%s%d, b%s%d); \\" % (h, i, h, i, h, j, h, k))
+    body.append("    aL0 ^= (RCL); aH0 ^= (RCH); }")
+    L.append("#define VG_KECCAK_ROUND32(RCL, RCH) { \\")
     L.extend(body)
     L.append("")
     ps = primes(64)

@@ -1533,7 +1533,9 @@ extern "C" int vg_gkr_create(vg_ctx *ctx, const vg_circuit *c, vg_gkr **out)
     if (cudaMalloc(&g->vu, sizeof(fe)) != cudaSuccess) return fail("v_u");
     if (cudaMalloc(&g->heavy_parts, (size_t)MAX_HEAVY * HEAVY_PARTS * 4 * sizeof(fe)) != cudaSuccess)
         return fail("heavy partials");
-    if (cudaMemset(g->round_counter, 0, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
+    // on the context's stream: the streams are non-blocking, so a memset on
+    // the legacy stream would not be ordered before the first round kernel
+    if (cudaMemsetAsync(g->round_counter, 0, sizeof(unsigned), ctx->stream) != cudaSuccess) return fail("round counter");
     int rc = gkr_bind(g, c);
     if (rc != VG_OK) {
         vg_gkr_destroy(g);
@@ -2213,7 +2215,8 @@ int vg_gkr_tables_create(vg_ctx *ctx, long max_n, int max_records, vg_gkr **out)
     if (cudaMalloc(&g->round_parts, 3 * 148 * 8 * sizeof(fe)) != cudaSuccess) return fail("round partials");
     if (cudaMalloc(&g->round_out, 16 * sizeof(fe)) != cudaSuccess) return fail("round sums");
     if (cudaMalloc(&g->round_counter, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
-    if (cudaMemset(g->round_counter, 0, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
+    // ordered on the context's (non-blocking) stream before the first round
+    if (cudaMemsetAsync(g->round_counter, 0, sizeof(unsigned), ctx->stream) != cudaSuccess) return fail("round counter");
     g->deferred = true;
     const int rc = vg_gkr_tables_reserve(g, max_n, max_records);
     if (rc != VG_OK) {
