@@ -230,6 +230,10 @@ def load_from_pinned(session, pinned, index_bytes=4):
     vb.check(vb.lib().vg_session_load(session.h, d, ns.ctypes.data, tys, us, vs, index_bytes), "vg_session_load")
 
 
+def local_device():
+    return int(os.environ.get("VIRGO_DEVICE", "0"))
+
+
 def ours(args, layers, rank, world):
     import virgo_b200 as vb
     L = vb.lib()
@@ -244,6 +248,18 @@ def ours(args, layers, rank, world):
     # warm-up: every session proves once per warm-up step
     for w in range(args.warmup):
         vb.prove_batch(sessions, [seed0 + w * args.batch + i for i in range(args.batch)])
+
+    # launch shapes: the autotuner times whole batches of the sessions under
+    # each candidate (before any timed region; proofs are bit-identical under
+    # every choice)
+    tune = None
+    if not args.no_autotune:
+        defaults = vb.tune_get(local_device())
+        chosen, trials = vb.autotune(sessions, seed=seed0 + 900, reps=2)
+        tune = {"objective": "wall time of %d proofs in flight (best of 2 after 1 warm-up per candidate)"
+                             % len(sessions),
+                "defaults": defaults, "chosen": chosen,
+                "trials": [[k, v, round(ms, 2), c] for k, v, ms, c in trials]}
 
     # ---- plain: one proof at a time on one stream (device time by CUDA events) ----
     barrier(world)
@@ -340,7 +356,7 @@ def ours(args, layers, rank, world):
     base.close()
     return {"t_plain": t_plain, "t_batch": t_batch, "t_e2e": t_e2e, "t_e2e_circuit": t_e2e_circuit,
             "clocks": clocks.summary(), "families": fam, "launches": n_launch,
-            "stages": {k: v / args.steps for k, v in stages.items()},
+            "stages": {k: v / args.steps for k, v in stages.items()}, "autotune": tune,
             "h2d": int(u0.nbytes) * args.batch, "h2d_circuit": h2d_circuit * args.batch, "d2h": d2h}
 
 
@@ -601,6 +617,7 @@ def main():
     ap.add_argument("--batch", type=int, default=8, help="proofs in flight at once (one stream each)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-served", action="store_true", help="skip the batched-random and served measurements")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -653,6 +670,7 @@ def main():
             "roofline": roofline(r["families"], hbm, kind),
             "stages_s": r["stages"],
             "kernel_families": fam,
+            "autotune": r["autotune"],
         }
         if not args.no_served and world == 1:
             line["commit_path"] = {"note": "config 2, best of 3 calls, wall clock incl. host<->device copies",

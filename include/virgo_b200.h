@@ -396,6 +396,52 @@ int vg_session_ctx(vg_session *s, vg_ctx **out);
 int vg_session_commit_ctx(vg_session *s, vg_ctx **out);
 void vg_free(void *p);
 
+/* ---- launch-shape tuning (no reference counterpart: the reference's loops
+ * have no launch shapes).  One set of parameters per device, process-wide,
+ * read by every launch on that device.  Every value gives bit-identical
+ * results; only speed changes.  Defaults are the shapes measured best on the
+ * 256x256 matmul proof. */
+enum {
+    VG_TUNE_GROUP_START = 0,   /* sumcheck tile: table length (power of two, 2^11 .. 2^22) at
+                                  which a phase's remaining rounds run as round groups (chunks of
+                                  2048 entries folded up to 10 rounds in shared memory, one CTA
+                                  per chunk) instead of one launch per round */
+    VG_TUNE_ROUND_THREADS = 1, /* threads per CTA of the one-round kernel (128, 256, 512) */
+    VG_TUNE_NTT_MAX_LOG = 2,   /* NTT radix: log2 of the largest sub-DFT one pass runs in shared
+                                  memory (6 .. 10); a 2^n transform takes ceil(n / this) passes */
+    VG_TUNE_NTT_TILE_LOG = 3,  /* NTT stage fusion width: log2 of the elements one CTA holds in a
+                                  pass (10 .. 13; sub-DFTs of several columns share a CTA) */
+    VG_TUNE_LEAF_THREADS = 4,  /* threads per CTA of the per-thread leaf-chain kernels (64, 128, 256) */
+    VG_TUNE_LEAF_WARP_MAX = 5, /* Merkle leaf hashing: launches of at most this many SHA3 leaf
+                                  chains hash each chain with a whole warp (25 lanes of the
+                                  Keccak state, one per thread) instead of one thread per chain;
+                                  0 = never (0 .. 2^24) */
+    VG_TUNE_COUNT = 6
+};
+int vg_tune_get(int device, int key, long *value);
+/* VG_ERR_ARG for a value outside the key's range. */
+int vg_tune_set(int device, int key, long value);
+int vg_tune_reset(int device);
+int vg_tune_range(int key, long *lo, long *hi, long *def);
+
+/* Autotuner: for each parameter in turn (the others fixed at their best so
+ * far) times every candidate value by proving with the given sessions
+ * (vg_session_prove_batch over all n at once: n = 1 tunes one proof's
+ * latency, n > 1 the throughput of n proofs in flight), `reps` timed batches
+ * after one warm-up batch per candidate, the best of them counting; keeps a
+ * candidate only if it beats the value in force by more than 1%, and leaves
+ * the winners set for the sessions' device.  trials (optional, up to
+ * max_trials) receives every timing.  Do not prove on the same device from
+ * other threads meanwhile. */
+typedef struct {
+    int key;
+    long value;
+    double ms;      /* best wall time of one batch */
+    int chosen;     /* 1 for the value the tuner kept */
+} vg_tune_trial;
+int vg_autotune(vg_session *const *ss, int n, unsigned seed, int reps, vg_tune_trial *trials, int max_trials,
+                int *n_trials);
+
 /* ---- the fft_gkr side prover (src/VPD/fft_circuit_GKR.cpp) ----
  * The reference verifier runs it as a process, `fft_gkr <L-6> <file>`
  * (vpd_verifier.cpp:89-99), and adds its prover time to Prove Time; main

@@ -42,6 +42,38 @@ def test_no_device_fails_loudly(built):
     assert b"CUDA" in built.vg_last_error() or b"device" in built.vg_last_error()
 
 
+def test_tuning_table_validates_and_resets(built):
+    """Launch-shape parameters are host state: defaults, range checks,
+    per-device values and reset need no GPU."""
+    vb.tune_reset(0)
+    vb.tune_reset(1)
+    d = vb.tune_get(0)
+    assert d == {"group_start": 1 << 17, "round_threads": 128, "ntt_max_log": 10, "ntt_tile_log": 12,
+                 "leaf_threads": 256, "leaf_warp_max": 0}
+    vb.tune_set(0, group_start=1 << 13, ntt_max_log=8, leaf_warp_max=4096)
+    assert vb.tune_get(0)["group_start"] == 1 << 13 and vb.tune_get(1) == d
+    for bad in ({"group_start": 3000}, {"group_start": 1 << 10}, {"round_threads": 1024}, {"ntt_max_log": 11},
+                {"ntt_tile_log": 14}, {"leaf_threads": 96}, {"leaf_warp_max": -1}):
+        with pytest.raises(vb.VirgoError):
+            vb.tune_set(0, **bad)
+    assert vb.tune_get(0)["ntt_max_log"] == 8   # a rejected value changes nothing
+    lo, hi, df = ctypes.c_long(), ctypes.c_long(), ctypes.c_long()
+    assert built.vg_tune_range(2, ctypes.byref(lo), ctypes.byref(hi), ctypes.byref(df)) == 0
+    assert (lo.value, hi.value, df.value) == (6, 10, 10)
+    assert built.vg_tune_range(6, None, None, None) == 2
+    assert built.vg_tune_set(64, 0, 2048) == 2 and built.vg_tune_get(-1, 0, ctypes.byref(lo)) == 2
+    vb.tune_reset(0)
+    assert vb.tune_get(0) == d
+
+
+def test_autotune_rejects_bad_arguments(built):
+    n = ctypes.c_int()
+    assert built.vg_autotune(None, 1, 1, 1, None, 0, ctypes.byref(n)) == 2
+    hs = (ctypes.c_void_p * 1)(None)
+    assert built.vg_autotune(hs, 1, 1, 1, None, 0, ctypes.byref(n)) == 2
+    assert built.vg_autotune(hs, 1, 1, 0, None, 0, ctypes.byref(n)) == 2
+
+
 def test_matmul_generator_shapes():
     L = circuits.matmul_addtree(4, 16, seed=0)
     assert [len(t) for t, _, _ in L] == [32, 64, 32, 16]

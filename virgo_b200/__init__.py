@@ -51,6 +51,15 @@ class vg_job_info(ctypes.Structure):
                 ("latency_s", ctypes.c_double), ("footprint", ctypes.c_size_t), ("stats", vg_proof_stats)]
 
 
+class vg_tune_trial(ctypes.Structure):
+    _fields_ = [("key", ctypes.c_int), ("value", ctypes.c_long), ("ms", ctypes.c_double), ("chosen", ctypes.c_int)]
+
+
+# launch-shape parameters (VG_TUNE_* in include/virgo_b200.h)
+TUNE_KEYS = {"group_start": 0, "round_threads": 1, "ntt_max_log": 2, "ntt_tile_log": 3, "leaf_threads": 4,
+             "leaf_warp_max": 5}
+
+
 def lib():
     """Loads the library (raises VirgoError when it has not been built)."""
     global _lib
@@ -146,6 +155,12 @@ def lib():
             "vg_session_load": (c_i, [c_p, c_i, c_p, c_p, c_p, c_p, c_i]),
             "vg_circuit_build": (c_i, [c_p, c_i, c_p, c_p, c_p, c_p, c_i, ctypes.POINTER(c_p), c_p]),
             "vg_free": (None, [c_p]),
+            "vg_tune_get": (c_i, [c_i, c_i, ctypes.POINTER(c_l)]),
+            "vg_tune_set": (c_i, [c_i, c_i, c_l]),
+            "vg_tune_reset": (c_i, [c_i]),
+            "vg_tune_range": (c_i, [c_i, ctypes.POINTER(c_l), ctypes.POINTER(c_l), ctypes.POINTER(c_l)]),
+            "vg_autotune": (c_i, [c_p, c_i, ctypes.c_uint, c_i, ctypes.POINTER(vg_tune_trial), c_i,
+                                  ctypes.POINTER(c_i)]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -333,6 +348,43 @@ def prove_batch(sessions, seeds, transcript: bool = True):
         lib().vg_free(bufs[i])
         out.append((st[i], data))
     return out
+
+
+def tune_get(device: int = 0) -> dict:
+    """The device's launch-shape parameters by name."""
+    out = {}
+    for name, k in TUNE_KEYS.items():
+        v = ctypes.c_long()
+        check(lib().vg_tune_get(device, k, ctypes.byref(v)), "vg_tune_get")
+        out[name] = v.value
+    return out
+
+
+def tune_set(device: int = 0, **values):
+    for name, v in values.items():
+        check(lib().vg_tune_set(device, TUNE_KEYS[name], int(v)), "vg_tune_set %s" % name)
+
+
+def tune_reset(device: int = 0):
+    check(lib().vg_tune_reset(device), "vg_tune_reset")
+
+
+def autotune(sessions, seed: int = 1, reps: int = 2):
+    """Runs vg_autotune over the sessions (all proving at once).  Returns the
+    chosen parameters by name and every trial as (name, value, ms, chosen)."""
+    n = len(sessions)
+    hs = (ctypes.c_void_p * n)(*[s.h.value for s in sessions])
+    cap = 64
+    tr = (vg_tune_trial * cap)()
+    nt = ctypes.c_int()
+    check(lib().vg_autotune(hs, n, seed, reps, tr, cap, ctypes.byref(nt)), "vg_autotune")
+    names = {k: name for name, k in TUNE_KEYS.items()}
+    trials = [(names[tr[i].key], tr[i].value, tr[i].ms, bool(tr[i].chosen)) for i in range(nt.value)]
+    dev = ctypes.c_int()
+    ctx = ctypes.c_void_p()
+    check(lib().vg_session_ctx(sessions[0].h, ctypes.byref(ctx)), "vg_session_ctx")
+    check(lib().vg_ctx_device(ctx, ctypes.byref(dev)), "vg_ctx_device")
+    return tune_get(dev.value), trials
 
 
 def _layer_arrays(layers, index_bytes):

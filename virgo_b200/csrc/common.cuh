@@ -185,3 +185,6 @@ int vg_reduce_partials(vg_ctx *ctx, const fe *parts, int nparts, int K, fe *out_
 // the total; tmp holds vg_scan_tmp_words(n) words.
 long vg_scan_tmp_words(long n);
 int vg_scan_u32(vg_ctx *c, uint32_t *d, long n, uint32_t *tmp);
+
+// The device's launch-shape parameter `key` (VG_TUNE_*; tune.cu).
+long vg_tune_value(int device, int key);

@@ -95,6 +95,11 @@ def main():
     L.append("// Lanes a[x + 5*y] are held as 32-bit halves aL<i>, aH<i>.")
     L.append("#define VG_KECCAK_RC_LO { " + ", ".join("0x%08xu" % (v & 0xFFFFFFFF) for v in rc) + " }")
     L.append("#define VG_KECCAK_RC_HI { " + ", ".join("0x%08xu" % (v >> 32) for v in rc) + " }")
+    # per-lane tables of the warp formulation (lane x + 5y holds A[x, y]):
+    # its rho rotation, and the lane pi takes its value from, since
+    # B[y, 2x + 3y] = A[x, y] puts A[(X + 3Y) % 5, X] at lane X + 5Y
+    L.append("#define VG_KECCAK_RHO { " + ", ".join(str(rot[i % 5][i // 5]) for i in range(25)) + " }")
+    L.append("#define VG_KECCAK_PI_SRC { " + ", ".join(str(((i % 5) + 3 * (i // 5)) % 5 + 5 * (i % 5)) for i in range(25)) + " }")
     L.append("")
     body = []
     for h in "LH":

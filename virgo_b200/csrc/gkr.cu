@@ -591,9 +591,9 @@ __global__ void __launch_bounds__(GKR_THREADS) k_heavy_finish(HeavyKeys H, const
 // contiguous chunk of the three tables can run several consecutive rounds on
 // it without any other CTA: a chunk of 2 RG_CHUNK entries folds into shared
 // memory (RG_CHUNK entries) and keeps folding there until two entries are
-// left, i.e. up to 11 rounds per launch.  The challenges of all those rounds
+// left, i.e. up to 10 rounds per launch.  The challenges of all those rounds
 // are known in advance (they come from the verifier's rand() stream), so one
-// launch replaces up to 11 round launches and each table is read from HBM
+// launch replaces up to 10 round launches and each table is read from HBM
 // once per group instead of once per round.  Per-round partial sums are
 // reduced by the last CTA to finish; every round's sums go to its record.
 constexpr int RG_LOG = 10, RG_CHUNK = 1 << RG_LOG, RG_THREADS = 256, RG_MAX = 12;
@@ -627,21 +627,26 @@ __device__ __forceinline__ void rg_sums(fe v0, fe v1, fe a0, fe a1, fe m0, fe m1
     acc[2] = acc[2] + p0 + a0;
 }
 
-// warp sums of acc into sm[step][warp][3]; warps without an active lane
-// (first thread >= active) only store zeros
-__device__ __forceinline__ void rg_warp_store(fe (&acc)[3], fe *sm, int step, long active)
+// warp sums of acc added into sm[step][warp][3] (a CTA's chunks accumulate
+// there); warps without an active lane (first thread >= active) add nothing
+__device__ __forceinline__ void rg_warp_add(fe (&acc)[3], fe *sm, int step, long active)
 {
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    if ((long)(threadIdx.x & ~31) < active) {
+    if ((long)(threadIdx.x & ~31) >= active) return;
 #pragma unroll
-        for (int k = 0; k < 3; ++k) acc[k] = warp_sum(acc[k]);
-    }
+    for (int k = 0; k < 3; ++k) acc[k] = warp_sum(acc[k]);
     if (lane == 0) {
 #pragma unroll
-        for (int k = 0; k < 3; ++k) sm[(step * (RG_THREADS / 32) + wid) * 3 + k] = acc[k];
+        for (int k = 0; k < 3; ++k) {
+            fe *o = &sm[(step * (RG_THREADS / 32) + wid) * 3 + k];
+            *o = *o + acc[k];
+        }
     }
 }
 
+// CTAs loop over the chunks (chunk q at q * cin of the input), so the grid
+// stays within what is resident at once and the last CTA's reduction reads
+// at most gridDim.x partials per round.
 __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict__ xV, const fe *__restrict__ xA,
                                                             const fe *__restrict__ xM, long n_in, RoundGroup G,
                                                             fe *__restrict__ yV, fe *__restrict__ yA, fe *__restrict__ yM,
@@ -652,70 +657,78 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
     fe *sV = smem, *sA = smem + RG_TABLE, *sM = smem + 2 * RG_TABLE;
     fe *wsum = smem + 3 * RG_TABLE;   // [RG_MAX][warps][3]
     __shared__ bool last;
+    constexpr int NW = RG_THREADS / 32;
     const int t = threadIdx.x;
-    // first step: from global into shared
+    for (int i = t; i < RG_MAX * NW * 3; i += RG_THREADS) wsum[i] = vg::fe_zero();
     const long chunk = 1L << G.chunk_log;
     const long cin = G.first_nofold ? min(n_in, chunk) : min(n_in, 2L * chunk);
-    const long base = (long)blockIdx.x * cin;
-    long m = G.first_nofold ? cin : cin / 2;   // entries in shared after the first step
-    {
-        fe acc[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
-        const fe r = G.r[0];
-        for (long k = t; k < m / 2; k += RG_THREADS) {
-            fe v0, v1, a0, a1, m0, m1;
-            if (G.first_nofold) {
-                const long b = base + 2 * k;
-                v0 = xV[b]; v1 = xV[b + 1];
-                a0 = xA[b]; a1 = xA[b + 1];
-                m0 = xM[b]; m1 = xM[b + 1];
-            } else {
-                const long b = base + 4 * k;
-                v0 = rg_fold(xV[b], xV[b + 1], r); v1 = rg_fold(xV[b + 2], xV[b + 3], r);
-                a0 = rg_fold(xA[b], xA[b + 1], r); a1 = rg_fold(xA[b + 2], xA[b + 3], r);
-                m0 = rg_fold(xM[b], xM[b + 1], r); m1 = rg_fold(xM[b + 2], xM[b + 3], r);
+    const long nchunks = n_in / cin;
+    const long m0 = G.first_nofold ? cin : cin / 2;   // entries in shared after the first step
+    long m = m0;
+    for (long q = blockIdx.x; q < nchunks; q += gridDim.x) {
+        const long base = q * cin;
+        m = m0;
+        __syncthreads();   // wsum zeroed; the previous chunk's tables written out
+        // first step: from global into shared
+        {
+            fe acc[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+            const fe r = G.r[0];
+            for (long k = t; k < m / 2; k += RG_THREADS) {
+                fe v0, v1, a0, a1, m0v, m1v;
+                if (G.first_nofold) {
+                    const long b = base + 2 * k;
+                    v0 = xV[b]; v1 = xV[b + 1];
+                    a0 = xA[b]; a1 = xA[b + 1];
+                    m0v = xM[b]; m1v = xM[b + 1];
+                } else {
+                    const long b = base + 4 * k;
+                    v0 = rg_fold(xV[b], xV[b + 1], r); v1 = rg_fold(xV[b + 2], xV[b + 3], r);
+                    a0 = rg_fold(xA[b], xA[b + 1], r); a1 = rg_fold(xA[b + 2], xA[b + 3], r);
+                    m0v = rg_fold(xM[b], xM[b + 1], r); m1v = rg_fold(xM[b + 2], xM[b + 3], r);
+                }
+                const int i0 = rg_ix(2 * k), i1 = rg_ix(2 * k + 1);
+                sV[i0] = v0; sV[i1] = v1;
+                sA[i0] = a0; sA[i1] = a1;
+                sM[i0] = m0v; sM[i1] = m1v;
+                rg_sums(v0, v1, a0, a1, m0v, m1v, acc);
             }
-            const int i0 = rg_ix(2 * k), i1 = rg_ix(2 * k + 1);
-            sV[i0] = v0; sV[i1] = v1;
-            sA[i0] = a0; sA[i1] = a1;
-            sM[i0] = m0; sM[i1] = m1;
-            rg_sums(v0, v1, a0, a1, m0, m1, acc);
+            rg_warp_add(acc, wsum, 0, m / 2);
         }
-        rg_warp_store(acc, wsum, 0, m / 2);
-    }
-    // further steps in shared memory: fold m -> m/2, sums over m/4 pairs
-    for (int st = 1; st < G.nsteps; ++st) {
-        const fe r = G.r[st];
-        fe acc[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
-        fe v0, v1, a0, a1, m0, m1;
-        const long npairs = m / 4;
+        // further steps in shared memory: fold m -> m/2, sums over m/4 pairs
+        for (int st = 1; st < G.nsteps; ++st) {
+            const fe r = G.r[st];
+            fe acc[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+            fe v0, v1, a0, a1, m0v, m1v;
+            const long npairs = m / 4;
+            __syncthreads();
+            const bool act = t < npairs;   // m / 4 <= RG_CHUNK / 4 = RG_THREADS: at most one pair per thread
+            if (act) {
+                const int b0 = rg_ix(4 * t), b1 = rg_ix(4 * t + 1), b2 = rg_ix(4 * t + 2), b3 = rg_ix(4 * t + 3);
+                v0 = rg_fold(sV[b0], sV[b1], r); v1 = rg_fold(sV[b2], sV[b3], r);
+                a0 = rg_fold(sA[b0], sA[b1], r); a1 = rg_fold(sA[b2], sA[b3], r);
+                m0v = rg_fold(sM[b0], sM[b1], r); m1v = rg_fold(sM[b2], sM[b3], r);
+                rg_sums(v0, v1, a0, a1, m0v, m1v, acc);
+            }
+            __syncthreads();
+            if (act) {
+                const int i0 = rg_ix(2 * t), i1 = rg_ix(2 * t + 1);
+                sV[i0] = v0; sV[i1] = v1;
+                sA[i0] = a0; sA[i1] = a1;
+                sM[i0] = m0v; sM[i1] = m1v;
+            }
+            m >>= 1;
+            rg_warp_add(acc, wsum, st, npairs);
+        }
         __syncthreads();
-        const bool act = t < npairs;   // m / 4 <= RG_CHUNK / 4 = RG_THREADS: at most one pair per thread
-        if (act) {
-            const int b0 = rg_ix(4 * t), b1 = rg_ix(4 * t + 1), b2 = rg_ix(4 * t + 2), b3 = rg_ix(4 * t + 3);
-            v0 = rg_fold(sV[b0], sV[b1], r); v1 = rg_fold(sV[b2], sV[b3], r);
-            a0 = rg_fold(sA[b0], sA[b1], r); a1 = rg_fold(sA[b2], sA[b3], r);
-            m0 = rg_fold(sM[b0], sM[b1], r); m1 = rg_fold(sM[b2], sM[b3], r);
-            rg_sums(v0, v1, a0, a1, m0, m1, acc);
+        // the chunk's remaining m entries (none when the group folded nothing)
+        for (long k = t; yV && k < m; k += RG_THREADS) {
+            yV[q * m + k] = sV[rg_ix(k)];
+            yA[q * m + k] = sA[rg_ix(k)];
+            yM[q * m + k] = sM[rg_ix(k)];
         }
-        __syncthreads();
-        if (act) {
-            const int i0 = rg_ix(2 * t), i1 = rg_ix(2 * t + 1);
-            sV[i0] = v0; sV[i1] = v1;
-            sA[i0] = a0; sA[i1] = a1;
-            sM[i0] = m0; sM[i1] = m1;
-        }
-        m >>= 1;
-        rg_warp_store(acc, wsum, st, npairs);
     }
     __syncthreads();
-    // the chunk's remaining m entries (none when the group folded nothing)
-    for (long k = t; yV && k < m; k += RG_THREADS) {
-        yV[(long)blockIdx.x * m + k] = sV[rg_ix(k)];
-        yA[(long)blockIdx.x * m + k] = sA[rg_ix(k)];
-        yM[(long)blockIdx.x * m + k] = sM[rg_ix(k)];
-    }
     // CTA partials per round
-    constexpr int NW = RG_THREADS / 32;
     if ((t & 31) < 3) {
         const int k = t & 31;
         for (int st = t >> 5; st < G.nsteps; st += NW) {
@@ -724,7 +737,7 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
             parts[((long)st * gridDim.x + blockIdx.x) * 3 + k] = x;
         }
     }
-    if (G.last6 && gridDim.x == 1 && m == 2 && t == 0) {
+    if (G.last6 && nchunks == 1 && m == 2 && t == 0) {
         fe *l6 = rec + 9 * (G.slot0 + G.nsteps - 1) + 3;
         l6[0] = sV[0]; l6[1] = sV[1]; l6[2] = sA[0]; l6[3] = sA[1]; l6[4] = sM[0]; l6[5] = sM[1];   // rg_ix(0, 1) = 0, 1
     }
@@ -734,19 +747,30 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
     __syncthreads();
     if (!last) return;
     __threadfence();
-    // warp st sums round st over all CTAs
+    // warp st sums round st over all CTAs, four partials in flight per lane
     const int wid = t >> 5, lane = t & 31;
     for (int st = wid; st < G.nsteps; st += NW) {
         fe tot[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
-        for (long b = lane; b < gridDim.x; b += 32) {
+        for (long b0 = lane; b0 < gridDim.x; b0 += 4 * 32) {
+            fe x[4][3];
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                const fe *p = &parts[((long)st * gridDim.x + b) * 3 + k];
-                fe x;
-                x.img = __ldcg(&p->img);
-                x.real = __ldcg(&p->real);
-                tot[k] = tot[k] + x;
+            for (int j = 0; j < 4; ++j) {
+                const long b = b0 + 32 * j;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    if (b < gridDim.x) {
+                        const fe *p = &parts[((long)st * gridDim.x + b) * 3 + k];
+                        x[j][k].img = __ldcg(&p->img);
+                        x[j][k].real = __ldcg(&p->real);
+                    } else {
+                        x[j][k] = vg::fe_zero();
+                    }
+                }
             }
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int k = 0; k < 3; ++k) tot[k] = tot[k] + x[j][k];
         }
 #pragma unroll
         for (int k = 0; k < 3; ++k) tot[k] = warp_sum(tot[k]);
@@ -823,8 +847,8 @@ __device__ __forceinline__ fe fold(fe x0, fe x1, fe r) { return x0 + r * (x1 - x
 
 // The block partials are reduced by the last block to finish (a counter in
 // device memory decides which one), so one launch returns the round sums.
-template <bool FOLD>
-__global__ void __launch_bounds__(GKR_THREADS) k_round(const fe *__restrict__ xV, const fe *__restrict__ xAV,
+template <bool FOLD, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_round(const fe *__restrict__ xV, const fe *__restrict__ xAV,
                                                        const fe *__restrict__ xAM, long npairs, fe r,
                                                        fe *__restrict__ yV, fe *__restrict__ yAV, fe *__restrict__ yAM,
                                                        fe *__restrict__ parts, unsigned *__restrict__ counter,
@@ -1923,17 +1947,12 @@ extern "C" int vg_gkr_phase1_init(vg_gkr *g, int layer, const vg_fe *r0, const v
     return finalize_tables(g, N);
 }
 
-// Table length at which a phase's remaining rounds become one single-CTA
-// group (at most one chunk); VIRGO_GROUP_START overrides it (a power of two).
-static long group_start()
-{
-    static const long v = [] {
-        const char *e = getenv("VIRGO_GROUP_START");
-        long x = e ? atol(e) : 2L * RG_CHUNK;
-        return (x >= 4 && !(x & (x - 1))) ? x : 2L * RG_CHUNK;
-    }();
-    return v;
-}
+// Table length at which a phase's remaining rounds become round groups: the
+// device's VG_TUNE_GROUP_START (at least 2 RG_CHUNK).  A group on a longer
+// table runs one CTA per chunk of 2 RG_CHUNK entries (RG_CHUNK for a group
+// whose first round does not fold), each folding its chunk in shared memory
+// for up to 10 rounds; groups follow one another until the phase ends.
+static long group_start(int device) { return vg_tune_value(device, VG_TUNE_GROUP_START); }
 
 // With VIRGO_TAIL_CHUNK = c (a power of two below RG_CHUNK), a group starting
 // on more than TAIL_SPLIT chunks' worth of entries uses chunks of c entries,
@@ -1976,8 +1995,8 @@ static int rg_smem_attribute(int dev)
     return VG_OK;
 }
 
-// Launches the pending deferred rounds as one group (a single CTA: the
-// group starts when the table fits one chunk).
+// Launches the pending deferred rounds as one group: one chunk per CTA when
+// the table fits the grid, CTAs looping over chunks beyond.
 static int flush_rounds(vg_gkr *g)
 {
     if (g->pend_r.empty()) return VG_OK;
@@ -1992,16 +2011,18 @@ static int flush_rounds(vg_gkr *g)
     for (int i = 0; i < G.nsteps; ++i) G.r[i] = g->pend_r[i];
     const long n_in = g->pend_n0;
     const long cin = G.first_nofold ? std::min(n_in, g->pend_chunk) : std::min(n_in, 2 * g->pend_chunk);
-    const long grid = n_in / cin;
+    const long nchunks = n_in / cin;
+    // CTAs loop over chunks: at most 3 resident per SM (60 KB of shared memory each)
+    const long grid = std::min(nchunks, 148L * 3L);
     const long m_final = (G.first_nofold ? cin : cin / 2) >> (G.nsteps - 1);
-    G.last6 = (grid == 1 && m_final == 2) ? 1 : 0;
+    G.last6 = (nchunks == 1 && m_final == 2) ? 1 : 0;
     const bool folds = !(G.first_nofold && G.nsteps == 1);
     fe *y[3] = {g->buf[g->next_buf][0], g->buf[g->next_buf][1], g->buf[g->next_buf][2]};
     const size_t smem = (3 * RG_TABLE + RG_MAX * (RG_THREADS / 32) * 3) * sizeof(fe);
     VG_TRY(rg_smem_attribute(c->device));
     {
         // every round of the group: the first reads 3 tables of n_in, writes nothing more than the chunk tails
-        ProfScope ps(c, KF_ROUND, 48.0 * (double)n_in + (folds ? 48.0 * (double)(grid * m_final) : 0.0));
+        ProfScope ps(c, KF_ROUND, 48.0 * (double)n_in + (folds ? 48.0 * (double)(nchunks * m_final) : 0.0));
         k_round_group<<<(unsigned)grid, RG_THREADS, smem, c->stream>>>(g->cur[0], g->cur[1], g->cur[2], n_in, G,
                                                                       folds ? y[0] : nullptr, folds ? y[1] : nullptr,
                                                                       folds ? y[2] : nullptr, g->rg_parts,
@@ -2130,11 +2151,14 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
     if (!fold && !g->round0_pending) return vg_fail(VG_ERR_STATE, "current_bit 0 only directly after an init");
     if (fold && g->round0_pending) return vg_fail(VG_ERR_STATE, "first round after an init must have current_bit 0");
     if (fold && g->n < 4) return vg_fail(VG_ERR_STATE, "no variables left to fold");
-    // deferred: once the table fits one CTA's chunk, the remaining rounds of
-    // the phase are queued and run as one single-CTA group; larger tables run
-    // one round per launch (their rounds are throughput bound, the group
-    // kernel's serial in-CTA steps are not)
-    const long lim = std::min(fold ? 2L * RG_CHUNK : (long)RG_CHUNK, group_start());
+    // deferred: once the table is at most the group start, the remaining
+    // rounds of the phase are queued and run as round groups (one CTA per
+    // chunk, the last group a single CTA); larger tables run one round per
+    // launch (their rounds are throughput bound, the group kernel's serial
+    // in-CTA steps are not).  A first round that does not fold reads its
+    // chunk unfolded, so it starts at half the length.
+    const long S = std::max(2L * RG_CHUNK, group_start(g->ctx->device));
+    const long lim = fold ? S : S / 2;
     if (g->deferred && (!g->pend_r.empty() || g->n <= lim)) {
         if (g->pend_r.empty()) {
             g->pend_n0 = g->n;
@@ -2153,7 +2177,11 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
     vg_ctx *c = g->ctx;
     const long n_out = fold ? g->n / 2 : g->n;   // table length the sums are taken over
     const long npairs = n_out / 2;
-    unsigned grid = std::min<unsigned>(grid_for(npairs, GKR_THREADS), 148u * 8u);
+    // threads per CTA from the device's tuning; the grid covers at most
+    // 148 x 2048 threads and at most 148 x 8 CTAs (the partials buffer),
+    // looping beyond
+    const int T = (int)vg_tune_value(c->device, VG_TUNE_ROUND_THREADS);
+    unsigned grid = std::min<unsigned>(grid_for(npairs, T), std::min(148u * 8u, 148u * 2048u / (unsigned)T));
     fe *y[3] = {g->buf[g->next_buf][0], g->buf[g->next_buf][1], g->buf[g->next_buf][2]};
     fe r = tofe(previous_random);
     fe *o3 = g->deferred ? g->rec + 9 * g->rec_n : g->round_out;
@@ -2161,12 +2189,18 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
     {
         // fold: read 3 tables x 4 entries, write 3 x 2 per pair; else read 3 x 2
         ProfScope ps(c, KF_ROUND, (fold ? 288.0 : 96.0) * (double)npairs);
-        if (fold)
-            k_round<true><<<grid, GKR_THREADS, 0, c->stream>>>(g->cur[0], g->cur[1], g->cur[2], npairs, r, y[0], y[1], y[2],
-                                                               g->round_parts, g->round_counter, o3, o6);
-        else
-            k_round<false><<<grid, GKR_THREADS, 0, c->stream>>>(g->cur[0], g->cur[1], g->cur[2], npairs, r, nullptr, nullptr,
-                                                                nullptr, g->round_parts, g->round_counter, o3, o6);
+        const fe *x0 = g->cur[0], *x1 = g->cur[1], *x2 = g->cur[2];
+        fe *pr = g->round_parts;
+        unsigned *cnt = g->round_counter;
+#define VG_ROUND_LAUNCH(TT)                                                                                          \
+    if (fold)                                                                                                         \
+        k_round<true, TT><<<grid, TT, 0, c->stream>>>(x0, x1, x2, npairs, r, y[0], y[1], y[2], pr, cnt, o3, o6);      \
+    else                                                                                                              \
+        k_round<false, TT><<<grid, TT, 0, c->stream>>>(x0, x1, x2, npairs, r, nullptr, nullptr, nullptr, pr, cnt, o3, o6)
+        if (T == 128) VG_ROUND_LAUNCH(128);
+        else if (T == 512) VG_ROUND_LAUNCH(512);
+        else VG_ROUND_LAUNCH(256);
+#undef VG_ROUND_LAUNCH
     }
     VG_LAUNCHED(c);
     if (fold) {

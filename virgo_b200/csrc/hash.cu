@@ -83,9 +83,9 @@ __global__ void k_fill_pad(uint64_t *__restrict__ tree, long from, long to)
 // Leaf k of a codeword set with per-slice length n: h = 0; for s:
 // h = H(c[s][k] || c[s][k + n/2] || h).  One thread per leaf; a warp reads
 // 32 consecutive k of one slice, i.e. 512 contiguous bytes per load.
-template <int KIND>
-__global__ void __launch_bounds__(HASH_THREADS) k_leaf_chain(const fe *__restrict__ c, int n_slices, long n,
-                                                            uint64_t *__restrict__ leaves)
+template <int KIND, int T>
+__global__ void __launch_bounds__(T) k_leaf_chain(const fe *__restrict__ c, int n_slices, long n,
+                                                 uint64_t *__restrict__ leaves)
 {
     const long half = n >> 1;
     long k = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -103,8 +103,8 @@ __global__ void __launch_bounds__(HASH_THREADS) k_leaf_chain(const fe *__restric
 // Leaf chains of several codeword sets in one launch: thread t serves leaf
 // t - begin of the job whose range holds t.  The next slice's pair is loaded
 // before the current hash so the loads overlap the permutation.
-template <int KIND>
-__global__ void __launch_bounds__(HASH_THREADS) k_leaf_chains(ChainJobs jobs)
+template <int KIND, int T>
+__global__ void __launch_bounds__(T) k_leaf_chains(ChainJobs jobs)
 {
     const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
     if (t >= jobs.total) return;
@@ -126,6 +126,76 @@ __global__ void __launch_bounds__(HASH_THREADS) k_leaf_chains(ChainJobs jobs)
         b = nb;
     }
     store_digest(jobs.j[q].leaves + 4 * k, h);
+}
+
+// ---- leaf chains, one warp per chain (SHA3-256 only) ----
+// Lanes 0..3 load the chain's next pair (a.img, a.real, b.img, b.real) as the
+// first four message words; lanes 4..7 take the running digest, which the
+// previous permutation left in lanes 0..3; lanes 8 and 16 hold the padding.
+__device__ __forceinline__ uint64_t chain_word(const fe *__restrict__ c, long off, long half, int l)
+{
+    const uint64_t *p = (const uint64_t *)(c + off + (l < 2 ? 0 : half));
+    return p[l & 1];
+}
+
+__device__ __forceinline__ void warp_chain(const fe *__restrict__ c, int n_slices, long n, long k,
+                                           uint64_t *__restrict__ out)
+{
+    const unsigned FULL = 0xffffffffu;
+    const int l = threadIdx.x & 31;
+    const long half = n >> 1;
+    const vg::KeccakLanes K = vg::keccak_lanes(l);
+    uint32_t lo = 0, hi = 0;
+    uint64_t word = l < 4 ? chain_word(c, k, half, l) : 0;
+    for (int s = 0; s < n_slices; ++s) {
+        const uint64_t next = (l < 4 && s + 1 < n_slices) ? chain_word(c, (long)(s + 1) * n + k, half, l) : 0;
+        const uint32_t dl = __shfl_sync(FULL, lo, (l - 4) & 31), dh = __shfl_sync(FULL, hi, (l - 4) & 31);
+        if (l < 4) {
+            lo = (uint32_t)word;
+            hi = (uint32_t)(word >> 32);
+        } else if (l < 8) {
+            lo = dl;
+            hi = dh;
+        } else {
+            lo = l == 8 ? 0x06u : 0u;
+            hi = l == 16 ? 0x80000000u : 0u;
+        }
+        vg::keccak_f_warp(lo, hi, K);
+        word = next;
+    }
+    if (l < 4) out[l] = lo | ((uint64_t)hi << 32);
+}
+
+constexpr int WARP_CHAIN_THREADS = 128;
+
+__global__ void __launch_bounds__(WARP_CHAIN_THREADS) k_leaf_chains_warp(ChainJobs jobs)
+{
+    const long w = ((long)blockIdx.x * WARP_CHAIN_THREADS + threadIdx.x) >> 5;
+    if (w >= jobs.total) return;   // whole warps
+    int q = 0;
+    while (q + 1 < jobs.count && w >= jobs.j[q + 1].begin) ++q;
+    const long k = w - jobs.j[q].begin;
+    warp_chain(jobs.j[q].cw, 65, jobs.j[q].n, k, jobs.j[q].leaves + 4 * k);
+}
+
+__global__ void __launch_bounds__(WARP_CHAIN_THREADS) k_leaf_chain_warp(const fe *__restrict__ c, int n_slices, long n,
+                                                                       uint64_t *__restrict__ leaves)
+{
+    const long k = ((long)blockIdx.x * WARP_CHAIN_THREADS + threadIdx.x) >> 5;
+    if (k >= (n >> 1)) return;   // whole warps
+    warp_chain(c, n_slices, n, k, leaves + 4 * k);
+}
+
+static unsigned warp_chain_grid(long chains)
+{
+    return (unsigned)((chains * 32 + WARP_CHAIN_THREADS - 1) / WARP_CHAIN_THREADS);
+}
+
+// leaf hashing form for a launch of `chains` chains: one warp per chain when
+// SHA3 and at most VG_TUNE_LEAF_WARP_MAX chains
+static bool use_warp_chains(vg_ctx *c, long chains)
+{
+    return c->hash_kind == VG_HASH_SHA3_256 && chains <= vg_tune_value(c->device, VG_TUNE_LEAF_WARP_MAX);
 }
 
 // One Merkle level (parents of height `height`) of every tree that still has
@@ -177,10 +247,20 @@ int vg_leaf_chains(vg_ctx *c, const ChainJobs &jobs)
     double bytes = 0;
     for (int q = 0; q < jobs.count; ++q) bytes += 16.0 * 65.0 * (double)jobs.j[q].n + 32.0 * (double)(jobs.j[q].n >> 1);
     ProfScope ps(c, KF_LEAF_CHAIN, bytes);
-    if (c->hash_kind == VG_HASH_SHA256)
-        k_leaf_chains<VG_HASH_SHA256><<<grid_for(jobs.total, HASH_THREADS), HASH_THREADS, 0, c->stream>>>(jobs);
-    else
-        k_leaf_chains<VG_HASH_SHA3_256><<<grid_for(jobs.total, HASH_THREADS), HASH_THREADS, 0, c->stream>>>(jobs);
+    if (use_warp_chains(c, jobs.total)) {
+        k_leaf_chains_warp<<<warp_chain_grid(jobs.total), WARP_CHAIN_THREADS, 0, c->stream>>>(jobs);
+    } else {
+        const int T = (int)vg_tune_value(c->device, VG_TUNE_LEAF_THREADS);
+#define VG_CHAINS_LAUNCH(TT)                                                                                 \
+    if (c->hash_kind == VG_HASH_SHA256)                                                                       \
+        k_leaf_chains<VG_HASH_SHA256, TT><<<grid_for(jobs.total, TT), TT, 0, c->stream>>>(jobs);             \
+    else                                                                                                      \
+        k_leaf_chains<VG_HASH_SHA3_256, TT><<<grid_for(jobs.total, TT), TT, 0, c->stream>>>(jobs)
+        if (T == 64) VG_CHAINS_LAUNCH(64);
+        else if (T == 256) VG_CHAINS_LAUNCH(256);
+        else VG_CHAINS_LAUNCH(128);
+#undef VG_CHAINS_LAUNCH
+    }
     VG_LAUNCHED(c);
     return VG_OK;
 }
@@ -242,10 +322,20 @@ int vg_leaf_chain_dev(vg_ctx *c, const fe *cw, int n_slices, long n, uint64_t *l
     long half = n >> 1;
     if (half < 1) return VG_OK;
     ProfScope ps(c, KF_LEAF_CHAIN, 16.0 * (double)n_slices * (double)n + 32.0 * (double)half);
-    if (c->hash_kind == VG_HASH_SHA256)
-        k_leaf_chain<VG_HASH_SHA256><<<grid_for(half, HASH_THREADS), HASH_THREADS, 0, c->stream>>>(cw, n_slices, n, leaves);
-    else
-        k_leaf_chain<VG_HASH_SHA3_256><<<grid_for(half, HASH_THREADS), HASH_THREADS, 0, c->stream>>>(cw, n_slices, n, leaves);
+    if (use_warp_chains(c, half)) {
+        k_leaf_chain_warp<<<warp_chain_grid(half), WARP_CHAIN_THREADS, 0, c->stream>>>(cw, n_slices, n, leaves);
+    } else {
+        const int T = (int)vg_tune_value(c->device, VG_TUNE_LEAF_THREADS);
+#define VG_CHAIN_LAUNCH(TT)                                                                                           \
+    if (c->hash_kind == VG_HASH_SHA256)                                                                                \
+        k_leaf_chain<VG_HASH_SHA256, TT><<<grid_for(half, TT), TT, 0, c->stream>>>(cw, n_slices, n, leaves);          \
+    else                                                                                                               \
+        k_leaf_chain<VG_HASH_SHA3_256, TT><<<grid_for(half, TT), TT, 0, c->stream>>>(cw, n_slices, n, leaves)
+        if (T == 64) VG_CHAIN_LAUNCH(64);
+        else if (T == 256) VG_CHAIN_LAUNCH(256);
+        else VG_CHAIN_LAUNCH(128);
+#undef VG_CHAIN_LAUNCH
+    }
     VG_LAUNCHED(c);
     return VG_OK;
 }

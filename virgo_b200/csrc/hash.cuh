@@ -106,6 +106,78 @@ __device__ __forceinline__ void sha256_64(const uint64_t w[8], uint64_t d[4])
     for (int i = 0; i < 4; ++i) d[i] = (uint64_t)bswap32(H[2 * i]) | ((uint64_t)bswap32(H[2 * i + 1]) << 32);
 }
 
+// ---- Keccak-f[1600] on a whole warp ----
+// Lane l = x + 5y (l < 25) holds state word A[x, y] as two 32-bit halves;
+// lanes 25..31 take part in the shuffles and hold nothing used.  A round is
+// ten 64-bit shuffles: five for the column parity C[x], two for C[x-1] and
+// C[x+1], one for pi (each lane rotates its own word by its rho offset
+// first), two for the chi neighbours.  About a fifth of the per-thread
+// permutation's instructions per lane, at 32 lanes per permutation: it pays
+// only when too few chains exist to fill the GPU one thread each.
+struct KeccakLanes {
+    int col[5];      // lanes of column x: x + 5 y', y' < 5
+    int xm, xp, xp2; // lanes (x - 1, y), (x + 1, y), (x + 2, y)
+    int pi;          // lane whose rotated word pi moves here
+    int rn;          // rho rotation modulo 32
+    bool rswap;      // rho rotation >= 32: halves swap first
+    bool iota;       // lane 0
+};
+
+__device__ __forceinline__ KeccakLanes keccak_lanes(int l)
+{
+    const uint8_t RHO[25] = VG_KECCAK_RHO, PI[25] = VG_KECCAK_PI_SRC;
+    KeccakLanes K;
+    const bool in = l < 25;
+    const int x = l % 5, y = l / 5;
+#pragma unroll
+    for (int j = 0; j < 5; ++j) K.col[j] = in ? x + 5 * j : l;
+    K.xm = in ? (x + 4) % 5 + 5 * y : l;
+    K.xp = in ? (x + 1) % 5 + 5 * y : l;
+    K.xp2 = in ? (x + 2) % 5 + 5 * y : l;
+    K.pi = in ? PI[l] : l;
+    const int rho = in ? RHO[l] : 0;
+    K.rn = rho & 31;
+    K.rswap = rho >= 32;
+    K.iota = l == 0;
+    return K;
+}
+
+__device__ __forceinline__ void keccak_f_warp(uint32_t &lo, uint32_t &hi, const KeccakLanes &K)
+{
+    const uint32_t RCL[24] = VG_KECCAK_RC_LO, RCH[24] = VG_KECCAK_RC_HI;
+    const unsigned FULL = 0xffffffffu;
+#pragma unroll
+    for (int r = 0; r < 24; ++r) {
+        // theta
+        uint32_t s0l = __shfl_sync(FULL, lo, K.col[0]), s0h = __shfl_sync(FULL, hi, K.col[0]);
+        uint32_t s1l = __shfl_sync(FULL, lo, K.col[1]), s1h = __shfl_sync(FULL, hi, K.col[1]);
+        uint32_t s2l = __shfl_sync(FULL, lo, K.col[2]), s2h = __shfl_sync(FULL, hi, K.col[2]);
+        uint32_t s3l = __shfl_sync(FULL, lo, K.col[3]), s3h = __shfl_sync(FULL, hi, K.col[3]);
+        uint32_t s4l = __shfl_sync(FULL, lo, K.col[4]), s4h = __shfl_sync(FULL, hi, K.col[4]);
+        const uint32_t cl = vg_xor3(vg_xor3(s0l, s1l, s2l), s3l, s4l);
+        const uint32_t ch = vg_xor3(vg_xor3(s0h, s1h, s2h), s3h, s4h);
+        const uint32_t ml = __shfl_sync(FULL, cl, K.xm), mh = __shfl_sync(FULL, ch, K.xm);
+        const uint32_t pl = __shfl_sync(FULL, cl, K.xp), ph = __shfl_sync(FULL, ch, K.xp);
+        // D = C[x-1] ^ rotl(C[x+1], 1)
+        lo = vg_xor3(lo, ml, __funnelshift_l(ph, pl, 1));
+        hi = vg_xor3(hi, mh, __funnelshift_l(pl, ph, 1));
+        // rho (own word), then pi
+        uint32_t a = K.rswap ? hi : lo, b = K.rswap ? lo : hi;
+        const uint32_t rl = __funnelshift_l(b, a, K.rn), rh = __funnelshift_l(a, b, K.rn);
+        const uint32_t bl = __shfl_sync(FULL, rl, K.pi), bh = __shfl_sync(FULL, rh, K.pi);
+        // chi
+        const uint32_t b1l = __shfl_sync(FULL, bl, K.xp), b1h = __shfl_sync(FULL, bh, K.xp);
+        const uint32_t b2l = __shfl_sync(FULL, bl, K.xp2), b2h = __shfl_sync(FULL, bh, K.xp2);
+        lo = vg_chi(bl, b1l, b2l);
+        hi = vg_chi(bh, b1h, b2h);
+        // iota
+        if (K.iota) {
+            lo ^= RCL[r];
+            hi ^= RCH[r];
+        }
+    }
+}
+
 template <int KIND>
 __device__ __forceinline__ void hash64(const uint64_t w[8], uint64_t d[4])
 {

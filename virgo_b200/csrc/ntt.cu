@@ -22,7 +22,7 @@
 namespace {
 
 constexpr int NTT_THREADS = 256;
-constexpr int MAX_LM = 10;
+constexpr int MAX_LM = 10, MAX_TILE_LOG = 13;
 
 struct PassArgs {
     const fe *in;
@@ -192,21 +192,25 @@ __global__ void k_tw_build(fe w, fe w4096, fe *lo, fe *hi, int nhi)
     if (i < nhi) hi[i] = vg::fe_pow(w4096, (uint64_t)i);
 }
 
-void plan_factors(int logn, std::vector<int> &f)
+// n = 2^logn as ceil(logn / max_lm) factors of nearly equal size (the
+// radix: VG_TUNE_NTT_MAX_LOG, at most MAX_LM)
+void plan_factors(int logn, int max_lm, std::vector<int> &f)
 {
     f.clear();
-    if (logn <= MAX_LM) {
+    if (logn <= max_lm) {
         f.push_back(logn);
         return;
     }
-    int P = (logn + MAX_LM - 1) / MAX_LM;
+    int P = (logn + max_lm - 1) / max_lm;
     int base = logn / P, extra = logn % P;
     for (int q = 0; q < P; ++q) f.push_back(base + (q < extra ? 1 : 0));
 }
 
-int pick_logG(int lm, long avail_log)
+// columns (or whole items) per CTA: m * G ~ 2^tile_log elements
+// (VG_TUNE_NTT_TILE_LOG, at most MAX_TILE_LOG)
+int pick_logG(int lm, long avail_log, int tile_log)
 {
-    int lg = 12 - lm;               // m * G ~ 4096 elements (64 KB)
+    int lg = tile_log - lm;
     if (lg < 0) lg = 0;
     if (lg > avail_log) lg = (int)avail_log;
     return lg;
@@ -243,11 +247,12 @@ int vg_twiddles(vg_ctx *c, fe root, int logn, const fe **lo, const fe **hi)
     return VG_OK;
 }
 
-// Largest dynamic shared memory of a pass: m * G <= 4096 items (pick_logG)
-// plus m / 2 <= 512 twiddles.  The kernel attribute is process-wide per
-// device, so it is raised once to this bound: setting it per launch to the
-// launch's own size races with other threads' launches of other sizes.
-constexpr size_t NTT_MAX_SMEM = (4096 + 512) * sizeof(fe);
+// Largest dynamic shared memory of a pass: m * G <= 2^MAX_TILE_LOG items
+// (pick_logG) plus m / 2 <= 512 twiddles.  The kernel attribute is
+// process-wide per device, so it is raised once to this bound: setting it per
+// launch to the launch's own size races with other threads' launches of other
+// sizes.
+constexpr size_t NTT_MAX_SMEM = ((1 << MAX_TILE_LOG) + (1 << (MAX_LM - 1))) * sizeof(fe);
 
 static int ntt_smem_attribute(int dev)
 {
@@ -294,7 +299,9 @@ extern "C" int vg_ntt(vg_ctx *c, const vg_fe *in_, long in_len, long in_bstride,
     fe inv_n = vg::fe_inv(vg::fe_make((uint64_t)n % vg::P, 0));
 
     std::vector<int> f;
-    plan_factors(logn, f);
+    const int max_lm = std::min(MAX_LM, (int)vg_tune_value(c->device, VG_TUNE_NTT_MAX_LOG));
+    const int tile_log = std::min(MAX_TILE_LOG, (int)vg_tune_value(c->device, VG_TUNE_NTT_TILE_LOG));
+    plan_factors(logn, max_lm, f);
     const int P = (int)f.size();
 
     if (P == 1) {
@@ -302,7 +309,7 @@ extern "C" int vg_ntt(vg_ctx *c, const vg_fe *in_, long in_len, long in_bstride,
         a.in = in; a.out = out; a.in_len = in_len; a.in_bstride = in_bstride; a.out_bstride = out_bstride;
         a.logn = logn; a.lm = logn; a.kind = 2; a.tw_lo = lo; a.tw_hi = hi; a.scale = scale_inv_n; a.inv_n = inv_n;
         // G whole items per CTA, G must divide batch
-        int lg = pick_logG(logn, 30);
+        int lg = pick_logG(logn, 30, std::max(tile_log, logn));
         while (lg > 0 && (batch % (1 << lg)) != 0) --lg;
         a.logG = lg;
         VG_TRY(launch_pass(c, a, batch >> lg, 1));
@@ -331,7 +338,7 @@ extern "C" int vg_ntt(vg_ctx *c, const vg_fe *in_, long in_len, long in_bstride,
         a.logn = logn; a.lm = f[q]; a.kind = 0; a.logA = logA;
         a.tw_lo = lo; a.tw_hi = hi; a.scale = 0;
         long logC = logA - f[q];
-        a.logG = pick_logG(f[q], logC);
+        a.logG = pick_logG(f[q], logC, tile_log);
         long nblocks = (n >> logA) * ((1L << logC) >> a.logG);
         VG_TRY(launch_pass(c, a, nblocks, batch));
         logA -= f[q];
@@ -343,7 +350,7 @@ extern "C" int vg_ntt(vg_ctx *c, const vg_fe *in_, long in_len, long in_bstride,
         a.nfac = P - 1;
         for (int q = 0; q < P - 1; ++q) a.fac[q] = f[q];
         a.tw_lo = lo; a.tw_hi = hi; a.scale = scale_inv_n; a.inv_n = inv_n;
-        a.logG = pick_logG(f[P - 1], f[0]);
+        a.logG = pick_logG(f[P - 1], f[0], tile_log);
         long T_all = n >> f[P - 1];
         long nblocks = T_all >> a.logG;
         VG_TRY(launch_pass(c, a, nblocks, batch));
