@@ -255,8 +255,8 @@ def ours(args, layers, rank, world):
     tune = None
     if not args.no_autotune:
         defaults = vb.tune_get(local_device())
-        chosen, trials = vb.autotune(sessions, seed=seed0 + 900, reps=2)
-        tune = {"objective": "wall time of %d proofs in flight (best of 2 after 1 warm-up per candidate)"
+        chosen, trials = vb.autotune(sessions, seed=seed0 + 900, reps=3)
+        tune = {"objective": "wall time of %d proofs in flight (best of 3 after 1 warm-up per candidate)"
                              % len(sessions),
                 "defaults": defaults, "chosen": chosen,
                 "trials": [[k, v, round(ms, 2), c] for k, v, ms, c in trials]}

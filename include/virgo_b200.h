@@ -416,7 +416,13 @@ enum {
                                   chains hash each chain with a whole warp (25 lanes of the
                                   Keccak state, one per thread) instead of one thread per chain;
                                   0 = never (0 .. 2^24) */
-    VG_TUNE_COUNT = 6
+    VG_TUNE_ROUND_FUSE = 6,    /* sumcheck rounds per launch above the group start (1, 2): with 2,
+                                  consecutive rounds pair into one pass that reads the tables
+                                  once and writes a quarter of them */
+    VG_TUNE_LEAF_ROT = 7,      /* SHA3 leaf chains (per-thread form): 0 = every 64-bit rotation as
+                                  two funnel shifts (ALU pipe); 1 = every other rho rotation, 2 =
+                                  every rho rotation as multiplies by 2^n (integer-multiply pipe) */
+    VG_TUNE_COUNT = 8
 };
 int vg_tune_get(int device, int key, long *value);
 /* VG_ERR_ARG for a value outside the key's range. */
@@ -429,7 +435,7 @@ int vg_tune_range(int key, long *lo, long *hi, long *def);
  * (vg_session_prove_batch over all n at once: n = 1 tunes one proof's
  * latency, n > 1 the throughput of n proofs in flight), `reps` timed batches
  * after one warm-up batch per candidate, the best of them counting; keeps a
- * candidate only if it beats the value in force by more than 1%, and leaves
+ * candidate only if it beats the value in force by more than 2%, and leaves
  * the winners set for the sessions' device.  trials (optional, up to
  * max_trials) receives every timing.  Do not prove on the same device from
  * other threads meanwhile. */

@@ -82,3 +82,26 @@ def test_fft_gkr_matches_reference_binary(prover, tmp_path):
     st, msgs, _ = prover.prove(lg)
     assert (msgs == ref).all()
     assert st.proof_size == int(open(out).read().split()[1])
+
+
+def test_fft_gkr_graph_replays_match_golden(prover):
+    """A run repeating the previous one's size and seed is captured as a CUDA
+    graph and later ones replay it: every run (plain, capture, replays, and
+    after switching sizes and seeds in between) gives the recorded messages
+    and passes the checks, with the same kernel count."""
+    gold = {(c["lg"], c["seed"]): c for c in json.load(open(GOLD))["fft_gkr"]}
+    a, b = gold[(8, next(s for l, s in gold if l == 8))], gold[(10, next(s for l, s in gold if l == 10))]
+    launches = {}
+    for case in (a, a, a, a, b, b, b, a, a, a, b):
+        st, msgs, vals = prover.prove(case["lg"], case["seed"])
+        assert st.pass_ == 1 and _same(msgs, case["msgs"]) and vals.tobytes().hex() == case["vals"], case["lg"]
+        launches.setdefault(case["lg"], set()).add(st.launches)
+        assert st.gpu_s > 0
+    assert all(len(v) == 1 for v in launches.values()), launches
+    # another seed at the same size: a new key, never the other key's graph
+    for _ in range(3):
+        st, msgs, vals = prover.prove(a["lg"], 777)
+        ok, m, v, _ = O.fft_gkr(a["lg"], 777)
+        assert ok and st.pass_ == 1 and (msgs == m).all() and (vals == v).all()
+    st, msgs, _ = prover.prove(a["lg"], a["seed"])
+    assert _same(msgs, a["msgs"])

@@ -43,7 +43,7 @@ def golden_sessions():
     ("group_start", 1 << 11), ("group_start", 1 << 13), ("group_start", 1 << 15), ("group_start", 1 << 19),
     ("group_start", 1 << 22), ("round_threads", 256), ("round_threads", 512), ("ntt_max_log", 6),
     ("ntt_max_log", 8), ("ntt_max_log", 9), ("ntt_tile_log", 10), ("ntt_tile_log", 11), ("ntt_tile_log", 13),
-    ("leaf_threads", 64), ("leaf_threads", 128), ("leaf_warp_max", 1 << 24),
+    ("leaf_threads", 64), ("leaf_threads", 128), ("leaf_warp_max", 1 << 24), ("leaf_rot", 1), ("leaf_rot", 2),
 ])
 def test_golden_transcripts_under_every_tuning(golden_sessions, knob, value):
     vb.tune_set(0, **{knob: value})
@@ -51,6 +51,16 @@ def test_golden_transcripts_under_every_tuning(golden_sessions, knob, value):
     for s, c in golden_sessions:
         _, blob = s.prove(c["seed"])
         assert transcript.digest(transcript.parse(blob)) == c["digest"], (c["name"], knob, value)
+
+
+@pytest.mark.parametrize("group_start", [1 << 11, 1 << 13, 1 << 17])
+def test_golden_transcripts_with_paired_rounds(golden_sessions, group_start):
+    """Rounds above the group start paired into two-round passes (the group
+    start lowered so that the golden circuits have such rounds)."""
+    vb.tune_set(0, group_start=group_start, round_fuse=2)
+    for s, c in golden_sessions:
+        _, blob = s.prove(c["seed"])
+        assert transcript.digest(transcript.parse(blob)) == c["digest"], (c["name"], group_start)
 
 
 def test_round_groups_loop_over_chunks_on_large_tables():
@@ -67,6 +77,9 @@ def test_round_groups_loop_over_chunks_on_large_tables():
         assert s.prove(5)[1] == base
         vb.tune_set(0, group_start=1 << 11, round_threads=256)
         assert s.prove(5)[1] == base
+        for gs, t in ((1 << 11, 128), (1 << 13, 512), (1 << 17, 256)):
+            vb.tune_set(0, group_start=gs, round_threads=t, round_fuse=2)
+            assert s.prove(5)[1] == base, (gs, t)
     finally:
         s.close()
 
@@ -106,6 +119,22 @@ def test_leaf_chain_forms(ctx, mode, n_slices, n):
     assert (got == O.leaf_chain(0, cw, n_slices, n)).all()
 
 
+@pytest.mark.parametrize("rot,threads", [(1, 256), (2, 64), (2, 128)])
+def test_multiply_pipe_rotations_in_batched_chains(rot, threads):
+    """The SHA3 leaf chains with rho's rotations as multiplies: a proof's
+    batched chains (every codeword set of the proof in one launch) give the
+    golden transcript."""
+    gold = {c["name"]: c for c in json.load(open(GOLD))}
+    c = gold["random_5layer"]
+    vb.tune_set(0, leaf_rot=rot, leaf_threads=threads)
+    s = vb.Session(getattr(circuits, c["generator"])(**c["params"]))
+    try:
+        _, blob = s.prove(c["seed"])
+    finally:
+        s.close()
+    assert transcript.digest(transcript.parse(blob)) == c["digest"]
+
+
 def test_warp_leaf_chains_leave_sha256_per_thread(ctx):
     """The warp form is SHA3 only: with SHA-256 selected the same setting
     hashes per thread and still matches."""
@@ -127,7 +156,7 @@ def test_autotune_keeps_proofs_and_picks_candidates(golden_sessions):
     forks = [s0.fork() for _ in range(2)]
     try:
         chosen, trials = vb.autotune([s0] + forks, seed=3, reps=1)
-        assert len(trials) == 20
+        assert len(trials) == 25
         for name, v in chosen.items():
             assert any(t[0] == name and t[1] == v for t in trials) or v == vb.tune_get(0)[name]
             assert sum(1 for t in trials if t[0] == name and t[3]) == 1, name

@@ -349,6 +349,49 @@ struct vg_fft_gkr {
     long long launched = 0;
     const vg_fe *recs = nullptr;
     cudaEvent_t ev[2] = {nullptr, nullptr};   // around the run's device steps
+    // The device steps as a CUDA graph.  A run with the size, seed and
+    // buffers of the previous one enqueues exactly the same steps (every
+    // challenge comes from the seed), so the second such run is captured
+    // and later ones replay the graph: every kernel still runs, from one
+    // launch instead of one per kernel.
+    cudaGraphExec_t gexec = nullptr;
+    int g_lg = 0;
+    unsigned g_seed = 0;
+    const void *g_key[3] = {nullptr, nullptr, nullptr};   // dev, host, parts_host at capture
+    long long g_launched = 0;   // kernels in the graph
+    bool g_seen = false;        // the last plain run had the current key
+    bool g_off = false;         // a capture failed: plain launches from then on
+};
+
+// VIRGO_GRAPHS=0 turns the side proof's graph off (plain launches)
+static bool fg_graphs_enabled()
+{
+    static const bool on = [] {
+        const char *e = getenv("VIRGO_GRAPHS");
+        return !(e && e[0] == '0');
+    }();
+    return on;
+}
+
+static void fg_drop_graph(vg_fft_gkr *f)
+{
+    if (f->gexec) cudaGraphExecDestroy(f->gexec);
+    f->gexec = nullptr;
+    f->g_seen = false;
+}
+
+// Ends a stream capture left open by an early error return.
+struct CaptureGuard {
+    cudaStream_t s = nullptr;
+    bool active = false;
+    ~CaptureGuard()
+    {
+        if (!active) return;
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(s, &g);
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+    }
 };
 
 extern "C" int vg_fft_gkr_rounds(int lg) { return (lg + 6) + lg + 2 * lg * lg; }
@@ -388,6 +431,7 @@ int vg_fft_gkr_reserve(vg_fft_gkr *f, int max_lg)
         return vg_fail(VG_ERR_ARG, "vg_fft_gkr_reserve: max_lg %d outside 1..%d", max_lg, FG_MAX_LG);
     if (max_lg <= f->max_lg) return VG_OK;
     if (f->pending) return vg_fail(VG_ERR_STATE, "vg_fft_gkr_reserve: a run is in flight");
+    fg_drop_graph(f);   // the tables move
     VG_TRY(vg_gkr_tables_reserve(f->tables, 64L << max_lg, vg_fft_gkr_rounds(max_lg)));
     f->max_lg = max_lg;
     return VG_OK;
@@ -397,6 +441,7 @@ extern "C" int vg_fft_gkr_destroy(vg_fft_gkr *f)
 {
     if (!f) return VG_OK;
     cudaStreamSynchronize(f->ctx->stream);
+    fg_drop_graph(f);
     vg_gkr_destroy(f->tables);
     vg_release(f->ctx, f->dev);
     for (cudaEvent_t e : f->ev)
@@ -414,6 +459,19 @@ int vg_fft_gkr_launch(vg_fft_gkr *f, int lg, unsigned seed)
     if (f->pending) return vg_fail(VG_ERR_STATE, "vg_fft_gkr_launch: the previous run was not finished");
     vg_ctx *c = f->ctx;
     f->t0 = std::chrono::steady_clock::now();
+    const bool graphs = fg_graphs_enabled() && !f->g_off && !c->profiling;
+    if (graphs && f->gexec && f->g_lg == lg && f->g_seed == seed && f->g_key[0] == f->dev && f->g_key[1] == f->host &&
+        f->g_key[2] == f->parts_host) {
+        // H, prod_blocks and the host record pointer are those of the captured run
+        VG_CHECK_CUDA(cudaEventRecord(f->ev[0], c->stream));
+        VG_CHECK_CUDA(cudaGraphLaunch(f->gexec, c->stream));
+        VG_CHECK_CUDA(cudaEventRecord(f->ev[1], c->stream));
+        c->launches += f->g_launched;
+        f->launched = f->g_launched;
+        f->lg = lg;
+        f->pending = true;
+        return VG_OK;
+    }
     const long long launches0 = c->launches;
     const long N = 1L << lg, NE = 64L << lg;
     const int nrounds = vg_fft_gkr_rounds(lg);
@@ -521,6 +579,17 @@ int vg_fft_gkr_launch(vg_fft_gkr *f, int lg, unsigned seed)
         return b;
     };
     VG_CHECK_CUDA(cudaEventRecord(f->ev[0], c->stream));
+    // capture when the previous plain run had the same size, seed and buffers
+    const bool same_key = f->g_lg == lg && f->g_seed == seed && f->g_key[0] == f->dev && f->g_key[1] == f->host &&
+                          f->g_key[2] == f->parts_host;
+    const bool capture = graphs && f->g_seen && same_key;
+    CaptureGuard guard;
+    if (capture) {
+        fg_drop_graph(f);
+        VG_CHECK_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+        guard.s = c->stream;
+        guard.active = true;
+    }
     VG_CHECK_CUDA(cudaMemcpyAsync(D, f->host, up_bytes, cudaMemcpyHostToDevice, c->stream));
 
     // ---- circuit values ----
@@ -602,6 +671,31 @@ int vg_fft_gkr_launch(vg_fft_gkr *f, int lg, unsigned seed)
     int nrec;
     VG_TRY(vg_gkr_records(g, &f->recs, &nrec));
     if (nrec != nrounds) return vg_fail(VG_ERR_STATE, "fft_gkr: %d records for %d rounds", nrec, nrounds);
+    if (capture) {
+        guard.active = false;
+        cudaGraph_t graph = nullptr;
+        cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+        if (e == cudaSuccess) e = cudaGraphInstantiate(&f->gexec, graph, 0);
+        if (graph) cudaGraphDestroy(graph);
+        if (e != cudaSuccess) {
+            // nothing of this run executed: launch it plainly, and from now on
+            cudaGetLastError();
+            f->gexec = nullptr;
+            f->g_off = true;
+            c->launches = launches0;
+            return vg_fft_gkr_launch(f, lg, seed);
+        }
+        f->g_launched = c->launches - launches0;
+        VG_CHECK_CUDA(cudaGraphLaunch(f->gexec, c->stream));
+    } else if (graphs) {
+        if (!same_key) fg_drop_graph(f);   // a graph of another key must not be replayed for this one
+        f->g_seen = true;                  // the next run with this key is captured
+        f->g_lg = lg;
+        f->g_seed = seed;
+        f->g_key[0] = f->dev;
+        f->g_key[1] = f->host;
+        f->g_key[2] = f->parts_host;
+    }
     VG_CHECK_CUDA(cudaEventRecord(f->ev[1], c->stream));
     f->launched = c->launches - launches0;
     f->lg = lg;

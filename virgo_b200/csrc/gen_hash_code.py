@@ -32,6 +32,53 @@ def keccak_rotations():
     return rot
 
 
+def round32(rot, mode):
+    """One Keccak-f round on 32-bit lane halves as macro lines.  mode 0: every
+    rotation a pair of funnel shifts; 1 / 2: every other / every rho rotation
+    as multiplies by 2^n (VG_MROT_LO / VG_MROT_HI)."""
+    body = []
+    for h in "LH":
+        for x in range(5):
+            body.append("    uint32_t c%s%d = vg_xor3(vg_xor3(a%s%d, a%s%d, a%s%d), a%s%d, a%s%d); \\"
+                        % (h, x, h, x, h, x + 5, h, x + 10, h, x + 15, h, x + 20))
+    for x in range(5):   # rot1 of each column parity
+        body.append("    uint32_t rL%d = __funnelshift_l(cH%d, cL%d, 1), rH%d = __funnelshift_l(cL%d, cH%d, 1); \\"
+                    % (x, x, x, x, x, x))
+    for i in range(25):
+        x = i % 5
+        for h in "LH":
+            body.append("    a%s%d = vg_xor3(a%s%d, c%s%d, r%s%d); \\" % (h, i, h, i, h, (x + 4) % 5, h, (x + 1) % 5))
+    # rho + pi: b[y, 2x+3y] = rot(a[x, y], r[x][y])
+    k = 0
+    for x in range(5):
+        for y in range(5):
+            dst = y + 5 * ((2 * x + 3 * y) % 5)
+            src = x + 5 * y
+            n = rot[x][y]
+            if n == 0:
+                body.append("    uint32_t bL%d = aL%d, bH%d = aH%d; \\" % (dst, src, dst, src))
+                continue
+            mul = mode == 2 or (mode == 1 and k % 2 == 0)
+            k += 1
+            lo, hi = ("aL%d" % src, "aH%d" % src) if n < 32 else ("aH%d" % src, "aL%d" % src)   # >= 32: halves swap
+            m = n % 32
+            if mul:
+                body.append("    uint32_t bL%d = VG_MROT_LO(%s, %s, %d), bH%d = VG_MROT_HI(%s, %s, %d); \\"
+                            % (dst, lo, hi, m, dst, lo, hi, m))
+            else:
+                body.append("    uint32_t bL%d = __funnelshift_l(%s, %s, %d), bH%d = __funnelshift_l(%s, %s, %d); \\"
+                            % (dst, hi, lo, m, dst, lo, hi, m))
+    # chi
+    for y in range(5):
+        for x in range(5):
+            i = x + 5 * y
+            j, kk = (x + 1) % 5 + 5 * y, (x + 2) % 5 + 5 * y
+            for h in "LH":
+                body.append("    a%s%d = vg_chi(b%s%d, b%s%d, b%s%d); \\" % (h, i, h, i, h, j, h, kk))
+    body.append("    aL0 ^= (RCL); aH0 ^= (RCH); }")
+    return body
+
+
 def primes(n):
     ps, c = [], 2
     while len(ps) < n:
@@ -101,43 +148,16 @@ def main():
     L.append("#define VG_KECCAK_RHO { " + ", ".join(str(rot[i % 5][i // 5]) for i in range(25)) + " }")
     L.append("#define VG_KECCAK_PI_SRC { " + ", ".join(str(((i % 5) + 3 * (i // 5)) % 5 + 5 * (i % 5)) for i in range(25)) + " }")
     L.append("")
-    body = []
-    for h in "LH":
-        for x in range(5):
-            body.append("    uint32_t c%s%d = vg_xor3(vg_xor3(a%s%d, a%s%d, a%s%d), a%s%d, a%s%d); \\"
-                        % (h, x, h, x, h, x + 5, h, x + 10, h, x + 15, h, x + 20))
-    for x in range(5):   # rot1 of each column parity
-        body.append("    uint32_t rL%d = __funnelshift_l(cH%d, cL%d, 1), rH%d = __funnelshift_l(cL%d, cH%d, 1); \\"
-                    % (x, x, x, x, x, x))
-    for i in range(25):
-        x = i % 5
-        for h in "LH":
-            body.append("    a%s%d = vg_xor3(a%s%d, c%s%d, r%s%d); \\" % (h, i, h, i, h, (x + 4) % 5, h, (x + 1) % 5))
-    # rho + pi: b[y, 2x+3y] = rot(a[x, y], r[x][y])
-    for x in range(5):
-        for y in range(5):
-            dst = y + 5 * ((2 * x + 3 * y) % 5)
-            src = x + 5 * y
-            n = rot[x][y]
-            if n == 0:
-                body.append("    uint32_t bL%d = aL%d, bH%d = aH%d; \\" % (dst, src, dst, src))
-            elif n < 32:
-                body.append("    uint32_t bL%d = __funnelshift_l(aH%d, aL%d, %d), bH%d = __funnelshift_l(aL%d, aH%d, %d); \\"
-                            % (dst, src, src, n, dst, src, src, n))
-            else:   # rotation by 32 swaps the halves
-                body.append("    uint32_t bL%d = __funnelshift_l(aL%d, aH%d, %d), bH%d = __funnelshift_l(aH%d, aL%d, %d); \\"
-                            % (dst, src, src, n - 32, dst, src, src, n - 32))
-    # chi
-    for y in range(5):
-        for x in range(5):
-            i = x + 5 * y
-            j, k = (x + 1) % 5 + 5 * y, (x + 2) % 5 + 5 * y
-            for h in "LH":
-                body.append("    a%s%d = vg_chi(b%s%d, b%s%d, b%s%d); \\" % (h, i, h, i, h, j, h, k))
-    body.append("    aL0 ^= (RCL); aH0 ^= (RCH); }")
     L.append("#define VG_KECCAK_ROUND32(RCL, RCH) { \\")
-    L.extend(body)
+    L.extend(round32(rot, 0))
     L.append("")
+    # the same round with rho's rotations partly (1: every other one) or
+    # wholly (2) on the integer-multiply pipe (VG_MROT_*, hash.cuh), which
+    # the funnel-shift form leaves idle while the ALU pipe saturates
+    for mode in (1, 2):
+        L.append("#define VG_KECCAK_ROUND32_M%d(RCL, RCH) { \\" % mode)
+        L.extend(round32(rot, mode))
+        L.append("")
     ps = primes(64)
     k = [iroot(p << 96, 3) & 0xFFFFFFFF for p in ps]
     h0 = [iroot(p << 64, 2) & 0xFFFFFFFF for p in ps[:8]]

@@ -917,6 +917,84 @@ __global__ void __launch_bounds__(THREADS) k_round(const fe *__restrict__ xV, co
     }
 }
 
+// Two consecutive rounds in one pass over tables above the group start
+// (deferred mode): rounds only combine neighbouring entries and both
+// challenges are known, so a thread takes 8 consecutive entries of each table
+// (4 when the first round is the unfolded one after a phase init), folds them
+// with ra into 4, adds the first round's sums over those two pairs, folds
+// with rb into 2, adds the second round's sums over that pair and writes the
+// 2 entries: one read of the tables for two rounds, a quarter of them
+// written.  Both rounds' sums go through one block reduction and the
+// last-block pass (6 values per CTA).
+template <bool FOLD, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_round2(const fe *__restrict__ xV, const fe *__restrict__ xAV,
+                                                    const fe *__restrict__ xAM, long nquads, fe ra, fe rb,
+                                                    fe *__restrict__ yV, fe *__restrict__ yAV, fe *__restrict__ yAM,
+                                                    fe *__restrict__ parts, unsigned *__restrict__ counter,
+                                                    fe *__restrict__ out_a, fe *__restrict__ out_b)
+{
+    __shared__ fe sm[6 * 32];
+    __shared__ bool last;
+    fe sa[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()}, sb[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nquads; i += (long)gridDim.x * blockDim.x) {
+        fe v[4], a[4], m[4];
+        if (FOLD) {
+            const long b = 8 * i;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                v[k] = fold(xV[b + 2 * k], xV[b + 2 * k + 1], ra);
+                a[k] = fold(xAV[b + 2 * k], xAV[b + 2 * k + 1], ra);
+                m[k] = fold(xAM[b + 2 * k], xAM[b + 2 * k + 1], ra);
+            }
+        } else {
+            const long b = 4 * i;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                v[k] = xV[b + k];
+                a[k] = xAV[b + k];
+                m[k] = xAM[b + k];
+            }
+        }
+        rg_sums(v[0], v[1], a[0], a[1], m[0], m[1], sa);
+        rg_sums(v[2], v[3], a[2], a[3], m[2], m[3], sa);
+        const fe v0 = fold(v[0], v[1], rb), v1 = fold(v[2], v[3], rb);
+        const fe a0 = fold(a[0], a[1], rb), a1 = fold(a[2], a[3], rb);
+        const fe m0 = fold(m[0], m[1], rb), m1 = fold(m[2], m[3], rb);
+        rg_sums(v0, v1, a0, a1, m0, m1, sb);
+        yV[2 * i] = v0; yV[2 * i + 1] = v1;
+        yAV[2 * i] = a0; yAV[2 * i + 1] = a1;
+        yAM[2 * i] = m0; yAM[2 * i + 1] = m1;
+    }
+    fe acc[6] = {sa[0], sa[1], sa[2], sb[0], sb[1], sb[2]};
+    block_sum<6>(acc, sm);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) parts[6 * blockIdx.x + k] = acc[k];
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    fe tot[6] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            fe x;
+            x.img = __ldcg(&parts[6 * b + k].img);
+            x.real = __ldcg(&parts[6 * b + k].real);
+            tot[k] = tot[k] + x;
+        }
+    }
+    __syncthreads();
+    block_sum<6>(tot, sm);
+    if (threadIdx.x == 0) {
+        out_a[0] = tot[0]; out_a[1] = tot[1]; out_a[2] = tot[2];
+        out_b[0] = tot[3]; out_b[1] = tot[4]; out_b[2] = tot[5];
+        *counter = 0;
+    }
+}
+
 vg::fe tofe(vg_fe x) { return vg::fe_make(x.real, x.img); }
 vg_fe tovg(vg::fe x) { vg_fe r; r.real = x.real; r.img = x.img; return r; }
 
@@ -1040,6 +1118,13 @@ struct vg_gkr {
     long pend_chunk = 0;                 // a CTA's entries after its first step
     bool pend_nofold = false;
     fe *rg_parts = nullptr;              // per-CTA, per-round partial sums of a group
+    // deferred round above the group start held back to run together with
+    // the next round in one k_round2 pass (VG_TUNE_ROUND_FUSE = 2)
+    bool held = false;
+    bool held_fold = false;
+    fe held_r{};
+    int held_slot = 0;
+    long held_n = 0;                     // table length before the held round
     fe *heavy_parts = nullptr;           // per-CTA partial sums of heavy keys
 };
 
@@ -1551,7 +1636,7 @@ extern "C" int vg_gkr_create(vg_ctx *ctx, const vg_circuit *c, vg_gkr **out)
         return vg_fail(VG_ERR_OOM, "vg_gkr_create: %s allocation failed", what);
     };
     if (cudaMalloc(&g->rbuf, 3 * 64 * sizeof(fe)) != cudaSuccess) return fail("challenges");
-    if (cudaMalloc(&g->round_parts, 3 * 148 * 8 * sizeof(fe)) != cudaSuccess) return fail("round partials");
+    if (cudaMalloc(&g->round_parts, 6 * 148 * 8 * sizeof(fe)) != cudaSuccess) return fail("round partials");
     if (cudaMalloc(&g->round_out, 16 * sizeof(fe)) != cudaSuccess) return fail("round sums");
     if (cudaMalloc(&g->round_counter, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
     if (cudaMalloc(&g->vu, sizeof(fe)) != cudaSuccess) return fail("v_u");
@@ -1995,10 +2080,95 @@ static int rg_smem_attribute(int dev)
     return VG_OK;
 }
 
+// One round on the current tables of length n_in (before the round's fold):
+// k_round with its sums (and, when one pair remains, the folded pair) at o3
+// (and o6).
+static int launch_round(vg_gkr *g, long n_in, bool fold, fe r, fe *o3, fe *o6)
+{
+    vg_ctx *c = g->ctx;
+    const long n_out = fold ? n_in / 2 : n_in;   // table length the sums are taken over
+    const long npairs = n_out / 2;
+    // threads per CTA from the device's tuning; the grid covers at most
+    // 148 x 2048 threads and at most 148 x 8 CTAs (the partials buffer),
+    // looping beyond
+    const int T = (int)vg_tune_value(c->device, VG_TUNE_ROUND_THREADS);
+    unsigned grid = std::min<unsigned>(grid_for(npairs, T), std::min(148u * 8u, 148u * 2048u / (unsigned)T));
+    fe *y[3] = {g->buf[g->next_buf][0], g->buf[g->next_buf][1], g->buf[g->next_buf][2]};
+    {
+        // fold: read 3 tables x 4 entries, write 3 x 2 per pair; else read 3 x 2
+        ProfScope ps(c, KF_ROUND, (fold ? 288.0 : 96.0) * (double)npairs);
+        const fe *x0 = g->cur[0], *x1 = g->cur[1], *x2 = g->cur[2];
+        fe *pr = g->round_parts;
+        unsigned *cnt = g->round_counter;
+#define VG_ROUND_LAUNCH(TT)                                                                                          \
+    if (fold)                                                                                                         \
+        k_round<true, TT><<<grid, TT, 0, c->stream>>>(x0, x1, x2, npairs, r, y[0], y[1], y[2], pr, cnt, o3, o6);      \
+    else                                                                                                              \
+        k_round<false, TT><<<grid, TT, 0, c->stream>>>(x0, x1, x2, npairs, r, nullptr, nullptr, nullptr, pr, cnt, o3, o6)
+        if (T == 128) VG_ROUND_LAUNCH(128);
+        else if (T == 512) VG_ROUND_LAUNCH(512);
+        else VG_ROUND_LAUNCH(256);
+#undef VG_ROUND_LAUNCH
+    }
+    VG_LAUNCHED(c);
+    if (fold) {
+        g->cur[0] = y[0];
+        g->cur[1] = y[1];
+        g->cur[2] = y[2];
+        g->next_buf ^= 1;
+    }
+    return VG_OK;
+}
+
+// Two rounds in one k_round2 pass on the current tables of length n_in: the
+// first folds with ra when `fold` (else it is a phase's unfolded first
+// round), the second folds with rb; sums to oa and ob.
+static int launch_round2(vg_gkr *g, long n_in, bool fold, fe ra, fe rb, fe *oa, fe *ob)
+{
+    vg_ctx *c = g->ctx;
+    const long nquads = fold ? n_in / 8 : n_in / 4;
+    const int T = (int)vg_tune_value(c->device, VG_TUNE_ROUND_THREADS);
+    unsigned grid = std::min<unsigned>(grid_for(nquads, T), std::min(148u * 4u, 148u * 2048u / (unsigned)T));
+    fe *y[3] = {g->buf[g->next_buf][0], g->buf[g->next_buf][1], g->buf[g->next_buf][2]};
+    {
+        // per quad: read 3 tables x 8 (or 4) entries, write 3 x 2
+        ProfScope ps(c, KF_ROUND, (fold ? 480.0 : 288.0) * (double)nquads);
+        const fe *x0 = g->cur[0], *x1 = g->cur[1], *x2 = g->cur[2];
+        fe *pr = g->round_parts;
+        unsigned *cnt = g->round_counter;
+#define VG_ROUND2_LAUNCH(TT)                                                                                         \
+    if (fold)                                                                                                         \
+        k_round2<true, TT><<<grid, TT, 0, c->stream>>>(x0, x1, x2, nquads, ra, rb, y[0], y[1], y[2], pr, cnt, oa, ob); \
+    else                                                                                                              \
+        k_round2<false, TT><<<grid, TT, 0, c->stream>>>(x0, x1, x2, nquads, ra, rb, y[0], y[1], y[2], pr, cnt, oa, ob)
+        if (T == 128) VG_ROUND2_LAUNCH(128);
+        else if (T == 512) VG_ROUND2_LAUNCH(512);
+        else VG_ROUND2_LAUNCH(256);
+#undef VG_ROUND2_LAUNCH
+    }
+    VG_LAUNCHED(c);
+    g->cur[0] = y[0];
+    g->cur[1] = y[1];
+    g->cur[2] = y[2];
+    g->next_buf ^= 1;
+    return VG_OK;
+}
+
+// A held round with no partner (the next round starts a group, or the phase
+// ends): it runs alone.
+static int flush_held(vg_gkr *g)
+{
+    if (!g->held) return VG_OK;
+    g->held = false;
+    fe *o3 = g->rec + 9 * g->held_slot;
+    return launch_round(g, g->held_n, g->held_fold, g->held_r, o3, o3 + 3);
+}
+
 // Launches the pending deferred rounds as one group: one chunk per CTA when
 // the table fits the grid, CTAs looping over chunks beyond.
 static int flush_rounds(vg_gkr *g)
 {
+    VG_TRY(flush_held(g));
     if (g->pend_r.empty()) return VG_OK;
     vg_ctx *c = g->ctx;
     RoundGroup G{};
@@ -2160,6 +2330,7 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
     const long S = std::max(2L * RG_CHUNK, group_start(g->ctx->device));
     const long lim = fold ? S : S / 2;
     if (g->deferred && (!g->pend_r.empty() || g->n <= lim)) {
+        VG_TRY(flush_held(g));   // the round before this one ran alone
         if (g->pend_r.empty()) {
             g->pend_n0 = g->n;
             g->pend_nofold = !fold;
@@ -2175,41 +2346,33 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
         return VG_OK;
     }
     vg_ctx *c = g->ctx;
-    const long n_out = fold ? g->n / 2 : g->n;   // table length the sums are taken over
-    const long npairs = n_out / 2;
-    // threads per CTA from the device's tuning; the grid covers at most
-    // 148 x 2048 threads and at most 148 x 8 CTAs (the partials buffer),
-    // looping beyond
-    const int T = (int)vg_tune_value(c->device, VG_TUNE_ROUND_THREADS);
-    unsigned grid = std::min<unsigned>(grid_for(npairs, T), std::min(148u * 8u, 148u * 2048u / (unsigned)T));
-    fe *y[3] = {g->buf[g->next_buf][0], g->buf[g->next_buf][1], g->buf[g->next_buf][2]};
-    fe r = tofe(previous_random);
+    const fe r = tofe(previous_random);
+    if (g->deferred) {
+        if (g->held) {
+            // this round pairs with the held one: one pass for both
+            g->held = false;
+            VG_TRY(launch_round2(g, g->held_n, g->held_fold, g->held_r, r, g->rec + 9 * g->held_slot,
+                                 g->rec + 9 * g->rec_n));
+            ++g->rec_n;
+            g->n /= 2;   // a round after another always folds
+            g->round0_pending = false;
+            return VG_OK;
+        }
+        if (vg_tune_value(c->device, VG_TUNE_ROUND_FUSE) >= 2) {
+            g->held = true;
+            g->held_fold = fold;
+            g->held_r = r;
+            g->held_slot = g->rec_n;
+            g->held_n = g->n;
+            ++g->rec_n;
+            if (fold) g->n /= 2;
+            g->round0_pending = false;
+            return VG_OK;
+        }
+    }
     fe *o3 = g->deferred ? g->rec + 9 * g->rec_n : g->round_out;
-    fe *o6 = g->deferred ? o3 + 3 : nullptr;
-    {
-        // fold: read 3 tables x 4 entries, write 3 x 2 per pair; else read 3 x 2
-        ProfScope ps(c, KF_ROUND, (fold ? 288.0 : 96.0) * (double)npairs);
-        const fe *x0 = g->cur[0], *x1 = g->cur[1], *x2 = g->cur[2];
-        fe *pr = g->round_parts;
-        unsigned *cnt = g->round_counter;
-#define VG_ROUND_LAUNCH(TT)                                                                                          \
-    if (fold)                                                                                                         \
-        k_round<true, TT><<<grid, TT, 0, c->stream>>>(x0, x1, x2, npairs, r, y[0], y[1], y[2], pr, cnt, o3, o6);      \
-    else                                                                                                              \
-        k_round<false, TT><<<grid, TT, 0, c->stream>>>(x0, x1, x2, npairs, r, nullptr, nullptr, nullptr, pr, cnt, o3, o6)
-        if (T == 128) VG_ROUND_LAUNCH(128);
-        else if (T == 512) VG_ROUND_LAUNCH(512);
-        else VG_ROUND_LAUNCH(256);
-#undef VG_ROUND_LAUNCH
-    }
-    VG_LAUNCHED(c);
-    if (fold) {
-        g->cur[0] = y[0];
-        g->cur[1] = y[1];
-        g->cur[2] = y[2];
-        g->next_buf ^= 1;
-        g->n = n_out;
-    }
+    VG_TRY(launch_round(g, g->n, fold, r, o3, g->deferred ? o3 + 3 : nullptr));
+    if (fold) g->n /= 2;
     g->round0_pending = false;
     if (g->deferred) {
         ++g->rec_n;
@@ -2246,7 +2409,7 @@ int vg_gkr_tables_create(vg_ctx *ctx, long max_n, int max_records, vg_gkr **out)
         vg_gkr_destroy(g);
         return vg_fail(VG_ERR_OOM, "vg_gkr_tables_create: %s allocation failed", what);
     };
-    if (cudaMalloc(&g->round_parts, 3 * 148 * 8 * sizeof(fe)) != cudaSuccess) return fail("round partials");
+    if (cudaMalloc(&g->round_parts, 6 * 148 * 8 * sizeof(fe)) != cudaSuccess) return fail("round partials");
     if (cudaMalloc(&g->round_out, 16 * sizeof(fe)) != cudaSuccess) return fail("round sums");
     if (cudaMalloc(&g->round_counter, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
     // ordered on the context's (non-blocking) stream before the first round

@@ -1,7 +1,12 @@
 // Hash kernels: batched 64-byte hashing, Merkle trees and the FRI leaf hash
 // chains.  All are integer-ALU bound (Keccak-f[1600]: 24 rounds of 64-bit
 // xor/and-not/rotate; SHA-256: 2 x 64 rounds of 32-bit ops).
+#include <mutex>
 #include "common.cuh"
+// 2^n, n < 32, for the multiply-pipe rotations (VG_MROT_*); filled per device
+// at first use (pow2_table)
+#define VG_HASH_MULROT 1
+static __constant__ uint32_t vg_pow2c[32];
 #include "hash.cuh"
 #include "merkle.cuh"
 
@@ -103,7 +108,7 @@ __global__ void __launch_bounds__(T) k_leaf_chain(const fe *__restrict__ c, int 
 // Leaf chains of several codeword sets in one launch: thread t serves leaf
 // t - begin of the job whose range holds t.  The next slice's pair is loaded
 // before the current hash so the loads overlap the permutation.
-template <int KIND, int T>
+template <int KIND, int T, int ROT>
 __global__ void __launch_bounds__(T) k_leaf_chains(ChainJobs jobs)
 {
     const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
@@ -121,7 +126,7 @@ __global__ void __launch_bounds__(T) k_leaf_chains(ChainJobs jobs)
             nb = c[(long)(s + 1) * n + k + half];
         }
         uint64_t w[8] = {a.img, a.real, b.img, b.real, h[0], h[1], h[2], h[3]};
-        vg::hash64<KIND>(w, h);
+        vg::hash64_rot<KIND, ROT>(w, h);
         a = na;
         b = nb;
     }
@@ -241,6 +246,22 @@ __global__ void __launch_bounds__(MERKLE_TOP) k_merkle_tops(TreeJobs jobs, uint6
     if (threadIdx.x < 4) roots[4 * blockIdx.x + threadIdx.x] = tree[4 + threadIdx.x];
 }
 
+// fills vg_pow2c on the current device, once per device
+static int pow2_table(int dev)
+{
+    static std::mutex mu;
+    static std::vector<bool> done;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev >= (int)done.size()) done.resize(dev + 1, false);
+    if (!done[dev]) {
+        uint32_t p[32];
+        for (int i = 0; i < 32; ++i) p[i] = 1u << i;
+        VG_CHECK_CUDA(cudaMemcpyToSymbol(vg_pow2c, p, sizeof p));
+        done[dev] = true;
+    }
+    return VG_OK;
+}
+
 int vg_leaf_chains(vg_ctx *c, const ChainJobs &jobs)
 {
     if (jobs.total < 1) return VG_OK;
@@ -251,11 +272,17 @@ int vg_leaf_chains(vg_ctx *c, const ChainJobs &jobs)
         k_leaf_chains_warp<<<warp_chain_grid(jobs.total), WARP_CHAIN_THREADS, 0, c->stream>>>(jobs);
     } else {
         const int T = (int)vg_tune_value(c->device, VG_TUNE_LEAF_THREADS);
-#define VG_CHAINS_LAUNCH(TT)                                                                                 \
-    if (c->hash_kind == VG_HASH_SHA256)                                                                       \
-        k_leaf_chains<VG_HASH_SHA256, TT><<<grid_for(jobs.total, TT), TT, 0, c->stream>>>(jobs);             \
-    else                                                                                                      \
-        k_leaf_chains<VG_HASH_SHA3_256, TT><<<grid_for(jobs.total, TT), TT, 0, c->stream>>>(jobs)
+        const int rot = c->hash_kind == VG_HASH_SHA3_256 ? (int)vg_tune_value(c->device, VG_TUNE_LEAF_ROT) : 0;
+        if (rot) VG_TRY(pow2_table(c->device));
+#define VG_CHAINS_LAUNCH(TT)                                                                                    \
+    if (c->hash_kind == VG_HASH_SHA256)                                                                          \
+        k_leaf_chains<VG_HASH_SHA256, TT, 0><<<grid_for(jobs.total, TT), TT, 0, c->stream>>>(jobs);             \
+    else if (rot == 1)                                                                                           \
+        k_leaf_chains<VG_HASH_SHA3_256, TT, 1><<<grid_for(jobs.total, TT), TT, 0, c->stream>>>(jobs);          \
+    else if (rot == 2)                                                                                           \
+        k_leaf_chains<VG_HASH_SHA3_256, TT, 2><<<grid_for(jobs.total, TT), TT, 0, c->stream>>>(jobs);          \
+    else                                                                                                         \
+        k_leaf_chains<VG_HASH_SHA3_256, TT, 0><<<grid_for(jobs.total, TT), TT, 0, c->stream>>>(jobs)
         if (T == 64) VG_CHAINS_LAUNCH(64);
         else if (T == 256) VG_CHAINS_LAUNCH(256);
         else VG_CHAINS_LAUNCH(128);

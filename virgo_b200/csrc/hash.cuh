@@ -53,6 +53,45 @@ __device__ __forceinline__ void sha3_256_64(const uint64_t w[8], uint64_t d[4])
     d[3] = aL3 | ((uint64_t)aH3 << 32);
 }
 
+#ifdef VG_HASH_MULROT
+// 64-bit rotation left by n (0..31) of (hi:lo) on the integer-multiply pipe:
+// lo * 2^n keeps the bits that stay in the low word and umulhi(hi, 2^n)
+// brings in those crossing from the high word; they share no bit, so the
+// sum is their union.  The funnel-shift form runs on the ALU pipe, which the
+// permutation saturates while the multiply pipe idles.  2^n is read from
+// vg_pow2c (constant memory, filled at run time by the including file) so
+// that the compiler cannot turn the multiplies back into shifts.
+#define VG_MROT_LO(lo, hi, n) ((lo) * vg_pow2c[n] + __umulhi((hi), vg_pow2c[n]))
+#define VG_MROT_HI(lo, hi, n) ((hi) * vg_pow2c[n] + __umulhi((lo), vg_pow2c[n]))
+
+// sha3_256_64 with every other (MODE 1) or every (MODE 2) rho rotation on
+// the multiply pipe; the same digest
+template <int MODE>
+__device__ __forceinline__ void sha3_256_64_mrot(const uint64_t w[8], uint64_t d[4])
+{
+    const uint32_t RCL[24] = VG_KECCAK_RC_LO, RCH[24] = VG_KECCAK_RC_HI;
+    uint32_t aL0 = (uint32_t)w[0], aH0 = (uint32_t)(w[0] >> 32), aL1 = (uint32_t)w[1], aH1 = (uint32_t)(w[1] >> 32);
+    uint32_t aL2 = (uint32_t)w[2], aH2 = (uint32_t)(w[2] >> 32), aL3 = (uint32_t)w[3], aH3 = (uint32_t)(w[3] >> 32);
+    uint32_t aL4 = (uint32_t)w[4], aH4 = (uint32_t)(w[4] >> 32), aL5 = (uint32_t)w[5], aH5 = (uint32_t)(w[5] >> 32);
+    uint32_t aL6 = (uint32_t)w[6], aH6 = (uint32_t)(w[6] >> 32), aL7 = (uint32_t)w[7], aH7 = (uint32_t)(w[7] >> 32);
+    uint32_t aL8 = 0x06u, aH8 = 0, aL9 = 0, aH9 = 0, aL10 = 0, aH10 = 0, aL11 = 0, aH11 = 0, aL12 = 0, aH12 = 0;
+    uint32_t aL13 = 0, aH13 = 0, aL14 = 0, aH14 = 0, aL15 = 0, aH15 = 0, aL16 = 0, aH16 = 0x80000000u;
+    uint32_t aL17 = 0, aH17 = 0, aL18 = 0, aH18 = 0, aL19 = 0, aH19 = 0, aL20 = 0, aH20 = 0, aL21 = 0, aH21 = 0;
+    uint32_t aL22 = 0, aH22 = 0, aL23 = 0, aH23 = 0, aL24 = 0, aH24 = 0;
+    if (MODE == 1) {
+#pragma unroll
+        for (int r = 0; r < 24; ++r) VG_KECCAK_ROUND32_M1(RCL[r], RCH[r]);
+    } else {
+#pragma unroll
+        for (int r = 0; r < 24; ++r) VG_KECCAK_ROUND32_M2(RCL[r], RCH[r]);
+    }
+    d[0] = aL0 | ((uint64_t)aH0 << 32);
+    d[1] = aL1 | ((uint64_t)aH1 << 32);
+    d[2] = aL2 | ((uint64_t)aH2 << 32);
+    d[3] = aL3 | ((uint64_t)aH3 << 32);
+}
+#endif
+
 __device__ __forceinline__ uint32_t bswap32(uint32_t x) { return __byte_perm(x, 0, 0x0123); }
 __device__ __forceinline__ uint32_t ror32(uint32_t x, int n) { return __funnelshift_r(x, x, n); }
 
@@ -184,5 +223,16 @@ __device__ __forceinline__ void hash64(const uint64_t w[8], uint64_t d[4])
     if (KIND == HASH_SHA256) sha256_64(w, d);
     else sha3_256_64(w, d);
 }
+
+#ifdef VG_HASH_MULROT
+// hash64 with the SHA3 rotations in form ROT (0: funnel shifts; 1, 2: see
+// sha3_256_64_mrot)
+template <int KIND, int ROT>
+__device__ __forceinline__ void hash64_rot(const uint64_t w[8], uint64_t d[4])
+{
+    if (KIND == HASH_SHA256 || ROT == 0) hash64<KIND>(w, d);
+    else sha3_256_64_mrot<ROT>(w, d);
+}
+#endif
 
 }  // namespace vg

@@ -24,6 +24,8 @@ const Range RANGES[VG_TUNE_COUNT] = {
     {10, 13, 12, false},                    // NTT_TILE_LOG
     {64, 256, 256, true},                   // LEAF_THREADS
     {0, 1L << 24, 0, false},                // LEAF_WARP_MAX
+    {1, 2, 1, false},                       // ROUND_FUSE
+    {0, 2, 0, false},                       // LEAF_ROT
 };
 
 std::atomic<long> g_tune[MAX_DEVICES][VG_TUNE_COUNT];

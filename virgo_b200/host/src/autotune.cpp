@@ -10,7 +10,8 @@
 // commitment is not on the proof's critical path.  Every candidate gets one
 // warm-up batch, then `reps` timed batches of which the fastest counts; a
 // candidate replaces the value in force only when it is faster by more than
-// 1%, so timing noise leaves the defaults alone.
+// 2% (repeated batches of one setting vary by about 1%), so timing noise
+// leaves the defaults alone.
 //
 // Every parameter value gives bit-identical proofs (the tests prove each one
 // against the same transcripts), so the tuner never changes a result.
@@ -33,10 +34,12 @@ const std::vector<Knob> &knobs()
 {
     static const std::vector<Knob> k = {
         {VG_TUNE_GROUP_START, {1L << 11, 1L << 13, 1L << 15, 1L << 17, 1L << 19}},
+        {VG_TUNE_ROUND_FUSE, {1, 2}},
         {VG_TUNE_ROUND_THREADS, {128, 256, 512}},
         {VG_TUNE_NTT_MAX_LOG, {8, 9, 10}},
         {VG_TUNE_NTT_TILE_LOG, {11, 12, 13}},
         {VG_TUNE_LEAF_THREADS, {64, 128, 256}},
+        {VG_TUNE_LEAF_ROT, {0, 1, 2}},
         {VG_TUNE_LEAF_WARP_MAX, {0, 1024, 8192}},
     };
     return k;
@@ -106,7 +109,7 @@ extern "C" int vg_autotune(vg_session *const *ss, int n, unsigned seed, int reps
                 return rc;
             }
             const int t = record(kb.key, v, ms);
-            if (ms < best_ms && ms < 0.99 * cur_ms) {
+            if (ms < best_ms && ms < 0.98 * cur_ms) {
                 best = v;
                 best_ms = ms;
                 best_trial = t;
