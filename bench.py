@@ -618,6 +618,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-served", action="store_true", help="skip the batched-random and served measurements")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
+    ap.add_argument("--tune", default="", help="launch shapes to set first, e.g. round_fuse=2,group_start=2048")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -637,6 +638,9 @@ def main():
         import torch.distributed as dist
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    if args.tune:
+        import virgo_b200 as vb
+        vb.tune_set(local, **{k: int(v) for k, v in (kv.split("=") for kv in args.tune.split(","))})
     r = ours(args, layers, rank, world)
     if rank == 0:
         hbm, kind = peaks()
