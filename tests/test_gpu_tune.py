@@ -41,7 +41,7 @@ def golden_sessions():
 
 @pytest.mark.parametrize("knob,value", [
     ("group_start", 1 << 11), ("group_start", 1 << 13), ("group_start", 1 << 15), ("group_start", 1 << 19),
-    ("group_start", 1 << 22), ("round_threads", 256), ("round_threads", 512), ("ntt_max_log", 6),
+    ("group_start", 1 << 22), ("round_threads", 128), ("round_threads", 512), ("ntt_max_log", 6),
     ("ntt_max_log", 8), ("ntt_max_log", 9), ("ntt_tile_log", 10), ("ntt_tile_log", 11), ("ntt_tile_log", 13),
     ("leaf_threads", 64), ("leaf_threads", 128), ("leaf_warp_max", 1 << 24), ("leaf_rot", 1), ("leaf_rot", 2),
 ])
@@ -53,11 +53,13 @@ def test_golden_transcripts_under_every_tuning(golden_sessions, knob, value):
         assert transcript.digest(transcript.parse(blob)) == c["digest"], (c["name"], knob, value)
 
 
+@pytest.mark.parametrize("fuse", [1, 2])
 @pytest.mark.parametrize("group_start", [1 << 11, 1 << 13, 1 << 17])
-def test_golden_transcripts_with_paired_rounds(golden_sessions, group_start):
-    """Rounds above the group start paired into two-round passes (the group
-    start lowered so that the golden circuits have such rounds)."""
-    vb.tune_set(0, group_start=group_start, round_fuse=2)
+def test_golden_transcripts_with_paired_rounds(golden_sessions, group_start, fuse):
+    """Rounds above the group start one per launch or paired into two-round
+    passes (the group start lowered so that the golden circuits have such
+    rounds)."""
+    vb.tune_set(0, group_start=group_start, round_fuse=fuse)
     for s, c in golden_sessions:
         _, blob = s.prove(c["seed"])
         assert transcript.digest(transcript.parse(blob)) == c["digest"], (c["name"], group_start)
@@ -77,9 +79,9 @@ def test_round_groups_loop_over_chunks_on_large_tables():
         assert s.prove(5)[1] == base
         vb.tune_set(0, group_start=1 << 11, round_threads=256)
         assert s.prove(5)[1] == base
-        for gs, t in ((1 << 11, 128), (1 << 13, 512), (1 << 17, 256)):
-            vb.tune_set(0, group_start=gs, round_threads=t, round_fuse=2)
-            assert s.prove(5)[1] == base, (gs, t)
+        for gs, t, fuse in ((1 << 11, 128, 2), (1 << 13, 512, 2), (1 << 17, 256, 1), (1 << 11, 128, 1)):
+            vb.tune_set(0, group_start=gs, round_threads=t, round_fuse=fuse)
+            assert s.prove(5)[1] == base, (gs, t, fuse)
     finally:
         s.close()
 

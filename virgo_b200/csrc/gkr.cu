@@ -1091,7 +1091,7 @@ struct vg_gkr {
     unsigned long long *acc = nullptr;   // 2 tables x 4 words x 2^max_bl
     fe *eq = nullptr;                    // half tables
     fe *rbuf = nullptr;                  // challenges (device copy)
-    fe *round_parts = nullptr;           // block partials of the round kernel
+    fe *round_parts = nullptr;           // block partials of the round kernels (6 x 148 x 8 values)
     fe *round_out = nullptr;             // round sums (3) written by the last block
     unsigned *round_counter = nullptr;   // blocks finished, reset by the last one
     long eq_half = 0;
@@ -2089,10 +2089,10 @@ static int launch_round(vg_gkr *g, long n_in, bool fold, fe r, fe *o3, fe *o6)
     const long n_out = fold ? n_in / 2 : n_in;   // table length the sums are taken over
     const long npairs = n_out / 2;
     // threads per CTA from the device's tuning; the grid covers at most
-    // 148 x 2048 threads and at most 148 x 8 CTAs (the partials buffer),
-    // looping beyond
+    // 148 x 2048 threads and at most 148 x 16 CTAs (the partials buffer holds
+    // 3 sums for each), looping beyond
     const int T = (int)vg_tune_value(c->device, VG_TUNE_ROUND_THREADS);
-    unsigned grid = std::min<unsigned>(grid_for(npairs, T), std::min(148u * 8u, 148u * 2048u / (unsigned)T));
+    unsigned grid = std::min<unsigned>(grid_for(npairs, T), std::min(148u * 16u, 148u * 2048u / (unsigned)T));
     fe *y[3] = {g->buf[g->next_buf][0], g->buf[g->next_buf][1], g->buf[g->next_buf][2]};
     {
         // fold: read 3 tables x 4 entries, write 3 x 2 per pair; else read 3 x 2
@@ -2127,8 +2127,9 @@ static int launch_round2(vg_gkr *g, long n_in, bool fold, fe ra, fe rb, fe *oa, 
 {
     vg_ctx *c = g->ctx;
     const long nquads = fold ? n_in / 8 : n_in / 4;
+    // at most 148 x 2048 threads and 148 x 8 CTAs (6 sums each in the partials buffer)
     const int T = (int)vg_tune_value(c->device, VG_TUNE_ROUND_THREADS);
-    unsigned grid = std::min<unsigned>(grid_for(nquads, T), std::min(148u * 4u, 148u * 2048u / (unsigned)T));
+    unsigned grid = std::min<unsigned>(grid_for(nquads, T), std::min(148u * 8u, 148u * 2048u / (unsigned)T));
     fe *y[3] = {g->buf[g->next_buf][0], g->buf[g->next_buf][1], g->buf[g->next_buf][2]};
     {
         // per quad: read 3 tables x 8 (or 4) entries, write 3 x 2
