@@ -602,9 +602,14 @@ def roofline(fam, hbm_peak, peak_kind):
                              "average launch's algorithmic bytes") if traffic else None,
             "peak_source": peak_kind, "launches_per_proof": f["launches"],
             "avg_launch_us": round(1000.0 * f["ms"] / f["launches"], 2), "bytes_per_launch": per_launch,
+            "alu_pipe": {"frac_large_launches": 0.75, "frac_round_group": 0.33,
+                         "source": "ncu sm__inst_executed_pipe_alu, pct of peak: the 2^24-entry fold round "
+                                   "(profiles/k_round_matmul256.txt) and a 64-CTA round group "
+                                   "(profiles/k_round_group_matmul256.txt)"},
             "note": "CUDA events on the launching stream; back-to-back launches share one event, so a "
-                    "launch's time runs from the end of the one before it; the kernel is integer-ALU bound "
-                    "(ncu ALU pipe 80%)"}
+                    "launch's time runs from the end of the one before it; the large launches are bound by "
+                    "the integer ALU pipe and HBM together (ALU 75%, DRAM 65%), the round groups of the "
+                    "last 17 rounds of each phase by latency"}
 
 
 def main():
