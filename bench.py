@@ -307,6 +307,16 @@ def ours(args, layers, rank, world):
             tot_n, tot_t, tot_b = tot_n + n.value, tot_t + t.value, tot_b + b.value
         if tot_n:
             fam[name] = {"launches": tot_n / args.steps, "ms": tot_t / args.steps, "bytes": tot_b / args.steps}
+    # the sumcheck stream's launches one by one: round launches that move at
+    # least 100 MB (tables of 2^21 entries and up) against the rest
+    cap = 20000
+    tf, tm, tb = (ctypes.c_int * cap)(), (ctypes.c_double * cap)(), (ctypes.c_double * cap)()
+    nt = ctypes.c_long()
+    vb.check(L.vg_ctx_profile_trace(ctx0, tf, tm, tb, cap, ctypes.byref(nt)))
+    rounds = [(tm[i], tb[i]) for i in range(min(nt.value, cap)) if tf[i] == FAMILIES.index("sumcheck_round")]
+    big = [x for x in rounds if x[1] >= 100e6]
+    large_rounds = {"launches_per_proof": len(big) / args.steps,
+                    "ms": sum(t for t, _ in big) / args.steps, "bytes": sum(b for _, b in big) / args.steps} if big else None
     for cx in pctxs:
         vb.check(L.vg_ctx_profile(cx, 0))
     for s in sessions[1:]:
@@ -355,7 +365,7 @@ def ours(args, layers, rank, world):
         s.close()
     base.close()
     return {"t_plain": t_plain, "t_batch": t_batch, "t_e2e": t_e2e, "t_e2e_circuit": t_e2e_circuit,
-            "clocks": clocks.summary(), "families": fam, "launches": n_launch,
+            "clocks": clocks.summary(), "families": fam, "launches": n_launch, "large_rounds": large_rounds,
             "stages": {k: v / args.steps for k, v in stages.items()}, "autotune": tune,
             "h2d": int(u0.nbytes) * args.batch, "h2d_circuit": h2d_circuit * args.batch, "d2h": d2h}
 
@@ -586,7 +596,7 @@ def max_over_ranks(x, world):
     return replicas.max_over_ranks(x)
 
 
-def roofline(fam, hbm_peak, peak_kind):
+def roofline(fam, hbm_peak, peak_kind, large=None):
     mem = {k: v for k, v in fam.items() if k in HBM_BOUND}
     if not mem:
         return None
@@ -602,6 +612,13 @@ def roofline(fam, hbm_peak, peak_kind):
                              "average launch's algorithmic bytes") if traffic else None,
             "peak_source": peak_kind, "launches_per_proof": f["launches"],
             "avg_launch_us": round(1000.0 * f["ms"] / f["launches"], 2), "bytes_per_launch": per_launch,
+            "large_launches": ({"achieved": round(large["bytes"] / (large["ms"] / 1000.0) / 1e9, 1),
+                                "frac": round(large["bytes"] / (large["ms"] / 1000.0) / 1e9 / hbm_peak, 4),
+                                "launches_per_proof": large["launches_per_proof"],
+                                "share_of_family_ms": round(large["ms"] / f["ms"], 4),
+                                "note": "the round launches that move at least 100 MB each (tables of 2^21 "
+                                        "entries and up), same events"}
+                               if (large and top == "sumcheck_round" and large["ms"] > 0) else None),
             "alu_pipe": {"frac_large_launches": 0.75, "frac_round_group": 0.33,
                          "source": "ncu sm__inst_executed_pipe_alu, pct of peak: the 2^24-entry fold round "
                                    "(profiles/k_round_matmul256.txt) and a 64-CTA round group "
@@ -676,7 +693,7 @@ def main():
                                     "(uint32 wires, built and validated on the GPU)"},
             "gpu_launches": r["launches"],
             "clocks": r["clocks"],
-            "roofline": roofline(r["families"], hbm, kind),
+            "roofline": roofline(r["families"], hbm, kind, r["large_rounds"]),
             "stages_s": r["stages"],
             "kernel_families": fam,
             "autotune": r["autotune"],

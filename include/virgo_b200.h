@@ -435,7 +435,7 @@ int vg_tune_range(int key, long *lo, long *hi, long *def);
  * (vg_session_prove_batch over all n at once: n = 1 tunes one proof's
  * latency, n > 1 the throughput of n proofs in flight), `reps` timed batches
  * after one warm-up batch per candidate, the best of them counting; keeps a
- * candidate only if it beats the value in force by more than 2%, and leaves
+ * candidate only if it beats the value in force by more than 3%, and leaves
  * the winners set for the sessions' device.  trials (optional, up to
  * max_trials) receives every timing.  Do not prove on the same device from
  * other threads meanwhile. */
