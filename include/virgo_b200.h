@@ -422,7 +422,10 @@ enum {
     VG_TUNE_LEAF_ROT = 7,      /* SHA3 leaf chains (per-thread form): 0 = every 64-bit rotation as
                                   two funnel shifts (ALU pipe); 1 = every other rho rotation, 2 =
                                   every rho rotation as multiplies by 2^n (integer-multiply pipe) */
-    VG_TUNE_COUNT = 8
+    VG_TUNE_BETA_TABLE = 8,    /* phase-2 table builds read each gate's beta_g from a table the
+                                  phase-1 builds of the same layer wrote (1), or form it again
+                                  from the eq half tables (0) */
+    VG_TUNE_COUNT = 9
 };
 int vg_tune_get(int device, int key, long *value);
 /* VG_ERR_ARG for a value outside the key's range. */

@@ -179,8 +179,13 @@ struct BetaG {
     const fe *f0, *s0, *f1, *s1;   // alpha*eq(r0 low half), eq(r0 high half), beta*..., eq(r1 high)
     int fh;
     long mask;
+    // the layer's values by gate: phase 1's gathers store each gate's value
+    // there (save), phase 2's read it (tab) instead of forming it again
+    fe *save = nullptr;
+    const fe *tab = nullptr;
     __device__ __forceinline__ fe at(long i) const
     {
+        if (tab) return tab[i];
         return f0[i & mask] * s0[i >> fh] + f1[i & mask] * s1[i >> fh];
     }
 };
@@ -425,6 +430,7 @@ __device__ __forceinline__ void edge1(int tk, uint32_t gv, uint32_t o, const Bet
 {
     const int t = tk & 255;
     const fe b = bg.at(gv);
+    if (bg.save) bg.save[gv] = b;   // every edge of a gate stores the same value
     switch (t) {
     case 0: av = av + prev[o] * b; am = am + b; break;
     case 1: am = am + prev[o] * b; break;
@@ -1126,6 +1132,8 @@ struct vg_gkr {
     int held_slot = 0;
     long held_n = 0;                     // table length before the held round
     fe *heavy_parts = nullptr;           // per-CTA partial sums of heavy keys
+    fe *bgt = nullptr;                   // beta_g by gate of the current layer (2^max_bl entries)
+    int bgt_layer = -1;                  // the layer whose phase-1 gathers filled bgt, -1 none
 };
 
 static int flush_rounds(vg_gkr *g);
@@ -1594,7 +1602,8 @@ static int gkr_bind(vg_gkr *g, const vg_circuit *c)
             }
         vg_release(x, g->eq);
         vg_release(x, g->rg_parts);
-        g->eq = g->rg_parts = nullptr;
+        vg_release(x, g->bgt);
+        g->eq = g->rg_parts = g->bgt = nullptr;
         g->N_cap = 0;
         for (int b = 0; b < 2; ++b)
             for (int k = 0; k < 3; ++k)
@@ -1602,9 +1611,12 @@ static int gkr_bind(vg_gkr *g, const vg_circuit *c)
         if (vg_alloc(x, (void **)&g->eq, 6 * (1L << (c->max_bl / 2 + 1)) * sizeof(fe)) != VG_OK) return oom("eq tables");
         if (vg_alloc(x, (void **)&g->rg_parts, rg_parts_len(N) * sizeof(fe)) != VG_OK)
             return oom("group partials");
+        if (vg_alloc(x, (void **)&g->bgt, N * sizeof(fe)) != VG_OK) return oom("beta_g table");
         g->N_cap = N;
     }
     g->C = c;
+    g->bgt_layer = -1;
+    g->held = false;
     g->eq_half = 1L << (c->max_bl / 2 + 1);
     g->layer = -1;
     g->n = 0;
@@ -1677,6 +1689,7 @@ extern "C" int vg_gkr_destroy(vg_gkr *g)
     cudaFree(g->vu);
     cudaFree(g->heavy_parts);
     cudaFree(g->rg_parts);
+    cudaFree(g->bgt);
     cudaFree(g->rec);
     if (g->rec_host) cudaFreeHost(g->rec_host);
     delete g;
@@ -1929,7 +1942,7 @@ static int tables_ready(vg_gkr *g, long N)
 
 // phase tables by gathering over the layer's edge set (no atomics, no finalize)
 template <int PH>
-static int gather_tables(vg_gkr *g, const EdgeSet &E, long N, const fe *prev)
+static int gather_tables(vg_gkr *g, const EdgeSet &E, long N, const fe *prev, const BetaG &bg)
 {
     vg_ctx *c = g->ctx;
     const EdgeView ev{E.off, E.g, E.o, E.tk};
@@ -1937,7 +1950,7 @@ static int gather_tables(vg_gkr *g, const EdgeSet &E, long N, const fe *prev)
     {
         ProfScope ps(c, PH == 0 ? KF_SCATTER1 : KF_SCATTER2, 10.0 * (double)E.E + 4.0 * (double)N + 32.0 * (double)N);
         k_gather_keys<PH><<<std::min<unsigned>(grid_for(N, GKR_THREADS), 148u * 64u), GKR_THREADS, 0, c->stream>>>(
-            ev, N, g->bg, g->bu, prev, g->vu, out_m, out_v);
+            ev, N, bg, g->bu, prev, g->vu, out_m, out_v);
     }
     VG_LAUNCHED(c);
     const int nheavy = (int)(E.heavy_host.size() / 3);
@@ -1951,7 +1964,7 @@ static int gather_tables(vg_gkr *g, const EdgeSet &E, long N, const fe *prev)
         }
         const int nparts = HEAVY_PARTS;
         ProfScope ps(c, PH == 0 ? KF_SCATTER1 : KF_SCATTER2, 0.0);
-        k_gather_heavy<PH><<<dim3(nparts, H.count), GKR_THREADS, 0, c->stream>>>(ev, H, g->bg, g->bu, prev, g->heavy_parts);
+        k_gather_heavy<PH><<<dim3(nparts, H.count), GKR_THREADS, 0, c->stream>>>(ev, H, bg, g->bu, prev, g->heavy_parts);
         VG_LAUNCHED(c);
         k_heavy_finish<PH><<<H.count, GKR_THREADS, 0, c->stream>>>(H, g->heavy_parts, nparts, g->vu, out_m, out_v);
         VG_LAUNCHED(c);
@@ -1959,7 +1972,7 @@ static int gather_tables(vg_gkr *g, const EdgeSet &E, long N, const fe *prev)
     if (E.n_medium) {
         ProfScope ps(c, PH == 0 ? KF_SCATTER1 : KF_SCATTER2, 0.0);
         k_gather_long<PH><<<std::min<unsigned>(grid_for(E.n_medium * 32, GKR_THREADS), 148u * 64u), GKR_THREADS, 0,
-                            c->stream>>>(ev, E.medium, E.n_medium, g->bg, g->bu, prev, g->vu, out_m, out_v);
+                            c->stream>>>(ev, E.medium, E.n_medium, bg, g->bu, prev, g->vu, out_m, out_v);
         VG_LAUNCHED(c);
     }
     return VG_OK;
@@ -2012,8 +2025,18 @@ extern "C" int vg_gkr_phase1_init(vg_gkr *g, int layer, const vg_fe *r0, const v
     g->bg.s1 = e + 3 * H;
     g->bg.fh = fh;
     g->bg.mask = (1L << fh) - 1;
+    g->bg.save = nullptr;
+    g->bg.tab = nullptr;
+    g->bgt_layer = -1;
     if (D.ph[0].ok) {
-        VG_TRY(gather_tables<0>(g, D.ph[0], N, g->vals[layer - 1]));
+        // the gathers store every gate's beta_g for phase 2 (a gate with a
+        // phase-2 edge has a phase-1 edge: both need its u); every store of
+        // entry x holds beta_g(x), whichever edge made it
+        const bool table = vg_tune_value(c->device, VG_TUNE_BETA_TABLE) != 0;
+        BetaG b1 = g->bg;
+        b1.save = table ? g->bgt : nullptr;
+        VG_TRY(gather_tables<0>(g, D.ph[0], N, g->vals[layer - 1], b1));
+        g->bgt_layer = table ? layer : -1;
         g->cur[0] = g->vals[layer - 1];
         return tables_ready(g, N);
     }
@@ -2228,7 +2251,9 @@ static int phase2_tables(vg_gkr *g, const vg_fe *r_u, int length_u)
     bu.mask = (1L << fh) - 1;
     g->bu = bu;
     if (D.ph[1].ok) {
-        VG_TRY(gather_tables<1>(g, D.ph[1], N, nullptr));
+        BetaG b2 = g->bg;
+        if (g->bgt_layer == layer) b2.tab = g->bgt;
+        VG_TRY(gather_tables<1>(g, D.ph[1], N, nullptr, b2));
         g->cur[0] = g->vals[layer - 1];
         return tables_ready(g, N);
     }

@@ -27,6 +27,7 @@ const Range RANGES[VG_TUNE_COUNT] = {
     {0, 1L << 24, 0, false},                // LEAF_WARP_MAX
     {1, 2, 2, false},                       // ROUND_FUSE
     {0, 2, 0, false},                       // LEAF_ROT
+    {0, 1, 1, false},                       // BETA_TABLE
 };
 
 std::atomic<long> g_tune[MAX_DEVICES][VG_TUNE_COUNT];

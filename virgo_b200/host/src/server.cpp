@@ -82,6 +82,7 @@ extern "C" size_t vg_job_footprint(int d, const long *n)
     b += (gates + (size_t)maxw) * 9;        // gate records (type, u, v)
     b += 2 * (gates + (size_t)maxw) * 14;   // edge sets of both phases (gate, wire, type) + offsets
     b += (size_t)maxw * 16 * 9 / 2 * 2;     // sumcheck tables, ping-pong
+    b += (size_t)maxw * 16;                 // beta_g by gate
     b += 4 * 65 * S * 16;                   // l, h, q and virtual-oracle codewords
     b += 65 * S * 16 + 4 * S * 32;          // FRI levels, Merkle trees
     b += (size_t)64 << 20;                  // staging, scratch, twiddles
