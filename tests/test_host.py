@@ -236,3 +236,65 @@ def test_sha256_compression_and_circuit():
     for t, u, v in L[1:]:
         vals = O.eval_layer(t, u, v, vals)
     assert not vals.any()
+
+
+def _inc_table(name):
+    """A brace-initialised table of numbers from csrc/hash_code.inc."""
+    import re
+    src = open(os.path.join(ROOT, "virgo_b200", "csrc", "hash_code.inc")).read()
+    body = re.search(r"#define %s \{([^}]*)\}" % name, src).group(1)
+    return [int(x.strip().rstrip("u"), 0) for x in body.replace("\\", "").split(",") if x.strip()]
+
+
+def test_warp_keccak_lane_tables_give_sha3():
+    """The one-warp-per-chain Keccak (lane x + 5y holds A[x, y]; theta from
+    five column shuffles and two neighbour shuffles, rho on the own word, pi
+    through the PI_SRC lane, chi from two neighbour shuffles) emulated lane
+    by lane with the generated tables equals hashlib's SHA3-256; the
+    multiply form of a rotation equals the shift form."""
+    import hashlib
+    M64 = (1 << 64) - 1
+    rho, pi_src = _inc_table("VG_KECCAK_RHO"), _inc_table("VG_KECCAK_PI_SRC")
+    rcl, rch = _inc_table("VG_KECCAK_RC_LO"), _inc_table("VG_KECCAK_RC_HI")
+    assert len(rho) == len(pi_src) == 25 and sorted(pi_src) == list(range(25))
+
+    def rotl(v, n):
+        return ((v << n) | (v >> (64 - n))) & M64 if n else v
+
+    def shfl(vals, src):
+        return [vals[s] for s in src]
+
+    def perm(A):
+        A = A + [0] * 7
+        x = [l % 5 for l in range(32)]
+        y = [l // 5 for l in range(32)]
+        own = lambda f: [f(l) if l < 25 else l for l in range(32)]  # noqa: E731
+        for r in range(24):
+            C = [0] * 32
+            for yy in range(5):
+                s = shfl(A, own(lambda l: x[l] + 5 * yy))
+                C = [c ^ v for c, v in zip(C, s)]
+            cm = shfl(C, own(lambda l: (x[l] + 4) % 5 + 5 * y[l]))
+            cp = shfl(C, own(lambda l: (x[l] + 1) % 5 + 5 * y[l]))
+            A = [a ^ m ^ rotl(p, 1) for a, m, p in zip(A, cm, cp)]
+            R = [rotl(A[l], rho[l]) if l < 25 else 0 for l in range(32)]
+            B = shfl(R, own(lambda l: pi_src[l]))
+            b1 = shfl(B, own(lambda l: (x[l] + 1) % 5 + 5 * y[l]))
+            b2 = shfl(B, own(lambda l: (x[l] + 2) % 5 + 5 * y[l]))
+            A = [b ^ (~p & q & M64) for b, p, q in zip(B, b1, b2)]
+            A[0] ^= rcl[r] | (rch[r] << 32)
+        return A[:25]
+
+    rng = np.random.default_rng(3)
+    for _ in range(4):
+        msg = rng.integers(0, 256, 64, dtype=np.uint8).tobytes()
+        A = [int.from_bytes(msg[8 * i:8 * i + 8], "little") for i in range(8)] + [0] * 17
+        A[8], A[16] = 0x06, 1 << 63
+        out = perm(A)
+        assert b"".join(out[i].to_bytes(8, "little") for i in range(4)) == hashlib.sha3_256(msg).digest()
+    # VG_MROT_LO / VG_MROT_HI: lo * 2^n + umulhi(hi, 2^n) is the rotated low half
+    for lo, hi in rng.integers(0, 1 << 32, (200, 2), dtype=np.uint64).tolist():
+        for n in range(32):
+            v = rotl((hi << 32) | lo, n)
+            assert ((lo << n) & 0xFFFFFFFF) + ((hi << n) >> 32) == v & 0xFFFFFFFF
+            assert ((hi << n) & 0xFFFFFFFF) + ((lo << n) >> 32) == v >> 32
