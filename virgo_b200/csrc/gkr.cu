@@ -613,12 +613,16 @@ static inline size_t rg_parts_len(long N) { return ((size_t)N / RG_CHUNK + 1 + 2
 // of bank conflicts
 __device__ __forceinline__ int rg_ix(long i) { return (int)(i + (i >> 3)); }
 constexpr int RG_TABLE = RG_CHUNK + RG_CHUNK / 8;
+// dynamic shared memory of a group CTA (elements): three tables, per-warp
+// round sums, the folded pairs of the three-thread steps
+constexpr int RG_SMEM_FE = 3 * RG_TABLE + RG_MAX * (RG_THREADS / 32) * 3 + 6 * (RG_THREADS / 3);
 struct RoundGroup {
     int chunk_log;      // log2 of a CTA's entries after its first step (at most RG_LOG)
     int nsteps;         // rounds in this launch
     int first_nofold;   // the first round has no fold (the round right after a phase init)
     int slot0;          // record of the first round; the others follow
     int last6;          // write the final pair (the table ends at 2 entries) into the last record
+    int split3;         // steps with at most RG_THREADS / 3 pairs run three threads per pair
     fe r[RG_MAX];       // fold challenge of each round
 };
 
@@ -662,6 +666,7 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
     extern __shared__ fe smem[];
     fe *sV = smem, *sA = smem + RG_TABLE, *sM = smem + 2 * RG_TABLE;
     fe *wsum = smem + 3 * RG_TABLE;   // [RG_MAX][warps][3]
+    fe *stage = wsum + RG_MAX * (RG_THREADS / 32) * 3;   // [pair][6] of the three-thread steps
     __shared__ bool last;
     constexpr int NW = RG_THREADS / 32;
     const int t = threadIdx.x;
@@ -703,9 +708,47 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
         // further steps in shared memory: fold m -> m/2, sums over m/4 pairs
         for (int st = 1; st < G.nsteps; ++st) {
             const fe r = G.r[st];
+            const long npairs = m / 4;
+            if (G.split3 && 3 * npairs <= RG_THREADS) {
+                // few pairs: three threads per pair, one per table, each
+                // folding its table's two entries; the folded pairs meet in
+                // `stage`, and each thread adds one product's share of the
+                // three sums (p0 = m0 v0, p1 = m1 v1, p2 = (m1 - m0)(v1 - v0))
+                const int pp = t / 3, role = t - 3 * pp;
+                const bool act = pp < npairs;
+                fe *tab = role == 0 ? sV : (role == 1 ? sA : sM);
+                fe f0 = vg::fe_zero(), f1 = vg::fe_zero();
+                __syncthreads();
+                if (act) {
+                    f0 = rg_fold(tab[rg_ix(4 * pp)], tab[rg_ix(4 * pp + 1)], r);
+                    f1 = rg_fold(tab[rg_ix(4 * pp + 2)], tab[rg_ix(4 * pp + 3)], r);
+                    stage[6 * pp + 2 * role] = f0;
+                    stage[6 * pp + 2 * role + 1] = f1;
+                }
+                __syncthreads();   // every read of this step's tables is done
+                fe acc[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+                if (act) {
+                    tab[rg_ix(2 * pp)] = f0;
+                    tab[rg_ix(2 * pp + 1)] = f1;
+                    const fe *q = stage + 6 * pp;   // v0 v1 a0 a1 m0 m1
+                    if (role == 0) {
+                        const fe p0 = q[4] * q[0];
+                        acc[1] = -p0;
+                        acc[2] = p0 + q[2];
+                    } else if (role == 1) {
+                        acc[1] = q[5] * q[1] + (q[3] - q[2]);
+                    } else {
+                        const fe p2 = (q[5] - q[4]) * (q[1] - q[0]);
+                        acc[0] = p2;
+                        acc[1] = -p2;
+                    }
+                }
+                m >>= 1;
+                rg_warp_add(acc, wsum, st, 3 * npairs);
+                continue;
+            }
             fe acc[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
             fe v0, v1, a0, a1, m0v, m1v;
-            const long npairs = m / 4;
             __syncthreads();
             const bool act = t < npairs;   // m / 4 <= RG_CHUNK / 4 = RG_THREADS: at most one pair per thread
             if (act) {
@@ -2097,7 +2140,7 @@ static int rg_smem_attribute(int dev)
     if (dev >= (int)done.size()) done.resize(dev + 1, false);
     if (!done[dev]) {
         VG_CHECK_CUDA(cudaFuncSetAttribute(k_round_group, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)((3 * RG_TABLE + RG_MAX * (RG_THREADS / 32) * 3) * sizeof(fe))));
+                                          (int)(RG_SMEM_FE * sizeof(fe))));
         done[dev] = true;
     }
     return VG_OK;
@@ -2206,13 +2249,14 @@ static int flush_rounds(vg_gkr *g)
     const long n_in = g->pend_n0;
     const long cin = G.first_nofold ? std::min(n_in, g->pend_chunk) : std::min(n_in, 2 * g->pend_chunk);
     const long nchunks = n_in / cin;
-    // CTAs loop over chunks: at most 3 resident per SM (60 KB of shared memory each)
+    // CTAs loop over chunks: at most 3 resident per SM (68 KB of shared memory each)
     const long grid = std::min(nchunks, 148L * 3L);
     const long m_final = (G.first_nofold ? cin : cin / 2) >> (G.nsteps - 1);
     G.last6 = (nchunks == 1 && m_final == 2) ? 1 : 0;
+    G.split3 = vg_tune_value(c->device, VG_TUNE_GROUP_SPLIT) != 0 ? 1 : 0;
     const bool folds = !(G.first_nofold && G.nsteps == 1);
     fe *y[3] = {g->buf[g->next_buf][0], g->buf[g->next_buf][1], g->buf[g->next_buf][2]};
-    const size_t smem = (3 * RG_TABLE + RG_MAX * (RG_THREADS / 32) * 3) * sizeof(fe);
+    const size_t smem = RG_SMEM_FE * sizeof(fe);
     VG_TRY(rg_smem_attribute(c->device));
     {
         // every round of the group: the first reads 3 tables of n_in, writes nothing more than the chunk tails
