@@ -426,7 +426,7 @@ enum {
                                   phase-1 builds of the same layer wrote (1), or form it again
                                   from the eq half tables (0) */
     VG_TUNE_GROUP_SPLIT = 9,   /* round groups: steps with few pairs left spread each pair over three
-                                  threads, one per table (1), or one thread per pair (0) */
+                                  threads, one per table (1), or keep one thread per pair (0) */
     VG_TUNE_COUNT = 10
 };
 int vg_tune_get(int device, int key, long *value);

@@ -28,7 +28,7 @@ const Range RANGES[VG_TUNE_COUNT] = {
     {1, 2, 2, false},                       // ROUND_FUSE
     {0, 2, 0, false},                       // LEAF_ROT
     {0, 1, 1, false},                       // BETA_TABLE
-    {0, 1, 1, false},                       // GROUP_SPLIT
+    {0, 1, 0, false},                       // GROUP_SPLIT
 };
 
 std::atomic<long> g_tune[MAX_DEVICES][VG_TUNE_COUNT];
