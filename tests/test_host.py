@@ -298,3 +298,23 @@ def test_warp_keccak_lane_tables_give_sha3():
             v = rotl((hi << 32) | lo, n)
             assert ((lo << n) & 0xFFFFFFFF) + ((hi << n) >> 32) == v & 0xFFFFFFFF
             assert ((hi << n) & 0xFFFFFFFF) + ((lo << n) >> 32) == v >> 32
+
+
+def test_bench_roofline_fields():
+    """bench.py's roofline object from per-family profiles: the dominant
+    family, its fraction of the HBM peak, the large launches apart; JSON."""
+    import sys
+    sys.path.insert(0, ROOT)
+    import bench
+    fam = {"sumcheck_round": {"launches": 84.0, "ms": 5.3, "bytes": 7.5e9},
+           "ntt_pass": {"launches": 22.0, "ms": 1.5, "bytes": 8.5e8}}
+    large = {"launches_per_proof": 16.0, "ms": 2.3, "bytes": 6.0e9}
+    r = bench.roofline(fam, 6650.0, "fallback", large)
+    assert r["kernel"] == "sumcheck_round" and r["bound"] == "hbm"
+    assert abs(r["achieved"] - 7.5e9 / 5.3e-3 / 1e9) < 0.1 and 0 < r["frac"] < 1
+    assert r["large_launches"]["launches_per_proof"] == 16.0 and r["large_launches"]["frac"] > r["frac"]
+    assert r["traffic"] is not None and r["alu_pipe"]["frac_large_launches"] > 0
+    json.dumps(r)
+    assert bench.roofline(fam, 6650.0, "fallback", None)["large_launches"] is None
+    hbm, kind = bench.peaks()
+    assert hbm > 0 and kind in ("measured", "fallback")
