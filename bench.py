@@ -31,6 +31,7 @@ from concurrent.futures import ThreadPoolExecutor
 import json
 import os
 import re
+import shutil
 import statistics
 import subprocess
 import sys
@@ -83,7 +84,9 @@ def make_workload(args):
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """nvidia-smi samples during the timed region (clocks and throttle reasons)."""
+    """Clocks and throttle reasons during a timed region: one background
+    `nvidia-smi --query-gpu=... -lms 200` process for the whole region
+    (started before it, stopped after it), parsed afterwards."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -92,33 +95,37 @@ class ClockSampler:
     def __init__(self, device):
         self.device = device
         self.rows = []
-        self.stop = threading.Event()
-
-    def _run(self):
-        while not self.stop.is_set():
-            try:
-                out = subprocess.run(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
-                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
-                for line in out.stdout.strip().splitlines():
-                    self.rows.append([x.strip() for x in line.split(",")])
-            except Exception:
-                pass
-            self.stop.wait(0.2)
+        self.proc = None
 
     def __enter__(self):
-        self.t = threading.Thread(target=self._run, daemon=True)
-        self.t.start()
+        self.out = tempfile.TemporaryFile(mode="w+")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)   # first sample before the region starts
         return self
 
     def __exit__(self, *a):
-        self.stop.set()
-        self.t.join(timeout=10)
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=10)
+            except Exception:
+                self.proc.kill()
+                self.proc.wait()
+        self.out.seek(0)
+        for line in self.out.read().strip().splitlines():
+            self.rows.append([x.strip() for x in line.split(",")])
+        self.out.close()
 
     def summary(self):
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        sm = [float(r[1]) for r in self.rows if len(r) > 2 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 2 and r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = sorted({names[k] for r in self.rows for k in range(4) if len(r) > 5 + k and r[5 + k] == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
@@ -135,16 +142,23 @@ def ref_prover_seconds(workdir):
     return ev + prove, {"evaluate_s": ev, "gkr_s": gkr, "prove_time_s": prove, "fft_gkr_s": fft}
 
 
+def _ref_proof_dir():
+    d = tempfile.mkdtemp(prefix="virgo_ref_")
+    os.symlink(FFT_BIN, os.path.join(d, "fft_gkr"))   # the reference runs ./fft_gkr beside every proof
+    return d
+
+
+def _ref_launch(circuit, meta, seed):
+    d = _ref_proof_dir()
+    p = subprocess.Popen([REF_BIN, circuit, meta, os.path.join(d, "res.txt"), str(seed)], cwd=d,
+                         stdout=open(os.path.join(d, "out.txt"), "w"), stderr=open(os.path.join(d, "err.txt"), "w"))
+    return p, d
+
+
 def run_reference_proofs(circuit, meta, count, seed0):
     """`count` concurrent single-threaded reference proofs; returns per-proof
     prover seconds and stage details."""
-    procs = []
-    for k in range(count):
-        d = tempfile.mkdtemp(prefix="virgo_ref_")
-        os.symlink(FFT_BIN, os.path.join(d, "fft_gkr"))
-        p = subprocess.Popen([REF_BIN, circuit, meta, os.path.join(d, "res.txt"), str(seed0 + k)], cwd=d,
-                             stdout=open(os.path.join(d, "out.txt"), "w"), stderr=open(os.path.join(d, "err.txt"), "w"))
-        procs.append((p, d))
+    procs = [_ref_launch(circuit, meta, seed0 + k) for k in range(count)]
     res = []
     for p, d in procs:
         p.wait()
@@ -152,10 +166,64 @@ def run_reference_proofs(circuit, meta, count, seed0):
         secs, detail = ref_prover_seconds(d)
         detail["verified"] = ok
         res.append((secs, detail))
+        shutil.rmtree(d, ignore_errors=True)
     return res
 
 
+def run_reference_pool(circuit, meta, n_warm, n_timed, width, seed0):
+    """A pool of `width` concurrent single-threaded reference processes, one
+    proof each: first n_warm warm-up proofs, then n_timed timed proofs; once
+    every timed proof has started, filler proofs keep the pool full until the
+    last timed proof ends (fillers are then stopped and not counted), so every
+    timed proof runs beside width - 1 others.  Returns the timed proofs'
+    (prover seconds, detail) and the wall-clock span from the first timed
+    start to the last timed end."""
+    pending = [("warm", seed0 + k) for k in range(n_warm)] + \
+              [("timed", seed0 + n_warm + k) for k in range(n_timed)]
+    running = []            # (kind, popen, dir, t_start)
+    timed, t_first, t_last = [], None, None
+    timed_left = n_timed
+    filler_seed = seed0 + n_warm + n_timed
+    fillers = 0
+    while timed_left:
+        while len(running) < width and (pending or timed_left):
+            if pending:
+                kind, seed = pending.pop(0)
+            else:
+                kind, seed = "filler", filler_seed
+                filler_seed += 1
+                fillers += 1
+            p, d = _ref_launch(circuit, meta, seed)
+            t0 = time.perf_counter()
+            if kind == "timed" and t_first is None:
+                t_first = t0
+            running.append((kind, p, d, t0))
+        time.sleep(0.02)
+        still = []
+        for kind, p, d, t0 in running:
+            if p.poll() is None:
+                still.append((kind, p, d, t0))
+                continue
+            if p.returncode != 0:
+                raise RuntimeError("reference proof failed (rc %d) in %s" % (p.returncode, d))
+            if kind == "timed":
+                t_last = time.perf_counter()
+                secs, detail = ref_prover_seconds(d)
+                detail["verified"] = "Pass" in open(os.path.join(d, "out.txt")).read()
+                timed.append((secs, detail))
+                timed_left -= 1
+            shutil.rmtree(d, ignore_errors=True)
+        running = still
+    for kind, p, d, t0 in running:   # warm-up stragglers and fillers: this process's own children
+        p.kill()
+        p.wait()
+        shutil.rmtree(d, ignore_errors=True)
+    return timed, t_last - t_first, fillers
+
+
 def write_circuit_text(layers, circuit, meta):
+    """The circuit in the reference text format through the library's writer
+    (fast; used by this arm's cpu_baseline)."""
     import virgo_b200 as vb
     L = vb.lib()
     L.vg_circuit_write_text.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
@@ -168,38 +236,82 @@ def write_circuit_text(layers, circuit, meta):
     vb.check(L.vg_circuit_write_text(d, ns.ctypes.data, tys, us, vs, circuit.encode(), meta.encode()), "write text")
 
 
-def reference_arm(args, layers):
-    cores = os.cpu_count() or 1
+def bench_config(args, layers):
+    """The workload description, identical on both arms."""
+    return {"workload": WORKLOAD if args.workload == "matmul256" else args.workload,
+            "circuit_gates": int(sum(len(t) for t, _, _ in layers)), "input_log2": 17 if args.workload == "matmul256" else None,
+            "hash": "sha3-256", "proofs_per_step": args.batch,
+            "l2": "inputs larger than L2 (circuit + tables > 1 GB per proof), no flush needed"}
+
+
+def host_cores():
     try:
-        mem_gb = os.sysconf("SC_PAGE_SIZE") * os.sysconf("SC_PHYS_PAGES") / 2 ** 30
+        return len(os.sched_getaffinity(0))
     except Exception:
-        mem_gb = 64
+        return os.cpu_count() or 1
+
+
+def mem_available_gb():
+    try:
+        with open("/proc/meminfo") as f:
+            for line in f:
+                if line.startswith("MemAvailable:"):
+                    return int(line.split()[1]) / 2 ** 20
+    except Exception:
+        pass
+    return 64.0
+
+
+def reference_arm(args, layers):
+    """The reference prover (compiled from its own sources, unmodified apart
+    from a main that seeds rand()) on the host cores: a step is
+    `proofs_per_step` proofs, as on the GPU arm; W warm-up steps, then K timed
+    steps, through a pool of single-threaded processes as wide as the cores
+    (and memory) allow.  value = pool width x mean(1 / prover seconds) over
+    the timed proofs, each timed by the reference's own timers (Prove Time,
+    which includes the fft_gkr side proof, plus evaluate; zk_verifier.cpp
+    :1244-1248); ms_per_step = wall-clock span of the timed proofs / K.  No
+    library of this repository is loaded: the circuit file is written by the
+    pure-numpy writer."""
+    from virgo_b200 import circuits
     if not os.path.exists(REF_BIN):
         return {"impl": "reference", "unavailable": "reference prover not compiled (oracle/_ref missing)"}
+    cores = host_cores()
+    per_proof_gb = 4.5 if args.workload == "matmul256" else 1.0   # measured peak RSS 3.3 GB, plus margin
+    width = max(1, min(cores, int(0.85 * mem_available_gb() // per_proof_gb)))
     tmp = tempfile.mkdtemp(prefix="virgo_circ_")
     circuit, meta = os.path.join(tmp, "c.txt"), os.path.join(tmp, "m.txt")
-    write_circuit_text(layers, circuit, meta)
-    per_proof_gb = 5.0 if args.workload == "matmul256" else 1.0
-    width = max(1, min(cores, int(mem_gb // per_proof_gb), args.steps + args.warmup))
-    # warm-up proofs run in the same wave when cores allow; only the last K count
-    t0 = time.time()
-    results = run_reference_proofs(circuit, meta, width, seed0=1)
-    measured = results[-args.steps:] if len(results) > args.steps else results
-    wall = time.time() - t0
-    secs = [s for s, _ in measured]
-    value = sum(1.0 / s for s in secs)
+    circuits.write_text(layers, circuit, meta)
+    try:
+        timed, span, fillers = run_reference_pool(circuit, meta, args.warmup * args.batch, args.steps * args.batch,
+                                                  width, seed0=1)
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+    secs = [x for x, _ in timed]
+    value = width * statistics.mean(1.0 / x for x in secs)
+    stage_means = {k: statistics.mean(d[k] for _, d in timed) for k in ("evaluate_s", "gkr_s", "prove_time_s", "fft_gkr_s")}
     return {
         "metric": METRIC, "value": value, "unit": "proofs/s", "impl": "reference",
-        "n_gpus": args.gpus, "steps": len(measured), "warmup": len(results) - len(measured),
-        "ms_per_step": 1000.0 * statistics.mean(secs), "higher_is_better": True, "scaling": "weak",
+        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * span / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "u64 (F_{p^2}, p = 2^61 - 1)", "data": "synthetic (seeded)",
-        "config": {"workload": WORKLOAD if args.workload == "matmul256" else args.workload, "circuit_gates": int(sum(len(t) for t, _, _ in layers)),
-                   "concurrent_proofs": width, "input_log2": 17, "hash": "sha3-256"},
+        "config": bench_config(args, layers),
         "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": width, "kind": "reference",
-                         "sample": "%d concurrent single-threaded reference proofs of the workload, each timed by "
-                                   "its own Prove Time (fft_gkr side proof included) plus evaluate" % width},
+                         "sample": "%d timed proofs of the workload (%d steps x %d), %d single-threaded reference "
+                                   "processes at a time on %d host cores, each proof timed by its own Prove Time "
+                                   "(fft_gkr side proof included) plus evaluate"
+                                   % (len(timed), args.steps, args.batch, width, cores)},
         "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "reference_detail": [d for _, d in measured], "wall_s": wall,
+        "reference_pool": {"processes": width, "host_cores": cores, "proofs_timed": len(timed),
+                           "proofs_warmup": args.warmup * args.batch, "fillers_stopped": fillers,
+                           "timed_span_s": round(span, 2),
+                           "wall_proofs_s": round(len(timed) / span, 4),
+                           "wall_note": "timed proofs / wall-clock span; each process also reads the circuit text "
+                                        "and runs the verifier, which the prover timers exclude",
+                           "all_verified": all(d["verified"] for _, d in timed),
+                           "mean_stage_s": {k: round(v, 4) for k, v in stage_means.items()},
+                           "build": "reference sources compiled unchanged with g++ -O3 -march=x86-64-v3 (its CMake "
+                                    "uses -march=native; x86-64-v3 keeps AVX2/BMI2 and runs on any such host)"},
     }
 
 
@@ -608,8 +720,10 @@ def roofline(fam, hbm_peak, peak_kind, large=None):
     return {"bound": "hbm", "kernel": top, "achieved": round(gbs, 1), "peak": hbm_peak, "unit": "GB/s",
             "frac": round(gbs / hbm_peak, 4),
             "traffic": round(per_launch * traffic) if traffic else None,
-            "traffic_note": ("ncu dram read+write / algorithmic bytes on full-size launches (profiles/), times the "
-                             "average launch's algorithmic bytes") if traffic else None,
+            "traffic_source": ("profile-derived constant, not measured in this run: the ratio of ncu "
+                               "dram__bytes_read.sum + dram__bytes_write.sum to algorithmic bytes on a full-size "
+                               "launch (profiles/k_round_matmul256.txt, %.3f), times this run's average "
+                               "algorithmic bytes per launch" % traffic) if traffic else None,
             "peak_source": peak_kind, "launches_per_proof": f["launches"],
             "avg_launch_us": round(1000.0 * f["ms"] / f["launches"], 2), "bytes_per_launch": per_launch,
             "large_launches": ({"achieved": round(large["bytes"] / (large["ms"] / 1000.0) / 1e9, 1),
@@ -619,10 +733,11 @@ def roofline(fam, hbm_peak, peak_kind, large=None):
                                 "note": "the round launches that move at least 100 MB each (tables of 2^21 "
                                         "entries and up), same events"}
                                if (large and top == "sumcheck_round" and large["ms"] > 0) else None),
-            "alu_pipe": {"frac_large_launches": 0.75, "frac_round_group": 0.33,
-                         "source": "ncu sm__inst_executed_pipe_alu, pct of peak: the 2^24-entry fold round "
-                                   "(profiles/k_round_matmul256.txt) and a 64-CTA round group "
-                                   "(profiles/k_round_group_matmul256.txt)"},
+            "alu_pipe_profile": {"frac_large_launches": 0.75, "frac_round_group": 0.33,
+                                 "source": "profile-derived constants, not measured in this run: ncu "
+                                           "sm__inst_executed_pipe_alu, pct of peak, of the 2^24-entry fold round "
+                                           "(profiles/k_round_matmul256.txt) and a 64-CTA round group "
+                                           "(profiles/k_round_group_matmul256.txt)"},
             "note": "CUDA events on the launching stream; back-to-back launches share one event, so a "
                     "launch's time runs from the end of the one before it; the large launches are bound by "
                     "the integer ALU pipe and HBM together (ALU 75%, DRAM 65%), the round groups of the "
@@ -673,11 +788,8 @@ def main():
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1000.0 * r["t_batch"] / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "u64 (F_{p^2}, p = 2^61 - 1)", "data": "synthetic (seeded)",
-            "config": {"workload": WORKLOAD if args.workload == "matmul256" else args.workload,
-                       "circuit_gates": int(sum(len(t) for t, _, _ in layers)), "input_log2": 17,
-                       "hash": "sha3-256", "proofs_per_step": args.batch,
-                       "parallelism": ("replicas x%d, " % world if world > 1 else "") + "%d proofs in flight" % args.batch,
-                       "l2": "inputs larger than L2 (circuit + tables > 1 GB per proof)"},
+            "config": bench_config(args, layers),
+            "parallelism": ("replicas x%d, " % world if world > 1 else "") + "%d proofs in flight" % args.batch,
             "plain": {"value": args.steps * world / r["t_plain"], "unit": "proofs/s",
                       "ms_per_proof": 1000.0 * r["t_plain"] / args.steps,
                       "note": "one proof at a time on one stream, CUDA-event device time"},

@@ -4,7 +4,7 @@
  * The drop-in C++ classes (zk_prover, poly_commit::poly_commit_prover, the
  * fri:: functions, fast_fourier_transform, create_tree, my_hhash; headers under
  * virgo_b200/host/include) are thin wrappers over these entry points; a caller
- * in any language can bind them directly.
+ * in any language can bind them directly (ctypes, cgo, JNI, a C++ link).
  *
  * Conventions
  *  - Every entry point returns VG_OK (0) or a VG_ERR_* code; vg_last_error()
@@ -178,12 +178,16 @@ int vg_mle_eval(vg_ctx *ctx, const vg_fe *vals, long n, const vg_fe *r, int log_
  * counterpart in the reference.  It allocates nothing: its scratch (eq tables,
  * block partials) is one file-scope device array of 268,160 bytes that every
  * GPU loading this library keeps until exit.  vals device (n >= 2^log_n), r and
- * out host; log_n <= 26, larger is rejected with VG_ERR_ARG.  The first call on
- * a device looks up the array's address (cudaGetSymbolAddress, that device
- * current): make it before any stream capture.  All calls share the array,
- * which keeps the last call's contents (each call writes what it reads);
- * calls that overlap on the GPU race.  Runs on the legacy default stream and
- * returns after *out is written. */
+ * out host; log_n in [0, 26], anything else is rejected with VG_ERR_ARG.  The
+ * first call on a device looks up the array's address (cudaGetSymbolAddress,
+ * that device current) and caches it: make it before any stream capture, and
+ * do not use the entry point on a device again after cudaDeviceReset of it.
+ * All calls on a device share that device's array, which keeps the last
+ * call's contents (each call writes what it reads); calls on one device that
+ * overlap on the GPU race.  Runs on the legacy default stream, which does NOT
+ * wait for non-blocking streams such as this library's context streams:
+ * synchronise the stream that produced vals first (vg_ctx_sync).  Returns
+ * after *out is written. */
 int vg_mle_eval_noalloc(const vg_fe *vals, long n, const vg_fe *r, int log_n, vg_fe *out);
 /* Phase-1 bookkeeping of layer `layer` (zk_prover::sumcheck_phase1_init,
  * zk_prover.cpp:375-592): beta_g = alpha*eq(r0,g) + beta*eq(r1,g) over

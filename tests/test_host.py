@@ -313,8 +313,64 @@ def test_bench_roofline_fields():
     assert r["kernel"] == "sumcheck_round" and r["bound"] == "hbm"
     assert abs(r["achieved"] - 7.5e9 / 5.3e-3 / 1e9) < 0.1 and 0 < r["frac"] < 1
     assert r["large_launches"]["launches_per_proof"] == 16.0 and r["large_launches"]["frac"] > r["frac"]
-    assert r["traffic"] is not None and r["alu_pipe"]["frac_large_launches"] > 0
+    assert r["traffic"] is not None and r["alu_pipe_profile"]["frac_large_launches"] > 0
     json.dumps(r)
     assert bench.roofline(fam, 6650.0, "fallback", None)["large_launches"] is None
     hbm, kind = bench.peaks()
     assert hbm > 0 and kind in ("measured", "fallback")
+
+
+def test_text_writer_matches_library_writer(built, tmp_path):
+    """The pure-numpy text writer (used where no library of this repository
+    may be loaded) writes the same bytes as vg_circuit_write_text, negative
+    values and 32-bit inputs included."""
+    for k, L in enumerate([circuits.mixed_gates(4, log_width=5), circuits.matmul_addtree(8, 32, seed=2),
+                           circuits.random_layered([5, 6, 4], seed=3)]):
+        L = [(t, u.copy(), v.copy()) for t, u, v in L]
+        if k == 0:
+            L[0][1][:4] = [-1, -(1 << 31), (1 << 32) - 1, -123456789012]
+        a, am = str(tmp_path / "a.txt"), str(tmp_path / "am.txt")
+        b, bm = str(tmp_path / "b.txt"), str(tmp_path / "bm.txt")
+        circuits.write_text(L, a, am)
+        d = len(L)
+        ns = np.array([len(t) for t, _, _ in L], np.int64)
+        arrs = [(np.ascontiguousarray(t, np.uint8), np.ascontiguousarray(u, np.int64),
+                 np.ascontiguousarray(v, np.int64)) for t, u, v in L]
+        tys, us, vs = (ctypes.c_void_p * d)(), (ctypes.c_void_p * d)(), (ctypes.c_void_p * d)()
+        for i, (t, u, v) in enumerate(arrs):
+            tys[i], us[i], vs[i] = t.ctypes.data, u.ctypes.data, v.ctypes.data
+        built.vg_circuit_write_text.argtypes = [ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+                                                ctypes.c_void_p, ctypes.c_char_p, ctypes.c_char_p]
+        vb.check(built.vg_circuit_write_text(d, ns.ctypes.data, tys, us, vs, b.encode(), bm.encode()), "write")
+        assert open(a, "rb").read().split() == open(b, "rb").read().split()
+        assert open(am).read() == open(bm).read()
+    x = np.array([0, -1, 9, 10, 9999, 10000, -10 ** 17 + 1, 10 ** 17 - 1, 1 << 33], np.int64)
+    assert circuits._decimal_bytes(x, 32).decode().split() == [str(int(v)) for v in x]
+
+
+def test_reference_pool_keeps_width_and_counts_timed(tmp_path, monkeypatch):
+    """The reference arm's process pool: warm-up proofs first, then the timed
+    ones; fillers keep it full until the last timed proof ends and are then
+    stopped; only timed proofs are returned, each with its own timers.  A
+    stand-in script plays the reference binary (same output lines)."""
+    import sys
+    import time
+    sys.path.insert(0, ROOT)
+    import bench
+    fake = tmp_path / "fake_ref.sh"
+    fake.write_text("#!/bin/sh\n"
+                    "echo \"total evaluation time: 0.01 seconds.\" >&2\n"
+                    "echo \"GKR Prove Time 0.05\" >&2\n"
+                    "echo \"Prove Time 0.2\" >&2\n"
+                    "echo \"x y 0.02\" > log_fftgkr.txt\n"
+                    "sleep 0.3\n"
+                    "echo Pass\n")
+    fake.chmod(0o755)
+    monkeypatch.setattr(bench, "REF_BIN", str(fake))
+    monkeypatch.setattr(bench, "FFT_BIN", str(fake))
+    t0 = time.perf_counter()
+    timed, span, fillers = bench.run_reference_pool("c.txt", "m.txt", n_warm=3, n_timed=5, width=3, seed0=1)
+    assert len(timed) == 5 and all(d["verified"] for _, d in timed)
+    assert all(abs(s - 0.21) < 1e-9 for s, _ in timed)
+    assert 0 < span < time.perf_counter() - t0
+    assert fillers >= 1   # 8 proofs on 3 slots: the last wave is topped up

@@ -99,7 +99,7 @@ def test_oracle_matches_reference_routines():
     for lo in range(0, 13):
         for lc in range(0, lo + 1):
             if lo == 2 and lc == 2:
-                continue   # reference defect at order 4, documented in DESIGN.md
+                continue   # reference defect: its size-4 FFT returns stale scratch (RS_polynomial.cpp:125-146)
             co = O.fe_random(rng_seed, 1 << lc)
             rng_seed += 1
             out = np.zeros((1 << lo, 2), np.uint64)

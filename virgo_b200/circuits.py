@@ -117,20 +117,56 @@ def mixed_gates(seed: int, log_width: int = 6) -> list:
     return layers
 
 
+_DIGITS4 = np.array([list(b"%04d" % i) for i in range(10000)], np.uint8)
+_POW10 = np.array([10 ** k for k in range(1, 19)], np.int64)
+
+
+def _decimal_bytes(vals: np.ndarray, sep: int) -> bytes:
+    """Integers (|x| < 10^18) as ASCII decimal, each followed by the byte
+    `sep`, formatted with array operations: one fixed-width slot per number
+    filled four digits at a time from a table, then the leading zeros masked
+    out."""
+    x = np.ascontiguousarray(vals, dtype=np.int64)
+    if x.size == 0:
+        return b""
+    neg = x < 0
+    a = np.abs(x)
+    ndig = np.searchsorted(_POW10, a, side="right") + 1          # digits of |x|
+    groups = (int(ndig.max()) + 3) // 4
+    width = 4 * groups + 1                                        # sign + digits
+    slots = np.empty((x.size, width + 1), np.uint8)
+    slots[:, 0] = 45                                              # '-'
+    slots[:, width] = sep
+    q = a
+    for g in range(groups - 1, -1, -1):
+        q, r = np.divmod(q, 10000)
+        slots[:, 1 + 4 * g:5 + 4 * g] = _DIGITS4[r]
+    keep = np.empty((x.size, width + 1), bool)
+    keep[:, 1:width] = np.arange(width - 1)[None, :] >= (width - 1 - ndig)[:, None]
+    keep[:, 0] = neg
+    keep[:, width] = True
+    return slots[keep].tobytes()
+
+
 def write_text(layers: list, circuit_path: str, meta_path: str) -> None:
-    """Writes the reference text format (one line per layer)."""
-    with open(circuit_path, "w") as f:
-        f.write("%d\n" % len(layers))
+    """Writes the reference text format (one line per layer: the gate count,
+    then type, gate index, u, v of every gate), pure Python and numpy."""
+    with open(circuit_path, "wb") as f:
+        f.write(b"%d\n" % len(layers))
         for ty, u, v in layers:
             n = len(ty)
-            rows = np.empty((n, 4), dtype=np.int64)
-            rows[:, 0] = ty
-            rows[:, 1] = np.arange(n)
-            rows[:, 2] = u
-            rows[:, 3] = v
-            f.write("%d " % n)
-            f.write(" ".join(map(str, rows.ravel().tolist())))
-            f.write("\n")
+            f.write(b"%d " % n)
+            chunk = 1 << 22
+            for lo in range(0, n, chunk):
+                hi = min(n, lo + chunk)
+                rows = np.empty((hi - lo, 4), dtype=np.int64)
+                rows[:, 0] = ty[lo:hi]
+                rows[:, 1] = np.arange(lo, hi)
+                rows[:, 2] = u[lo:hi]
+                rows[:, 3] = v[lo:hi]
+                b = _decimal_bytes(rows.ravel(), 32)
+                f.write(b[:-1] if hi == n else b)
+            f.write(b"\n")
     with open(meta_path, "w") as f:
         for _ in layers:
             f.write("0 0 1 0 0\n")

@@ -5,22 +5,28 @@
 // (cudaMalloc would fail), code that must not take the device-wide
 // synchronisation of cudaFree on a latency-critical path, and embedders with a
 // fixed device-memory budget.  The call works entirely in one file-scope
-// device array of 16,760 field elements (268,160 bytes), held by every GPU
-// that loads this library until the process exits.
+// device array of 16,760 field elements (268,160 bytes); every GPU that loads
+// this library holds its own copy of the array until the process exits.
 //
 // Contract (also in include/virgo_b200.h):
 //   - vals is device memory (n >= 2^log_n entries), r and out host memory;
 //   - log_n <= NOALLOC_MAX_LOG (26); larger sizes are rejected with
-//     VG_ERR_ARG and a message;
+//     VG_ERR_ARG and a message before anything touches the GPU;
+//   - the kernels run on the legacy default stream, which does not wait for
+//     work on non-blocking streams (this library's context streams are
+//     non-blocking): a caller whose vals come from such a stream must
+//     synchronise it first (vg_ctx_sync for a library context);
 //   - the first call on a device looks up the array's device address with
 //     cudaGetSymbolAddress (with that device current) and caches it, so make
-//     that first call before any stream capture;
-//   - every call reuses the same array and it keeps the previous call's
-//     contents; each call writes every region before reading it, so nothing
-//     has to start at zero.  Calls that overlap on the GPU (two host threads,
-//     or two devices' work on one array) race: serialise them;
-//   - the work runs on the legacy default stream and the call returns after
-//     the result is copied to out.
+//     that first call before any stream capture.  The cache is per device and
+//     per process: after cudaDeviceReset of a device the cached address is
+//     no longer valid, so do not call this entry point on that device again
+//     in the same process;
+//   - every call on a device reuses that device's array and it keeps the
+//     previous call's contents; each call writes every region before reading
+//     it, so nothing has to start at zero.  Calls on the same device that
+//     overlap on the GPU (two host threads, two streams) race: serialise them;
+//   - the call returns after the result is copied to out.
 #include "common.cuh"
 #include <mutex>
 
@@ -74,11 +80,11 @@ fe *g_na_addr[64] = {nullptr};   // per device, looked up on first use
 
 extern "C" int vg_mle_eval_noalloc(const vg_fe *vals, long n, const vg_fe *r, int log_n, vg_fe *out)
 {
-    if (!vals || !r || !out || log_n < 0 || n < (1L << log_n))
-        return vg_fail(VG_ERR_ARG, "vg_mle_eval_noalloc: bad argument (n=%ld log_n=%d)", n, log_n);
-    if (log_n > NOALLOC_MAX_LOG)
-        return vg_fail(VG_ERR_ARG, "vg_mle_eval_noalloc: log_n %d exceeds the fixed scratch limit %d", log_n,
+    if (log_n < 0 || log_n > NOALLOC_MAX_LOG)   // checked before any shift by log_n
+        return vg_fail(VG_ERR_ARG, "vg_mle_eval_noalloc: log_n %d outside the fixed scratch limit [0, %d]", log_n,
                        NOALLOC_MAX_LOG);
+    if (!vals || !r || !out || n < (1L << log_n))
+        return vg_fail(VG_ERR_ARG, "vg_mle_eval_noalloc: bad argument (n=%ld log_n=%d)", n, log_n);
     {
         cudaPointerAttributes a;
         if (cudaPointerGetAttributes(&a, vals) != cudaSuccess || a.type != cudaMemoryTypeDevice) {
