@@ -54,6 +54,7 @@ WORKLOAD = "matmul256_addtree_32bit"
 METRIC = "proofs/s (256x256 matmul circuit, 2^24 product gates, full prover)"
 REF_BIN = os.path.join(ROOT, "oracle", "_ref", "zk_proof_ref")
 FFT_BIN = os.path.join(ROOT, "oracle", "_ref", "fft_gkr")
+COMMIT_BIN = os.path.join(ROOT, "oracle", "_ref", "commit_ref")
 FAMILIES = ["ntt_pass", "leaf_chain", "merkle_level", "fri_fold_leaf", "virtual_oracle", "eval_layer",
             "phase1_scatter", "phase2_scatter", "acc_finalize", "sumcheck_round", "reduce", "other"]
 # DRAM bytes / algorithmic bytes measured by ncu on full-size launches
@@ -219,6 +220,79 @@ def run_reference_pool(circuit, meta, n_warm, n_timed, width, seed0):
         p.wait()
         shutil.rmtree(d, ignore_errors=True)
     return timed, t_last - t_first, fillers
+
+
+def reference_sample(jobs):
+    """Proves each (name, layers, seed) job with the reference prover, all
+    jobs at once (one single-threaded process each); the circuit files are
+    written by the library's text writer.  Returns (name, prover seconds,
+    detail) per job, prover seconds from the reference's own timers (Prove
+    Time, fft_gkr side proof included, plus evaluate)."""
+    tmp = tempfile.mkdtemp(prefix="virgo_sample_")
+    width = max(1, min(host_cores(), len(jobs)))
+    try:
+        files = []
+        for k, (name, layers, seed) in enumerate(jobs):
+            c, m = os.path.join(tmp, "c%d.txt" % k), os.path.join(tmp, "m%d.txt" % k)
+            write_circuit_text(layers, c, m)
+            files.append((name, c, m, seed))
+        out, running = [], []
+        while files or running:
+            while files and len(running) < width:   # at most one process per core
+                name, c, m, seed = files.pop(0)
+                running.append((name, _ref_launch(c, m, seed)))
+            time.sleep(0.02)
+            still = []
+            for name, (p, d) in running:
+                if p.poll() is None:
+                    still.append((name, (p, d)))
+                    continue
+                if p.returncode != 0:
+                    raise RuntimeError("reference proof of %s failed (rc %d)" % (name, p.returncode))
+                secs, detail = ref_prover_seconds(d)
+                detail["verified"] = "Pass" in open(os.path.join(d, "out.txt")).read()
+                out.append((name, secs, detail))
+                shutil.rmtree(d, ignore_errors=True)
+            running = still
+        return out
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def cpu_baselines_batched_served(sample_random=8, seed_batch=4):
+    """Bounded reference samples for the batched (64 random circuits) and
+    served (job mix) workloads, all proved at once on the host cores:
+    `sample_random` circuits drawn (seeded) from the 64 of the batch, and one
+    job of each class of the served mix.  Throughput on all host cores is
+    projected as cores / mean prover seconds (equal shares of the classes for
+    the mix)."""
+    from virgo_b200 import circuits, sha256_circuit
+    cores = host_cores()
+    batch = circuits.random_batch(64, seed_batch)
+    pick = [int(i) for i in np.random.default_rng(17).choice(64, size=sample_random, replace=False)]
+    jobs = [("random64[%d]" % i, batch[i], 100 + i) for i in pick]
+    mix = [("random_2^14", circuits.random_by_gates(14, 16, seed=14000)),
+           ("random_2^18", circuits.random_by_gates(18, 16, seed=18000)),
+           ("random_2^22", circuits.random_by_gates(22, 16, seed=22000)),
+           ("sha256_16_blocks", sha256_circuit.sha256_blocks(16, seed=41)),
+           ("sha256_64_blocks", sha256_circuit.sha256_blocks(64, seed=61))]
+    jobs += [(n, c, 500 + k) for k, (n, c) in enumerate(mix)]
+    t0 = time.perf_counter()
+    res = reference_sample(jobs)
+    wall = time.perf_counter() - t0
+    rnd = [(n, s) for n, s, _ in res if n.startswith("random64")]
+    srv = [(n, s) for n, s, _ in res if not n.startswith("random64")]
+    mean_r = statistics.mean(s for _, s in rnd)
+    mean_s = statistics.mean(s for _, s in srv)
+    common = {"unit": "proofs/s", "kind": "reference", "cores": cores,
+              "note": "projected to all %d host cores as cores / mean prover seconds; the sample ran %d "
+                      "single-threaded reference processes, at most one per core (%.1f s wall)"
+                      % (cores, len(jobs), wall),
+              "all_verified": all(d["verified"] for _, _, d in res)}
+    return (dict(common, value=cores / mean_r, sample="%d of the 64 circuits (indices %s), prover seconds %s"
+                 % (len(rnd), pick, [round(s, 3) for _, s in rnd])),
+            dict(common, value=cores / mean_s, sample="one job of each class of the mix, prover seconds %s"
+                 % {n: round(s, 3) for n, s in srv}))
 
 
 def write_circuit_text(layers, circuit, meta):
@@ -645,7 +719,30 @@ def served(n_jobs, seed, slots, rate_factor=3.0, budget_ms=500.0, slo_factors=(0
             "timing": "wall clock, submit to transcript on the host (circuit upload included)"}
 
 
-def commit_path(sizes=(20, 22, 24), reps=3):
+def reference_commit_seconds(log_len, priv, pub, mask, pub_mask, which, pos):
+    """The reference's commit path (oracle/_ref/commit_ref: commit_private_array,
+    commit_public_array, commit_phase and the query answers through its
+    poly_commit API) on the given inputs, one host core; returns its own
+    stage timers in seconds."""
+    import struct
+    tmp = tempfile.mkdtemp(prefix="virgo_commit_")
+    try:
+        fin, fout = os.path.join(tmp, "in.bin"), os.path.join(tmp, "out.bin")
+        with open(fin, "wb") as f:
+            f.write(struct.pack("<iiiIi", log_len, len(mask), len(pub_mask), 1, len(which)))
+            for w, p in zip(which, pos):
+                f.write(struct.pack("<iq", int(w), int(p)))
+            for a in (priv, pub, mask, pub_mask):
+                f.write(np.ascontiguousarray(a, np.uint64).tobytes())
+        subprocess.run([COMMIT_BIN, fin, fout], check=True, capture_output=True)
+        with open(fout, "rb") as f:
+            f.seek(-24, 2)
+            return struct.unpack("<ddd", f.read(24))
+    finally:
+        shutil.rmtree(tmp, ignore_errors=True)
+
+
+def commit_path(sizes=(20, 22, 24), reps=3, cpu_sizes=(20,)):
     """Config 2: the kernel-level commit path alone (vg_pc_commit_all: RS
     encodings of a private and a public vector of 2^L seeded F_p2 values,
     the virtual oracle, every FRI fold to 32 entries per slice, every leaf
@@ -669,7 +766,10 @@ def commit_path(sizes=(20, 22, 24), reps=3):
             M = S // gap
             priv, pub, mask, pub_mask, fri_r = fe(n), fe(n), fe(300), fe(M), fe(nlevels)
             which = np.array([0, 1] + [2 + t for t in range(nlevels)], np.int32)
-            pos = rng.integers(0, S // 2, len(which)).astype(np.int64)
+            # positions below half the queried set's per-slice length (S for
+            # the two committed oracles, S / 2^(t+1) for FRI level t)
+            half = np.array([S // 2, S // 2] + [max(1, (S >> (t + 1)) // 2) for t in range(nlevels)], np.int64)
+            pos = (rng.integers(0, 1 << 62, len(which)) % half).astype(np.int64)
             nq = len(which)
             roots = np.zeros((2 + nlevels, 32), np.uint8)
             sums, inner = np.zeros((65, 2), np.uint64), np.zeros(2, np.uint64)
@@ -690,9 +790,17 @@ def commit_path(sizes=(20, 22, 24), reps=3):
                 L.vg_pc_destroy(pc)
             t = min(ts[1:])
             leaves = 2 * (n >> 2) + sum(n >> (3 + i) for i in range(nlevels))
-            out.append({"log_len": log_len, "ms": round(1000 * t, 2), "keccak_f": 65 * leaves,
-                        "keccak_f_per_s": round(65 * leaves / t / 1e9, 3), "unit": "G Keccak-f/s",
-                        "h2d_bytes": int(priv.nbytes + pub.nbytes + mask.nbytes + pub_mask.nbytes)})
+            row = {"log_len": log_len, "ms": round(1000 * t, 2), "keccak_f": 65 * leaves,
+                   "keccak_f_per_s": round(65 * leaves / t / 1e9, 3), "unit": "G Keccak-f/s",
+                   "h2d_bytes": int(priv.nbytes + pub.nbytes + mask.nbytes + pub_mask.nbytes)}
+            if log_len in cpu_sizes and os.path.exists(COMMIT_BIN):
+                secs = reference_commit_seconds(log_len, priv, pub, mask, pub_mask, which, pos)
+                row["cpu_baseline"] = {"value": round(1.0 / sum(secs), 5), "unit": "commits/s", "cores": 1,
+                                       "kind": "reference",
+                                       "sample": "the same inputs through the reference's poly_commit API on one "
+                                                 "host core (commit_private_array %.2f s, commit_public_array "
+                                                 "%.2f s, commit_phase %.2f s, its own timers)" % secs}
+            out.append(row)
     finally:
         ctx.close()
     return out
@@ -825,6 +933,11 @@ def main():
                                               "the fft_gkr side proof, plus evaluate)", "detail": detail}
         else:
             line["cpu_baseline"] = None
+        if (not args.no_cpu_baseline and not args.no_served and world == 1 and os.path.exists(REF_BIN)
+                and args.workload == "matmul256"):
+            cb_batch, cb_served = cpu_baselines_batched_served()
+            line["batched_random64"]["cpu_baseline"] = cb_batch
+            line["served"]["cpu_baseline"] = cb_served
         print(json.dumps(line))
     if world > 1:
         import torch.distributed as dist

@@ -220,3 +220,53 @@ def test_fft_gkr_other_seed():
     ok1, m1, _, _ = O.fft_gkr(6, 1)
     ok2, m2, _, _ = O.fft_gkr(6, 12345)
     assert ok1 and ok2 and not (m1 == m2).all()
+
+
+def _commit_cases():
+    path = os.path.join(GOLD, "commit_ref.json")
+    return {c["log_len"]: c for c in json.load(open(path))} if os.path.exists(path) else {}
+
+
+@pytest.mark.parametrize("log_len", [11, 15])
+def test_commit_path_restatement_matches_reference(log_len):
+    """The restatement's commit path (RS encodings, virtual oracle, FRI folds
+    with the reference's own randomness, leaf chains, trees, query answers)
+    against the reference run through its poly_commit API
+    (tests/golden/commit_ref.json, oracle/commit_ref.cpp): every root,
+    all_sum, the final codeword and every query answer."""
+    import sys
+    sys.path.insert(0, GOLD)
+    import make_commit_golden as G
+    case = _commit_cases()[log_len]
+    x = G.case_inputs(log_len)
+    S = 1 << (log_len - 1)
+    l_exp, M = O.commit_private(x["priv"], log_len, x["pri_mask"])
+    assert M == case["n_pub_mask"]
+    tree_l = O.merkle_tree(0, O.leaf_chain(0, l_exp, 65, S))
+    assert tree_l[1].tobytes().hex() == case["roots"][0]
+    _, h_exp, vo, sums = O.commit_public(l_exp, x["pub"], log_len, x["pub_mask"])
+    assert sums.tobytes().hex() == case["all_sum"]
+    tree_h = O.merkle_tree(0, O.leaf_chain(0, h_exp, 65, S))
+    assert tree_h[1].tobytes().hex() == case["roots"][1]
+    fri_r = np.frombuffer(bytes.fromhex(case["fri_r"]), np.uint64).reshape(-1, 2)
+    sets = [(l_exp, S, tree_l), (h_exp, S, tree_h)]
+    cw, n = vo, S
+    for t in range(len(fri_r)):
+        cw = O.fri_fold(cw, 65, n, O.root_of_unity(n.bit_length() - 1), fri_r[t])
+        n //= 2
+        tree = O.merkle_tree(0, O.leaf_chain(0, cw, 65, n))
+        assert tree[1].tobytes().hex() == case["roots"][2 + t], ("level", t)
+        sets.append((cw, n, tree))
+    assert n == case["final_n"]
+    assert hashlib.sha256(cw.tobytes()).hexdigest() == case["final_slice_major"]
+    for q, (which, pos) in enumerate(zip(case["which"], case["pos"])):
+        src, n, tree = sets[which]
+        p = pos % (n // 2)
+        vals = np.array([src[s * n + p + b * (n // 2)] for s in range(65) for b in (0, 1)], np.uint64)
+        node, path = p + n // 2, []
+        while node != 1:
+            path.append(tree[node ^ 1].tobytes())
+            node //= 2
+        path.append(tree[p + n // 2].tobytes())
+        assert len(path) == case["queries"][q]["path_len"]
+        assert G.query_digest(vals, path) == case["queries"][q]["digest"], ("query", q, which)
