@@ -298,6 +298,8 @@ typedef struct {
     double fft_gkr_s;       /* the fft_gkr side proof: device time of its stream (0 when not run) */
     int fft_gkr_lg;         /* its size L - 6, 0 when not run */
     int fft_gkr_proof_size; /* its bytes as the reference counts them (the verifier adds them) */
+    int graph_replays;      /* sumcheck phases whose round launches were replayed from a captured CUDA graph */
+    int graph_captures;     /* sumcheck phases captured as a graph during this proof */
 } vg_proof_stats;
 /* From file-level layers as in the circuit text format (src/linear_gkr/README.md):
  * d layers, the input layer first (types 2/3, u = value), layer i has n[i]

@@ -37,6 +37,7 @@ class vg_proof_stats(ctypes.Structure):
         ("launch_s", ctypes.c_double), ("wait_s", ctypes.c_double), ("replay_s", ctypes.c_double),
         ("total_s", ctypes.c_double), ("prove_time", ctypes.c_double), ("proof_size", ctypes.c_longlong), ("launches", ctypes.c_longlong),
         ("fft_gkr_s", ctypes.c_double), ("fft_gkr_lg", ctypes.c_int), ("fft_gkr_proof_size", ctypes.c_int),
+        ("graph_replays", ctypes.c_int), ("graph_captures", ctypes.c_int),
     ]
 
 

@@ -623,7 +623,7 @@ struct RoundGroup {
     int slot0;          // record of the first round; the others follow
     int last6;          // write the final pair (the table ends at 2 entries) into the last record
     int split3;         // steps with at most RG_THREADS / 3 pairs run three threads per pair
-    fe r[RG_MAX];       // fold challenge of each round
+    const fe *r;        // fold challenge of each round (device memory, nsteps values)
 };
 
 __device__ __forceinline__ fe rg_fold(fe x0, fe x1, fe r) { return x0 + r * (x1 - x0); }
@@ -896,15 +896,19 @@ __device__ __forceinline__ fe fold(fe x0, fe x1, fe r) { return x0 + r * (x1 - x
 
 // The block partials are reduced by the last block to finish (a counter in
 // device memory decides which one), so one launch returns the round sums.
+// The fold challenge comes from device memory (rp), so a captured launch
+// sequence can be replayed with the next proof's challenges.
 template <bool FOLD, int THREADS>
 __global__ void __launch_bounds__(THREADS) k_round(const fe *__restrict__ xV, const fe *__restrict__ xAV,
-                                                       const fe *__restrict__ xAM, long npairs, fe r,
+                                                       const fe *__restrict__ xAM, long npairs,
+                                                       const fe *__restrict__ rp,
                                                        fe *__restrict__ yV, fe *__restrict__ yAV, fe *__restrict__ yAM,
                                                        fe *__restrict__ parts, unsigned *__restrict__ counter,
                                                        fe *__restrict__ out3, fe *__restrict__ last6)
 {
     __shared__ fe sm[3 * 32];
     __shared__ bool last;
+    const fe r = FOLD ? *rp : vg::fe_zero();
     fe acc[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < npairs; i += (long)gridDim.x * blockDim.x) {
         fe v0, v1, a0, a1, m0, m1;
@@ -975,15 +979,19 @@ __global__ void __launch_bounds__(THREADS) k_round(const fe *__restrict__ xV, co
 // 2 entries: one read of the tables for two rounds, a quarter of them
 // written.  Both rounds' sums go through one block reduction and the
 // last-block pass (6 values per CTA).
+// (both challenges from device memory: rp[0] for the first fold, rp[1] for
+// the second)
 template <bool FOLD, int THREADS>
 __global__ void __launch_bounds__(THREADS) k_round2(const fe *__restrict__ xV, const fe *__restrict__ xAV,
-                                                    const fe *__restrict__ xAM, long nquads, fe ra, fe rb,
+                                                    const fe *__restrict__ xAM, long nquads,
+                                                    const fe *__restrict__ rp,
                                                     fe *__restrict__ yV, fe *__restrict__ yAV, fe *__restrict__ yAM,
                                                     fe *__restrict__ parts, unsigned *__restrict__ counter,
                                                     fe *__restrict__ out_a, fe *__restrict__ out_b)
 {
     __shared__ fe sm[6 * 32];
     __shared__ bool last;
+    const fe ra = FOLD ? rp[0] : vg::fe_zero(), rb = rp[1];
     fe sa[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()}, sb[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nquads; i += (long)gridDim.x * blockDim.x) {
         fe v[4], a[4], m[4];
@@ -1130,6 +1138,33 @@ struct vg_circuit {
     std::vector<unsigned long long> edge_stats_host;
 };
 
+// One deferred round launch (k_round, k_round2 or k_round_group), held until
+// the next flush so that a phase's rounds are issued together: after one H2D
+// copy of their challenges, plainly or as a captured CUDA graph.
+struct RoundLaunch {
+    int kind = 0;               // 0 k_round, 1 k_round2, 2 k_round_group
+    bool fold = false;
+    int threads = 0;
+    unsigned grid = 0;
+    long count = 0;             // pairs (k_round), quads (k_round2), input entries (group)
+    const fe *x[3] = {nullptr, nullptr, nullptr};
+    fe *y[3] = {nullptr, nullptr, nullptr};
+    int slot = 0;               // challenge slot of the (first) round
+    fe *oa = nullptr, *ob = nullptr;   // k_round: sums, folded pair; k_round2: the two rounds' sums
+    RoundGroup G{};             // k_round_group (G.r set when issued)
+    double prof_bytes = 0;
+};
+
+// A phase's round launches captured once and replayed: the key lists every
+// pointer, size and shape the graph's nodes use, so a replay does exactly
+// what issuing the same launches would.
+struct PhaseGraph {
+    std::vector<uint64_t> key;
+    uint64_t hash = 0;
+    cudaGraphExec_t exec = nullptr;
+    long launches = 0;
+};
+
 struct vg_gkr {
     vg_ctx *ctx = nullptr;
     const vg_circuit *C = nullptr;
@@ -1171,15 +1206,31 @@ struct vg_gkr {
     // the next round in one k_round2 pass (VG_TUNE_ROUND_FUSE = 2)
     bool held = false;
     bool held_fold = false;
-    fe held_r{};
     int held_slot = 0;
     long held_n = 0;                     // table length before the held round
     fe *heavy_parts = nullptr;           // per-CTA partial sums of heavy keys
     fe *bgt = nullptr;                   // beta_g by gate of the current layer (2^max_bl entries)
     int bgt_layer = -1;                  // the layer whose phase-1 gathers filled bgt, -1 none
+    // fold challenges of the deferred rounds: record slot k's at rhost[k]
+    // (pinned, written when the round is queued) and rdev[k] (copied once per
+    // flush); a synchronous round's at rsync_host / rsync_dev
+    fe *rdev = nullptr, *rhost = nullptr;
+    size_t rhost_cap = 0;                // bytes
+    int r_cap = 0;                       // slots of rdev
+    fe *rsync_dev = nullptr, *rsync_host = nullptr;
+    // deferred round launches not issued yet, and the challenge slots they read
+    std::vector<RoundLaunch> pend_launch;
+    int pend_lo = 0, pend_hi = 0;
+    // captured phase graphs; keys seen once (a key is captured the second
+    // time it comes, replayed from then on)
+    std::vector<PhaseGraph> graphs;
+    std::vector<uint64_t> seen;
+    bool graphs_off = false;
+    long long graph_replays = 0, graph_captures = 0;
 };
 
 static int flush_rounds(vg_gkr *g);
+static void destroy_graphs(vg_gkr *g);
 
 // ------------------------------------------------------------------ circuit
 static int grow_u32(vg_ctx *c, uint32_t **p, long *cap, long n)
@@ -1695,6 +1746,8 @@ extern "C" int vg_gkr_create(vg_ctx *ctx, const vg_circuit *c, vg_gkr **out)
     if (cudaMalloc(&g->round_out, 16 * sizeof(fe)) != cudaSuccess) return fail("round sums");
     if (cudaMalloc(&g->round_counter, sizeof(unsigned)) != cudaSuccess) return fail("round counter");
     if (cudaMalloc(&g->vu, sizeof(fe)) != cudaSuccess) return fail("v_u");
+    if (cudaMalloc(&g->rsync_dev, sizeof(fe)) != cudaSuccess) return fail("round challenge");
+    if (cudaMallocHost(&g->rsync_host, sizeof(fe)) != cudaSuccess) return fail("round challenge (pinned)");
     if (cudaMalloc(&g->heavy_parts, (size_t)MAX_HEAVY * HEAVY_PARTS * 4 * sizeof(fe)) != cudaSuccess)
         return fail("heavy partials");
     // on the context's stream: the streams are non-blocking, so a memset on
@@ -1735,6 +1788,11 @@ extern "C" int vg_gkr_destroy(vg_gkr *g)
     cudaFree(g->bgt);
     cudaFree(g->rec);
     if (g->rec_host) cudaFreeHost(g->rec_host);
+    destroy_graphs(g);
+    cudaFree(g->rdev);
+    if (g->rhost) cudaFreeHost(g->rhost);
+    cudaFree(g->rsync_dev);
+    if (g->rsync_host) cudaFreeHost(g->rsync_host);
     delete g;
     return VG_OK;
 }
@@ -1742,6 +1800,7 @@ extern "C" int vg_gkr_destroy(vg_gkr *g)
 extern "C" int vg_gkr_evaluate(vg_gkr *g)
 {
     if (!g) return vg_fail(VG_ERR_ARG, "null gkr");
+    VG_TRY(flush_rounds(g));
     vg_ctx *c = g->ctx;
     for (int i = 1; i < g->C->depth; ++i) {
         const DevLayer &D = g->C->L[i];
@@ -2146,10 +2205,187 @@ static int rg_smem_attribute(int dev)
     return VG_OK;
 }
 
+// Issues one round launch on the context stream (rp: its challenge(s) in
+// device memory).
+static int issue_launch(vg_gkr *g, const RoundLaunch &L, const fe *rp)
+{
+    vg_ctx *c = g->ctx;
+    {
+        ProfScope ps(c, KF_ROUND, L.prof_bytes);
+        fe *pr = g->round_parts;
+        unsigned *cnt = g->round_counter;
+        if (L.kind == 0) {
+#define VG_ROUND_LAUNCH(TT)                                                                                          \
+    if (L.fold)                                                                                                       \
+        k_round<true, TT><<<L.grid, TT, 0, c->stream>>>(L.x[0], L.x[1], L.x[2], L.count, rp, L.y[0], L.y[1], L.y[2], \
+                                                        pr, cnt, L.oa, L.ob);                                         \
+    else                                                                                                              \
+        k_round<false, TT><<<L.grid, TT, 0, c->stream>>>(L.x[0], L.x[1], L.x[2], L.count, rp, nullptr, nullptr,      \
+                                                         nullptr, pr, cnt, L.oa, L.ob)
+            if (L.threads == 128) VG_ROUND_LAUNCH(128);
+            else if (L.threads == 512) VG_ROUND_LAUNCH(512);
+            else VG_ROUND_LAUNCH(256);
+#undef VG_ROUND_LAUNCH
+        } else if (L.kind == 1) {
+#define VG_ROUND2_LAUNCH(TT)                                                                                         \
+    if (L.fold)                                                                                                       \
+        k_round2<true, TT><<<L.grid, TT, 0, c->stream>>>(L.x[0], L.x[1], L.x[2], L.count, rp, L.y[0], L.y[1], L.y[2], \
+                                                         pr, cnt, L.oa, L.ob);                                        \
+    else                                                                                                              \
+        k_round2<false, TT><<<L.grid, TT, 0, c->stream>>>(L.x[0], L.x[1], L.x[2], L.count, rp, L.y[0], L.y[1],       \
+                                                          L.y[2], pr, cnt, L.oa, L.ob)
+            if (L.threads == 128) VG_ROUND2_LAUNCH(128);
+            else if (L.threads == 512) VG_ROUND2_LAUNCH(512);
+            else VG_ROUND2_LAUNCH(256);
+#undef VG_ROUND2_LAUNCH
+        } else {
+            RoundGroup G = L.G;
+            G.r = rp;
+            k_round_group<<<L.grid, RG_THREADS, RG_SMEM_FE * sizeof(fe), c->stream>>>(
+                L.x[0], L.x[1], L.x[2], L.count, G, L.y[0], L.y[1], L.y[2], g->rg_parts, g->round_counter, g->rec);
+        }
+    }
+    VG_LAUNCHED(c);
+    return VG_OK;
+}
+
+// A round launch: issued now on a synchronous object (its challenge staged
+// through rsync), queued until the next flush on a deferred one (challenges
+// from the record slots).
+static int add_launch(vg_gkr *g, RoundLaunch &L, int nslots, fe r_sync)
+{
+    if (!g->deferred) {
+        if (!g->rsync_host) return vg_fail(VG_ERR_STATE, "synchronous round on a tables object");
+        *g->rsync_host = r_sync;
+        VG_CHECK_CUDA(cudaMemcpyAsync(g->rsync_dev, g->rsync_host, sizeof(fe), cudaMemcpyHostToDevice, g->ctx->stream));
+        return issue_launch(g, L, g->rsync_dev);
+    }
+    if (g->pend_launch.empty()) {
+        g->pend_lo = L.slot;
+        g->pend_hi = L.slot + nslots;
+    } else {
+        g->pend_lo = std::min(g->pend_lo, L.slot);
+        g->pend_hi = std::max(g->pend_hi, L.slot + nslots);
+    }
+    g->pend_launch.push_back(L);
+    return VG_OK;
+}
+
+// VIRGO_GRAPHS=0 issues every deferred round launch plainly
+static bool rg_graphs_enabled()
+{
+    static int on = -1;
+    if (on < 0) {
+        const char *e = getenv("VIRGO_GRAPHS");
+        on = (e && e[0] == '0') ? 0 : 1;
+    }
+    return on != 0;
+}
+
+static void destroy_graphs(vg_gkr *g)
+{
+    for (auto &pg : g->graphs)
+        if (pg.exec) cudaGraphExecDestroy(pg.exec);
+    g->graphs.clear();
+    g->seen.clear();
+}
+
+// Issues the queued round launches: one H2D copy of the challenge slots they
+// read, then the launches.  A sequence seen before (same pointers, sizes,
+// shapes and slots: the same phase of the same circuit in a later proof) is
+// captured as a graph the second time and replayed from then on; a stream
+// already being captured (the fft_gkr side proof's graph) or the per-launch
+// profiler gets plain launches.
+static int exec_pending(vg_gkr *g)
+{
+    if (g->pend_launch.empty()) return VG_OK;
+    vg_ctx *c = g->ctx;
+    const int lo = g->pend_lo, hi = g->pend_hi;
+    std::vector<RoundLaunch> launches;
+    launches.swap(g->pend_launch);
+    auto issue = [&]() -> int {
+        if (hi > lo)
+            VG_CHECK_CUDA(cudaMemcpyAsync(g->rdev + lo, g->rhost + lo, (size_t)(hi - lo) * sizeof(fe),
+                                          cudaMemcpyHostToDevice, c->stream));
+        for (const RoundLaunch &L : launches) VG_TRY(issue_launch(g, L, g->rdev + L.slot));
+        return VG_OK;
+    };
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    VG_CHECK_CUDA(cudaStreamIsCapturing(c->stream, &cs));
+    if (!rg_graphs_enabled() || g->graphs_off || c->profiling || cs != cudaStreamCaptureStatusNone) return issue();
+
+    std::vector<uint64_t> key;
+    key.reserve(4 + 24 * launches.size());
+    key.push_back((uint64_t)(uintptr_t)g->rdev);
+    key.push_back((uint64_t)(uintptr_t)g->rhost);
+    key.push_back((uint64_t)lo);
+    key.push_back((uint64_t)hi);
+    for (const RoundLaunch &L : launches) {
+        key.push_back((uint64_t)L.kind | ((uint64_t)L.fold << 8) | ((uint64_t)L.threads << 16) | ((uint64_t)L.grid << 32));
+        key.push_back((uint64_t)L.count);
+        for (int k = 0; k < 3; ++k) key.push_back((uint64_t)(uintptr_t)L.x[k]);
+        for (int k = 0; k < 3; ++k) key.push_back((uint64_t)(uintptr_t)L.y[k]);
+        key.push_back((uint64_t)L.slot);
+        key.push_back((uint64_t)(uintptr_t)L.oa);
+        key.push_back((uint64_t)(uintptr_t)L.ob);
+        key.push_back(((uint64_t)L.G.chunk_log) | ((uint64_t)L.G.nsteps << 8) | ((uint64_t)L.G.first_nofold << 16) |
+                      ((uint64_t)L.G.last6 << 24) | ((uint64_t)L.G.split3 << 32));
+        key.push_back((uint64_t)L.G.slot0);
+    }
+    key.push_back((uint64_t)(uintptr_t)g->round_parts);
+    key.push_back((uint64_t)(uintptr_t)g->round_counter);
+    key.push_back((uint64_t)(uintptr_t)g->rg_parts);
+    key.push_back((uint64_t)(uintptr_t)g->rec);
+    uint64_t h = 1469598103934665603ull;   // FNV-1a over the key words
+    for (uint64_t w : key) {
+        h ^= w;
+        h *= 1099511628211ull;
+    }
+    for (PhaseGraph &pg : g->graphs)
+        if (pg.hash == h && pg.key == key) {
+            VG_CHECK_CUDA(cudaGraphLaunch(pg.exec, c->stream));
+            c->launches += pg.launches;
+            ++g->graph_replays;
+            return VG_OK;
+        }
+    if (std::find(g->seen.begin(), g->seen.end(), h) == g->seen.end()) {
+        if (g->seen.size() >= 1024) g->seen.clear();
+        g->seen.push_back(h);   // first sight: plain launches
+        return issue();
+    }
+    // second sight: capture, instantiate, launch
+    if (g->graphs.size() >= 256) destroy_graphs(g);
+    const long launches0 = c->launches;
+    VG_CHECK_CUDA(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeRelaxed));
+    const int rc = issue();
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(c->stream, &graph);
+    cudaGraphExec_t exec = nullptr;
+    if (rc == VG_OK && e == cudaSuccess) e = cudaGraphInstantiate(&exec, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    if (rc != VG_OK || e != cudaSuccess) {
+        // nothing of the capture ran: issue plainly, and no graphs from now on
+        cudaGetLastError();
+        if (exec) cudaGraphExecDestroy(exec);
+        g->graphs_off = true;
+        c->launches = launches0;
+        return issue();
+    }
+    PhaseGraph pg;
+    pg.key.swap(key);
+    pg.hash = h;
+    pg.exec = exec;
+    pg.launches = c->launches - launches0;
+    g->graphs.push_back(std::move(pg));
+    ++g->graph_captures;
+    VG_CHECK_CUDA(cudaGraphLaunch(exec, c->stream));
+    return VG_OK;
+}
+
 // One round on the current tables of length n_in (before the round's fold):
 // k_round with its sums (and, when one pair remains, the folded pair) at o3
-// (and o6).
-static int launch_round(vg_gkr *g, long n_in, bool fold, fe r, fe *o3, fe *o6)
+// (and o6); its challenge is record slot `slot`'s (deferred) or r.
+static int launch_round(vg_gkr *g, long n_in, bool fold, fe r, int slot, fe *o3, fe *o6)
 {
     vg_ctx *c = g->ctx;
     const long n_out = fold ? n_in / 2 : n_in;   // table length the sums are taken over
@@ -2157,66 +2393,52 @@ static int launch_round(vg_gkr *g, long n_in, bool fold, fe r, fe *o3, fe *o6)
     // threads per CTA from the device's tuning; the grid covers at most
     // 148 x 2048 threads and at most 148 x 16 CTAs (the partials buffer holds
     // 3 sums for each), looping beyond
-    const int T = (int)vg_tune_value(c->device, VG_TUNE_ROUND_THREADS);
-    unsigned grid = std::min<unsigned>(grid_for(npairs, T), std::min(148u * 16u, 148u * 2048u / (unsigned)T));
-    fe *y[3] = {g->buf[g->next_buf][0], g->buf[g->next_buf][1], g->buf[g->next_buf][2]};
-    {
-        // fold: read 3 tables x 4 entries, write 3 x 2 per pair; else read 3 x 2
-        ProfScope ps(c, KF_ROUND, (fold ? 288.0 : 96.0) * (double)npairs);
-        const fe *x0 = g->cur[0], *x1 = g->cur[1], *x2 = g->cur[2];
-        fe *pr = g->round_parts;
-        unsigned *cnt = g->round_counter;
-#define VG_ROUND_LAUNCH(TT)                                                                                          \
-    if (fold)                                                                                                         \
-        k_round<true, TT><<<grid, TT, 0, c->stream>>>(x0, x1, x2, npairs, r, y[0], y[1], y[2], pr, cnt, o3, o6);      \
-    else                                                                                                              \
-        k_round<false, TT><<<grid, TT, 0, c->stream>>>(x0, x1, x2, npairs, r, nullptr, nullptr, nullptr, pr, cnt, o3, o6)
-        if (T == 128) VG_ROUND_LAUNCH(128);
-        else if (T == 512) VG_ROUND_LAUNCH(512);
-        else VG_ROUND_LAUNCH(256);
-#undef VG_ROUND_LAUNCH
+    RoundLaunch L;
+    L.kind = 0;
+    L.fold = fold;
+    L.threads = (int)vg_tune_value(c->device, VG_TUNE_ROUND_THREADS);
+    L.grid = std::min<unsigned>(grid_for(npairs, L.threads), std::min(148u * 16u, 148u * 2048u / (unsigned)L.threads));
+    L.count = npairs;
+    for (int k = 0; k < 3; ++k) {
+        L.x[k] = g->cur[k];
+        L.y[k] = fold ? g->buf[g->next_buf][k] : nullptr;
     }
-    VG_LAUNCHED(c);
+    L.slot = slot;
+    L.oa = o3;
+    L.ob = o6;
+    L.prof_bytes = (fold ? 288.0 : 96.0) * (double)npairs;   // fold: read 3 tables x 4 entries, write 3 x 2 per pair
+    VG_TRY(add_launch(g, L, 1, r));
     if (fold) {
-        g->cur[0] = y[0];
-        g->cur[1] = y[1];
-        g->cur[2] = y[2];
+        for (int k = 0; k < 3; ++k) g->cur[k] = L.y[k];
         g->next_buf ^= 1;
     }
     return VG_OK;
 }
 
 // Two rounds in one k_round2 pass on the current tables of length n_in: the
-// first folds with ra when `fold` (else it is a phase's unfolded first
-// round), the second folds with rb; sums to oa and ob.
-static int launch_round2(vg_gkr *g, long n_in, bool fold, fe ra, fe rb, fe *oa, fe *ob)
+// first (record slot `slot`) folds when `fold` (else it is a phase's unfolded
+// first round), the second (slot + 1) folds; sums to their records.
+static int launch_round2(vg_gkr *g, long n_in, bool fold, int slot)
 {
     vg_ctx *c = g->ctx;
     const long nquads = fold ? n_in / 8 : n_in / 4;
     // at most 148 x 2048 threads and 148 x 8 CTAs (6 sums each in the partials buffer)
-    const int T = (int)vg_tune_value(c->device, VG_TUNE_ROUND_THREADS);
-    unsigned grid = std::min<unsigned>(grid_for(nquads, T), std::min(148u * 8u, 148u * 2048u / (unsigned)T));
-    fe *y[3] = {g->buf[g->next_buf][0], g->buf[g->next_buf][1], g->buf[g->next_buf][2]};
-    {
-        // per quad: read 3 tables x 8 (or 4) entries, write 3 x 2
-        ProfScope ps(c, KF_ROUND, (fold ? 480.0 : 288.0) * (double)nquads);
-        const fe *x0 = g->cur[0], *x1 = g->cur[1], *x2 = g->cur[2];
-        fe *pr = g->round_parts;
-        unsigned *cnt = g->round_counter;
-#define VG_ROUND2_LAUNCH(TT)                                                                                         \
-    if (fold)                                                                                                         \
-        k_round2<true, TT><<<grid, TT, 0, c->stream>>>(x0, x1, x2, nquads, ra, rb, y[0], y[1], y[2], pr, cnt, oa, ob); \
-    else                                                                                                              \
-        k_round2<false, TT><<<grid, TT, 0, c->stream>>>(x0, x1, x2, nquads, ra, rb, y[0], y[1], y[2], pr, cnt, oa, ob)
-        if (T == 128) VG_ROUND2_LAUNCH(128);
-        else if (T == 512) VG_ROUND2_LAUNCH(512);
-        else VG_ROUND2_LAUNCH(256);
-#undef VG_ROUND2_LAUNCH
+    RoundLaunch L;
+    L.kind = 1;
+    L.fold = fold;
+    L.threads = (int)vg_tune_value(c->device, VG_TUNE_ROUND_THREADS);
+    L.grid = std::min<unsigned>(grid_for(nquads, L.threads), std::min(148u * 8u, 148u * 2048u / (unsigned)L.threads));
+    L.count = nquads;
+    for (int k = 0; k < 3; ++k) {
+        L.x[k] = g->cur[k];
+        L.y[k] = g->buf[g->next_buf][k];
     }
-    VG_LAUNCHED(c);
-    g->cur[0] = y[0];
-    g->cur[1] = y[1];
-    g->cur[2] = y[2];
+    L.slot = slot;
+    L.oa = g->rec + 9 * slot;
+    L.ob = g->rec + 9 * (slot + 1);
+    L.prof_bytes = (fold ? 480.0 : 288.0) * (double)nquads;   // per quad: read 3 x 8 (or 4) entries, write 3 x 2
+    VG_TRY(add_launch(g, L, 2, vg::fe_zero()));
+    for (int k = 0; k < 3; ++k) g->cur[k] = L.y[k];
     g->next_buf ^= 1;
     return VG_OK;
 }
@@ -2228,53 +2450,59 @@ static int flush_held(vg_gkr *g)
     if (!g->held) return VG_OK;
     g->held = false;
     fe *o3 = g->rec + 9 * g->held_slot;
-    return launch_round(g, g->held_n, g->held_fold, g->held_r, o3, o3 + 3);
+    return launch_round(g, g->held_n, g->held_fold, vg::fe_zero(), g->held_slot, o3, o3 + 3);
 }
 
-// Launches the pending deferred rounds as one group: one chunk per CTA when
+// Queues the pending deferred rounds as one group: one chunk per CTA when
 // the table fits the grid, CTAs looping over chunks beyond.
-static int flush_rounds(vg_gkr *g)
+static int group_rounds(vg_gkr *g)
 {
     VG_TRY(flush_held(g));
     if (g->pend_r.empty()) return VG_OK;
     vg_ctx *c = g->ctx;
-    RoundGroup G{};
+    RoundLaunch L;
+    L.kind = 2;
+    RoundGroup &G = L.G;
     int cl = 0;
     while ((1L << cl) < g->pend_chunk) ++cl;
     G.chunk_log = cl;
     G.nsteps = (int)g->pend_r.size();
     G.first_nofold = g->pend_nofold ? 1 : 0;
     G.slot0 = g->pend_slot0;
-    for (int i = 0; i < G.nsteps; ++i) G.r[i] = g->pend_r[i];
+    G.r = nullptr;
     const long n_in = g->pend_n0;
     const long cin = G.first_nofold ? std::min(n_in, g->pend_chunk) : std::min(n_in, 2 * g->pend_chunk);
     const long nchunks = n_in / cin;
     // CTAs loop over chunks: at most 3 resident per SM (68 KB of shared memory each)
-    const long grid = std::min(nchunks, 148L * 3L);
+    L.grid = (unsigned)std::min(nchunks, 148L * 3L);
     const long m_final = (G.first_nofold ? cin : cin / 2) >> (G.nsteps - 1);
     G.last6 = (nchunks == 1 && m_final == 2) ? 1 : 0;
     G.split3 = vg_tune_value(c->device, VG_TUNE_GROUP_SPLIT) != 0 ? 1 : 0;
     const bool folds = !(G.first_nofold && G.nsteps == 1);
-    fe *y[3] = {g->buf[g->next_buf][0], g->buf[g->next_buf][1], g->buf[g->next_buf][2]};
-    const size_t smem = RG_SMEM_FE * sizeof(fe);
-    VG_TRY(rg_smem_attribute(c->device));
-    {
-        // every round of the group: the first reads 3 tables of n_in, writes nothing more than the chunk tails
-        ProfScope ps(c, KF_ROUND, 48.0 * (double)n_in + (folds ? 48.0 * (double)(nchunks * m_final) : 0.0));
-        k_round_group<<<(unsigned)grid, RG_THREADS, smem, c->stream>>>(g->cur[0], g->cur[1], g->cur[2], n_in, G,
-                                                                      folds ? y[0] : nullptr, folds ? y[1] : nullptr,
-                                                                      folds ? y[2] : nullptr, g->rg_parts,
-                                                                      g->round_counter, g->rec);
+    L.threads = RG_THREADS;
+    L.count = n_in;
+    for (int k = 0; k < 3; ++k) {
+        L.x[k] = g->cur[k];
+        L.y[k] = folds ? g->buf[g->next_buf][k] : nullptr;
     }
-    VG_LAUNCHED(c);
+    L.slot = G.slot0;
+    // every round of the group: the first reads 3 tables of n_in, writes nothing more than the chunk tails
+    L.prof_bytes = 48.0 * (double)n_in + (folds ? 48.0 * (double)(nchunks * m_final) : 0.0);
+    VG_TRY(rg_smem_attribute(c->device));   // before any capture
+    VG_TRY(add_launch(g, L, G.nsteps, vg::fe_zero()));
     if (folds) {
-        g->cur[0] = y[0];
-        g->cur[1] = y[1];
-        g->cur[2] = y[2];
+        for (int k = 0; k < 3; ++k) g->cur[k] = L.y[k];
         g->next_buf ^= 1;
     }
     g->pend_r.clear();
     return VG_OK;
+}
+
+// Every queued round: held and grouped rounds into launches, then issued.
+static int flush_rounds(vg_gkr *g)
+{
+    VG_TRY(group_rounds(g));
+    return exec_pending(g);
 }
 
 // phase-2 tables for the current layer once g->vu holds v_u
@@ -2343,6 +2571,21 @@ int vg_gkr_phase2_init_deferred(vg_gkr *g, const vg_fe *r_u, int length_u, vg_fe
     return phase2_tables(g, r_u, length_u);
 }
 
+// challenge slots for n records: device copy from the pool, pinned host side
+static int grow_challenges(vg_gkr *g, int n)
+{
+    if (n <= g->r_cap) return VG_OK;
+    vg_release(g->ctx, g->rdev);
+    g->rdev = nullptr;
+    g->r_cap = 0;
+    VG_TRY(vg_alloc(g->ctx, (void **)&g->rdev, (size_t)n * sizeof(fe)));
+    void *h = g->rhost;
+    VG_TRY(vg_pinned_grow(g->ctx, &h, &g->rhost_cap, (size_t)n * sizeof(fe)));
+    g->rhost = (fe *)h;
+    g->r_cap = n;
+    return VG_OK;
+}
+
 int vg_gkr_defer(vg_gkr *g, int on)
 {
     if (!g) return vg_fail(VG_ERR_ARG, "null gkr");
@@ -2360,6 +2603,7 @@ int vg_gkr_defer(vg_gkr *g, int on)
         VG_TRY(vg_alloc(g->ctx, (void **)&g->rec, (size_t)need * 9 * sizeof(fe)));
         g->rec_cap = need;
     }
+    VG_TRY(grow_challenges(g, g->rec_cap));
     return VG_OK;
 }
 
@@ -2399,6 +2643,10 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
     // chunk unfolded, so it starts at half the length.
     const long S = std::max(2L * RG_CHUNK, group_start(g->ctx->device));
     const long lim = fold ? S : S / 2;
+    if (g->deferred) {
+        if (g->rec_n >= g->r_cap) return vg_fail(VG_ERR_STATE, "challenge slots full");
+        g->rhost[g->rec_n] = tofe(previous_random);   // this round's record slot; copied at the next flush
+    }
     if (g->deferred && (!g->pend_r.empty() || g->n <= lim)) {
         VG_TRY(flush_held(g));   // the round before this one ran alone
         if (g->pend_r.empty()) {
@@ -2412,7 +2660,7 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
         ++g->rec_n;
         if (fold) g->n /= 2;
         g->round0_pending = false;
-        if ((int)g->pend_r.size() >= group_capacity(g->pend_n0, g->pend_nofold, g->pend_chunk)) VG_TRY(flush_rounds(g));
+        if ((int)g->pend_r.size() >= group_capacity(g->pend_n0, g->pend_nofold, g->pend_chunk)) VG_TRY(group_rounds(g));
         return VG_OK;
     }
     vg_ctx *c = g->ctx;
@@ -2421,8 +2669,8 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
         if (g->held) {
             // this round pairs with the held one: one pass for both
             g->held = false;
-            VG_TRY(launch_round2(g, g->held_n, g->held_fold, g->held_r, r, g->rec + 9 * g->held_slot,
-                                 g->rec + 9 * g->rec_n));
+            if (g->rec_n != g->held_slot + 1) return vg_fail(VG_ERR_STATE, "paired rounds in non-adjacent records");
+            VG_TRY(launch_round2(g, g->held_n, g->held_fold, g->held_slot));
             ++g->rec_n;
             g->n /= 2;   // a round after another always folds
             g->round0_pending = false;
@@ -2431,7 +2679,6 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
         if (vg_tune_value(c->device, VG_TUNE_ROUND_FUSE) >= 2) {
             g->held = true;
             g->held_fold = fold;
-            g->held_r = r;
             g->held_slot = g->rec_n;
             g->held_n = g->n;
             ++g->rec_n;
@@ -2441,7 +2688,7 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
         }
     }
     fe *o3 = g->deferred ? g->rec + 9 * g->rec_n : g->round_out;
-    VG_TRY(launch_round(g, g->n, fold, r, o3, g->deferred ? o3 + 3 : nullptr));
+    VG_TRY(launch_round(g, g->n, fold, r, g->deferred ? g->rec_n : 0, o3, g->deferred ? o3 + 3 : nullptr));
     if (fold) g->n /= 2;
     g->round0_pending = false;
     if (g->deferred) {
@@ -2525,6 +2772,7 @@ int vg_gkr_tables_reserve(vg_gkr *g, long max_n, int max_records)
         VG_TRY(vg_alloc(x, (void **)&g->rec, (size_t)max_records * 9 * sizeof(fe)));
         g->rec_cap = max_records;
     }
+    VG_TRY(grow_challenges(g, g->rec_cap));
     return VG_OK;
 }
 
@@ -2552,4 +2800,9 @@ int vg_gkr_tables_begin(vg_gkr *g, const vg_fe *V, long n, vg_fe **AV, vg_fe **A
 }
 
 const vg_fe *vg_gkr_records_dev(const vg_gkr *g) { return (const vg_fe *)g->rec; }
+void vg_gkr_graph_counts(const vg_gkr *g, long long *replays, long long *captures)
+{
+    *replays = g ? g->graph_replays : 0;
+    *captures = g ? g->graph_captures : 0;
+}
 int vg_gkr_record_count(const vg_gkr *g) { return g->rec_n; }

@@ -17,6 +17,9 @@ int vg_gkr_defer(vg_gkr *g, int on);
 int vg_gkr_phase2_init_deferred(vg_gkr *g, const vg_fe *r_u, int length_u, vg_fe r_last, vg_fe addend);
 // Enqueues the copy of all records to pinned host memory (*host, 9 * *n values).
 int vg_gkr_records(vg_gkr *g, const vg_fe **host, int *n);
+// Phase round sequences issued from a captured CUDA graph so far (replays)
+// and captured so far (captures), counted over the object's life.
+void vg_gkr_graph_counts(const vg_gkr *g, long long *replays, long long *captures);
 
 // Sumcheck tables without a circuit: vg_gkr_round (deferred) over tables the
 // caller fills.  vg_gkr_tables_begin flushes the rounds still queued, hands

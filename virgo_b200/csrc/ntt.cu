@@ -9,8 +9,9 @@
 // decomposition applied recursively, so no separate bit-reversal pass is
 // needed and every pass reads and writes runs of >= G contiguous elements.
 //
-// Inside a CTA each sub-DFT is a radix-2 decimation-in-time transform in
-// shared memory (bit-reversed load, natural-order result).
+// Inside a CTA each sub-DFT is a decimation-in-time transform in shared
+// memory (bit-reversed load, natural-order result) with radix-4 butterflies
+// (two radix-2 stages each, three twiddle products per four entries).
 //
 // Twiddles: w^e for e < n comes from two small tables, lo[e & 4095] *
 // hi[e >> 12], built once per root and cached in the context.
@@ -119,10 +120,49 @@ __global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(PassArgs a)
     }
     __syncthreads();
 
-    // ---- radix-2 DIT stages ----
-    // stage 0 multiplies by w^0 = 1 and stage 1 by 1 or w_m^(m/4), the
-    // square root of -1, which is +-i in F_p2 (i^2 = -1): no products there
-    for (int s = 0; s < a.lm && s < 2; ++s) {
+    // ---- DIT stages, two radix-2 stages at a time (radix 4) ----
+    // For the stage pair (s, s+1), position pos < 2^s inside a group of
+    // 2^(s+2) entries and u = w_m^e, e = pos 2^(lm-2-s), the two radix-2
+    // butterfly layers equal
+    //   t1 = x1 u^2, t2 = x2 u, t3 = x3 u^3,
+    //   y0 = (x0 + t1) + (t2 + t3), y2 = (x0 + t1) - (t2 + t3),
+    //   y1 = (x0 - t1) + J (t2 - t3), y3 = (x0 - t1) - J (t2 - t3),
+    // with J = w_m^(m/4), a square root of -1 in F_p2, i.e. +-i, whose
+    // product is a swap and a negation: three products per four entries
+    // instead of four, and one shared-memory round trip and barrier per two
+    // stages.  The first pair (s = 0) has u = 1 and no products.  u^3 = w^(3e)
+    // with 3e >= m/2 is -T[3e - m/2].  An odd lm ends with one radix-2 stage.
+    const bool j_plus = a.lm >= 2 && T[m >> 2].img == 1;
+    int s = 0;
+    for (; s + 1 < a.lm; s += 2) {
+        const int quarter = 1 << s;
+        for (int b = threadIdx.x; b < (mg >> 2); b += blockDim.x) {
+            const int g = b & (G - 1), q = b >> a.logG;
+            const int pos = q & (quarter - 1), grp = q >> s;
+            const int i0 = (grp << (s + 2)) + pos;
+            fe *p0 = &S[(i0 << a.logG) + g];
+            const int st = quarter << a.logG;
+            fe x0 = p0[0], t1 = p0[st], t2 = p0[2 * st], t3 = p0[3 * st];
+            bool neg3 = false;
+            if (s) {
+                const int e = pos << (a.lm - 2 - s), e3 = 3 * e, h = m >> 1;
+                t1 = t1 * T[2 * e];
+                t2 = t2 * T[e];
+                neg3 = e3 >= h;
+                t3 = t3 * T[neg3 ? e3 - h : e3];
+            }
+            const fe E = x0 + t1, O = x0 - t1;
+            const fe F = neg3 ? t2 - t3 : t2 + t3;
+            const fe Dm = neg3 ? t2 + t3 : t2 - t3;
+            const fe D = j_plus ? vg::fe_make(vg::negp(Dm.img), Dm.real) : vg::fe_make(Dm.img, vg::negp(Dm.real));
+            p0[0] = E + F;
+            p0[2 * st] = E - F;
+            p0[st] = O + D;
+            p0[3 * st] = O - D;
+        }
+        __syncthreads();
+    }
+    if (s < a.lm) {
         const int half = 1 << s;
         for (int b = threadIdx.x; b < (mg >> 1); b += blockDim.x) {
             const int g = b & (G - 1), q = b >> a.logG;
@@ -130,24 +170,7 @@ __global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(PassArgs a)
             const int i0 = (grp << (s + 1)) + pos, i1 = i0 + half;
             fe x0 = S[(i0 << a.logG) + g];
             fe x1 = S[(i1 << a.logG) + g];
-            if (pos) {   // times T[m/4] = +-i: (x.real + i x.img) i = -x.img + i x.real
-                const fe w = T[pos << (a.lm - 1 - s)];
-                x1 = w.img == 1 ? vg::fe_make(vg::negp(x1.img), x1.real) : vg::fe_make(x1.img, vg::negp(x1.real));
-            }
-            S[(i0 << a.logG) + g] = x0 + x1;
-            S[(i1 << a.logG) + g] = x0 - x1;
-        }
-        __syncthreads();
-    }
-    for (int s = 2; s < a.lm; ++s) {
-        const int half = 1 << s;
-        for (int b = threadIdx.x; b < (mg >> 1); b += blockDim.x) {
-            const int g = b & (G - 1), q = b >> a.logG;
-            const int pos = q & (half - 1), grp = q >> s;
-            const int i0 = (grp << (s + 1)) + pos, i1 = i0 + half;
-            fe w = T[pos << (a.lm - 1 - s)];
-            fe x0 = S[(i0 << a.logG) + g];
-            fe x1 = S[(i1 << a.logG) + g] * w;
+            if (pos) x1 = x1 * T[pos << (a.lm - 1 - s)];
             S[(i0 << a.logG) + g] = x0 + x1;
             S[(i1 << a.logG) + g] = x0 - x1;
         }

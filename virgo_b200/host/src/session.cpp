@@ -880,6 +880,8 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
         launches0 += l2;
     }
     zk_prover &p = *s->p;
+    long long greplay0 = 0, gcap0 = 0;
+    vg_gkr_graph_counts(p.dev_gkr, &greplay0, &gcap0);
 
     // launch pass: the whole proof enqueued on the session's stream
     PassResults res;
@@ -943,6 +945,12 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
         launches1 += l2;
     }
     st.launches = launches1 - launches0;
+    {
+        long long gr = 0, gc = 0;
+        vg_gkr_graph_counts(p.dev_gkr, &gr, &gc);
+        st.graph_replays = (int)(gr - greplay0);
+        st.graph_captures = (int)(gc - gcap0);
+    }
     if (stats) *stats = st;
     if (transcript && transcript_len) {
         *transcript_len = tr.bytes.size();
