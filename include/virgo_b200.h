@@ -365,6 +365,26 @@ int vg_session_set_inputs(vg_session *s, const int64_t *values, long n);
  * stats, transcripts and transcript_lens have n entries (or are NULL). */
 int vg_session_prove_batch(vg_session *const *ss, int n, const unsigned *seeds, int want_transcript,
                            vg_proof_stats *stats, uint8_t **transcripts, size_t *transcript_lens);
+/* The session's last proof as a file, for a verifier in another process
+ * (no counterpart in the reference, whose prover and verifier share one
+ * process and talk through method calls, zk_verifier.cpp:910-1253 and
+ * vpd_verifier.cpp:80-335).  The file holds every device result the prover's
+ * host replay consumes; with the circuit file and the seed (in the file), a
+ * process running the reference verifier and the drop-in prover classes over
+ * these results, no GPU, reproduces the proof: the verifier draws the same
+ * rand() values and receives the same messages.  Valid after vg_session_prove
+ * until the next proof or load.  Format (little-endian):
+ *   char "VGPF"; uint32 version (1); uint32 seed; int32 depth;
+ *   int32 bit_length[depth]  (the padded circuit's layers, input first);
+ *   int32 nrec; int32 levels; int32 nq; int64 n_final; int32 proof_size;
+ *   vg_fe records[9 * nrec]  (V_res, then every sumcheck round in call order:
+ *                             its 3 sums, then the folded V, addV, add_mult
+ *                             pairs when one pair remained);
+ *   vg_digest roots[2 + levels] (l, h, FRI level t); vg_fe all_sum[65];
+ *   vg_fe inner; vg_fe fri_r[levels]; vg_fe final_cw[65 * n_final]
+ *   (slice-major); int32 which[nq]; int64 pos[nq] (as for vg_pc_query_batch);
+ *   vg_fe qvals[130 * nq]; vg_digest qpaths[32 * nq]. */
+int vg_session_write_proof(vg_session *s, const char *path);
 /* A session with a context and no circuit yet (vg_session_load gives it one). */
 int vg_session_new(vg_session **out);
 

@@ -389,3 +389,46 @@ def test_reference_verifier_accepts_matmul256(tmp_path):
     assert len(got) > 400
     assert transcript.first_difference(got, ref) is None
     assert runs["gpu"][-1][0] == "V" and runs["gpu"][-1] == runs["ref"][-1]
+
+
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF, "zk_verify_file")), reason="replay verifier not built here")
+@pytest.mark.parametrize("case", ["matmul16_seed1", "random_5layer", "matmul8_32bit"])
+def test_serialized_proof_verified_in_another_process(tmp_path, case):
+    """A GPU session's proof written to a file (vg_session_write_proof) and
+    checked by the reference verifier, compiled unchanged, in a process of
+    its own with no GPU (oracle/_ref/zk_verify_file: the drop-in prover
+    classes answered from the file).  It prints Pass with the session's proof
+    size, and a proof file with one flipped bit in a sumcheck message is
+    rejected."""
+    c = next(x for x in _golden() if x["name"] == case)
+    layers = getattr(circuits, c["generator"])(**c["params"])
+    s = vb.Session(layers)
+    proof = str(tmp_path / "proof.vgpf")
+    try:
+        st, blob = s.prove(c["seed"])
+        s.write_proof(proof)
+    finally:
+        s.close()
+    assert transcript.digest(transcript.parse(blob)) == c["digest"]
+    cpath, mpath = str(tmp_path / "c.txt"), str(tmp_path / "m.txt")
+    circuits.write_text(layers, cpath, mpath)
+    os.symlink(os.path.join(REF, "fft_gkr"), tmp_path / "fft_gkr")
+
+    def verify(path, tag):
+        return subprocess.run([os.path.join(REF, "zk_verify_file"), cpath, mpath, path, str(tmp_path / (tag + ".txt"))],
+                              cwd=str(tmp_path), capture_output=True, text=True, timeout=600)
+
+    out = verify(proof, "res")
+    assert out.returncode == 0 and "Pass" in out.stdout, (out.stdout[-2000:], out.stderr[-2000:])
+    fields = open(tmp_path / "res.txt").read().split()
+    assert int(fields[-1]) == st.proof_size + st.fft_gkr_proof_size
+
+    # one flipped bit in the second record (the first sumcheck round's sums)
+    data = bytearray(open(proof, "rb").read())
+    depth = int.from_bytes(data[12:16], "little")
+    off = 16 + 4 * depth + 4 * 4 + 8 + 9 * 16 + 8   # header, then record 1, its first sum's real part
+    data[off] ^= 1
+    bad = str(tmp_path / "bad.vgpf")
+    open(bad, "wb").write(bytes(data))
+    out = verify(bad, "bad")
+    assert out.returncode != 0 and "Pass" not in out.stdout

@@ -374,3 +374,25 @@ def test_reference_pool_keeps_width_and_counts_timed(tmp_path, monkeypatch):
     assert all(abs(s - 0.21) < 1e-9 for s, _ in timed)
     assert 0 < span < time.perf_counter() - t0
     assert fillers >= 1   # 8 proofs on 3 slots: the last wave is topped up
+
+
+def test_replay_verifier_rejects_malformed_proof_files(tmp_path):
+    """The verifier process for serialized proofs (oracle/_ref/zk_verify_file)
+    refuses files that are not complete VGPF proofs before it verifies
+    anything: wrong magic, a truncated body, trailing bytes."""
+    binary = os.path.join(ROOT, "oracle", "_ref", "zk_verify_file")
+    if not os.path.exists(binary):
+        pytest.skip("replay verifier not built here")
+    L = circuits.matmul_addtree(4, 8, seed=1)
+    c, m = str(tmp_path / "c.txt"), str(tmp_path / "m.txt")
+    circuits.write_text(L, c, m)
+    header = b"VGPF" + (1).to_bytes(4, "little") + (5).to_bytes(4, "little") + (1).to_bytes(4, "little") + \
+        (17).to_bytes(4, "little")
+    cases = {"magic": b"XXXX" + header[4:] + bytes(64), "truncated": header + bytes(8),
+             "trailing": header + (0).to_bytes(4, "little") * 3 + (1).to_bytes(8, "little") +
+             (0).to_bytes(4, "little") + bytes(2 * 32 + 16 * (65 + 1 + 65)) + b"x"}
+    for name, data in cases.items():
+        p = str(tmp_path / (name + ".vgpf"))
+        open(p, "wb").write(data)
+        out = subprocess.run([binary, c, m, p, str(tmp_path / "r.txt")], capture_output=True, text=True, timeout=60)
+        assert out.returncode == 2 and "VGPF" in out.stderr, (name, out.stderr)

@@ -122,6 +122,7 @@ def lib():
             "vg_session_from_file": (c_i, [ctypes.c_char_p, ctypes.POINTER(c_p)]),
             "vg_session_destroy": (c_i, [c_p]),
             "vg_session_depth": (c_i, [c_p, ctypes.POINTER(c_i), ctypes.POINTER(c_i)]),
+            "vg_session_write_proof": (c_i, [c_p, ctypes.c_char_p]),
             "vg_session_prove": (c_i, [c_p, ctypes.c_uint, c_i, ctypes.POINTER(vg_proof_stats),
                                        ctypes.POINTER(c_p), ctypes.POINTER(c_sz)]),
             "vg_session_fork": (c_i, [c_p, ctypes.POINTER(c_p)]),
@@ -299,6 +300,10 @@ class Session:
             check(lib().vg_session_set_inputs(self.h, v.ctypes.data, len(v)), "vg_session_set_inputs")
         else:   # a pinned torch tensor
             check(lib().vg_session_set_inputs(self.h, values.data_ptr(), values.numel()), "vg_session_set_inputs")
+
+    def write_proof(self, path: str):
+        """The last proof as a file (vg_session_write_proof)."""
+        check(lib().vg_session_write_proof(self.h, path.encode()), "vg_session_write_proof")
 
     def set_fft_gkr(self, on: bool):
         """Run the fft_gkr side proof beside every proof (default on)."""

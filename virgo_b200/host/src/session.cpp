@@ -105,6 +105,18 @@ struct CircuitData {
 
 // A session owns its context (CUDA stream, scratch), its commitment state and
 // its prover tables, so sessions prove concurrently from different threads.
+// Device results of the launch pass, read by the replay pass.
+struct PassResults {
+    const F *rec = nullptr;   // GKR records (9 values each)
+    int nrec = 0;
+    vg_pc_results pc{};
+    int levels = 0;
+    // the replay pass's FRI challenges and query plan (kept for the proof file)
+    std::vector<F> fri_r;
+    std::vector<int> which;
+    std::vector<long> pos;
+};
+
 struct vg_session {
     std::shared_ptr<CircuitData> circuit;
     vg_ctx *ctx = nullptr;
@@ -124,6 +136,12 @@ struct vg_session {
     vg_fft_gkr *fft = nullptr;
     int fft_max_lg = 0;
     bool fft_on = true;
+    // the last proof, for vg_session_write_proof: the device results stay in
+    // the objects' pinned buffers until the next proof
+    bool last_valid = false;
+    unsigned last_seed = 0;
+    int last_proof_size = 0;
+    PassResults last;
 };
 
 // The verifier runs `./fft_gkr <L - 6>` next to every proof of input size
@@ -242,6 +260,7 @@ extern "C" int vg_session_load(vg_session *s, int d, const long *n, const uint8_
                                const void *const *v, int index_bytes)
 {
     if (!s || !s->ctx || d < 1 || !n || !ty || !u || !v) return vg_fail(VG_ERR_ARG, "vg_session_load: bad argument");
+    s->last_valid = false;
     int dev = 0;
     vg_ctx_device(s->ctx, &dev);
     cudaSetDevice(dev);
@@ -533,14 +552,6 @@ public:
     }
 };
 
-// Device results of the launch pass, read by the replay pass.
-struct PassResults {
-    const F *rec = nullptr;   // GKR records (9 values each)
-    int nrec = 0;
-    vg_pc_results pc{};
-    int levels = 0;
-};
-
 // One run of the protocol from srand(seed).  launch: every device step is
 // enqueued and nothing is read back (the transcript is off); replay: no
 // device work, every device result comes from `res`, and the transcript,
@@ -766,6 +777,9 @@ static int prove_pass(vg_session *s, unsigned seed, bool launch, PassResults &re
 
     // ---- replay: commitment messages ----
     const vg_pc_results &pr = res.pc;
+    res.fri_r = fri_r;
+    res.which = which;
+    res.pos = pos;
     // the claimed inner product the reference asserts (poly_commit.h:193)
     const F target = alpha_beta_sum - p.Zu * p.sumRc.eval(p.preu1) + all_mask_sum;
     const F inner = *(const F *)pr.inner;
@@ -879,6 +893,7 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
         if (x) vg_ctx_launch_count(x, &l2);
         launches0 += l2;
     }
+    s->last_valid = false;   // the objects' result buffers are about to be reused
     zk_prover &p = *s->p;
     long long greplay0 = 0, gcap0 = 0;
     vg_gkr_graph_counts(p.dev_gkr, &greplay0, &gcap0);
@@ -934,6 +949,10 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
     p.replay = nullptr;
     if (rc != VG_OK) return rc;
     st.replay_s = since(t0);
+    s->last = std::move(res);
+    s->last_seed = seed;
+    s->last_proof_size = proof_size;
+    s->last_valid = true;
 
     st.total_s = since(t_all);
     st.proof_size = proof_size;
@@ -957,6 +976,61 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
         *transcript = (uint8_t *)malloc(tr.bytes.size() ? tr.bytes.size() : 1);
         if (tr.bytes.size()) memcpy(*transcript, tr.bytes.data(), tr.bytes.size());
     }
+    return VG_OK;
+}
+
+// The last proof as a file (format in include/virgo_b200.h): every device
+// result the prover's replay consumes, so a process with the circuit and the
+// seed can answer the reference verifier's calls without a GPU.
+extern "C" int vg_session_write_proof(vg_session *s, const char *path)
+{
+    if (!s || !path) return vg_fail(VG_ERR_ARG, "vg_session_write_proof: null argument");
+    if (!s->last_valid) return vg_fail(VG_ERR_STATE, "vg_session_write_proof: no proof since the last load");
+    const PassResults &r = s->last;
+    const layered_circuit &C = s->circuit->C;
+    const int depth = C.total_depth, levels = r.levels, nq = (int)r.which.size();
+    const int64_t n_final = r.pc.n_final;
+    if ((int)r.fri_r.size() != levels || (int)r.pos.size() != nq)
+        return vg_fail(VG_ERR_STATE, "vg_session_write_proof: inconsistent proof state");
+    FILE *f = fopen(path, "wb");
+    if (!f) return vg_fail(VG_ERR_ARG, "vg_session_write_proof: cannot open %s", path);
+    bool ok = true;
+    auto put = [&](const void *p, size_t n) {
+        if (ok && n && fwrite(p, 1, n, f) != n) ok = false;
+    };
+    const uint32_t version = 1, seed = s->last_seed;
+    put("VGPF", 4);
+    put(&version, 4);
+    put(&seed, 4);
+    put(&depth, 4);
+    for (int i = 0; i < depth; ++i) {
+        const int32_t bl = C.circuit[i].bit_length;
+        put(&bl, 4);
+    }
+    const int32_t nrec = r.nrec, psize = s->last_proof_size;
+    put(&nrec, 4);
+    put(&levels, 4);
+    put(&nq, 4);
+    put(&n_final, 8);
+    put(&psize, 4);
+    put(r.rec, (size_t)nrec * 9 * sizeof(F));
+    put(r.pc.roots, (size_t)(2 + levels) * sizeof(vg_digest));
+    put(r.pc.all_sum, (size_t)(slice_number + 1) * sizeof(vg_fe));
+    put(r.pc.inner, sizeof(vg_fe));
+    put(r.fri_r.data(), (size_t)levels * sizeof(F));
+    put(r.pc.final_cw, (size_t)(slice_number + 1) * n_final * sizeof(vg_fe));
+    for (int q = 0; q < nq; ++q) {
+        const int32_t w = r.which[q];
+        put(&w, 4);
+    }
+    for (int q = 0; q < nq; ++q) {
+        const int64_t p = r.pos[q];
+        put(&p, 8);
+    }
+    put(r.pc.qvals, (size_t)nq * 130 * sizeof(vg_fe));
+    put(r.pc.qpaths, (size_t)nq * 32 * sizeof(vg_digest));
+    if (fclose(f) != 0) ok = false;
+    if (!ok) return vg_fail(VG_ERR_ARG, "vg_session_write_proof: writing %s failed", path);
     return VG_OK;
 }
 
