@@ -456,24 +456,35 @@ __device__ __forceinline__ void edge1(int tk, uint32_t gv, uint32_t o, const Bet
 }
 
 // contribution to the phase-2 tables, split into the parts with and without
-// the factor v_u (applied once per key): am = am1 + amv v_u, av = av1 + avv v_u
-__device__ __forceinline__ void edge2(int tk, uint32_t gv, uint32_t o, const BetaG &bg, const BetaU &bu, fe (&a)[4])
+// the factor v_u (applied once per key): am = am1 + amv v_u, av = av1 + avv v_u.
+// `used` collects which parts an edge touched (bit q for a[q]): a part no
+// edge touched is zero, so its product with v_u can be skipped.
+__device__ __forceinline__ void edge2(int tk, uint32_t gv, uint32_t o, const BetaG &bg, const BetaU &bu, fe (&a)[4],
+                                      unsigned &used)
 {
     const int t = tk & 255;
     const fe x = bg.at(gv) * bu.at(o);
     switch (t) {
-    case 1: a[1] = a[1] + x; break;
-    case 0: a[0] = a[0] + x; a[3] = a[3] + x; break;
+    case 1: a[1] = a[1] + x; used |= 2; break;
+    case 0: a[0] = a[0] + x; a[3] = a[3] + x; used |= 9; break;
     case 5:
-    case 10: a[3] = a[3] + x; break;
-    case 12: a[3] = a[3] + vg::fe_mul_pow2(x, tk >> 8); break;
-    case 6: a[2] = a[2] + x; a[3] = a[3] - x; break;
-    case 7: a[0] = a[0] - x; a[3] = a[3] + x; break;
-    case 8: a[0] = a[0] + x; a[1] = a[1] - (x + x); a[3] = a[3] + x; break;
-    case 13: a[1] = a[1] - x; a[3] = a[3] + x; break;
-    case 9: a[0] = a[0] + x; a[1] = a[1] - x; break;
+    case 10: a[3] = a[3] + x; used |= 8; break;
+    case 12: a[3] = a[3] + vg::fe_mul_pow2(x, tk >> 8); used |= 8; break;
+    case 6: a[2] = a[2] + x; a[3] = a[3] - x; used |= 12; break;
+    case 7: a[0] = a[0] - x; a[3] = a[3] + x; used |= 9; break;
+    case 8: a[0] = a[0] + x; a[1] = a[1] - (x + x); a[3] = a[3] + x; used |= 11; break;
+    case 13: a[1] = a[1] - x; a[3] = a[3] + x; used |= 10; break;
+    case 9: a[0] = a[0] + x; a[1] = a[1] - x; used |= 3; break;
     default: break;
     }
+}
+
+// the phase-2 entries from the parts: am1 + amv v_u and av1 + avv v_u, the
+// product skipped for a part no edge touched (it is zero)
+__device__ __forceinline__ void phase2_out(const fe (&a)[4], unsigned used, fe vu, fe &m, fe &v)
+{
+    m = (used & 2) ? a[0] + a[1] * vu : a[0];
+    v = (used & 8) ? a[2] + a[3] * vu : a[2];
 }
 
 struct EdgeView {
@@ -501,10 +512,9 @@ __global__ void __launch_bounds__(GKR_THREADS) k_gather_keys(EdgeView e, long N,
             out_v[k] = vg::fe_zero();
         } else {
             fe a[4] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
-            for (uint32_t p = s; p < t; ++p) edge2(e.tk[p], e.g[p], e.o[p], bg, bu, a);
-            const fe vu = *vu_ptr;
-            out_m[k] = a[0] + a[1] * vu;
-            out_v[k] = a[2] + a[3] * vu;
+            unsigned used = 0;
+            for (uint32_t p = s; p < t; ++p) edge2(e.tk[p], e.g[p], e.o[p], bg, bu, a, used);
+            phase2_out(a, used, *vu_ptr, out_m[k], out_v[k]);
         }
     }
 }
@@ -531,14 +541,12 @@ __global__ void __launch_bounds__(GKR_THREADS) k_gather_long(EdgeView e, const u
             }
         } else {
             fe a[4] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
-            for (uint32_t p = s + lane; p < t; p += 32) edge2(e.tk[p], e.g[p], e.o[p], bg, bu, a);
+            unsigned used = 0;
+            for (uint32_t p = s + lane; p < t; p += 32) edge2(e.tk[p], e.g[p], e.o[p], bg, bu, a, used);
 #pragma unroll
             for (int q = 0; q < 4; ++q) a[q] = warp_sum(a[q]);
-            if (lane == 0) {
-                const fe vu = *vu_ptr;
-                out_m[k] = a[0] + a[1] * vu;
-                out_v[k] = a[2] + a[3] * vu;
-            }
+            used = __reduce_or_sync(0xffffffffu, used);
+            if (lane == 0) phase2_out(a, used, *vu_ptr, out_m[k], out_v[k]);
         }
     }
 }
@@ -560,8 +568,9 @@ __global__ void __launch_bounds__(GKR_THREADS) k_gather_heavy(EdgeView e, HeavyK
     fe a[4] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
     for (long p = H.s[q] + blockIdx.x * (long)blockDim.x + threadIdx.x; p < (long)H.e[q];
          p += (long)gridDim.x * blockDim.x) {
+        unsigned used = 0;
         if (PH == 0) edge1(e.tk[p], e.g[p], e.o[p], bg, prev, a[0], a[1]);
-        else edge2(e.tk[p], e.g[p], e.o[p], bg, bu, a);
+        else edge2(e.tk[p], e.g[p], e.o[p], bg, bu, a, used);
     }
     block_sum<4>(a, sm);
     if (threadIdx.x == 0)
