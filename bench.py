@@ -544,14 +544,17 @@ def ours(args, layers, rank, world):
             d2h = step(seed0 + 200 + k * args.batch)
         return max_over_ranks(time.perf_counter() - t0, world), d2h
 
-    t_e2e, d2h = e2e_run(False)
+    # the clock sampler runs here too, so that both timed regions see the
+    # same background NVML queries
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clocks_e2e:
+        t_e2e, d2h = e2e_run(False)
     t_e2e_circuit, _ = e2e_run(True)
     pool.shutdown()
     for s in sessions[1:]:
         s.close()
     base.close()
     return {"t_plain": t_plain, "t_batch": t_batch, "t_e2e": t_e2e, "t_e2e_circuit": t_e2e_circuit,
-            "clocks": clocks.summary(), "families": fam, "launches": n_launch, "large_rounds": large_rounds,
+            "clocks": clocks.summary(), "clocks_e2e": clocks_e2e.summary(), "families": fam, "launches": n_launch, "large_rounds": large_rounds,
             "stages": {k: v / args.steps for k, v in stages.items()}, "autotune": tune,
             "h2d": int(u0.nbytes) * args.batch, "h2d_circuit": h2d_circuit * args.batch, "d2h": d2h}
 
@@ -902,7 +905,7 @@ def main():
                       "ms_per_proof": 1000.0 * r["t_plain"] / args.steps,
                       "note": "one proof at a time on one stream, CUDA-event device time"},
             "e2e": {"value": args.steps * args.batch * world / r["t_e2e"], "unit": "proofs/s",
-                    "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"],
+                    "h2d_bytes_per_step": r["h2d"], "d2h_bytes_per_step": r["d2h"], "clocks": r["clocks_e2e"],
                     "note": "%d proofs per step, wall clock: each session takes a new witness (the 2^17 input "
                             "values, int64) from pinned host memory with the wiring resident, proves, downloads "
                             "its transcript (the reference's timed Prove Time likewise excludes reading the "

@@ -40,6 +40,25 @@ extern "C" int vg_ctx_create(int device, vg_ctx **out)
     return VG_OK;
 }
 
+// Gives the context's stream the device's highest scheduling priority (a new
+// stream; the old one is drained and destroyed).  For a stream that carries
+// a proof's critical path, so that concurrent work on other streams fills
+// the SMs it leaves idle instead of delaying it.
+int vg_ctx_raise_priority(vg_ctx *c)
+{
+    if (!c) return vg_fail(VG_ERR_ARG, "vg_ctx_raise_priority: null context");
+    VG_CHECK_CUDA(cudaSetDevice(c->device));
+    int least = 0, greatest = 0;
+    VG_CHECK_CUDA(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+    if (greatest == least) return VG_OK;
+    cudaStream_t s;
+    VG_CHECK_CUDA(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, greatest));
+    VG_CHECK_CUDA(cudaStreamSynchronize(c->stream));
+    cudaStreamDestroy(c->stream);
+    c->stream = s;
+    return VG_OK;
+}
+
 static cudaEvent_t get_event(vg_ctx *c)
 {
     if (!c->event_pool.empty()) {

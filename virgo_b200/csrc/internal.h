@@ -55,6 +55,10 @@ int vg_h2d_staged(vg_ctx *c, void *dst, const void *src, size_t bytes);
 // far on signaler's.
 int vg_ctx_wait_for(vg_ctx *waiter, vg_ctx *signaler);
 
+// Replaces c's stream by one of the device's highest priority (drains the
+// old one first).
+int vg_ctx_raise_priority(vg_ctx *c);
+
 // Grows a device buffer from the stream-ordered pool on c's stream.
 int vg_ctx_grow_dev(vg_ctx *c, void **p, size_t *cap, size_t bytes);
 

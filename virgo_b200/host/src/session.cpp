@@ -217,11 +217,24 @@ extern "C" int vg_session_set_fft_gkr(vg_session *s, int on)
     return VG_OK;
 }
 
+// The sumcheck stream carries a proof's critical path (the layers' chain of
+// phases); the commitment and the side proof run beside it on their own
+// streams with room to spare.  So the sumcheck stream gets the device's
+// highest priority and the others fill the SMs it leaves idle
+// (VIRGO_STREAM_PRIORITY=0: all streams at the default priority).
+static bool prioritise_sumcheck()
+{
+    const char *e = getenv("VIRGO_STREAM_PRIORITY");
+    return !(e && e[0] == '0');
+}
+
 static int session_device(vg_ctx **ctx)
 {
     int dev = 0;
     if (const char *e = getenv("VIRGO_DEVICE")) dev = atoi(e);
-    return vg_ctx_create(dev, ctx);
+    int rc = vg_ctx_create(dev, ctx);
+    if (rc == VG_OK && prioritise_sumcheck()) rc = vg_ctx_raise_priority(*ctx);
+    return rc;
 }
 
 // own context, commitment state and prover over a (possibly shared) circuit
