@@ -786,19 +786,23 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
         }
     }
     __syncthreads();
-    // CTA partials per round
+    if (G.last6 && nchunks == 1 && m == 2 && t == 0) {
+        fe *l6 = rec + 9 * (G.slot0 + G.nsteps - 1) + 3;
+        l6[0] = sV[0]; l6[1] = sV[1]; l6[2] = sA[0]; l6[3] = sA[1]; l6[4] = sM[0]; l6[5] = sM[1];   // rg_ix(0, 1) = 0, 1
+    }
+    // CTA partials per round; a single CTA (a phase's tail group) writes its
+    // warp sums straight into the records, without the cross-CTA pass
+    const bool alone = gridDim.x == 1;
     if ((t & 31) < 3) {
         const int k = t & 31;
         for (int st = t >> 5; st < G.nsteps; st += NW) {
             fe x = vg::fe_zero();
             for (int w = 0; w < NW; ++w) x = x + wsum[(st * NW + w) * 3 + k];
-            parts[((long)st * gridDim.x + blockIdx.x) * 3 + k] = x;
+            if (alone) rec[9 * (G.slot0 + st) + k] = x;
+            else parts[((long)st * gridDim.x + blockIdx.x) * 3 + k] = x;
         }
     }
-    if (G.last6 && nchunks == 1 && m == 2 && t == 0) {
-        fe *l6 = rec + 9 * (G.slot0 + G.nsteps - 1) + 3;
-        l6[0] = sV[0]; l6[1] = sV[1]; l6[2] = sA[0]; l6[3] = sA[1]; l6[4] = sM[0]; l6[5] = sM[1];   // rg_ix(0, 1) = 0, 1
-    }
+    if (alone) return;
     __threadfence();
     __syncthreads();
     if (t == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
