@@ -20,14 +20,22 @@ GOLD = os.path.join(ROOT, "tests", "golden", "transcripts.json")
 
 
 def test_phase_graph_replays_match_golden():
+    """matmul16_seed1 and matmul16_seed7 share the wiring and differ in their
+    input values (and proof seed): one session proves both, switching the
+    witness with set_inputs, between proofs of another circuit."""
     gold = {c["name"]: c for c in json.load(open(GOLD))}
     a1, a7, b = gold["matmul16_seed1"], gold["matmul16_seed7"], gold["random_3layer_pad15"]
-    sa = vb.Session(getattr(circuits, a1["generator"])(**a1["params"]))
+    la1 = getattr(circuits, a1["generator"])(**a1["params"])
+    la7 = getattr(circuits, a7["generator"])(**a7["params"])
+    inputs = {a1["name"]: la1[0][1], a7["name"]: la7[0][1]}
+    sa = vb.Session(la1)
     sb = vb.Session(getattr(circuits, b["generator"])(**b["params"]))
     replays = captures = 0
     try:
         for it in range(4):
             for s, c in ((sa, a1), (sb, b), (sa, a7)):
+                if s is sa:
+                    s.set_inputs(inputs[c["name"]])
                 st, blob = s.prove(c["seed"])
                 assert transcript.digest(transcript.parse(blob)) == c["digest"], (it, c["name"])
                 if it == 0 and c is not a7:
