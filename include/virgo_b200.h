@@ -453,7 +453,11 @@ enum {
                                   from the eq half tables (0) */
     VG_TUNE_GROUP_SPLIT = 9,   /* round groups: steps with few pairs left spread each pair over three
                                   threads, one per table (1), or keep one thread per pair (0) */
-    VG_TUNE_COUNT = 10
+    VG_TUNE_LAZY_FOLD = 10,    /* sumcheck folds x0 + r (x1 - x0): 0 = canonical difference and the
+                                  three-product (Karatsuba) F_p2 product; 1 = the difference left
+                                  unreduced (x1 + 2p - x0) and a four-product (schoolbook) one,
+                                  fewer integer-ALU steps for more multiply-pipe work */
+    VG_TUNE_COUNT = 11
 };
 int vg_tune_get(int device, int key, long *value);
 /* VG_ERR_ARG for a value outside the key's range. */

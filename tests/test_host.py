@@ -63,7 +63,7 @@ def test_tuning_table_validates_and_resets(built):
     lo, hi, df = ctypes.c_long(), ctypes.c_long(), ctypes.c_long()
     assert built.vg_tune_range(2, ctypes.byref(lo), ctypes.byref(hi), ctypes.byref(df)) == 0
     assert (lo.value, hi.value, df.value) == (6, 10, 10)
-    assert built.vg_tune_range(10, None, None, None) == 2
+    assert built.vg_tune_range(11, None, None, None) == 2
     assert built.vg_tune_set(64, 0, 2048) == 2 and built.vg_tune_get(-1, 0, ctypes.byref(lo)) == 2
     vb.tune_reset(0)
     assert vb.tune_get(0) == d

@@ -635,7 +635,14 @@ struct RoundGroup {
     const fe *r;        // fold challenge of each round (device memory, nsteps values)
 };
 
-__device__ __forceinline__ fe rg_fold(fe x0, fe x1, fe r) { return x0 + r * (x1 - x0); }
+// x0 + r (x1 - x0); LAZY: the unreduced difference and the four-product
+// form (vg::fold_lazy), the same canonical value
+template <bool LAZY>
+__device__ __forceinline__ fe rg_fold(fe x0, fe x1, fe r)
+{
+    if (LAZY) return vg::fold_lazy(x0, x1, r);
+    return x0 + r * (x1 - x0);
+}
 
 __device__ __forceinline__ void rg_sums(fe v0, fe v1, fe a0, fe a1, fe m0, fe m1, fe (&acc)[3])
 {
@@ -666,6 +673,7 @@ __device__ __forceinline__ void rg_warp_add(fe (&acc)[3], fe *sm, int step, long
 // CTAs loop over the chunks (chunk q at q * cin of the input), so the grid
 // stays within what is resident at once and the last CTA's reduction reads
 // at most gridDim.x partials per round.
+template <bool LAZY>
 __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict__ xV, const fe *__restrict__ xA,
                                                             const fe *__restrict__ xM, long n_in, RoundGroup G,
                                                             fe *__restrict__ yV, fe *__restrict__ yA, fe *__restrict__ yM,
@@ -702,9 +710,9 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
                     m0v = xM[b]; m1v = xM[b + 1];
                 } else {
                     const long b = base + 4 * k;
-                    v0 = rg_fold(xV[b], xV[b + 1], r); v1 = rg_fold(xV[b + 2], xV[b + 3], r);
-                    a0 = rg_fold(xA[b], xA[b + 1], r); a1 = rg_fold(xA[b + 2], xA[b + 3], r);
-                    m0v = rg_fold(xM[b], xM[b + 1], r); m1v = rg_fold(xM[b + 2], xM[b + 3], r);
+                    v0 = rg_fold<LAZY>(xV[b], xV[b + 1], r); v1 = rg_fold<LAZY>(xV[b + 2], xV[b + 3], r);
+                    a0 = rg_fold<LAZY>(xA[b], xA[b + 1], r); a1 = rg_fold<LAZY>(xA[b + 2], xA[b + 3], r);
+                    m0v = rg_fold<LAZY>(xM[b], xM[b + 1], r); m1v = rg_fold<LAZY>(xM[b + 2], xM[b + 3], r);
                 }
                 const int i0 = rg_ix(2 * k), i1 = rg_ix(2 * k + 1);
                 sV[i0] = v0; sV[i1] = v1;
@@ -729,8 +737,8 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
                 fe f0 = vg::fe_zero(), f1 = vg::fe_zero();
                 __syncthreads();
                 if (act) {
-                    f0 = rg_fold(tab[rg_ix(4 * pp)], tab[rg_ix(4 * pp + 1)], r);
-                    f1 = rg_fold(tab[rg_ix(4 * pp + 2)], tab[rg_ix(4 * pp + 3)], r);
+                    f0 = rg_fold<LAZY>(tab[rg_ix(4 * pp)], tab[rg_ix(4 * pp + 1)], r);
+                    f1 = rg_fold<LAZY>(tab[rg_ix(4 * pp + 2)], tab[rg_ix(4 * pp + 3)], r);
                     stage[6 * pp + 2 * role] = f0;
                     stage[6 * pp + 2 * role + 1] = f1;
                 }
@@ -762,9 +770,9 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
             const bool act = t < npairs;   // m / 4 <= RG_CHUNK / 4 = RG_THREADS: at most one pair per thread
             if (act) {
                 const int b0 = rg_ix(4 * t), b1 = rg_ix(4 * t + 1), b2 = rg_ix(4 * t + 2), b3 = rg_ix(4 * t + 3);
-                v0 = rg_fold(sV[b0], sV[b1], r); v1 = rg_fold(sV[b2], sV[b3], r);
-                a0 = rg_fold(sA[b0], sA[b1], r); a1 = rg_fold(sA[b2], sA[b3], r);
-                m0v = rg_fold(sM[b0], sM[b1], r); m1v = rg_fold(sM[b2], sM[b3], r);
+                v0 = rg_fold<LAZY>(sV[b0], sV[b1], r); v1 = rg_fold<LAZY>(sV[b2], sV[b3], r);
+                a0 = rg_fold<LAZY>(sA[b0], sA[b1], r); a1 = rg_fold<LAZY>(sA[b2], sA[b3], r);
+                m0v = rg_fold<LAZY>(sM[b0], sM[b1], r); m1v = rg_fold<LAZY>(sM[b2], sM[b3], r);
                 rg_sums(v0, v1, a0, a1, m0v, m1v, acc);
             }
             __syncthreads();
@@ -905,13 +913,18 @@ __global__ void k_vu(const fe *__restrict__ last6, fe r, fe addend, fe *__restri
 }
 
 // ------------------------------------------------------------ round kernel
-__device__ __forceinline__ fe fold(fe x0, fe x1, fe r) { return x0 + r * (x1 - x0); }
+template <bool LAZY>
+__device__ __forceinline__ fe fold(fe x0, fe x1, fe r)
+{
+    if (LAZY) return vg::fold_lazy(x0, x1, r);
+    return x0 + r * (x1 - x0);
+}
 
 // The block partials are reduced by the last block to finish (a counter in
 // device memory decides which one), so one launch returns the round sums.
 // The fold challenge comes from device memory (rp), so a captured launch
 // sequence can be replayed with the next proof's challenges.
-template <bool FOLD, int THREADS>
+template <bool FOLD, int THREADS, bool LAZY>
 __global__ void __launch_bounds__(THREADS) k_round(const fe *__restrict__ xV, const fe *__restrict__ xAV,
                                                        const fe *__restrict__ xAM, long npairs,
                                                        const fe *__restrict__ rp,
@@ -927,12 +940,12 @@ __global__ void __launch_bounds__(THREADS) k_round(const fe *__restrict__ xV, co
         fe v0, v1, a0, a1, m0, m1;
         if (FOLD) {
             const long b = 4 * i;
-            v0 = fold(xV[b], xV[b + 1], r);
-            v1 = fold(xV[b + 2], xV[b + 3], r);
-            a0 = fold(xAV[b], xAV[b + 1], r);
-            a1 = fold(xAV[b + 2], xAV[b + 3], r);
-            m0 = fold(xAM[b], xAM[b + 1], r);
-            m1 = fold(xAM[b + 2], xAM[b + 3], r);
+            v0 = fold<LAZY>(xV[b], xV[b + 1], r);
+            v1 = fold<LAZY>(xV[b + 2], xV[b + 3], r);
+            a0 = fold<LAZY>(xAV[b], xAV[b + 1], r);
+            a1 = fold<LAZY>(xAV[b + 2], xAV[b + 3], r);
+            m0 = fold<LAZY>(xAM[b], xAM[b + 1], r);
+            m1 = fold<LAZY>(xAM[b + 2], xAM[b + 3], r);
             yV[2 * i] = v0; yV[2 * i + 1] = v1;
             yAV[2 * i] = a0; yAV[2 * i + 1] = a1;
             yAM[2 * i] = m0; yAM[2 * i + 1] = m1;
@@ -994,7 +1007,7 @@ __global__ void __launch_bounds__(THREADS) k_round(const fe *__restrict__ xV, co
 // last-block pass (6 values per CTA).
 // (both challenges from device memory: rp[0] for the first fold, rp[1] for
 // the second)
-template <bool FOLD, int THREADS>
+template <bool FOLD, int THREADS, bool LAZY>
 __global__ void __launch_bounds__(THREADS) k_round2(const fe *__restrict__ xV, const fe *__restrict__ xAV,
                                                     const fe *__restrict__ xAM, long nquads,
                                                     const fe *__restrict__ rp,
@@ -1012,9 +1025,9 @@ __global__ void __launch_bounds__(THREADS) k_round2(const fe *__restrict__ xV, c
             const long b = 8 * i;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                v[k] = fold(xV[b + 2 * k], xV[b + 2 * k + 1], ra);
-                a[k] = fold(xAV[b + 2 * k], xAV[b + 2 * k + 1], ra);
-                m[k] = fold(xAM[b + 2 * k], xAM[b + 2 * k + 1], ra);
+                v[k] = fold<LAZY>(xV[b + 2 * k], xV[b + 2 * k + 1], ra);
+                a[k] = fold<LAZY>(xAV[b + 2 * k], xAV[b + 2 * k + 1], ra);
+                m[k] = fold<LAZY>(xAM[b + 2 * k], xAM[b + 2 * k + 1], ra);
             }
         } else {
             const long b = 4 * i;
@@ -1027,9 +1040,9 @@ __global__ void __launch_bounds__(THREADS) k_round2(const fe *__restrict__ xV, c
         }
         rg_sums(v[0], v[1], a[0], a[1], m[0], m[1], sa);
         rg_sums(v[2], v[3], a[2], a[3], m[2], m[3], sa);
-        const fe v0 = fold(v[0], v[1], rb), v1 = fold(v[2], v[3], rb);
-        const fe a0 = fold(a[0], a[1], rb), a1 = fold(a[2], a[3], rb);
-        const fe m0 = fold(m[0], m[1], rb), m1 = fold(m[2], m[3], rb);
+        const fe v0 = fold<LAZY>(v[0], v[1], rb), v1 = fold<LAZY>(v[2], v[3], rb);
+        const fe a0 = fold<LAZY>(a[0], a[1], rb), a1 = fold<LAZY>(a[2], a[3], rb);
+        const fe m0 = fold<LAZY>(m[0], m[1], rb), m1 = fold<LAZY>(m[2], m[3], rb);
         rg_sums(v0, v1, a0, a1, m0, m1, sb);
         yV[2 * i] = v0; yV[2 * i + 1] = v1;
         yAV[2 * i] = a0; yAV[2 * i + 1] = a1;
@@ -1157,6 +1170,7 @@ struct vg_circuit {
 struct RoundLaunch {
     int kind = 0;               // 0 k_round, 1 k_round2, 2 k_round_group
     bool fold = false;
+    bool lazy = false;          // folds in the unreduced four-product form (VG_TUNE_LAZY_FOLD)
     int threads = 0;
     unsigned grid = 0;
     long count = 0;             // pairs (k_round), quads (k_round2), input entries (group)
@@ -2211,7 +2225,9 @@ static int rg_smem_attribute(int dev)
     std::lock_guard<std::mutex> lock(mu);
     if (dev >= (int)done.size()) done.resize(dev + 1, false);
     if (!done[dev]) {
-        VG_CHECK_CUDA(cudaFuncSetAttribute(k_round_group, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        VG_CHECK_CUDA(cudaFuncSetAttribute(k_round_group<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                          (int)(RG_SMEM_FE * sizeof(fe))));
+        VG_CHECK_CUDA(cudaFuncSetAttribute(k_round_group<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                           (int)(RG_SMEM_FE * sizeof(fe))));
         done[dev] = true;
     }
@@ -2228,34 +2244,46 @@ static int issue_launch(vg_gkr *g, const RoundLaunch &L, const fe *rp)
         fe *pr = g->round_parts;
         unsigned *cnt = g->round_counter;
         if (L.kind == 0) {
-#define VG_ROUND_LAUNCH(TT)                                                                                          \
+#define VG_ROUND_LAUNCH(TT, LZ)                                                                                      \
     if (L.fold)                                                                                                       \
-        k_round<true, TT><<<L.grid, TT, 0, c->stream>>>(L.x[0], L.x[1], L.x[2], L.count, rp, L.y[0], L.y[1], L.y[2], \
-                                                        pr, cnt, L.oa, L.ob);                                         \
+        k_round<true, TT, LZ><<<L.grid, TT, 0, c->stream>>>(L.x[0], L.x[1], L.x[2], L.count, rp, L.y[0], L.y[1],     \
+                                                            L.y[2], pr, cnt, L.oa, L.ob);                             \
     else                                                                                                              \
-        k_round<false, TT><<<L.grid, TT, 0, c->stream>>>(L.x[0], L.x[1], L.x[2], L.count, rp, nullptr, nullptr,      \
-                                                         nullptr, pr, cnt, L.oa, L.ob)
-            if (L.threads == 128) VG_ROUND_LAUNCH(128);
-            else if (L.threads == 512) VG_ROUND_LAUNCH(512);
-            else VG_ROUND_LAUNCH(256);
+        k_round<false, TT, LZ><<<L.grid, TT, 0, c->stream>>>(L.x[0], L.x[1], L.x[2], L.count, rp, nullptr, nullptr,  \
+                                                             nullptr, pr, cnt, L.oa, L.ob)
+#define VG_ROUND_LAUNCH_T(LZ)                     \
+    if (L.threads == 128) VG_ROUND_LAUNCH(128, LZ); \
+    else if (L.threads == 512) VG_ROUND_LAUNCH(512, LZ); \
+    else VG_ROUND_LAUNCH(256, LZ)
+            if (L.lazy) { VG_ROUND_LAUNCH_T(true); }
+            else { VG_ROUND_LAUNCH_T(false); }
+#undef VG_ROUND_LAUNCH_T
 #undef VG_ROUND_LAUNCH
         } else if (L.kind == 1) {
-#define VG_ROUND2_LAUNCH(TT)                                                                                         \
+#define VG_ROUND2_LAUNCH(TT, LZ)                                                                                     \
     if (L.fold)                                                                                                       \
-        k_round2<true, TT><<<L.grid, TT, 0, c->stream>>>(L.x[0], L.x[1], L.x[2], L.count, rp, L.y[0], L.y[1], L.y[2], \
-                                                         pr, cnt, L.oa, L.ob);                                        \
+        k_round2<true, TT, LZ><<<L.grid, TT, 0, c->stream>>>(L.x[0], L.x[1], L.x[2], L.count, rp, L.y[0], L.y[1],    \
+                                                             L.y[2], pr, cnt, L.oa, L.ob);                            \
     else                                                                                                              \
-        k_round2<false, TT><<<L.grid, TT, 0, c->stream>>>(L.x[0], L.x[1], L.x[2], L.count, rp, L.y[0], L.y[1],       \
-                                                          L.y[2], pr, cnt, L.oa, L.ob)
-            if (L.threads == 128) VG_ROUND2_LAUNCH(128);
-            else if (L.threads == 512) VG_ROUND2_LAUNCH(512);
-            else VG_ROUND2_LAUNCH(256);
+        k_round2<false, TT, LZ><<<L.grid, TT, 0, c->stream>>>(L.x[0], L.x[1], L.x[2], L.count, rp, L.y[0], L.y[1],   \
+                                                              L.y[2], pr, cnt, L.oa, L.ob)
+#define VG_ROUND2_LAUNCH_T(LZ)                     \
+    if (L.threads == 128) VG_ROUND2_LAUNCH(128, LZ); \
+    else if (L.threads == 512) VG_ROUND2_LAUNCH(512, LZ); \
+    else VG_ROUND2_LAUNCH(256, LZ)
+            if (L.lazy) { VG_ROUND2_LAUNCH_T(true); }
+            else { VG_ROUND2_LAUNCH_T(false); }
+#undef VG_ROUND2_LAUNCH_T
 #undef VG_ROUND2_LAUNCH
         } else {
             RoundGroup G = L.G;
             G.r = rp;
-            k_round_group<<<L.grid, RG_THREADS, RG_SMEM_FE * sizeof(fe), c->stream>>>(
-                L.x[0], L.x[1], L.x[2], L.count, G, L.y[0], L.y[1], L.y[2], g->rg_parts, g->round_counter, g->rec);
+            if (L.lazy)
+                k_round_group<true><<<L.grid, RG_THREADS, RG_SMEM_FE * sizeof(fe), c->stream>>>(
+                    L.x[0], L.x[1], L.x[2], L.count, G, L.y[0], L.y[1], L.y[2], g->rg_parts, g->round_counter, g->rec);
+            else
+                k_round_group<false><<<L.grid, RG_THREADS, RG_SMEM_FE * sizeof(fe), c->stream>>>(
+                    L.x[0], L.x[1], L.x[2], L.count, G, L.y[0], L.y[1], L.y[2], g->rg_parts, g->round_counter, g->rec);
         }
     }
     VG_LAUNCHED(c);
@@ -2334,7 +2362,8 @@ static int exec_pending(vg_gkr *g)
     key.push_back((uint64_t)lo);
     key.push_back((uint64_t)hi);
     for (const RoundLaunch &L : launches) {
-        key.push_back((uint64_t)L.kind | ((uint64_t)L.fold << 8) | ((uint64_t)L.threads << 16) | ((uint64_t)L.grid << 32));
+        key.push_back((uint64_t)L.kind | ((uint64_t)L.fold << 4) | ((uint64_t)L.lazy << 5) | ((uint64_t)L.threads << 16) |
+                      ((uint64_t)L.grid << 32));
         key.push_back((uint64_t)L.count);
         for (int k = 0; k < 3; ++k) key.push_back((uint64_t)(uintptr_t)L.x[k]);
         for (int k = 0; k < 3; ++k) key.push_back((uint64_t)(uintptr_t)L.y[k]);
@@ -2409,6 +2438,7 @@ static int launch_round(vg_gkr *g, long n_in, bool fold, fe r, int slot, fe *o3,
     RoundLaunch L;
     L.kind = 0;
     L.fold = fold;
+    L.lazy = vg_tune_value(c->device, VG_TUNE_LAZY_FOLD) != 0;
     L.threads = (int)vg_tune_value(c->device, VG_TUNE_ROUND_THREADS);
     L.grid = std::min<unsigned>(grid_for(npairs, L.threads), std::min(148u * 16u, 148u * 2048u / (unsigned)L.threads));
     L.count = npairs;
@@ -2439,6 +2469,7 @@ static int launch_round2(vg_gkr *g, long n_in, bool fold, int slot)
     RoundLaunch L;
     L.kind = 1;
     L.fold = fold;
+    L.lazy = vg_tune_value(c->device, VG_TUNE_LAZY_FOLD) != 0;
     L.threads = (int)vg_tune_value(c->device, VG_TUNE_ROUND_THREADS);
     L.grid = std::min<unsigned>(grid_for(nquads, L.threads), std::min(148u * 8u, 148u * 2048u / (unsigned)L.threads));
     L.count = nquads;
@@ -2475,6 +2506,7 @@ static int group_rounds(vg_gkr *g)
     vg_ctx *c = g->ctx;
     RoundLaunch L;
     L.kind = 2;
+    L.lazy = vg_tune_value(c->device, VG_TUNE_LAZY_FOLD) != 0;
     RoundGroup &G = L.G;
     int cl = 0;
     while ((1L << cl) < g->pend_chunk) ++cl;

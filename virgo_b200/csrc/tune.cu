@@ -29,6 +29,7 @@ const Range RANGES[VG_TUNE_COUNT] = {
     {0, 2, 0, false},                       // LEAF_ROT
     {0, 1, 1, false},                       // BETA_TABLE
     {0, 1, 0, false},                       // GROUP_SPLIT
+    {0, 1, 0, false},                       // LAZY_FOLD
 };
 
 std::atomic<long> g_tune[MAX_DEVICES][VG_TUNE_COUNT];
