@@ -43,7 +43,7 @@ def golden_sessions():
     ("group_start", 1 << 11), ("group_start", 1 << 13), ("group_start", 1 << 15), ("group_start", 1 << 19),
     ("group_start", 1 << 22), ("round_threads", 128), ("round_threads", 512), ("ntt_max_log", 6),
     ("ntt_max_log", 8), ("ntt_max_log", 9), ("ntt_tile_log", 10), ("ntt_tile_log", 11), ("ntt_tile_log", 13),
-    ("leaf_threads", 64), ("leaf_threads", 128), ("leaf_warp_max", 1 << 24), ("leaf_rot", 1), ("leaf_rot", 2),
+    ("leaf_threads", 64), ("leaf_threads", 128), ("leaf_warp_max", 1 << 24), ("leaf_rot", 1), ("leaf_rot", 2), ("leaf_rot", 3),
     ("beta_table", 0), ("group_split", 1), ("lazy_fold", 1),
 ])
 def test_golden_transcripts_under_every_tuning(golden_sessions, knob, value):
@@ -163,7 +163,7 @@ def test_autotune_keeps_proofs_and_picks_candidates(golden_sessions):
     forks = [s0.fork() for _ in range(2)]
     try:
         chosen, trials = vb.autotune([s0] + forks, seed=3, reps=1)
-        assert len(trials) == 31   # every candidate of every key (autotune.cpp), the defaults included
+        assert len(trials) == 32   # every candidate of every key (autotune.cpp), the defaults included
         for name, v in chosen.items():
             assert any(t[0] == name and t[1] == v for t in trials) or v == vb.tune_get(0)[name]
             assert sum(1 for t in trials if t[0] == name and t[3]) == 1, name

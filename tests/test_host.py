@@ -55,7 +55,7 @@ def test_tuning_table_validates_and_resets(built):
     assert vb.tune_get(0)["group_start"] == 1 << 13 and vb.tune_get(1) == d
     for bad in ({"group_start": 3000}, {"group_start": 1 << 10}, {"round_threads": 1024}, {"ntt_max_log": 11},
                 {"ntt_tile_log": 14}, {"leaf_threads": 96}, {"leaf_warp_max": -1}, {"round_fuse": 3},
-                {"round_fuse": 0}, {"leaf_rot": 3},
+                {"round_fuse": 0}, {"leaf_rot": 4},
                 {"beta_table": 2}, {"group_split": -1}):
         with pytest.raises(vb.VirgoError):
             vb.tune_set(0, **bad)

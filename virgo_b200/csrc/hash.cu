@@ -273,7 +273,7 @@ int vg_leaf_chains(vg_ctx *c, const ChainJobs &jobs)
     } else {
         const int T = (int)vg_tune_value(c->device, VG_TUNE_LEAF_THREADS);
         const int rot = c->hash_kind == VG_HASH_SHA3_256 ? (int)vg_tune_value(c->device, VG_TUNE_LEAF_ROT) : 0;
-        if (rot) VG_TRY(pow2_table(c->device));
+        if (rot == 1 || rot == 2) VG_TRY(pow2_table(c->device));
 #define VG_CHAINS_LAUNCH(TT)                                                                                    \
     if (c->hash_kind == VG_HASH_SHA256)                                                                          \
         k_leaf_chains<VG_HASH_SHA256, TT, 0><<<grid_for(jobs.total, TT), TT, 0, c->stream>>>(jobs);             \
@@ -281,6 +281,8 @@ int vg_leaf_chains(vg_ctx *c, const ChainJobs &jobs)
         k_leaf_chains<VG_HASH_SHA3_256, TT, 1><<<grid_for(jobs.total, TT), TT, 0, c->stream>>>(jobs);          \
     else if (rot == 2)                                                                                           \
         k_leaf_chains<VG_HASH_SHA3_256, TT, 2><<<grid_for(jobs.total, TT), TT, 0, c->stream>>>(jobs);          \
+    else if (rot == 3)                                                                                           \
+        k_leaf_chains<VG_HASH_SHA3_256, TT, 3><<<grid_for(jobs.total, TT), TT, 0, c->stream>>>(jobs);          \
     else                                                                                                         \
         k_leaf_chains<VG_HASH_SHA3_256, TT, 0><<<grid_for(jobs.total, TT), TT, 0, c->stream>>>(jobs)
         if (T == 64) VG_CHAINS_LAUNCH(64);

@@ -54,6 +54,28 @@ __device__ __forceinline__ void sha3_256_64(const uint64_t w[8], uint64_t d[4])
 }
 
 #ifdef VG_HASH_MULROT
+// sha3_256_64 with the 24 rounds in a loop unrolled four times (round
+// constants from constant memory): a sixth of the fully unrolled code, for
+// kernels whose permutation body would not stay in the instruction cache
+__constant__ uint32_t vg_keccak_rcl[24] = VG_KECCAK_RC_LO, vg_keccak_rch[24] = VG_KECCAK_RC_HI;
+__device__ __forceinline__ void sha3_256_64_compact(const uint64_t w[8], uint64_t d[4])
+{
+    uint32_t aL0 = (uint32_t)w[0], aH0 = (uint32_t)(w[0] >> 32), aL1 = (uint32_t)w[1], aH1 = (uint32_t)(w[1] >> 32);
+    uint32_t aL2 = (uint32_t)w[2], aH2 = (uint32_t)(w[2] >> 32), aL3 = (uint32_t)w[3], aH3 = (uint32_t)(w[3] >> 32);
+    uint32_t aL4 = (uint32_t)w[4], aH4 = (uint32_t)(w[4] >> 32), aL5 = (uint32_t)w[5], aH5 = (uint32_t)(w[5] >> 32);
+    uint32_t aL6 = (uint32_t)w[6], aH6 = (uint32_t)(w[6] >> 32), aL7 = (uint32_t)w[7], aH7 = (uint32_t)(w[7] >> 32);
+    uint32_t aL8 = 0x06u, aH8 = 0, aL9 = 0, aH9 = 0, aL10 = 0, aH10 = 0, aL11 = 0, aH11 = 0, aL12 = 0, aH12 = 0;
+    uint32_t aL13 = 0, aH13 = 0, aL14 = 0, aH14 = 0, aL15 = 0, aH15 = 0, aL16 = 0, aH16 = 0x80000000u;
+    uint32_t aL17 = 0, aH17 = 0, aL18 = 0, aH18 = 0, aL19 = 0, aH19 = 0, aL20 = 0, aH20 = 0, aL21 = 0, aH21 = 0;
+    uint32_t aL22 = 0, aH22 = 0, aL23 = 0, aH23 = 0, aL24 = 0, aH24 = 0;
+#pragma unroll 4
+    for (int r = 0; r < 24; ++r) VG_KECCAK_ROUND32(vg_keccak_rcl[r], vg_keccak_rch[r]);
+    d[0] = aL0 | ((uint64_t)aH0 << 32);
+    d[1] = aL1 | ((uint64_t)aH1 << 32);
+    d[2] = aL2 | ((uint64_t)aH2 << 32);
+    d[3] = aL3 | ((uint64_t)aH3 << 32);
+}
+
 // 64-bit rotation left by n (0..31) of (hi:lo) on the integer-multiply pipe:
 // lo * 2^n keeps the bits that stay in the low word and umulhi(hi, 2^n)
 // brings in those crossing from the high word; they share no bit, so the
@@ -226,11 +248,12 @@ __device__ __forceinline__ void hash64(const uint64_t w[8], uint64_t d[4])
 
 #ifdef VG_HASH_MULROT
 // hash64 with the SHA3 rotations in form ROT (0: funnel shifts; 1, 2: see
-// sha3_256_64_mrot)
+// sha3_256_64_mrot; 3: funnel shifts, rounds in a loop unrolled four times)
 template <int KIND, int ROT>
 __device__ __forceinline__ void hash64_rot(const uint64_t w[8], uint64_t d[4])
 {
     if (KIND == HASH_SHA256 || ROT == 0) hash64<KIND>(w, d);
+    else if (ROT == 3) sha3_256_64_compact(w, d);
     else sha3_256_64_mrot<ROT>(w, d);
 }
 #endif

@@ -42,7 +42,7 @@ const std::vector<Knob> &knobs()
         {VG_TUNE_NTT_MAX_LOG, {8, 9, 10}},
         {VG_TUNE_NTT_TILE_LOG, {11, 12, 13}},
         {VG_TUNE_LEAF_THREADS, {64, 128, 256}},
-        {VG_TUNE_LEAF_ROT, {0, 1, 2}},
+        {VG_TUNE_LEAF_ROT, {0, 1, 2, 3}},
         {VG_TUNE_LEAF_WARP_MAX, {0, 1024, 8192}},
     };
     return k;
