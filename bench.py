@@ -57,10 +57,11 @@ FFT_BIN = os.path.join(ROOT, "oracle", "_ref", "fft_gkr")
 COMMIT_BIN = os.path.join(ROOT, "oracle", "_ref", "commit_ref")
 FAMILIES = ["ntt_pass", "leaf_chain", "merkle_level", "fri_fold_leaf", "virtual_oracle", "eval_layer",
             "phase1_scatter", "phase2_scatter", "acc_finalize", "sumcheck_round", "reduce", "other"]
-# DRAM bytes / algorithmic bytes measured by ncu on full-size launches
-# (profiles/k_round_matmul256.txt: (805.4 + 376.0) MB read + written for
-# 1208 MB algorithmic on a 2^24-entry folding round)
-TRAFFIC_RATIO = {"sumcheck_round": 0.978}
+# DRAM bytes / algorithmic bytes measured by ncu on a full-size launch of
+# the family's default kernel (profiles/k_round2_matmul256.txt: (403.0 +
+# 173.3) MB read + written for 604 MB algorithmic on a 2^23-entry paired
+# round)
+TRAFFIC_RATIO = {"sumcheck_round": 0.954}
 HBM_BOUND = {"ntt_pass", "virtual_oracle", "eval_layer", "phase1_scatter", "phase2_scatter", "acc_finalize",
              "sumcheck_round", "reduce"}
 
@@ -842,7 +843,7 @@ def roofline(fam, hbm_peak, peak_kind, large=None):
             "traffic": round(per_launch * traffic) if traffic else None,
             "traffic_source": ("profile-derived constant, not measured in this run: the ratio of ncu "
                                "dram__bytes_read.sum + dram__bytes_write.sum to algorithmic bytes on a full-size "
-                               "launch (profiles/k_round_matmul256.txt, %.3f), times this run's average "
+                               "launch (profiles/k_round2_matmul256.txt, %.3f), times this run's average "
                                "algorithmic bytes per launch" % traffic) if traffic else None,
             "peak_source": peak_kind, "launches_per_proof": f["launches"],
             "avg_launch_us": round(1000.0 * f["ms"] / f["launches"], 2), "bytes_per_launch": per_launch,
@@ -853,15 +854,15 @@ def roofline(fam, hbm_peak, peak_kind, large=None):
                                 "note": "the round launches that move at least 100 MB each (tables of 2^21 "
                                         "entries and up), same events"}
                                if (large and top == "sumcheck_round" and large["ms"] > 0) else None),
-            "alu_pipe_profile": {"frac_large_launches": 0.75, "frac_round_group": 0.33,
+            "alu_pipe_profile": {"frac_large_launches": 0.735, "frac_round_group": 0.33,
                                  "source": "profile-derived constants, not measured in this run: ncu "
-                                           "sm__inst_executed_pipe_alu, pct of peak, of the 2^24-entry fold round "
-                                           "(profiles/k_round_matmul256.txt) and a 64-CTA round group "
-                                           "(profiles/k_round_group_matmul256.txt)"},
+                                           "sm__inst_executed_pipe_alu, pct of peak, of a paired round on a "
+                                           "2^23-entry table (profiles/k_round2_matmul256.txt) and a 64-CTA "
+                                           "round group (profiles/k_round_group_matmul256.txt)"},
             "note": "CUDA events on the launching stream; back-to-back launches share one event, so a "
                     "launch's time runs from the end of the one before it; the large launches are bound by "
-                    "the integer ALU pipe and HBM together (ALU 75%, DRAM 65%), the round groups of the "
-                    "last 17 rounds of each phase by latency"}
+                    "the integer ALU pipe (ALU 73.5%, math-pipe throttle the top stall), the round groups of "
+                    "the last 17 rounds of each phase by latency"}
 
 
 def main():
