@@ -448,8 +448,9 @@ enum {
     VG_TUNE_LEAF_ROT = 7,      /* SHA3 leaf chains (per-thread form): 0 = every 64-bit rotation as
                                   two funnel shifts (ALU pipe); 1 = every other rho rotation, 2 =
                                   every rho rotation as multiplies by 2^n (integer-multiply pipe);
-                                  3 = funnel shifts with the 24 rounds in a loop unrolled four
-                                  times (a sixth of the code, for the instruction cache) */
+                                  3 (default) = funnel shifts with the 24 rounds in a loop
+                                  unrolled four times (a sixth of the code: the fully unrolled
+                                  permutation stalled on instruction fetch) */
     VG_TUNE_BETA_TABLE = 8,    /* phase-2 table builds read each gate's beta_g from a table the
                                   phase-1 builds of the same layer wrote (1), or form it again
                                   from the eq half tables (0) */

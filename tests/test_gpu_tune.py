@@ -43,7 +43,7 @@ def golden_sessions():
     ("group_start", 1 << 11), ("group_start", 1 << 13), ("group_start", 1 << 15), ("group_start", 1 << 19),
     ("group_start", 1 << 22), ("round_threads", 128), ("round_threads", 512), ("ntt_max_log", 6),
     ("ntt_max_log", 8), ("ntt_max_log", 9), ("ntt_tile_log", 10), ("ntt_tile_log", 11), ("ntt_tile_log", 13),
-    ("leaf_threads", 64), ("leaf_threads", 128), ("leaf_warp_max", 1 << 24), ("leaf_rot", 1), ("leaf_rot", 2), ("leaf_rot", 3),
+    ("leaf_threads", 64), ("leaf_threads", 128), ("leaf_warp_max", 1 << 24), ("leaf_rot", 0), ("leaf_rot", 1), ("leaf_rot", 2),
     ("beta_table", 0), ("group_split", 1), ("lazy_fold", 1),
 ])
 def test_golden_transcripts_under_every_tuning(golden_sessions, knob, value):

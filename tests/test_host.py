@@ -49,7 +49,7 @@ def test_tuning_table_validates_and_resets(built):
     vb.tune_reset(1)
     d = vb.tune_get(0)
     assert d == {"group_start": 1 << 17, "round_threads": 256, "ntt_max_log": 10, "ntt_tile_log": 12,
-                 "leaf_threads": 256, "leaf_warp_max": 0, "round_fuse": 2, "leaf_rot": 0,
+                 "leaf_threads": 256, "leaf_warp_max": 0, "round_fuse": 2, "leaf_rot": 3,
                  "beta_table": 1, "group_split": 0, "lazy_fold": 0}
     vb.tune_set(0, group_start=1 << 13, ntt_max_log=8, leaf_warp_max=4096)
     assert vb.tune_get(0)["group_start"] == 1 << 13 and vb.tune_get(1) == d

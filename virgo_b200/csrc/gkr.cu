@@ -764,41 +764,6 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
                 rg_warp_add(acc, wsum, st, 3 * npairs);
                 continue;
             }
-            if (npairs <= 32) {
-                // every remaining step has at most 32 pairs: warp 0 runs them
-                // alone, synchronised per warp (lane t reads entries 4t..4t+3
-                // and writes 2t, 2t+1, all within the warp's pairs), while
-                // the other warps go on to the barrier after the steps
-                __syncthreads();   // the previous step's writes are visible
-                if (t < 32) {
-                    for (; st < G.nsteps; ++st) {
-                        const fe rs = G.r[st];
-                        const long np = m / 4;
-                        fe acc[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
-                        fe v0, v1, a0, a1, m0v, m1v;
-                        const bool act = t < np;
-                        if (act) {
-                            const int b0 = rg_ix(4 * t), b1 = rg_ix(4 * t + 1), b2 = rg_ix(4 * t + 2), b3 = rg_ix(4 * t + 3);
-                            v0 = rg_fold<LAZY>(sV[b0], sV[b1], rs); v1 = rg_fold<LAZY>(sV[b2], sV[b3], rs);
-                            a0 = rg_fold<LAZY>(sA[b0], sA[b1], rs); a1 = rg_fold<LAZY>(sA[b2], sA[b3], rs);
-                            m0v = rg_fold<LAZY>(sM[b0], sM[b1], rs); m1v = rg_fold<LAZY>(sM[b2], sM[b3], rs);
-                            rg_sums(v0, v1, a0, a1, m0v, m1v, acc);
-                        }
-                        __syncwarp();   // every read of this step is done
-                        if (act) {
-                            const int i0 = rg_ix(2 * t), i1 = rg_ix(2 * t + 1);
-                            sV[i0] = v0; sV[i1] = v1;
-                            sA[i0] = a0; sA[i1] = a1;
-                            sM[i0] = m0v; sM[i1] = m1v;
-                        }
-                        __syncwarp();   // the writes are visible to the next step
-                        m >>= 1;
-                        rg_warp_add(acc, wsum, st, np);
-                    }
-                }
-                m = m0 >> (G.nsteps - 1);
-                break;
-            }
             fe acc[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
             fe v0, v1, a0, a1, m0v, m1v;
             __syncthreads();

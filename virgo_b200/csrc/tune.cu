@@ -26,7 +26,7 @@ const Range RANGES[VG_TUNE_COUNT] = {
     {64, 256, 256, true},                   // LEAF_THREADS
     {0, 1L << 24, 0, false},                // LEAF_WARP_MAX
     {1, 2, 2, false},                       // ROUND_FUSE
-    {0, 3, 0, false},                       // LEAF_ROT
+    {0, 3, 3, false},                       // LEAF_ROT
     {0, 1, 1, false},                       // BETA_TABLE
     {0, 1, 0, false},                       // GROUP_SPLIT
     {0, 1, 0, false},                       // LAZY_FOLD
