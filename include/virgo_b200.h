@@ -446,7 +446,8 @@ enum {
                                   consecutive rounds pair into one pass that reads the tables
                                   once and writes a quarter of them */
     VG_TUNE_LEAF_ROT = 7,      /* SHA3 leaf chains (per-thread form): 0 = every 64-bit rotation as
-                                  two funnel shifts (ALU pipe); 1 = every other rho rotation, 2 =
+                                  two funnel shifts (ALU pipe), the 24 rounds fully unrolled;
+                                  1 = every other rho rotation, 2 =
                                   every rho rotation as multiplies by 2^n (integer-multiply pipe);
                                   3 (default) = funnel shifts with the 24 rounds in a loop
                                   unrolled four times (a sixth of the code: the fully unrolled

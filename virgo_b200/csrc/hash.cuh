@@ -53,7 +53,6 @@ __device__ __forceinline__ void sha3_256_64(const uint64_t w[8], uint64_t d[4])
     d[3] = aL3 | ((uint64_t)aH3 << 32);
 }
 
-#ifdef VG_HASH_MULROT
 // sha3_256_64 with the 24 rounds in a loop unrolled four times (round
 // constants from constant memory): a sixth of the fully unrolled code, for
 // kernels whose permutation body would not stay in the instruction cache
@@ -76,6 +75,7 @@ __device__ __forceinline__ void sha3_256_64_compact(const uint64_t w[8], uint64_
     d[3] = aL3 | ((uint64_t)aH3 << 32);
 }
 
+#ifdef VG_HASH_MULROT
 // 64-bit rotation left by n (0..31) of (hi:lo) on the integer-multiply pipe:
 // lo * 2^n keeps the bits that stay in the low word and umulhi(hi, 2^n)
 // brings in those crossing from the high word; they share no bit, so the
@@ -239,11 +239,13 @@ __device__ __forceinline__ void keccak_f_warp(uint32_t &lo, uint32_t &hi, const 
     }
 }
 
+// The digest of 64 bytes; SHA3-256 in the compact form (the rounds in a
+// loop: the fully unrolled permutation stalls on instruction fetch)
 template <int KIND>
 __device__ __forceinline__ void hash64(const uint64_t w[8], uint64_t d[4])
 {
     if (KIND == HASH_SHA256) sha256_64(w, d);
-    else sha3_256_64(w, d);
+    else sha3_256_64_compact(w, d);
 }
 
 #ifdef VG_HASH_MULROT
@@ -252,8 +254,8 @@ __device__ __forceinline__ void hash64(const uint64_t w[8], uint64_t d[4])
 template <int KIND, int ROT>
 __device__ __forceinline__ void hash64_rot(const uint64_t w[8], uint64_t d[4])
 {
-    if (KIND == HASH_SHA256 || ROT == 0) hash64<KIND>(w, d);
-    else if (ROT == 3) sha3_256_64_compact(w, d);
+    if (KIND == HASH_SHA256 || ROT == 3) hash64<KIND>(w, d);
+    else if (ROT == 0) sha3_256_64(w, d);
     else sha3_256_64_mrot<ROT>(w, d);
 }
 #endif
