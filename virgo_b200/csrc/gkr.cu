@@ -673,7 +673,10 @@ __device__ __forceinline__ void rg_warp_add(fe (&acc)[3], fe *sm, int step, long
 // CTAs loop over the chunks (chunk q at q * cin of the input), so the grid
 // stays within what is resident at once and the last CTA's reduction reads
 // at most gridDim.x partials per round.
-template <bool LAZY>
+// SPLIT: the three-thread steps (VG_TUNE_GROUP_SPLIT) are compiled in only
+// when asked for, which keeps the default kernel's code small enough for the
+// instruction cache
+template <bool LAZY, bool SPLIT>
 __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict__ xV, const fe *__restrict__ xA,
                                                             const fe *__restrict__ xM, long n_in, RoundGroup G,
                                                             fe *__restrict__ yV, fe *__restrict__ yA, fe *__restrict__ yM,
@@ -726,7 +729,7 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
         for (int st = 1; st < G.nsteps; ++st) {
             const fe r = G.r[st];
             const long npairs = m / 4;
-            if (G.split3 && 3 * npairs <= RG_THREADS) {
+            if (SPLIT && 3 * npairs <= RG_THREADS) {
                 // few pairs: three threads per pair, one per table, each
                 // folding its table's two entries; the folded pairs meet in
                 // `stage`, and each thread adds one product's share of the
@@ -2225,10 +2228,11 @@ static int rg_smem_attribute(int dev)
     std::lock_guard<std::mutex> lock(mu);
     if (dev >= (int)done.size()) done.resize(dev + 1, false);
     if (!done[dev]) {
-        VG_CHECK_CUDA(cudaFuncSetAttribute(k_round_group<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)(RG_SMEM_FE * sizeof(fe))));
-        VG_CHECK_CUDA(cudaFuncSetAttribute(k_round_group<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                          (int)(RG_SMEM_FE * sizeof(fe))));
+        const int bytes = (int)(RG_SMEM_FE * sizeof(fe));
+        VG_CHECK_CUDA(cudaFuncSetAttribute(k_round_group<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        VG_CHECK_CUDA(cudaFuncSetAttribute(k_round_group<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        VG_CHECK_CUDA(cudaFuncSetAttribute(k_round_group<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+        VG_CHECK_CUDA(cudaFuncSetAttribute(k_round_group<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
         done[dev] = true;
     }
     return VG_OK;
@@ -2278,12 +2282,14 @@ static int issue_launch(vg_gkr *g, const RoundLaunch &L, const fe *rp)
         } else {
             RoundGroup G = L.G;
             G.r = rp;
-            if (L.lazy)
-                k_round_group<true><<<L.grid, RG_THREADS, RG_SMEM_FE * sizeof(fe), c->stream>>>(
-                    L.x[0], L.x[1], L.x[2], L.count, G, L.y[0], L.y[1], L.y[2], g->rg_parts, g->round_counter, g->rec);
-            else
-                k_round_group<false><<<L.grid, RG_THREADS, RG_SMEM_FE * sizeof(fe), c->stream>>>(
-                    L.x[0], L.x[1], L.x[2], L.count, G, L.y[0], L.y[1], L.y[2], g->rg_parts, g->round_counter, g->rec);
+#define VG_GROUP_LAUNCH(LZ, SP)                                                                                      \
+    k_round_group<LZ, SP><<<L.grid, RG_THREADS, RG_SMEM_FE * sizeof(fe), c->stream>>>(                               \
+        L.x[0], L.x[1], L.x[2], L.count, G, L.y[0], L.y[1], L.y[2], g->rg_parts, g->round_counter, g->rec)
+            if (L.lazy && G.split3) VG_GROUP_LAUNCH(true, true);
+            else if (L.lazy) VG_GROUP_LAUNCH(true, false);
+            else if (G.split3) VG_GROUP_LAUNCH(false, true);
+            else VG_GROUP_LAUNCH(false, false);
+#undef VG_GROUP_LAUNCH
         }
     }
     VG_LAUNCHED(c);
