@@ -115,6 +115,11 @@ struct PassResults {
     std::vector<F> fri_r;
     std::vector<int> which;
     std::vector<long> pos;
+    // replay: the commitment's stream, synchronised only when the replay
+    // reaches the commitment (the GKR part overlaps its tail), and the time
+    // spent waiting for it
+    vg_ctx *commit_ctx = nullptr;
+    double commit_wait_s = 0;
 };
 
 struct vg_session {
@@ -789,6 +794,12 @@ static int prove_pass(vg_session *s, unsigned seed, bool launch, PassResults &re
     }
 
     // ---- replay: commitment messages ----
+    if (res.commit_ctx) {
+        const auto w0 = std::chrono::steady_clock::now();
+        const int rc = vg_ctx_sync(res.commit_ctx);
+        res.commit_wait_s += std::chrono::duration<double>(std::chrono::steady_clock::now() - w0).count();
+        if (rc != VG_OK) return rc;
+    }
     const vg_pc_results &pr = res.pc;
     res.fri_r = fri_r;
     res.which = which;
@@ -931,37 +942,52 @@ extern "C" int vg_session_prove(vg_session *s, unsigned seed, int want_transcrip
     auto t0 = clk::now();
     int fft_lg = 0;
     const int rc_fft = fft_side_launch(s, &fft_lg);   // host work hidden behind the proof's device time
-    rc = vg_ctx_sync(s->ctx);
-    if (rc == VG_OK) rc = vg_ctx_sync(s->cctx);
-    if (rc == VG_OK) rc = rc_fft;
-    if (rc != VG_OK) {
-        if (fft_lg) {   // wait for the side proof and clear its run
-            vg_fft_gkr_stats fs;
-            vg_fft_gkr_finish(s->fft, &fs, nullptr, nullptr);
-        }
-        return rc;
-    }
-    if (fft_lg) {
+    // the side proof's own stream is waited for after the replay, which also
+    // overlaps its tail
+    auto finish_side = [&](bool check) -> int {
+        if (!fft_lg) return VG_OK;
         vg_fft_gkr_stats fs;
-        rc = vg_fft_gkr_finish(s->fft, &fs, nullptr, nullptr);
-        if (rc != VG_OK) return rc;
+        const int r = vg_fft_gkr_finish(s->fft, &fs, nullptr, nullptr);
+        fft_lg = check ? fft_lg : 0;
+        if (!check || r != VG_OK) return r;
         if (!fs.pass) return vg_fail(VG_ERR_STATE, "fft_gkr side proof (lg %d) failed its checks", fft_lg);
         st.fft_gkr_s = fs.gpu_s;
         st.fft_gkr_lg = fft_lg;
         st.fft_gkr_proof_size = fs.proof_size;
+        return VG_OK;
+    };
+    // the GKR records are on the host once the sumcheck stream is done; the
+    // replay's commitment part waits for the commitment stream itself
+    rc = vg_ctx_sync(s->ctx);
+    if (rc == VG_OK) rc = rc_fft;
+    if (rc != VG_OK) {
+        vg_ctx_sync(s->cctx);
+        finish_side(false);   // wait for the side proof and clear its run
+        return rc;
     }
     st.wait_s = since(t0);
-    st.prove_time = since(t_all);
 
     // replay pass: messages, checks and the transcript from the device results
     t0 = clk::now();
     res.rec = (const F *)recs;
+    res.commit_ctx = s->cctx;
+    res.commit_wait_s = 0;
     tr.on = want_transcript != 0;
     rc = prove_pass(s, seed, false, res, tr, proof_size);
     p.defer_mode = zk_prover::DEFER_OFF;
     p.replay = nullptr;
+    if (rc != VG_OK) {
+        vg_ctx_sync(s->cctx);
+        finish_side(false);
+        return rc;
+    }
+    const auto t1 = clk::now();
+    rc = finish_side(true);
     if (rc != VG_OK) return rc;
-    st.replay_s = since(t0);
+    const double side_wait = std::chrono::duration<double>(clk::now() - t1).count();
+    st.replay_s = since(t0) - res.commit_wait_s - side_wait;
+    st.wait_s += res.commit_wait_s + side_wait;
+    st.prove_time = st.launch_s + st.wait_s;
     s->last = std::move(res);
     s->last_seed = seed;
     s->last_proof_size = proof_size;
