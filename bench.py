@@ -56,14 +56,14 @@ REF_BIN = os.path.join(ROOT, "oracle", "_ref", "zk_proof_ref")
 FFT_BIN = os.path.join(ROOT, "oracle", "_ref", "fft_gkr")
 COMMIT_BIN = os.path.join(ROOT, "oracle", "_ref", "commit_ref")
 FAMILIES = ["ntt_pass", "leaf_chain", "merkle_level", "fri_fold_leaf", "virtual_oracle", "eval_layer",
-            "phase1_scatter", "phase2_scatter", "acc_finalize", "sumcheck_round", "reduce", "other"]
+            "phase1_scatter", "phase2_scatter", "acc_finalize", "sumcheck_round", "reduce", "other", "gather_round"]
 # DRAM bytes / algorithmic bytes measured by ncu on a full-size launch of
 # the family's default kernel (profiles/k_round2_matmul256.txt: (403.0 +
 # 173.3) MB read + written for 604 MB algorithmic on a 2^23-entry paired
 # round)
 TRAFFIC_RATIO = {"sumcheck_round": 0.954}
 HBM_BOUND = {"ntt_pass", "virtual_oracle", "eval_layer", "phase1_scatter", "phase2_scatter", "acc_finalize",
-             "sumcheck_round", "reduce"}
+             "sumcheck_round", "reduce", "gather_round"}
 
 
 def peaks():

@@ -461,7 +461,11 @@ enum {
                                   three-product (Karatsuba) F_p2 product; 1 = the difference left
                                   unreduced (x1 + 2p - x0) and a four-product (schoolbook) one,
                                   fewer integer-ALU steps for more multiply-pipe work */
-    VG_TUNE_COUNT = 11
+    VG_TUNE_GATHER_FUSE = 11,  /* deferred proofs with paired rounds: a phase's table build over
+                                  the layer's edges runs inside the pass of its first two rounds
+                                  when the table is above the group start (1: the two tables it
+                                  builds are never written in full), or as a launch of its own (0) */
+    VG_TUNE_COUNT = 12
 };
 int vg_tune_get(int device, int key, long *value);
 /* VG_ERR_ARG for a value outside the key's range. */

@@ -284,17 +284,25 @@ def test_sha256_circuit_matches_reference(tmp_path):
     bit-test, range-sum and relay gates; in phase 2 table entry 0 collects
     55 000 summation edges, so the split heavy-entry path runs): the
     reference verifier accepts the reference prover's proof, and the GPU
-    transcript equals it."""
+    transcript equals it; also with the group start lowered to 2^11, so that
+    the phase table builds run inside the phases' first paired passes
+    (reading the long and heavy keys' entries that their own kernels
+    summed), and with those builds as launches of their own."""
     from virgo_b200 import sha256_circuit
     layers = sha256_circuit.sha256_blocks(4, seed=7)
     out, ref = _run_binary(os.path.join(REF, "zk_proof_ref"), layers, 77, tmp_path)
     assert out.returncode == 0 and "Pass" in out.stdout, out.stdout[-2000:]
+    ref = transcript.prover_records(ref)
     s = vb.Session(layers)
     try:
-        _, blob = s.prove(77)
+        for tune in ({}, {"group_start": 1 << 11}, {"group_start": 1 << 11, "gather_fuse": 0}):
+            vb.tune_reset(0)
+            vb.tune_set(0, **tune)
+            _, blob = s.prove(77)
+            assert transcript.first_difference(transcript.parse(blob), ref) is None, tune
     finally:
+        vb.tune_reset(0)
         s.close()
-    assert transcript.first_difference(transcript.parse(blob), transcript.prover_records(ref)) is None
 
 
 def test_session_set_inputs_equals_fresh_circuit():

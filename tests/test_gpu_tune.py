@@ -2,6 +2,7 @@
 same results bit for bit (golden transcripts, oracle kernels), including the
 one-warp-per-chain SHA3 leaf hashing and round groups that start on large
 tables with CTAs looping over chunks; the autotuner keeps proofs unchanged."""
+import ctypes
 import json
 import os
 
@@ -44,7 +45,7 @@ def golden_sessions():
     ("group_start", 1 << 22), ("round_threads", 128), ("round_threads", 512), ("ntt_max_log", 6),
     ("ntt_max_log", 8), ("ntt_max_log", 9), ("ntt_tile_log", 10), ("ntt_tile_log", 11), ("ntt_tile_log", 13),
     ("leaf_threads", 64), ("leaf_threads", 128), ("leaf_warp_max", 1 << 24), ("leaf_rot", 0), ("leaf_rot", 1), ("leaf_rot", 2),
-    ("beta_table", 0), ("group_split", 1), ("lazy_fold", 1),
+    ("beta_table", 0), ("group_split", 1), ("lazy_fold", 1), ("gather_fuse", 0),
 ])
 def test_golden_transcripts_under_every_tuning(golden_sessions, knob, value):
     vb.tune_set(0, **{knob: value})
@@ -163,7 +164,7 @@ def test_autotune_keeps_proofs_and_picks_candidates(golden_sessions):
     forks = [s0.fork() for _ in range(2)]
     try:
         chosen, trials = vb.autotune([s0] + forks, seed=3, reps=1)
-        assert len(trials) == 32   # every candidate of every key (autotune.cpp), the defaults included
+        assert len(trials) == 34   # every candidate of every key (autotune.cpp), the defaults included
         for name, v in chosen.items():
             assert any(t[0] == name and t[1] == v for t in trials) or v == vb.tune_get(0)[name]
             assert sum(1 for t in trials if t[0] == name and t[3]) == 1, name
@@ -176,3 +177,36 @@ def test_autotune_keeps_proofs_and_picks_candidates(golden_sessions):
     finally:
         for f in forks:
             f.close()
+
+
+def _family_launches(ctx, family):
+    n, t, b = ctypes.c_longlong(), ctypes.c_double(), ctypes.c_double()
+    vb.check(vb.lib().vg_ctx_profile_read(ctx, family, ctypes.byref(n), ctypes.byref(t), ctypes.byref(b)))
+    return n.value
+
+
+def test_table_builds_fused_into_first_paired_pass():
+    """Tables above the group start (2^18, 2^19 entries): with the default
+    shapes each phase's table build runs inside its first paired pass (the
+    gather_round family of the per-launch profiler, 12 in common.cuh, counts
+    those launches and the separate builds' families count none of them);
+    with VG_TUNE_GATHER_FUSE = 0 the builds are launches of their own; the
+    proofs are equal."""
+    layers = circuits.random_layered([18, 19, 18, 17], seed=21)
+    s = vb.Session(layers)
+    try:
+        base = s.prove(9)[1]
+        cx = s.ctx()
+        for fuse in (1, 0):
+            vb.tune_set(0, gather_fuse=fuse)
+            vb.check(vb.lib().vg_ctx_profile(cx, 1))
+            blob = s.prove(9)[1]
+            fused, builds = _family_launches(cx, 12), _family_launches(cx, 6) + _family_launches(cx, 7)
+            vb.check(vb.lib().vg_ctx_profile(cx, 0))
+            assert blob == base, fuse
+            if fuse:
+                assert fused >= 4, fused   # both phases of the layers over 2^18 and 2^19 entries
+            else:
+                assert fused == 0 and builds > 0
+    finally:
+        s.close()

@@ -50,20 +50,20 @@ def test_tuning_table_validates_and_resets(built):
     d = vb.tune_get(0)
     assert d == {"group_start": 1 << 17, "round_threads": 256, "ntt_max_log": 10, "ntt_tile_log": 12,
                  "leaf_threads": 256, "leaf_warp_max": 0, "round_fuse": 2, "leaf_rot": 3,
-                 "beta_table": 1, "group_split": 0, "lazy_fold": 0}
+                 "beta_table": 1, "group_split": 0, "lazy_fold": 0, "gather_fuse": 1}
     vb.tune_set(0, group_start=1 << 13, ntt_max_log=8, leaf_warp_max=4096)
     assert vb.tune_get(0)["group_start"] == 1 << 13 and vb.tune_get(1) == d
     for bad in ({"group_start": 3000}, {"group_start": 1 << 10}, {"round_threads": 1024}, {"ntt_max_log": 11},
                 {"ntt_tile_log": 14}, {"leaf_threads": 96}, {"leaf_warp_max": -1}, {"round_fuse": 3},
                 {"round_fuse": 0}, {"leaf_rot": 4},
-                {"beta_table": 2}, {"group_split": -1}):
+                {"beta_table": 2}, {"group_split": -1}, {"gather_fuse": 2}):
         with pytest.raises(vb.VirgoError):
             vb.tune_set(0, **bad)
     assert vb.tune_get(0)["ntt_max_log"] == 8   # a rejected value changes nothing
     lo, hi, df = ctypes.c_long(), ctypes.c_long(), ctypes.c_long()
     assert built.vg_tune_range(2, ctypes.byref(lo), ctypes.byref(hi), ctypes.byref(df)) == 0
     assert (lo.value, hi.value, df.value) == (6, 10, 10)
-    assert built.vg_tune_range(11, None, None, None) == 2
+    assert built.vg_tune_range(12, None, None, None) == 2
     assert built.vg_tune_set(64, 0, 2048) == 2 and built.vg_tune_get(-1, 0, ctypes.byref(lo)) == 2
     vb.tune_reset(0)
     assert vb.tune_get(0) == d

@@ -60,7 +60,7 @@ class vg_tune_trial(ctypes.Structure):
 TUNE_KEYS = {"group_start": 0, "round_threads": 1, "ntt_max_log": 2, "ntt_tile_log": 3, "leaf_threads": 4,
              "leaf_warp_max": 5, "round_fuse": 6,
              "leaf_rot": 7, "beta_table": 8,
-             "group_split": 9, "lazy_fold": 10}
+             "group_split": 9, "lazy_fold": 10, "gather_fuse": 11}
 
 
 def lib():

@@ -21,7 +21,7 @@ struct TwEntry {
 // Kernel families timed by the optional per-launch profiler (vg_ctx_profile).
 enum KernelFamily {
     KF_NTT = 0, KF_LEAF_CHAIN, KF_MERKLE, KF_FRI_FOLD, KF_VIRTUAL_ORACLE, KF_EVAL, KF_SCATTER1, KF_SCATTER2,
-    KF_FINALIZE, KF_ROUND, KF_REDUCE, KF_OTHER, KF_COUNT
+    KF_FINALIZE, KF_ROUND, KF_REDUCE, KF_OTHER, KF_GATHER_ROUND, KF_COUNT
 };
 struct ProfRec {
     int fam;

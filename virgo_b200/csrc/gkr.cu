@@ -999,6 +999,43 @@ __global__ void __launch_bounds__(THREADS) k_round(const fe *__restrict__ xV, co
     }
 }
 
+// The two rounds' sums of a paired pass: one block reduction of the six
+// values, a CTA's partials into parts, and the last CTA to finish (a counter
+// in device memory decides which) adds every CTA's into the two records.
+__device__ __forceinline__ void round2_finish(const fe (&sa)[3], const fe (&sb)[3], fe *sm, bool &last,
+                                              fe *__restrict__ parts, unsigned *__restrict__ counter,
+                                              fe *__restrict__ out_a, fe *__restrict__ out_b)
+{
+    fe acc[6] = {sa[0], sa[1], sa[2], sb[0], sb[1], sb[2]};
+    block_sum<6>(acc, sm);
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) parts[6 * blockIdx.x + k] = acc[k];
+        __threadfence();
+        last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    fe tot[6] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+#pragma unroll
+        for (int k = 0; k < 6; ++k) {
+            fe x;
+            x.img = __ldcg(&parts[6 * b + k].img);
+            x.real = __ldcg(&parts[6 * b + k].real);
+            tot[k] = tot[k] + x;
+        }
+    }
+    __syncthreads();
+    block_sum<6>(tot, sm);
+    if (threadIdx.x == 0) {
+        out_a[0] = tot[0]; out_a[1] = tot[1]; out_a[2] = tot[2];
+        out_b[0] = tot[3]; out_b[1] = tot[4]; out_b[2] = tot[5];
+        *counter = 0;
+    }
+}
+
 // Two consecutive rounds in one pass over tables above the group start
 // (deferred mode): rounds only combine neighbouring entries and both
 // challenges are known, so a thread takes 8 consecutive entries of each table
@@ -1051,34 +1088,74 @@ __global__ void __launch_bounds__(THREADS) k_round2(const fe *__restrict__ xV, c
         yAV[2 * i] = a0; yAV[2 * i + 1] = a1;
         yAM[2 * i] = m0; yAM[2 * i + 1] = m1;
     }
-    fe acc[6] = {sa[0], sa[1], sa[2], sb[0], sb[1], sb[2]};
-    block_sum<6>(acc, sm);
-    if (threadIdx.x == 0) {
+    round2_finish(sa, sb, sm, last, parts, counter, out_a, out_b);
+}
+
+// The phase's table build fused with its first two rounds (deferred mode,
+// paired rounds, tables above the group start).  A thread takes a quad of
+// consecutive keys, sums each key's edges as k_gather_keys does (a key with
+// more than LIGHT_MAX edges was summed beforehand by k_gather_long or
+// k_gather_heavy into tm / tv, read here), reads the quad's V entries and
+// runs k_round2's unfolded body on them: the addV and add_mult tables are
+// never written in full, and the pass after it starts from the folded
+// quarter.
+struct GatherArgs {
+    EdgeView e;
+    BetaG bg;
+    BetaU bu;
+    const fe *prev;   // phase 1: the layer below's values, the edges' other operand
+    const fe *vu;     // phase 2: v_u (device scalar)
+    fe *tm, *tv;      // the add_mult and addV tables: here only the long and heavy keys' entries are read
+};
+
+template <int PH, int THREADS>
+__global__ void __launch_bounds__(THREADS) k_gather_round2(GatherArgs ga, const fe *__restrict__ xV, long nquads,
+                                                           const fe *__restrict__ rp, fe *__restrict__ yV,
+                                                           fe *__restrict__ yAV, fe *__restrict__ yAM,
+                                                           fe *__restrict__ parts, unsigned *__restrict__ counter,
+                                                           fe *__restrict__ out_a, fe *__restrict__ out_b)
+{
+    __shared__ fe sm[6 * 32];
+    __shared__ bool last;
+    const fe rb = rp[1];
+    const fe vu = PH == 1 ? *ga.vu : vg::fe_zero();
+    fe sa[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()}, sb[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+    for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < nquads; i += (long)gridDim.x * blockDim.x) {
+        const long b = 4 * i;
+        fe v[4], a[4], m[4];
+        uint32_t off[5];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) parts[6 * blockIdx.x + k] = acc[k];
-        __threadfence();
-        last = atomicAdd(counter, 1u) == gridDim.x - 1;
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    fe tot[6] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
-    for (int b = threadIdx.x; b < (int)gridDim.x; b += blockDim.x) {
+        for (int k = 0; k < 5; ++k) off[k] = ga.e.off[b + k];
 #pragma unroll
-        for (int k = 0; k < 6; ++k) {
-            fe x;
-            x.img = __ldcg(&parts[6 * b + k].img);
-            x.real = __ldcg(&parts[6 * b + k].real);
-            tot[k] = tot[k] + x;
+        for (int k = 0; k < 4; ++k) {
+            v[k] = xV[b + k];
+            const uint32_t s = off[k], t = off[k + 1];
+            if (t - s > (uint32_t)LIGHT_MAX) {
+                m[k] = ga.tm[b + k];
+                a[k] = ga.tv[b + k];
+            } else if (PH == 0) {
+                fe am = vg::fe_zero(), av = vg::fe_zero();
+                for (uint32_t p = s; p < t; ++p) edge1(ga.e.tk[p], ga.e.g[p], ga.e.o[p], ga.bg, ga.prev, am, av);
+                m[k] = am;
+                a[k] = av;
+            } else {
+                fe q[4] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+                unsigned used = 0;
+                for (uint32_t p = s; p < t; ++p) edge2(ga.e.tk[p], ga.e.g[p], ga.e.o[p], ga.bg, ga.bu, q, used);
+                phase2_out(q, used, vu, m[k], a[k]);
+            }
         }
+        rg_sums(v[0], v[1], a[0], a[1], m[0], m[1], sa);
+        rg_sums(v[2], v[3], a[2], a[3], m[2], m[3], sa);
+        const fe v0 = fold<false>(v[0], v[1], rb), v1 = fold<false>(v[2], v[3], rb);
+        const fe a0 = fold<false>(a[0], a[1], rb), a1 = fold<false>(a[2], a[3], rb);
+        const fe m0 = fold<false>(m[0], m[1], rb), m1 = fold<false>(m[2], m[3], rb);
+        rg_sums(v0, v1, a0, a1, m0, m1, sb);
+        yV[2 * i] = v0; yV[2 * i + 1] = v1;
+        yAV[2 * i] = a0; yAV[2 * i + 1] = a1;
+        yAM[2 * i] = m0; yAM[2 * i + 1] = m1;
     }
-    __syncthreads();
-    block_sum<6>(tot, sm);
-    if (threadIdx.x == 0) {
-        out_a[0] = tot[0]; out_a[1] = tot[1]; out_a[2] = tot[2];
-        out_b[0] = tot[3]; out_b[1] = tot[4]; out_b[2] = tot[5];
-        *counter = 0;
-    }
+    round2_finish(sa, sb, sm, last, parts, counter, out_a, out_b);
 }
 
 vg::fe tofe(vg_fe x) { return vg::fe_make(x.real, x.img); }
@@ -1171,7 +1248,7 @@ struct vg_circuit {
 // the next flush so that a phase's rounds are issued together: after one H2D
 // copy of their challenges, plainly or as a captured CUDA graph.
 struct RoundLaunch {
-    int kind = 0;               // 0 k_round, 1 k_round2, 2 k_round_group
+    int kind = 0;               // 0 k_round, 1 k_round2, 2 k_round_group, 3 k_gather_round2
     bool fold = false;
     bool lazy = false;          // folds in the unreduced four-product form (VG_TUNE_LAZY_FOLD)
     int threads = 0;
@@ -1182,6 +1259,8 @@ struct RoundLaunch {
     int slot = 0;               // challenge slot of the (first) round
     fe *oa = nullptr, *ob = nullptr;   // k_round: sums, folded pair; k_round2: the two rounds' sums
     RoundGroup G{};             // k_round_group (G.r set when issued)
+    GatherArgs ga{};            // k_gather_round2: the table build's operands
+    int ph = 0;                 // k_gather_round2: the phase
     double prof_bytes = 0;
 };
 
@@ -1241,6 +1320,14 @@ struct vg_gkr {
     fe *heavy_parts = nullptr;           // per-CTA partial sums of heavy keys
     fe *bgt = nullptr;                   // beta_g by gate of the current layer (2^max_bl entries)
     int bgt_layer = -1;                  // the layer whose phase-1 gathers filled bgt, -1 none
+    // a deferred phase's table build left to run inside its first paired
+    // pass (k_gather_round2, VG_TUNE_GATHER_FUSE): the build's operands until
+    // that pass is queued, or until another launch needs the tables whole
+    bool gather_pending = false;
+    int gather_ph = 0;
+    long gather_n = 0;                   // table length
+    double gather_bytes = 0;             // the build's algorithmic bytes
+    GatherArgs gather{};
     // fold challenges of the deferred rounds: record slot k's at rhost[k]
     // (pinned, written when the round is queued) and rdev[k] (copied once per
     // flush); a synchronous round's at rsync_host / rsync_dev
@@ -2072,19 +2159,46 @@ static int tables_ready(vg_gkr *g, long N)
     return VG_OK;
 }
 
-// phase tables by gathering over the layer's edge set (no atomics, no finalize)
+static bool fuse_gather(vg_gkr *g, long N);
+
+// The pending table build (gather_tables) as a plain k_gather_keys launch,
+// for a launch that reads the tables whole.
+static int gather_now(vg_gkr *g)
+{
+    if (!g->gather_pending) return VG_OK;
+    g->gather_pending = false;
+    vg_ctx *c = g->ctx;
+    const GatherArgs &a = g->gather;
+    const long N = g->gather_n;
+    const unsigned grid = std::min<unsigned>(grid_for(N, GKR_THREADS), 148u * 64u);
+    {
+        ProfScope ps(c, g->gather_ph == 0 ? KF_SCATTER1 : KF_SCATTER2, g->gather_bytes + 32.0 * (double)N);
+        if (g->gather_ph == 0)
+            k_gather_keys<0><<<grid, GKR_THREADS, 0, c->stream>>>(a.e, N, a.bg, a.bu, a.prev, a.vu, a.tm, a.tv);
+        else
+            k_gather_keys<1><<<grid, GKR_THREADS, 0, c->stream>>>(a.e, N, a.bg, a.bu, a.prev, a.vu, a.tm, a.tv);
+    }
+    VG_LAUNCHED(c);
+    return VG_OK;
+}
+
+// phase tables by gathering over the layer's edge set (no atomics, no
+// finalize).  The keys with more than LIGHT_MAX edges are summed now; the
+// others by k_gather_keys now, or, when the phase's first two rounds will
+// run as one pass (fuse_gather), inside that pass (k_gather_round2).
 template <int PH>
 static int gather_tables(vg_gkr *g, const EdgeSet &E, long N, const fe *prev, const BetaG &bg)
 {
     vg_ctx *c = g->ctx;
     const EdgeView ev{E.off, E.g, E.o, E.tk};
     fe *out_m = g->buf[0][2], *out_v = g->buf[0][1];
-    {
-        ProfScope ps(c, PH == 0 ? KF_SCATTER1 : KF_SCATTER2, 10.0 * (double)E.E + 4.0 * (double)N + 32.0 * (double)N);
-        k_gather_keys<PH><<<std::min<unsigned>(grid_for(N, GKR_THREADS), 148u * 64u), GKR_THREADS, 0, c->stream>>>(
-            ev, N, bg, g->bu, prev, g->vu, out_m, out_v);
-    }
-    VG_LAUNCHED(c);
+    VG_TRY(gather_now(g));
+    g->gather_pending = true;
+    g->gather_ph = PH;
+    g->gather_n = N;
+    g->gather_bytes = 10.0 * (double)E.E + 4.0 * (double)N;   // edge records and key offsets
+    g->gather = GatherArgs{ev, bg, g->bu, prev, g->vu, out_m, out_v};
+    if (!fuse_gather(g, N)) VG_TRY(gather_now(g));
     const int nheavy = (int)(E.heavy_host.size() / 3);
     for (int h0 = 0; h0 < nheavy; h0 += MAX_HEAVY) {   // heavy keys, split over many CTAs
         HeavyKeys H{};
@@ -2194,6 +2308,20 @@ extern "C" int vg_gkr_phase1_init(vg_gkr *g, int layer, const vg_fe *r0, const v
 // for up to 10 rounds; groups follow one another until the phase ends.
 static long group_start(int device) { return vg_tune_value(device, VG_TUNE_GROUP_START); }
 
+// Whether a deferred phase's table build of N entries runs inside its first
+// paired pass: builds fused (VG_TUNE_GATHER_FUSE = 1), paired rounds
+// (VG_TUNE_ROUND_FUSE = 2) and a table above the group start, so that the
+// phase's unfolded first round is held and pairs with the second
+// (vg_gkr_round).  Should the rounds go otherwise, the first launch that
+// reads the tables builds them plainly before it (add_launch).
+static bool fuse_gather(vg_gkr *g, long N)
+{
+    const int d = g->ctx->device;
+    const long S = std::max(2L * RG_CHUNK, group_start(d));
+    return g->deferred && vg_tune_value(d, VG_TUNE_GATHER_FUSE) != 0 && vg_tune_value(d, VG_TUNE_ROUND_FUSE) >= 2 &&
+           N > S && N >= 8;
+}
+
 // With VIRGO_TAIL_CHUNK = c (a power of two below RG_CHUNK), a group starting
 // on more than TAIL_SPLIT chunks' worth of entries uses chunks of c entries,
 // so several CTAs share its first rounds, and the few entries left continue
@@ -2244,7 +2372,7 @@ static int issue_launch(vg_gkr *g, const RoundLaunch &L, const fe *rp)
 {
     vg_ctx *c = g->ctx;
     {
-        ProfScope ps(c, KF_ROUND, L.prof_bytes);
+        ProfScope ps(c, L.kind == 3 ? KF_GATHER_ROUND : KF_ROUND, L.prof_bytes);
         fe *pr = g->round_parts;
         unsigned *cnt = g->round_counter;
         if (L.kind == 0) {
@@ -2279,6 +2407,18 @@ static int issue_launch(vg_gkr *g, const RoundLaunch &L, const fe *rp)
             else { VG_ROUND2_LAUNCH_T(false); }
 #undef VG_ROUND2_LAUNCH_T
 #undef VG_ROUND2_LAUNCH
+        } else if (L.kind == 3) {
+#define VG_GR2_LAUNCH(TT, PH)                                                                                       \
+    k_gather_round2<PH, TT><<<L.grid, TT, 0, c->stream>>>(L.ga, L.x[0], L.count, rp, L.y[0], L.y[1], L.y[2], pr, cnt, \
+                                                          L.oa, L.ob)
+#define VG_GR2_LAUNCH_T(PH)                     \
+    if (L.threads == 128) VG_GR2_LAUNCH(128, PH); \
+    else if (L.threads == 512) VG_GR2_LAUNCH(512, PH); \
+    else VG_GR2_LAUNCH(256, PH)
+            if (L.ph == 0) { VG_GR2_LAUNCH_T(0); }
+            else { VG_GR2_LAUNCH_T(1); }
+#undef VG_GR2_LAUNCH_T
+#undef VG_GR2_LAUNCH
         } else {
             RoundGroup G = L.G;
             G.r = rp;
@@ -2301,6 +2441,7 @@ static int issue_launch(vg_gkr *g, const RoundLaunch &L, const fe *rp)
 // from the record slots).
 static int add_launch(vg_gkr *g, RoundLaunch &L, int nslots, fe r_sync)
 {
+    if (L.kind != 3) VG_TRY(gather_now(g));   // this launch reads the tables whole
     if (!g->deferred) {
         if (!g->rsync_host) return vg_fail(VG_ERR_STATE, "synchronous round on a tables object");
         *g->rsync_host = r_sync;
@@ -2379,6 +2520,15 @@ static int exec_pending(vg_gkr *g)
         key.push_back(((uint64_t)L.G.chunk_log) | ((uint64_t)L.G.nsteps << 8) | ((uint64_t)L.G.first_nofold << 16) |
                       ((uint64_t)L.G.last6 << 24) | ((uint64_t)L.G.split3 << 32));
         key.push_back((uint64_t)L.G.slot0);
+        if (L.kind == 3) {
+            const GatherArgs &a = L.ga;
+            const void *ptrs[] = {a.e.off, a.e.g, a.e.o, a.e.tk, a.bg.f0, a.bg.s0, a.bg.f1, a.bg.s1, a.bg.save,
+                                  a.bg.tab, a.bu.f, a.bu.s, a.prev, a.vu, a.tm, a.tv};
+            for (const void *q : ptrs) key.push_back((uint64_t)(uintptr_t)q);
+            key.push_back((uint64_t)(uint32_t)a.bg.fh | ((uint64_t)(uint32_t)a.bu.fh << 16) | ((uint64_t)L.ph << 32));
+            key.push_back((uint64_t)a.bg.mask);
+            key.push_back((uint64_t)a.bu.mask);
+        }
     }
     key.push_back((uint64_t)(uintptr_t)g->round_parts);
     key.push_back((uint64_t)(uintptr_t)g->round_counter);
@@ -2472,10 +2622,12 @@ static int launch_round2(vg_gkr *g, long n_in, bool fold, int slot)
     vg_ctx *c = g->ctx;
     const long nquads = fold ? n_in / 8 : n_in / 4;
     // at most 148 x 2048 threads and 148 x 8 CTAs (6 sums each in the partials buffer)
+    // the phase's pending table build runs inside its unfolded first pass
+    const bool fused = g->gather_pending && !fold && n_in == g->gather_n;
     RoundLaunch L;
-    L.kind = 1;
+    L.kind = fused ? 3 : 1;
     L.fold = fold;
-    L.lazy = vg_tune_value(c->device, VG_TUNE_LAZY_FOLD) != 0;
+    L.lazy = !fused && vg_tune_value(c->device, VG_TUNE_LAZY_FOLD) != 0;
     L.threads = (int)vg_tune_value(c->device, VG_TUNE_ROUND_THREADS);
     L.grid = std::min<unsigned>(grid_for(nquads, L.threads), std::min(148u * 8u, 148u * 2048u / (unsigned)L.threads));
     L.count = nquads;
@@ -2487,6 +2639,13 @@ static int launch_round2(vg_gkr *g, long n_in, bool fold, int slot)
     L.oa = g->rec + 9 * slot;
     L.ob = g->rec + 9 * (slot + 1);
     L.prof_bytes = (fold ? 480.0 : 288.0) * (double)nquads;   // per quad: read 3 x 8 (or 4) entries, write 3 x 2
+    if (fused) {
+        L.ga = g->gather;
+        L.ph = g->gather_ph;
+        g->gather_pending = false;
+        // the build's edge records and offsets, then per quad: V read (4 entries), 3 x 2 entries written
+        L.prof_bytes = g->gather_bytes + 160.0 * (double)nquads;
+    }
     VG_TRY(add_launch(g, L, 2, vg::fe_zero()));
     for (int k = 0; k < 3; ++k) g->cur[k] = L.y[k];
     g->next_buf ^= 1;
@@ -2553,6 +2712,7 @@ static int group_rounds(vg_gkr *g)
 static int flush_rounds(vg_gkr *g)
 {
     VG_TRY(group_rounds(g));
+    VG_TRY(gather_now(g));   // a build no round took in
     return exec_pending(g);
 }
 

@@ -30,6 +30,7 @@ const Range RANGES[VG_TUNE_COUNT] = {
     {0, 1, 1, false},                       // BETA_TABLE
     {0, 1, 0, false},                       // GROUP_SPLIT
     {0, 1, 0, false},                       // LAZY_FOLD
+    {0, 1, 1, false},                       // GATHER_FUSE
 };
 
 std::atomic<long> g_tune[MAX_DEVICES][VG_TUNE_COUNT];

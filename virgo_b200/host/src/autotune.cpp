@@ -39,6 +39,7 @@ const std::vector<Knob> &knobs()
         {VG_TUNE_BETA_TABLE, {0, 1}},
         {VG_TUNE_GROUP_SPLIT, {0, 1}},
         {VG_TUNE_LAZY_FOLD, {0, 1}},
+        {VG_TUNE_GATHER_FUSE, {0, 1}},
         {VG_TUNE_NTT_MAX_LOG, {8, 9, 10}},
         {VG_TUNE_NTT_TILE_LOG, {11, 12, 13}},
         {VG_TUNE_LEAF_THREADS, {64, 128, 256}},
