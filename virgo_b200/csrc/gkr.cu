@@ -644,13 +644,41 @@ __device__ __forceinline__ fe rg_fold(fe x0, fe x1, fe r)
     return x0 + r * (x1 - x0);
 }
 
+// A round's sums over one pair: (m0 + ma x)(v0 + va x) + a0 + aa x has x^2
+// term ma va, x term ma v0 + m0 va + aa = m1 v1 - m0 v0 - ma va + aa (three
+// products, not four) and constant m0 v0 + a0.  FULL = false leaves out the
+// x term (rg_derive forms it from the round's claim): two products.
+template <bool FULL = true>
 __device__ __forceinline__ void rg_sums(fe v0, fe v1, fe a0, fe a1, fe m0, fe m1, fe (&acc)[3])
 {
     const fe va = v1 - v0, ma = m1 - m0;
-    const fe p2 = ma * va, p0 = m0 * v0, p1 = m1 * v1;
+    const fe p2 = ma * va, p0 = m0 * v0;
     acc[0] = acc[0] + p2;
-    acc[1] = acc[1] + ((p1 - p0 - p2) + (a1 - a0));
+    if (FULL) acc[1] = acc[1] + ((m1 * v1 - p0 - p2) + (a1 - a0));
     acc[2] = acc[2] + p0 + a0;
+}
+
+// The x term of a round that follows another round of its phase, from the
+// others: the round's polynomial s(x) = a x^2 + b x + c sums to the claim
+// s(0) + s(1) = 2c + a + b, and the claim is the previous round's
+// polynomial at this round's fold challenge r (the tables folded with r sum
+// to exactly that), so b = prev(r) - 2c - a, the same field element as the
+// sum of the pairs' x terms (zk_prover.cpp:596-787 sums them).
+__device__ __forceinline__ void rg_derive(fe (&rec)[3], const fe (&prev)[3], fe r)
+{
+    const fe claim = (prev[0] * r + prev[1]) * r + prev[2];
+    rec[1] = claim - (rec[2] + rec[2]) - rec[0];
+}
+
+// a record's three sums, read at L2 (written by other threads of this
+// launch, or by an earlier launch)
+__device__ __forceinline__ void ld_rec3(fe (&x)[3], const fe *p)
+{
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        x[k].img = __ldcg(&p[k].img);
+        x[k].real = __ldcg(&p[k].real);
+    }
 }
 
 // warp sums of acc added into sm[step][warp][3] (a CTA's chunks accumulate
@@ -667,6 +695,23 @@ __device__ __forceinline__ void rg_warp_add(fe (&acc)[3], fe *sm, int step, long
             fe *o = &sm[(step * (RG_THREADS / 32) + wid) * 3 + k];
             *o = *o + acc[k];
         }
+    }
+}
+
+// The x terms of a group's rounds after its first, in order (each round's
+// claim is the record before it at the round's challenge); the first round's
+// was summed (rg_sums<true>), whether or not it folds.
+__device__ __forceinline__ void rg_group_derive(fe *rec, const RoundGroup &G)
+{
+    fe prev[3];
+    ld_rec3(prev, rec + 9 * G.slot0);
+    for (int st = 1; st < G.nsteps; ++st) {
+        fe *o = rec + 9 * (G.slot0 + st);
+        fe x[3];
+        ld_rec3(x, o);
+        rg_derive(x, prev, G.r[st]);
+        o[1] = x[1];
+        prev[0] = x[0]; prev[1] = x[1]; prev[2] = x[2];
     }
 }
 
@@ -732,8 +777,9 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
             if (SPLIT && 3 * npairs <= RG_THREADS) {
                 // few pairs: three threads per pair, one per table, each
                 // folding its table's two entries; the folded pairs meet in
-                // `stage`, and each thread adds one product's share of the
-                // three sums (p0 = m0 v0, p1 = m1 v1, p2 = (m1 - m0)(v1 - v0))
+                // `stage`, and the V and add_mult threads add the x^0 and x^2
+                // sums (p0 = m0 v0 plus a0, p2 = (m1 - m0)(v1 - v0)); the x
+                // term follows from the claim (rg_derive)
                 const int pp = t / 3, role = t - 3 * pp;
                 const bool act = pp < npairs;
                 fe *tab = role == 0 ? sV : (role == 1 ? sA : sM);
@@ -751,17 +797,8 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
                     tab[rg_ix(2 * pp)] = f0;
                     tab[rg_ix(2 * pp + 1)] = f1;
                     const fe *q = stage + 6 * pp;   // v0 v1 a0 a1 m0 m1
-                    if (role == 0) {
-                        const fe p0 = q[4] * q[0];
-                        acc[1] = -p0;
-                        acc[2] = p0 + q[2];
-                    } else if (role == 1) {
-                        acc[1] = q[5] * q[1] + (q[3] - q[2]);
-                    } else {
-                        const fe p2 = (q[5] - q[4]) * (q[1] - q[0]);
-                        acc[0] = p2;
-                        acc[1] = -p2;
-                    }
+                    if (role == 0) acc[2] = q[4] * q[0] + q[2];
+                    else if (role == 2) acc[0] = (q[5] - q[4]) * (q[1] - q[0]);
                 }
                 m >>= 1;
                 rg_warp_add(acc, wsum, st, 3 * npairs);
@@ -776,7 +813,7 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
                 v0 = rg_fold<LAZY>(sV[b0], sV[b1], r); v1 = rg_fold<LAZY>(sV[b2], sV[b3], r);
                 a0 = rg_fold<LAZY>(sA[b0], sA[b1], r); a1 = rg_fold<LAZY>(sA[b2], sA[b3], r);
                 m0v = rg_fold<LAZY>(sM[b0], sM[b1], r); m1v = rg_fold<LAZY>(sM[b2], sM[b3], r);
-                rg_sums(v0, v1, a0, a1, m0v, m1v, acc);
+                rg_sums<false>(v0, v1, a0, a1, m0v, m1v, acc);
             }
             __syncthreads();
             if (act) {
@@ -813,7 +850,11 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
             else parts[((long)st * gridDim.x + blockIdx.x) * 3 + k] = x;
         }
     }
-    if (alone) return;
+    if (alone) {
+        __syncthreads();
+        if (t == 0) rg_group_derive(rec, G);
+        return;
+    }
     __threadfence();
     __syncthreads();
     if (t == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
@@ -852,7 +893,11 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
             o[0] = tot[0]; o[1] = tot[1]; o[2] = tot[2];
         }
     }
-    if (t == 0) *counter = 0;
+    __syncthreads();
+    if (t == 0) {
+        rg_group_derive(rec, G);
+        *counter = 0;
+    }
 }
 
 // ------------------------------------------------ verifier's wiring predicates
@@ -927,13 +972,16 @@ __device__ __forceinline__ fe fold(fe x0, fe x1, fe r)
 // device memory decides which one), so one launch returns the round sums.
 // The fold challenge comes from device memory (rp), so a captured launch
 // sequence can be replayed with the next proof's challenges.
+// A folding round's x term follows from the claim (rg_derive): prev3 holds
+// the previous round's sums (the record before it, or on a synchronous
+// object the sums buffer out3 itself, read before it is written).
 template <bool FOLD, int THREADS, bool LAZY>
 __global__ void __launch_bounds__(THREADS) k_round(const fe *__restrict__ xV, const fe *__restrict__ xAV,
                                                        const fe *__restrict__ xAM, long npairs,
                                                        const fe *__restrict__ rp,
                                                        fe *__restrict__ yV, fe *__restrict__ yAV, fe *__restrict__ yAM,
                                                        fe *__restrict__ parts, unsigned *__restrict__ counter,
-                                                       fe *__restrict__ out3, fe *__restrict__ last6)
+                                                       fe *out3, fe *__restrict__ last6, const fe *prev3)
 {
     __shared__ fe sm[3 * 32];
     __shared__ bool last;
@@ -960,13 +1008,7 @@ __global__ void __launch_bounds__(THREADS) k_round(const fe *__restrict__ xV, co
         if (last6 && npairs == 1) {   // the folded pairs the last round of a phase needs
             last6[0] = v0; last6[1] = v1; last6[2] = a0; last6[3] = a1; last6[4] = m0; last6[5] = m1;
         }
-        // (m0 + ma x)(v0 + va x) + a0 + aa x: x^2 term ma va, x term
-        // ma v0 + m0 va = m1 v1 - m0 v0 - ma va (three products, not four)
-        const fe va = v1 - v0, ma = m1 - m0;
-        const fe p2 = ma * va, p0 = m0 * v0, p1 = m1 * v1;
-        acc[0] = acc[0] + p2;
-        acc[1] = acc[1] + ((p1 - p0 - p2) + (a1 - a0));
-        acc[2] = acc[2] + p0 + a0;
+        rg_sums<!FOLD>(v0, v1, a0, a1, m0, m1, acc);
     }
     block_sum<3>(acc, sm);
     if (threadIdx.x == 0) {
@@ -992,6 +1034,11 @@ __global__ void __launch_bounds__(THREADS) k_round(const fe *__restrict__ xV, co
     __syncthreads();
     block_sum<3>(tot, sm);
     if (threadIdx.x == 0) {
+        if (FOLD) {
+            fe prev[3];
+            ld_rec3(prev, prev3);
+            rg_derive(tot, prev, r);
+        }
         out3[0] = tot[0];
         out3[1] = tot[1];
         out3[2] = tot[2];
@@ -1002,9 +1049,12 @@ __global__ void __launch_bounds__(THREADS) k_round(const fe *__restrict__ xV, co
 // The two rounds' sums of a paired pass: one block reduction of the six
 // values, a CTA's partials into parts, and the last CTA to finish (a counter
 // in device memory decides which) adds every CTA's into the two records.
+// The second round's x term, and the first's when it folds (derive_a), follow
+// from the claims (rg_derive): the first round's claim is the record before
+// out_a at ra, the second's the first round's polynomial at rb.
 __device__ __forceinline__ void round2_finish(const fe (&sa)[3], const fe (&sb)[3], fe *sm, bool &last,
                                               fe *__restrict__ parts, unsigned *__restrict__ counter,
-                                              fe *__restrict__ out_a, fe *__restrict__ out_b)
+                                              fe *out_a, fe *__restrict__ out_b, bool derive_a, fe ra, fe rb)
 {
     fe acc[6] = {sa[0], sa[1], sa[2], sb[0], sb[1], sb[2]};
     block_sum<6>(acc, sm);
@@ -1030,8 +1080,15 @@ __device__ __forceinline__ void round2_finish(const fe (&sa)[3], const fe (&sb)[
     __syncthreads();
     block_sum<6>(tot, sm);
     if (threadIdx.x == 0) {
-        out_a[0] = tot[0]; out_a[1] = tot[1]; out_a[2] = tot[2];
-        out_b[0] = tot[3]; out_b[1] = tot[4]; out_b[2] = tot[5];
+        fe A[3] = {tot[0], tot[1], tot[2]}, B[3] = {tot[3], tot[4], tot[5]};
+        if (derive_a) {
+            fe prev[3];
+            ld_rec3(prev, out_a - 9);
+            rg_derive(A, prev, ra);
+        }
+        rg_derive(B, A, rb);
+        out_a[0] = A[0]; out_a[1] = A[1]; out_a[2] = A[2];
+        out_b[0] = B[0]; out_b[1] = B[1]; out_b[2] = B[2];
         *counter = 0;
     }
 }
@@ -1078,17 +1135,17 @@ __global__ void __launch_bounds__(THREADS) k_round2(const fe *__restrict__ xV, c
                 m[k] = xAM[b + k];
             }
         }
-        rg_sums(v[0], v[1], a[0], a[1], m[0], m[1], sa);
-        rg_sums(v[2], v[3], a[2], a[3], m[2], m[3], sa);
+        rg_sums<!FOLD>(v[0], v[1], a[0], a[1], m[0], m[1], sa);
+        rg_sums<!FOLD>(v[2], v[3], a[2], a[3], m[2], m[3], sa);
         const fe v0 = fold<LAZY>(v[0], v[1], rb), v1 = fold<LAZY>(v[2], v[3], rb);
         const fe a0 = fold<LAZY>(a[0], a[1], rb), a1 = fold<LAZY>(a[2], a[3], rb);
         const fe m0 = fold<LAZY>(m[0], m[1], rb), m1 = fold<LAZY>(m[2], m[3], rb);
-        rg_sums(v0, v1, a0, a1, m0, m1, sb);
+        rg_sums<false>(v0, v1, a0, a1, m0, m1, sb);
         yV[2 * i] = v0; yV[2 * i + 1] = v1;
         yAV[2 * i] = a0; yAV[2 * i + 1] = a1;
         yAM[2 * i] = m0; yAM[2 * i + 1] = m1;
     }
-    round2_finish(sa, sb, sm, last, parts, counter, out_a, out_b);
+    round2_finish(sa, sb, sm, last, parts, counter, out_a, out_b, FOLD, ra, rb);
 }
 
 // The phase's table build fused with its first two rounds (deferred mode,
@@ -1150,12 +1207,12 @@ __global__ void __launch_bounds__(THREADS) k_gather_round2(GatherArgs ga, const 
         const fe v0 = fold<false>(v[0], v[1], rb), v1 = fold<false>(v[2], v[3], rb);
         const fe a0 = fold<false>(a[0], a[1], rb), a1 = fold<false>(a[2], a[3], rb);
         const fe m0 = fold<false>(m[0], m[1], rb), m1 = fold<false>(m[2], m[3], rb);
-        rg_sums(v0, v1, a0, a1, m0, m1, sb);
+        rg_sums<false>(v0, v1, a0, a1, m0, m1, sb);
         yV[2 * i] = v0; yV[2 * i + 1] = v1;
         yAV[2 * i] = a0; yAV[2 * i + 1] = a1;
         yAM[2 * i] = m0; yAM[2 * i + 1] = m1;
     }
-    round2_finish(sa, sb, sm, last, parts, counter, out_a, out_b);
+    round2_finish(sa, sb, sm, last, parts, counter, out_a, out_b, false, vg::fe_zero(), rb);
 }
 
 vg::fe tofe(vg_fe x) { return vg::fe_make(x.real, x.img); }
@@ -1258,6 +1315,7 @@ struct RoundLaunch {
     fe *y[3] = {nullptr, nullptr, nullptr};
     int slot = 0;               // challenge slot of the (first) round
     fe *oa = nullptr, *ob = nullptr;   // k_round: sums, folded pair; k_round2: the two rounds' sums
+    const fe *prev = nullptr;   // k_round that folds: the previous round's sums
     RoundGroup G{};             // k_round_group (G.r set when issued)
     GatherArgs ga{};            // k_gather_round2: the table build's operands
     int ph = 0;                 // k_gather_round2: the phase
@@ -2379,10 +2437,10 @@ static int issue_launch(vg_gkr *g, const RoundLaunch &L, const fe *rp)
 #define VG_ROUND_LAUNCH(TT, LZ)                                                                                      \
     if (L.fold)                                                                                                       \
         k_round<true, TT, LZ><<<L.grid, TT, 0, c->stream>>>(L.x[0], L.x[1], L.x[2], L.count, rp, L.y[0], L.y[1],     \
-                                                            L.y[2], pr, cnt, L.oa, L.ob);                             \
+                                                            L.y[2], pr, cnt, L.oa, L.ob, L.prev);                     \
     else                                                                                                              \
         k_round<false, TT, LZ><<<L.grid, TT, 0, c->stream>>>(L.x[0], L.x[1], L.x[2], L.count, rp, nullptr, nullptr,  \
-                                                             nullptr, pr, cnt, L.oa, L.ob)
+                                                             nullptr, pr, cnt, L.oa, L.ob, nullptr)
 #define VG_ROUND_LAUNCH_T(LZ)                     \
     if (L.threads == 128) VG_ROUND_LAUNCH(128, LZ); \
     else if (L.threads == 512) VG_ROUND_LAUNCH(512, LZ); \
@@ -2517,6 +2575,7 @@ static int exec_pending(vg_gkr *g)
         key.push_back((uint64_t)L.slot);
         key.push_back((uint64_t)(uintptr_t)L.oa);
         key.push_back((uint64_t)(uintptr_t)L.ob);
+        key.push_back((uint64_t)(uintptr_t)L.prev);
         key.push_back(((uint64_t)L.G.chunk_log) | ((uint64_t)L.G.nsteps << 8) | ((uint64_t)L.G.first_nofold << 16) |
                       ((uint64_t)L.G.last6 << 24) | ((uint64_t)L.G.split3 << 32));
         key.push_back((uint64_t)L.G.slot0);
@@ -2605,6 +2664,8 @@ static int launch_round(vg_gkr *g, long n_in, bool fold, fe r, int slot, fe *o3,
     L.slot = slot;
     L.oa = o3;
     L.ob = o6;
+    // the previous round's sums: its record, or (synchronous object) the sums buffer itself
+    L.prev = fold ? (g->deferred ? o3 - 9 : o3) : nullptr;
     L.prof_bytes = (fold ? 288.0 : 96.0) * (double)npairs;   // fold: read 3 tables x 4 entries, write 3 x 2 per pair
     VG_TRY(add_launch(g, L, 1, r));
     if (fold) {
