@@ -606,12 +606,17 @@ __global__ void __launch_bounds__(GKR_THREADS) k_heavy_finish(HeavyKeys H, const
 // contiguous chunk of the three tables can run several consecutive rounds on
 // it without any other CTA: a chunk of 2 RG_CHUNK entries folds into shared
 // memory (RG_CHUNK entries) and keeps folding there until two entries are
-// left, i.e. up to 10 rounds per launch.  The challenges of all those rounds
-// are known in advance (they come from the verifier's rand() stream), so one
-// launch replaces up to 10 round launches and each table is read from HBM
-// once per group instead of once per round.  Per-round partial sums are
-// reduced by the last CTA to finish; every round's sums go to its record.
-constexpr int RG_LOG = 10, RG_CHUNK = 1 << RG_LOG, RG_THREADS = 256, RG_MAX = 12;
+// left, i.e. up to 10 rounds.  The challenges of all those rounds are known
+// in advance (they come from the verifier's rand() stream), so one launch
+// replaces up to 10 round launches and each table is read from HBM once per
+// group instead of once per round.  Per-round partial sums are reduced by
+// the last CTA to finish, which then runs the group's tail: the entries the
+// chunks left (at most 2 RG_CHUNK, written out by every CTA) fold on in its
+// shared memory for up to 10 more rounds, so the rounds of a phase below the
+// group start take one launch.  Every round's sums go to its record.
+constexpr int RG_LOG = 10, RG_CHUNK = 1 << RG_LOG, RG_THREADS = 256;
+// rounds of the chunks (RG_MAX) and of a whole launch with its tail (RG_STEPS)
+constexpr int RG_MAX = 12, RG_STEPS = 20;
 // Per-round partial sums of a group's CTAs ([round][CTA][3]): a group on
 // tables of up to N entries has at most N / RG_CHUNK CTAs, and a group split
 // into small chunks (at most 2 RG_CHUNK entries) at most 2 RG_CHUNK.
@@ -623,11 +628,13 @@ static inline size_t rg_parts_len(long N) { return ((size_t)N / RG_CHUNK + 1 + 2
 __device__ __forceinline__ int rg_ix(long i) { return (int)(i + (i >> 3)); }
 constexpr int RG_TABLE = RG_CHUNK + RG_CHUNK / 8;
 // dynamic shared memory of a group CTA (elements): three tables, per-warp
-// round sums, the folded pairs of the three-thread steps
-constexpr int RG_SMEM_FE = 3 * RG_TABLE + RG_MAX * (RG_THREADS / 32) * 3 + 6 * (RG_THREADS / 3);
+// round sums, each round's totals and challenge, the folded pairs of the
+// three-thread steps
+constexpr int RG_SMEM_FE = 3 * RG_TABLE + RG_STEPS * (RG_THREADS / 32) * 3 + RG_STEPS * 4 + 6 * (RG_THREADS / 3);
 struct RoundGroup {
     int chunk_log;      // log2 of a CTA's entries after its first step (at most RG_LOG)
-    int nsteps;         // rounds in this launch
+    int nsteps;         // rounds in this launch, the tail's included (at most RG_STEPS)
+    int tail;           // of those, the rounds the last CTA runs on the chunks' remaining entries
     int first_nofold;   // the first round has no fold (the round right after a phase init)
     int slot0;          // record of the first round; the others follow
     int last6;          // write the final pair (the table ends at 2 entries) into the last record
@@ -647,7 +654,7 @@ __device__ __forceinline__ fe rg_fold(fe x0, fe x1, fe r)
 // A round's sums over one pair: (m0 + ma x)(v0 + va x) + a0 + aa x has x^2
 // term ma va, x term ma v0 + m0 va + aa = m1 v1 - m0 v0 - ma va + aa (three
 // products, not four) and constant m0 v0 + a0.  FULL = false leaves out the
-// x term (rg_derive forms it from the round's claim): two products.
+// x term (the group's epilogue forms it from the round's claim): two products.
 template <bool FULL = true>
 __device__ __forceinline__ void rg_sums(fe v0, fe v1, fe a0, fe a1, fe m0, fe m1, fe (&acc)[3])
 {
@@ -670,15 +677,22 @@ __device__ __forceinline__ void rg_derive(fe (&rec)[3], const fe (&prev)[3], fe 
     rec[1] = claim - (rec[2] + rec[2]) - rec[0];
 }
 
-// a record's three sums, read at L2 (written by other threads of this
-// launch, or by an earlier launch)
+// a field element read at L2 (written by other CTAs of this launch, or by an
+// earlier launch)
+__device__ __forceinline__ fe ld_fe_cg(const fe *p)
+{
+    const ulonglong2 v = __ldcg(reinterpret_cast<const ulonglong2 *>(p));
+    fe x;
+    x.img = v.x;
+    x.real = v.y;
+    return x;
+}
+
+// a record's three sums, read at L2
 __device__ __forceinline__ void ld_rec3(fe (&x)[3], const fe *p)
 {
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        x[k].img = __ldcg(&p[k].img);
-        x[k].real = __ldcg(&p[k].real);
-    }
+    for (int k = 0; k < 3; ++k) x[k] = ld_fe_cg(p + k);
 }
 
 // warp sums of acc added into sm[step][warp][3] (a CTA's chunks accumulate
@@ -698,69 +712,143 @@ __device__ __forceinline__ void rg_warp_add(fe (&acc)[3], fe *sm, int step, long
     }
 }
 
-// The x terms of a group's rounds after its first, in order (each round's
-// claim is the record before it at the round's challenge); the first round's
-// was summed (rg_sums<true>), whether or not it folds.
-__device__ __forceinline__ void rg_group_derive(fe *rec, const RoundGroup &G)
+// The x terms of a group's rounds after its first (rg_derive), in shared
+// memory:
+//   b_st = a_{st-1} r^2 + b_{st-1} r + c_{st-1} - 2 c_st - a_st.
+// The terms without b_{st-1} are formed
+// by one thread per round, then one thread runs the chain b_st = r b_{st-1}
+// + d_st.  tot: [round][3]; sr: the challenges; d: scratch [round].
+__device__ __forceinline__ void rg_derive_smem(fe *tot, const fe *sr, fe *d, int nsteps)
 {
-    fe prev[3];
-    ld_rec3(prev, rec + 9 * G.slot0);
-    for (int st = 1; st < G.nsteps; ++st) {
-        fe *o = rec + 9 * (G.slot0 + st);
-        fe x[3];
-        ld_rec3(x, o);
-        rg_derive(x, prev, G.r[st]);
-        o[1] = x[1];
-        prev[0] = x[0]; prev[1] = x[1]; prev[2] = x[2];
+    const int t = threadIdx.x;
+    if (t >= 1 && t < nsteps) {
+        const fe r = sr[t];
+        const fe *p = tot + 3 * (t - 1), *o = tot + 3 * t;
+        d[t] = ((p[0] * (r * r) + p[2]) - (o[2] + o[2])) - o[0];
     }
+    __syncthreads();
+    if (t == 0) {
+        fe b = tot[1];
+        for (int st = 1; st < nsteps; ++st) {
+            b = sr[st] * b + d[st];
+            tot[3 * st + 1] = b;
+        }
+    }
+    __syncthreads();
 }
 
 // CTAs loop over the chunks (chunk q at q * cin of the input), so the grid
 // stays within what is resident at once and the last CTA's reduction reads
-// at most gridDim.x partials per round.
+// at most gridDim.x partials per round.  Each CTA runs its chunks as jobs,
+// and the last one then runs the tail as one more job through the same step
+// code (one copy of it: the default kernel stays small enough for the
+// instruction cache).  The tail reads the chunks' remaining entries at L2,
+// after the fence and counter that order every CTA's writes before it.
 // SPLIT: the three-thread steps (VG_TUNE_GROUP_SPLIT) are compiled in only
-// when asked for, which keeps the default kernel's code small enough for the
-// instruction cache
+// when asked for, for the same reason
 template <bool LAZY, bool SPLIT>
 __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict__ xV, const fe *__restrict__ xA,
                                                             const fe *__restrict__ xM, long n_in, RoundGroup G,
-                                                            fe *__restrict__ yV, fe *__restrict__ yA, fe *__restrict__ yM,
-                                                            fe *__restrict__ parts, unsigned *__restrict__ counter,
-                                                            fe *__restrict__ rec)
+                                                            fe *yV, fe *yA, fe *yM, fe *__restrict__ parts,
+                                                            unsigned *__restrict__ counter, fe *__restrict__ rec)
 {
     extern __shared__ fe smem[];
-    fe *sV = smem, *sA = smem + RG_TABLE, *sM = smem + 2 * RG_TABLE;
-    fe *wsum = smem + 3 * RG_TABLE;   // [RG_MAX][warps][3]
-    fe *stage = wsum + RG_MAX * (RG_THREADS / 32) * 3;   // [pair][6] of the three-thread steps
-    __shared__ bool last;
     constexpr int NW = RG_THREADS / 32;
-    const int t = threadIdx.x;
-    for (int i = t; i < RG_MAX * NW * 3; i += RG_THREADS) wsum[i] = vg::fe_zero();
+    fe *sV = smem, *sA = smem + RG_TABLE, *sM = smem + 2 * RG_TABLE;
+    fe *wsum = smem + 3 * RG_TABLE;        // [RG_STEPS][warps][3]
+    fe *tot = wsum + RG_STEPS * NW * 3;    // [RG_STEPS][3]: each round's sums over the whole table
+    fe *sr = tot + RG_STEPS * 3;           // [RG_STEPS]: the rounds' challenges
+    fe *stage = sr + RG_STEPS;             // [pair][6] of the three-thread steps; the epilogue's scratch
+    __shared__ bool last;
+    const int t = threadIdx.x, lane = t & 31, wid = t >> 5;
+    for (int i = t; i < RG_STEPS * NW * 3; i += RG_THREADS) wsum[i] = vg::fe_zero();
+    if (t < G.nsteps) sr[t] = ld_fe_cg(G.r + t);
+    const int k1 = G.nsteps - G.tail;      // rounds of the chunks
     const long chunk = 1L << G.chunk_log;
     const long cin = G.first_nofold ? min(n_in, chunk) : min(n_in, 2L * chunk);
     const long nchunks = n_in / cin;
-    const long m0 = G.first_nofold ? cin : cin / 2;   // entries in shared after the first step
-    long m = m0;
-    for (long q = blockIdx.x; q < nchunks; q += gridDim.x) {
-        const long base = q * cin;
-        m = m0;
-        __syncthreads();   // wsum zeroed; the previous chunk's tables written out
+    const long mfin = (G.first_nofold ? cin : cin / 2) >> (k1 - 1);   // entries a chunk leaves
+    const bool alone = gridDim.x == 1;
+    long m = 0;          // entries in shared memory
+    bool tail = false;   // the job is the tail (after every chunk)
+    for (long q = blockIdx.x;;) {
+        if (!tail && q >= nchunks) {
+            // every chunk of this CTA is done: its round sums
+            __syncthreads();
+            if (alone) {   // a single CTA: its sums are the totals
+                if (t < 3 * k1) {
+                    fe x = vg::fe_zero();
+                    for (int w = 0; w < NW; ++w) x = x + wsum[((t / 3) * NW + w) * 3 + t % 3];
+                    tot[t] = x;
+                }
+            } else {
+                if (t < 3 * k1) {
+                    fe x = vg::fe_zero();
+                    for (int w = 0; w < NW; ++w) x = x + wsum[((t / 3) * NW + w) * 3 + t % 3];
+                    parts[((long)(t / 3) * gridDim.x + blockIdx.x) * 3 + t % 3] = x;
+                }
+                __threadfence();
+                __syncthreads();
+                if (t == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+                __syncthreads();
+                if (!last) return;
+                __threadfence();
+                // warp st sums round st over all CTAs, four partials in flight per lane
+                for (int st = wid; st < k1; st += NW) {
+                    fe s3[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
+                    for (long b0 = lane; b0 < gridDim.x; b0 += 4 * 32) {
+                        fe x[4][3];
+#pragma unroll
+                        for (int j = 0; j < 4; ++j) {
+                            const long b = b0 + 32 * j;
+#pragma unroll
+                            for (int k = 0; k < 3; ++k)
+                                x[j][k] = b < gridDim.x ? ld_fe_cg(&parts[((long)st * gridDim.x + b) * 3 + k])
+                                                        : vg::fe_zero();
+                        }
+#pragma unroll
+                        for (int j = 0; j < 4; ++j)
+#pragma unroll
+                            for (int k = 0; k < 3; ++k) s3[k] = s3[k] + x[j][k];
+                    }
+#pragma unroll
+                    for (int k = 0; k < 3; ++k) s3[k] = warp_sum(s3[k]);
+                    if (lane == 0) {
+                        tot[3 * st] = s3[0];
+                        tot[3 * st + 1] = s3[1];
+                        tot[3 * st + 2] = s3[2];
+                    }
+                }
+            }
+            if (!G.tail) break;
+            tail = true;
+        }
+        // one job: chunk q (rounds 0 .. k1-1), or the tail (rounds k1 .. nsteps-1)
+        const fe *X0 = tail ? yV : xV, *X1 = tail ? yA : xA, *X2 = tail ? yM : xM;
+        const long base = tail ? 0 : q * cin, nin = tail ? nchunks * mfin : cin;
+        const bool nofold = !tail && G.first_nofold;
+        const int st0 = tail ? k1 : 0, st1 = tail ? G.nsteps : k1;
+        m = nofold ? nin : nin / 2;   // entries in shared memory after the first step
+        __syncthreads();   // wsum zeroed, sr loaded; the previous job's tables written out
         // first step: from global into shared
         {
             fe acc[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
-            const fe r = G.r[0];
+            const fe r = sr[st0];
             for (long k = t; k < m / 2; k += RG_THREADS) {
                 fe v0, v1, a0, a1, m0v, m1v;
-                if (G.first_nofold) {
+                if (nofold) {
                     const long b = base + 2 * k;
-                    v0 = xV[b]; v1 = xV[b + 1];
-                    a0 = xA[b]; a1 = xA[b + 1];
-                    m0v = xM[b]; m1v = xM[b + 1];
+                    v0 = ld_fe_cg(X0 + b); v1 = ld_fe_cg(X0 + b + 1);
+                    a0 = ld_fe_cg(X1 + b); a1 = ld_fe_cg(X1 + b + 1);
+                    m0v = ld_fe_cg(X2 + b); m1v = ld_fe_cg(X2 + b + 1);
                 } else {
                     const long b = base + 4 * k;
-                    v0 = rg_fold<LAZY>(xV[b], xV[b + 1], r); v1 = rg_fold<LAZY>(xV[b + 2], xV[b + 3], r);
-                    a0 = rg_fold<LAZY>(xA[b], xA[b + 1], r); a1 = rg_fold<LAZY>(xA[b + 2], xA[b + 3], r);
-                    m0v = rg_fold<LAZY>(xM[b], xM[b + 1], r); m1v = rg_fold<LAZY>(xM[b + 2], xM[b + 3], r);
+                    v0 = rg_fold<LAZY>(ld_fe_cg(X0 + b), ld_fe_cg(X0 + b + 1), r);
+                    v1 = rg_fold<LAZY>(ld_fe_cg(X0 + b + 2), ld_fe_cg(X0 + b + 3), r);
+                    a0 = rg_fold<LAZY>(ld_fe_cg(X1 + b), ld_fe_cg(X1 + b + 1), r);
+                    a1 = rg_fold<LAZY>(ld_fe_cg(X1 + b + 2), ld_fe_cg(X1 + b + 3), r);
+                    m0v = rg_fold<LAZY>(ld_fe_cg(X2 + b), ld_fe_cg(X2 + b + 1), r);
+                    m1v = rg_fold<LAZY>(ld_fe_cg(X2 + b + 2), ld_fe_cg(X2 + b + 3), r);
                 }
                 const int i0 = rg_ix(2 * k), i1 = rg_ix(2 * k + 1);
                 sV[i0] = v0; sV[i1] = v1;
@@ -768,18 +856,18 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
                 sM[i0] = m0v; sM[i1] = m1v;
                 rg_sums(v0, v1, a0, a1, m0v, m1v, acc);
             }
-            rg_warp_add(acc, wsum, 0, m / 2);
+            rg_warp_add(acc, wsum, st0, m / 2);
         }
         // further steps in shared memory: fold m -> m/2, sums over m/4 pairs
-        for (int st = 1; st < G.nsteps; ++st) {
-            const fe r = G.r[st];
+        for (int st = st0 + 1; st < st1; ++st) {
+            const fe r = sr[st];
             const long npairs = m / 4;
             if (SPLIT && 3 * npairs <= RG_THREADS) {
                 // few pairs: three threads per pair, one per table, each
                 // folding its table's two entries; the folded pairs meet in
                 // `stage`, and the V and add_mult threads add the x^0 and x^2
                 // sums (p0 = m0 v0 plus a0, p2 = (m1 - m0)(v1 - v0)); the x
-                // term follows from the claim (rg_derive)
+                // term follows from the claim (rg_derive_smem)
                 const int pp = t / 3, role = t - 3 * pp;
                 const bool act = pp < npairs;
                 fe *tab = role == 0 ? sV : (role == 1 ? sA : sM);
@@ -796,9 +884,9 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
                 if (act) {
                     tab[rg_ix(2 * pp)] = f0;
                     tab[rg_ix(2 * pp + 1)] = f1;
-                    const fe *q = stage + 6 * pp;   // v0 v1 a0 a1 m0 m1
-                    if (role == 0) acc[2] = q[4] * q[0] + q[2];
-                    else if (role == 2) acc[0] = (q[5] - q[4]) * (q[1] - q[0]);
+                    const fe *s6 = stage + 6 * pp;   // v0 v1 a0 a1 m0 m1
+                    if (role == 0) acc[2] = s6[4] * s6[0] + s6[2];
+                    else if (role == 2) acc[0] = (s6[5] - s6[4]) * (s6[1] - s6[0]);
                 }
                 m >>= 1;
                 rg_warp_add(acc, wsum, st, 3 * npairs);
@@ -826,78 +914,33 @@ __global__ void __launch_bounds__(RG_THREADS) k_round_group(const fe *__restrict
             rg_warp_add(acc, wsum, st, npairs);
         }
         __syncthreads();
-        // the chunk's remaining m entries (none when the group folded nothing)
+        // the job's remaining m entries (none when the group folded nothing);
+        // the tail's go to the start of the same tables, every read of them done
+        const long yo = tail ? 0 : q * m;
         for (long k = t; yV && k < m; k += RG_THREADS) {
-            yV[q * m + k] = sV[rg_ix(k)];
-            yA[q * m + k] = sA[rg_ix(k)];
-            yM[q * m + k] = sM[rg_ix(k)];
+            yV[yo + k] = sV[rg_ix(k)];
+            yA[yo + k] = sA[rg_ix(k)];
+            yM[yo + k] = sM[rg_ix(k)];
         }
+        if (tail) break;
+        q += gridDim.x;
     }
+    // a single CTA or the last one: the tail's sums (its own warps'), the
+    // final pair, the x terms, the records
     __syncthreads();
-    if (G.last6 && nchunks == 1 && m == 2 && t == 0) {
+    if (tail && t < 3 * G.tail) {
+        fe x = vg::fe_zero();
+        for (int w = 0; w < NW; ++w) x = x + wsum[((k1 + t / 3) * NW + w) * 3 + t % 3];
+        tot[3 * k1 + t] = x;
+    }
+    if (G.last6 && m == 2 && t == 0) {
         fe *l6 = rec + 9 * (G.slot0 + G.nsteps - 1) + 3;
         l6[0] = sV[0]; l6[1] = sV[1]; l6[2] = sA[0]; l6[3] = sA[1]; l6[4] = sM[0]; l6[5] = sM[1];   // rg_ix(0, 1) = 0, 1
     }
-    // CTA partials per round; a single CTA (a phase's tail group) writes its
-    // warp sums straight into the records, without the cross-CTA pass
-    const bool alone = gridDim.x == 1;
-    if ((t & 31) < 3) {
-        const int k = t & 31;
-        for (int st = t >> 5; st < G.nsteps; st += NW) {
-            fe x = vg::fe_zero();
-            for (int w = 0; w < NW; ++w) x = x + wsum[(st * NW + w) * 3 + k];
-            if (alone) rec[9 * (G.slot0 + st) + k] = x;
-            else parts[((long)st * gridDim.x + blockIdx.x) * 3 + k] = x;
-        }
-    }
-    if (alone) {
-        __syncthreads();
-        if (t == 0) rg_group_derive(rec, G);
-        return;
-    }
-    __threadfence();
     __syncthreads();
-    if (t == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    // warp st sums round st over all CTAs, four partials in flight per lane
-    const int wid = t >> 5, lane = t & 31;
-    for (int st = wid; st < G.nsteps; st += NW) {
-        fe tot[3] = {vg::fe_zero(), vg::fe_zero(), vg::fe_zero()};
-        for (long b0 = lane; b0 < gridDim.x; b0 += 4 * 32) {
-            fe x[4][3];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-                const long b = b0 + 32 * j;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    if (b < gridDim.x) {
-                        const fe *p = &parts[((long)st * gridDim.x + b) * 3 + k];
-                        x[j][k].img = __ldcg(&p->img);
-                        x[j][k].real = __ldcg(&p->real);
-                    } else {
-                        x[j][k] = vg::fe_zero();
-                    }
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < 4; ++j)
-#pragma unroll
-                for (int k = 0; k < 3; ++k) tot[k] = tot[k] + x[j][k];
-        }
-#pragma unroll
-        for (int k = 0; k < 3; ++k) tot[k] = warp_sum(tot[k]);
-        if (lane == 0) {
-            fe *o = rec + 9 * (G.slot0 + st);
-            o[0] = tot[0]; o[1] = tot[1]; o[2] = tot[2];
-        }
-    }
-    __syncthreads();
-    if (t == 0) {
-        rg_group_derive(rec, G);
-        *counter = 0;
-    }
+    rg_derive_smem(tot, sr, stage, G.nsteps);
+    for (int i = t; i < 3 * G.nsteps; i += RG_THREADS) rec[9 * (G.slot0 + i / 3) + i % 3] = tot[i];
+    if (!alone && t == 0) *counter = 0;
 }
 
 // ------------------------------------------------ verifier's wiring predicates
@@ -2397,14 +2440,46 @@ static long tail_chunk()
     return v;
 }
 
-// Rounds a group starting at table length n0 with chunks of `chunk` can hold
-// (see k_round_group).
+// Rounds the chunks of a group starting at table length n0 with chunks of
+// `chunk` can hold (see k_round_group).
 static int group_capacity(long n0, bool nofold, long chunk)
 {
     const long m0 = nofold ? std::min(n0, chunk) : std::min(n0, 2 * chunk) / 2;
     int k = 0;
     while ((1L << (k + 1)) <= m0) ++k;
     return std::min(k, RG_MAX);
+}
+
+// Shape of a group of nsteps rounds from table length n0: the chunks' rounds
+// (k1), the last CTA's tail rounds on the entries the chunks leave, and the
+// table length at the end.
+struct GroupShape {
+    long cin = 0, nchunks = 0;
+    int k1 = 0, tail = 0;
+    long final_n = 0;
+};
+static GroupShape group_shape(long n0, bool nofold, long chunk, int nsteps)
+{
+    GroupShape s;
+    s.cin = nofold ? std::min(n0, chunk) : std::min(n0, 2 * chunk);
+    s.nchunks = n0 / s.cin;
+    s.k1 = std::min(nsteps, group_capacity(n0, nofold, chunk));
+    const long mfin = (nofold ? s.cin : s.cin / 2) >> (s.k1 - 1);
+    s.tail = nsteps - s.k1;
+    const long rem = s.nchunks * mfin;   // entries the chunks leave
+    s.final_n = s.tail ? (rem / 2) >> (s.tail - 1) : rem;
+    return s;
+}
+
+// Rounds a whole group launch can hold: the chunks' rounds, then, when the
+// chunks leave between 4 and 2 RG_CHUNK entries in all, the rounds the last
+// CTA runs on them (a fold-first group of one chunk).
+static int group_total_capacity(long n0, bool nofold, long chunk)
+{
+    const int k1 = group_capacity(n0, nofold, chunk);
+    const GroupShape s = group_shape(n0, nofold, chunk, k1);
+    if (s.nchunks < 2 || s.final_n < 4 || s.final_n > 2L * RG_CHUNK) return k1;
+    return std::min(RG_STEPS, k1 + group_capacity(s.final_n, false, RG_CHUNK));
 }
 
 static int rg_smem_attribute(int dev)
@@ -2577,7 +2652,8 @@ static int exec_pending(vg_gkr *g)
         key.push_back((uint64_t)(uintptr_t)L.ob);
         key.push_back((uint64_t)(uintptr_t)L.prev);
         key.push_back(((uint64_t)L.G.chunk_log) | ((uint64_t)L.G.nsteps << 8) | ((uint64_t)L.G.first_nofold << 16) |
-                      ((uint64_t)L.G.last6 << 24) | ((uint64_t)L.G.split3 << 32));
+                      ((uint64_t)L.G.last6 << 24) | ((uint64_t)L.G.split3 << 32) |
+                      ((uint64_t)L.G.tail << 40));
         key.push_back((uint64_t)L.G.slot0);
         if (L.kind == 3) {
             const GatherArgs &a = L.ga;
@@ -2742,12 +2818,14 @@ static int group_rounds(vg_gkr *g)
     G.slot0 = g->pend_slot0;
     G.r = nullptr;
     const long n_in = g->pend_n0;
-    const long cin = G.first_nofold ? std::min(n_in, g->pend_chunk) : std::min(n_in, 2 * g->pend_chunk);
-    const long nchunks = n_in / cin;
-    // CTAs loop over chunks: at most 3 resident per SM (68 KB of shared memory each)
+    const GroupShape gs = group_shape(n_in, g->pend_nofold, g->pend_chunk, G.nsteps);
+    if (G.nsteps > RG_STEPS || (gs.tail && (gs.nchunks < 2 || gs.final_n < 2)))
+        return vg_fail(VG_ERR_STATE, "round group of %d rounds on %ld entries", G.nsteps, n_in);
+    G.tail = gs.tail;
+    const long nchunks = gs.nchunks;
+    // CTAs loop over chunks: at most 3 resident per SM (72 KB of shared memory each)
     L.grid = (unsigned)std::min(nchunks, 148L * 3L);
-    const long m_final = (G.first_nofold ? cin : cin / 2) >> (G.nsteps - 1);
-    G.last6 = (nchunks == 1 && m_final == 2) ? 1 : 0;
+    G.last6 = (gs.final_n == 2 && (gs.tail || nchunks == 1)) ? 1 : 0;
     G.split3 = vg_tune_value(c->device, VG_TUNE_GROUP_SPLIT) != 0 ? 1 : 0;
     const bool folds = !(G.first_nofold && G.nsteps == 1);
     L.threads = RG_THREADS;
@@ -2758,7 +2836,7 @@ static int group_rounds(vg_gkr *g)
     }
     L.slot = G.slot0;
     // every round of the group: the first reads 3 tables of n_in, writes nothing more than the chunk tails
-    L.prof_bytes = 48.0 * (double)n_in + (folds ? 48.0 * (double)(nchunks * m_final) : 0.0);
+    L.prof_bytes = 48.0 * (double)n_in + (folds ? 48.0 * (double)gs.final_n : 0.0);
     VG_TRY(rg_smem_attribute(c->device));   // before any capture
     VG_TRY(add_launch(g, L, G.nsteps, vg::fe_zero()));
     if (folds) {
@@ -2932,7 +3010,8 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
         ++g->rec_n;
         if (fold) g->n /= 2;
         g->round0_pending = false;
-        if ((int)g->pend_r.size() >= group_capacity(g->pend_n0, g->pend_nofold, g->pend_chunk)) VG_TRY(group_rounds(g));
+        if ((int)g->pend_r.size() >= group_total_capacity(g->pend_n0, g->pend_nofold, g->pend_chunk))
+            VG_TRY(group_rounds(g));
         return VG_OK;
     }
     vg_ctx *c = g->ctx;
