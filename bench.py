@@ -46,6 +46,10 @@ import numpy as np
 # gate type or table shape seen for the first time by the server) loads its
 # module mid-measurement
 os.environ.setdefault("CUDA_MODULE_LOADING", "EAGER")
+# every session runs three streams (sumcheck, commitment, side proof): 32
+# hardware work queues instead of CUDA's default 8, so that the streams of
+# the proofs in flight do not share queues (the package sets the same default)
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
 
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
@@ -64,6 +68,39 @@ FAMILIES = ["ntt_pass", "leaf_chain", "merkle_level", "fri_fold_leaf", "virtual_
 TRAFFIC_RATIO = {"sumcheck_round": 0.954}
 HBM_BOUND = {"ntt_pass", "virtual_oracle", "eval_layer", "phase1_scatter", "phase2_scatter", "acc_finalize",
              "sumcheck_round", "reduce", "gather_round"}
+
+
+# Integer-ALU work of one proof of the matmul workload: warp instructions on
+# the ALU pipe over every launch of a proof (ncu sm__inst_executed_pipe_alu
+# per launch times launches per proof, profiles/alu_instructions_matmul256_proof.txt),
+# a property of the code and the circuit, not of the run.  The pipe's peak is
+# ncu's sm__inst_executed_pipe_alu.avg.peak_sustained, 2 warp instructions
+# per SM cycle, on 148 SMs at the run's median SM clock.
+ALU_WARP_INST_PER_PROOF = {"matmul256": 2.538e9}
+# proofs the reference arm times per step (the step's sample)
+REF_SAMPLE_PER_STEP = 8
+ALU_PEAK_PER_SM_CYCLE = 2
+NUM_SMS = 148
+
+
+def alu_pipe(args, r):
+    """The integer ALU pipe as the roofline of the whole step: the proofs'
+    ALU instructions over the step's device time against the pipe's peak."""
+    n = ALU_WARP_INST_PER_PROOF.get(args.workload)
+    if not n:
+        return None
+    mhz = (r.get("clocks") or {}).get("sm_mhz") or 1965.0
+    peak = ALU_PEAK_PER_SM_CYCLE * NUM_SMS * mhz * 1e6           # warp instructions / s
+    floor_ms = 1e3 * n / peak                                      # one proof with the pipe always busy
+    batch_ms = 1e3 * r["t_batch"] / (args.steps * args.batch)      # per proof, per GPU
+    plain_ms = 1e3 * r["t_plain"] / args.steps
+    return {"bound": "int_alu", "unit": "G warp instructions/s", "achieved": round(n / batch_ms / 1e6, 1),
+            "peak": round(peak / 1e9, 1), "frac": round(floor_ms / batch_ms, 4),
+            "plain_frac": round(floor_ms / plain_ms, 4), "alu_warp_inst_per_proof": n,
+            "floor_ms_per_proof": round(floor_ms, 3), "max_batched_over_plain": round(plain_ms / floor_ms, 2),
+            "source": "instructions per proof: a profile-derived constant (ncu counters, "
+                      "profiles/alu_instructions_matmul256_proof.txt); times: this run's CUDA events; "
+                      "peak: 2 warp instructions per SM cycle x 148 SMs x the run's median SM clock"}
 
 
 def peaks():
@@ -339,10 +376,11 @@ def mem_available_gb():
 
 def reference_arm(args, layers):
     """The reference prover (compiled from its own sources, unmodified apart
-    from a main that seeds rand()) on the host cores: a step is
-    `proofs_per_step` proofs, as on the GPU arm; W warm-up steps, then K timed
-    steps, through a pool of single-threaded processes as wide as the cores
-    (and memory) allow.  value = pool width x mean(1 / prover seconds) over
+    from a main that seeds rand()) on the host cores: the same steps of
+    `proofs_per_step` proofs as on the GPU arm, each timed on a bounded sample
+    of at most REF_SAMPLE_PER_STEP of its proofs; W warm-up steps, then K
+    timed steps, through a pool of single-threaded processes as wide as the
+    cores (and memory) allow.  value = pool width x mean(1 / prover seconds) over
     the timed proofs, each timed by the reference's own timers (Prove Time,
     which includes the fft_gkr side proof, plus evaluate; zk_verifier.cpp
     :1244-1248); ms_per_step = wall-clock span of the timed proofs / K.  No
@@ -357,8 +395,12 @@ def reference_arm(args, layers):
     tmp = tempfile.mkdtemp(prefix="virgo_circ_")
     circuit, meta = os.path.join(tmp, "c.txt"), os.path.join(tmp, "m.txt")
     circuits.write_text(layers, circuit, meta)
+    # each step times a bounded sample of the step's proofs (at most
+    # REF_SAMPLE_PER_STEP of them; a reference proof takes about 10 s of one
+    # core), so that the K + W steps end within a few minutes
+    per_step = min(args.batch, REF_SAMPLE_PER_STEP)
     try:
-        timed, span, fillers = run_reference_pool(circuit, meta, args.warmup * args.batch, args.steps * args.batch,
+        timed, span, fillers = run_reference_pool(circuit, meta, args.warmup * per_step, args.steps * per_step,
                                                   width, seed0=1)
     finally:
         shutil.rmtree(tmp, ignore_errors=True)
@@ -372,13 +414,13 @@ def reference_arm(args, layers):
         "vs_baseline": None, "dtype": "u64 (F_{p^2}, p = 2^61 - 1)", "data": "synthetic (seeded)",
         "config": bench_config(args, layers),
         "cpu_baseline": {"value": value, "unit": "proofs/s", "cores": width, "kind": "reference",
-                         "sample": "%d timed proofs of the workload (%d steps x %d), %d single-threaded reference "
-                                   "processes at a time on %d host cores, each proof timed by its own Prove Time "
-                                   "(fft_gkr side proof included) plus evaluate"
-                                   % (len(timed), args.steps, args.batch, width, cores)},
+                         "sample": "%d timed proofs of the workload (%d steps x %d of each step's %d proofs), %d "
+                                   "single-threaded reference processes at a time on %d host cores, each proof "
+                                   "timed by its own Prove Time (fft_gkr side proof included) plus evaluate"
+                                   % (len(timed), args.steps, per_step, args.batch, width, cores)},
         "e2e": {"value": value, "unit": "proofs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "reference_pool": {"processes": width, "host_cores": cores, "proofs_timed": len(timed),
-                           "proofs_warmup": args.warmup * args.batch, "fillers_stopped": fillers,
+                           "proofs_warmup": args.warmup * per_step, "fillers_stopped": fillers,
                            "timed_span_s": round(span, 2),
                            "wall_proofs_s": round(len(timed) / span, 4),
                            "wall_note": "timed proofs / wall-clock span; each process also reads the circuit text "
@@ -872,7 +914,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["matmul256", "matmul16"], default="matmul256")
-    ap.add_argument("--batch", type=int, default=8, help="proofs in flight at once (one stream each)")
+    ap.add_argument("--batch", type=int, default=16, help="proofs in flight at once (one session each)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-served", action="store_true", help="skip the batched-random and served measurements")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default launch shapes")
@@ -927,6 +969,7 @@ def main():
             "gpu_launches": r["launches"],
             "clocks": r["clocks"],
             "roofline": roofline(r["families"], hbm, kind, r["large_rounds"]),
+            "roofline_alu": alu_pipe(args, r),
             "stages_s": r["stages"],
             "kernel_families": fam,
             "autotune": r["autotune"],

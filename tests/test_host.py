@@ -320,6 +320,27 @@ def test_bench_roofline_fields():
     assert hbm > 0 and kind in ("measured", "fallback")
 
 
+def test_bench_alu_roofline():
+    """bench.py's integer-pipe roofline: the proofs' ALU instructions over the
+    step's time against 2 warp instructions per SM cycle on 148 SMs; the
+    floor per proof bounds the batched / plain ratio."""
+    import argparse
+    import sys
+    sys.path.insert(0, ROOT)
+    import bench
+    args = argparse.Namespace(workload="matmul256", steps=10, batch=16)
+    r = {"t_batch": 10 * 16 * 6.6e-3, "t_plain": 10 * 9.1e-3, "clocks": {"sm_mhz": 1965.0}}
+    a = bench.alu_pipe(args, r)
+    peak = 2 * 148 * 1965e6
+    assert a["bound"] == "int_alu" and abs(a["peak"] - peak / 1e9) < 0.1
+    floor = bench.ALU_WARP_INST_PER_PROOF["matmul256"] / peak
+    assert abs(a["floor_ms_per_proof"] - 1e3 * floor) < 1e-3
+    assert abs(a["frac"] - floor / 6.6e-3) < 1e-3 and abs(a["plain_frac"] - floor / 9.1e-3) < 1e-3
+    assert abs(a["max_batched_over_plain"] - 9.1e-3 / floor) < 0.01
+    json.dumps(a)
+    assert bench.alu_pipe(argparse.Namespace(workload="matmul16", steps=1, batch=1), r) is None
+
+
 def test_text_writer_matches_library_writer(built, tmp_path):
     """The pure-numpy text writer (used where no library of this repository
     may be loaded) writes the same bytes as vg_circuit_write_text, negative

@@ -16,6 +16,12 @@ import os
 
 import numpy as np
 
+# Concurrent sessions run three streams each; CUDA's default of 8 hardware
+# work queues per device makes streams beyond the eighth share a queue (and
+# wait on each other's kernels).  Read when the process creates its CUDA
+# context; a value set by the caller is kept.
+os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", "32")
+
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "lib", "libvirgo_b200.so")
 HEADER = os.path.join(os.path.dirname(_HERE), "include", "virgo_b200.h")

@@ -1,3 +1,4 @@
+#include <cstdlib>
 #include <cstring>
 #include <algorithm>
 // Context, device memory, error reporting, elementwise field ops and the
@@ -20,9 +21,22 @@ int vg_fail(int code, const char *fmt, ...)
 
 extern "C" const char *vg_last_error(void) { return g_err.c_str(); }
 
+// Concurrent sessions run three streams each (sumcheck, commitment, side
+// proof); with CUDA's default of 8 hardware work queues per device, streams
+// beyond the eighth share a queue and their kernels wait on each other's.
+// The variable is read when the process creates its CUDA context, so it takes
+// effect only when this library makes the process's first CUDA call, and a
+// value the caller set is kept.
+static void default_connections()
+{
+    static std::once_flag once;
+    std::call_once(once, [] { setenv("CUDA_DEVICE_MAX_CONNECTIONS", "32", 0); });
+}
+
 extern "C" int vg_ctx_create(int device, vg_ctx **out)
 {
     if (!out) return vg_fail(VG_ERR_ARG, "vg_ctx_create: null out");
+    default_connections();
     int n = 0;
     cudaError_t e = cudaGetDeviceCount(&n);
     if (e != cudaSuccess || n == 0)
