@@ -104,6 +104,38 @@ def test_reference_verifier_accepts_gpu_proof(tmp_path, fft):
         assert open(tmp_path / "res.txt").read().split()[-1] == open(other / "res.txt").read().split()[-1]
 
 
+@pytest.mark.skipif(not os.path.exists(os.path.join(REF, "zk_proof_accept_gpred")), reason="acceptance binary not built")
+@pytest.mark.parametrize("case", ["mixed_gates", "random_5layer", "matmul16_seed7"])
+def test_reference_verifier_with_gpu_predicates(tmp_path, case):
+    """The reference verifier, compiled unchanged, with its wiring predicates
+    (zk_verifier::predicates) answered on the GPU from the prover's device
+    circuit (virgo_b200/host/bin_src/zk_verifier_predicates.cpp, linked over
+    the reference's definition made weak): Pass, every layer above the relay
+    layer answered there, and the same messages, verdict and proof size as
+    the reference prover's golden run (every gate type in mixed_gates)."""
+    c = next(x for x in _golden() if x["name"] == case)
+    layers = getattr(circuits, c["generator"])(**c["params"])
+    env = dict(os.environ, VIRGO_LOG_PREDICATES="1")
+    cpath, mpath = str(tmp_path / "c.txt"), str(tmp_path / "m.txt")
+    circuits.write_text(layers, cpath, mpath)
+    os.symlink(os.path.join(REF, "fft_gkr"), tmp_path / "fft_gkr")
+    tr = str(tmp_path / "t.bin")
+    out = subprocess.run([os.path.join(REF, "zk_proof_accept_gpred"), cpath, mpath, str(tmp_path / "res.txt"),
+                          str(c["seed"]), tr], cwd=str(tmp_path), capture_output=True, text=True, timeout=600, env=env)
+    assert out.returncode == 0 and "Pass" in out.stdout, (out.stdout[-2000:], out.stderr[-2000:])
+    answered = [l for l in out.stderr.splitlines() if l.startswith("virgo predicates: layer ")]
+    s = vb.Session(layers)   # the device circuit: the reader's layers, relay layer included
+    try:
+        depth, _ = s.depth()
+    finally:
+        s.close()
+    assert depth >= 3 and sorted(int(l.split()[3]) for l in answered) == list(range(2, depth))
+    recs = transcript.read(tr)
+    got = [[t, h] for t, h in transcript.record_hashes(transcript.prover_records(recs))]
+    assert transcript.first_difference(got, [r for r in c["records"] if r[0] != "C"]) is None
+    assert recs[-1][0] == "V" and recs[-1][1].hex() == c["verdict"][1]
+
+
 def test_session_runs_fft_gkr_side_proof():
     """Every proof runs the fft_gkr side proof for lg = L - 6 beside it (its
     own stream); turning it off leaves the transcript unchanged."""
@@ -380,8 +412,11 @@ def test_reference_verifier_accepts_matmul256(tmp_path):
     prints Pass, and every prover message and the verdict with its proof
     size equal the reference prover's own run on the same circuit and seed."""
     layers = circuits.matmul_addtree(256, 32, seed=1)
-    runs = {}
-    for name, binary in (("gpu", "zk_proof_accept"), ("ref", "zk_proof_ref")):
+    runs, pred_s = {}, {}
+    binaries = [("gpu", "zk_proof_accept"), ("ref", "zk_proof_ref")]
+    if os.path.exists(os.path.join(REF, "zk_proof_accept_gpred")):   # the verifier's predicates on the GPU too
+        binaries.append(("gpred", "zk_proof_accept_gpred"))
+    for name, binary in binaries:
         d = tmp_path / name
         d.mkdir()
         cpath, mpath = str(d / "c.txt"), str(d / "m.txt")
@@ -392,11 +427,17 @@ def test_reference_verifier_accepts_matmul256(tmp_path):
                              capture_output=True, text=True, timeout=900)
         assert out.returncode == 0 and "Pass" in out.stdout, (name, out.stdout[-1500:], out.stderr[-1500:])
         runs[name] = transcript.read(tr)
+        # the verifier's result line: prove time, verification time, predicates time, ...
+        pred_s[name] = float(open(d / "res.txt").read().split()[2])
     got = transcript.prover_records(runs["gpu"])
     ref = [r for r in transcript.prover_records(runs["ref"]) if r[0] != "C"]
     assert len(got) > 400
     assert transcript.first_difference(got, ref) is None
     assert runs["gpu"][-1][0] == "V" and runs["gpu"][-1] == runs["ref"][-1]
+    if "gpred" in runs:   # same proof and verdict with the predicates on the GPU, in less time
+        assert transcript.first_difference(transcript.prover_records(runs["gpred"]), ref) is None
+        assert runs["gpred"][-1] == runs["ref"][-1]
+        assert pred_s["gpred"] < pred_s["gpu"], pred_s
 
 
 @pytest.mark.skipif(not os.path.exists(os.path.join(REF, "zk_verify_file")), reason="replay verifier not built here")
