@@ -2,7 +2,7 @@
 
 bench.py times sessions in their deferred (launch pass + replay pass) mode: a
 session on the 256x256 matmul circuit (2^24 product gates, 8 add layers,
-32-bit entries) and seven forks of it, all proving at once, with paired
+32-bit entries) and fifteen forks of it, all proving at once, with paired
 sumcheck rounds, the beta_g table, the launch shapes the autotuner picks, and
 a new witness per proof through vg_session_set_inputs.  Here every prover
 record of those proofs (sumcheck messages, commitment roots, all_sum, FRI
@@ -71,7 +71,7 @@ def test_bench_session_path_matches_reference_matmul256(tmp_path):
 
     # the bench's session path while the reference runs
     base = vb.Session(layers)
-    sessions = [base] + [base.fork() for _ in range(7)]
+    sessions = [base] + [base.fork() for _ in range(15)]
     got = {}
     try:
         vb.tune_reset(0)
@@ -85,7 +85,7 @@ def test_bench_session_path_matches_reference_matmul256(tmp_path):
                 vb.tune_set(0, **shape)
             for i, s in enumerate(sessions):
                 s.set_inputs(witnesses[combos[i % 4][0]])
-            res = vb.prove_batch(sessions, [combos[i % 4][1] for i in range(8)])
+            res = vb.prove_batch(sessions, [combos[i % 4][1] for i in range(len(sessions))])
             for i, (st, blob) in enumerate(res):
                 assert blob, (name, i)
                 key = combos[i % 4]

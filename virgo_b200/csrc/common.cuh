@@ -16,6 +16,7 @@ struct TwEntry {
     int logn;
     fe *lo;   // w^i, i < 4096
     fe *hi;   // w^(4096 j), j < max(1, n / 4096)
+    fe *full = nullptr;   // w^e, e < n, for the NTT's column twiddles (small n only), or null
 };
 
 // Kernel families timed by the optional per-launch profiler (vg_ctx_profile).

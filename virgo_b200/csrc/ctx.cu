@@ -242,6 +242,7 @@ extern "C" int vg_ctx_destroy(vg_ctx *c)
     for (auto &t : c->tw_cache) {
         cudaFree(t.lo);
         cudaFree(t.hi);
+        if (t.full) cudaFree(t.full);
     }
     if (c->scratch) cudaFree(c->scratch);
     if (c->scratch2) cudaFree(c->scratch2);

@@ -14,7 +14,9 @@
 // (two radix-2 stages each, three twiddle products per four entries).
 //
 // Twiddles: w^e for e < n comes from two small tables, lo[e & 4095] *
-// hi[e >> 12], built once per root and cached in the context.
+// hi[e >> 12], built once per root and cached in the context; for n up to
+// 2^TW_FULL_MAX_LOG the column passes read w^e from a full table instead
+// (one load in place of two loads and a product per element).
 #include "common.cuh"
 #include <algorithm>
 #include <mutex>
@@ -36,6 +38,7 @@ struct PassArgs {
     int nfac;           // row pass: number of previous factors
     int fac[6];         // row pass: their logs, F_1 first
     const fe *tw_lo, *tw_hi;
+    const fe *tw_full;  // w^e for every e < n, or null
     int scale;
     fe inv_n;
 };
@@ -200,12 +203,19 @@ __global__ void __launch_bounds__(NTT_THREADS) k_ntt_pass(PassArgs a)
         if (a.kind == 0) {
             const long A = 1L << a.logA;
             const long c = (col_base % A) + g;
-            uint64_t e = ((uint64_t)c * (uint64_t)k) << (a.logn - a.logA);
-            if (e) y = y * tw_pow(a.tw_lo, a.tw_hi, e);
+            uint64_t e = ((uint64_t)c * (uint64_t)k) << (a.logn - a.logA);   // c k < A, so e < n
+            if (e) y = y * (a.tw_full ? a.tw_full[e] : tw_pow(a.tw_lo, a.tw_hi, e));
         }
         if (a.scale) y = y * a.inv_n;
         dst[gi] = y;
     }
+}
+
+// w^e for every e < n, from the two small tables
+__global__ void k_tw_full(const fe *__restrict__ lo, const fe *__restrict__ hi, long n, fe *__restrict__ full)
+{
+    for (long e = blockIdx.x * (long)blockDim.x + threadIdx.x; e < n; e += (long)gridDim.x * blockDim.x)
+        full[e] = tw_pow(lo, hi, (uint64_t)e);
 }
 
 __global__ void k_tw_build(fe w, fe w4096, fe *lo, fe *hi, int nhi)
@@ -262,11 +272,47 @@ int vg_twiddles(vg_ctx *c, fe root, int logn, const fe **lo, const fe **hi)
     if (c->tw_cache.size() >= 64) {
         vg_release(c, c->tw_cache.front().lo);
         vg_release(c, c->tw_cache.front().hi);
+        if (c->tw_cache.front().full) vg_release(c, c->tw_cache.front().full);
         c->tw_cache.erase(c->tw_cache.begin());
     }
     c->tw_cache.push_back(t);
     *lo = t.lo;
     *hi = t.hi;
+    return VG_OK;
+}
+
+// The full table w^e, e < 2^logn, of a cached root (built on first use), or
+// null when n is above 2^TW_FULL_MAX_LOG or the context's full tables would
+// pass TW_FULL_BUDGET bytes: the column passes then form w^e from lo and hi.
+constexpr int TW_FULL_MAX_LOG = 20;
+constexpr size_t TW_FULL_BUDGET = 64u << 20;
+
+static int twiddles_full(vg_ctx *c, fe root, int logn, const fe **full)
+{
+    *full = nullptr;
+    if (logn > TW_FULL_MAX_LOG) return VG_OK;
+    const fe *lo, *hi;
+    VG_TRY(vg_twiddles(c, root, logn, &lo, &hi));
+    size_t used = 0;
+    TwEntry *mine = nullptr;
+    for (auto &t : c->tw_cache) {
+        if (t.full) used += ((size_t)1 << t.logn) * sizeof(fe);
+        if (t.key_real == root.real && t.key_img == root.img && t.logn == logn) mine = &t;
+    }
+    if (!mine) return VG_OK;
+    if (!mine->full) {
+        const size_t bytes = ((size_t)1 << logn) * sizeof(fe);
+        if (used + bytes > TW_FULL_BUDGET) return VG_OK;
+        // never allocate inside a stream capture (the table would belong to the graph)
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        VG_CHECK_CUDA(cudaStreamIsCapturing(c->stream, &cs));
+        if (cs != cudaStreamCaptureStatusNone) return VG_OK;
+        VG_TRY(vg_alloc(c, (void **)&mine->full, bytes));
+        k_tw_full<<<std::min<unsigned>(grid_for(1L << logn, 256), 148u * 8u), 256, 0, c->stream>>>(mine->lo, mine->hi,
+                                                                                                   1L << logn, mine->full);
+        VG_LAUNCHED(c);
+    }
+    *full = mine->full;
     return VG_OK;
 }
 
@@ -317,8 +363,9 @@ extern "C" int vg_ntt(vg_ctx *c, const vg_fe *in_, long in_len, long in_bstride,
     root.real = root_.real;
     root.img = root_.img;
     const long n = 1L << logn;
-    const fe *lo, *hi;
+    const fe *lo, *hi, *full;
     VG_TRY(vg_twiddles(c, root, logn, &lo, &hi));
+    VG_TRY(twiddles_full(c, root, logn, &full));
     fe inv_n = vg::fe_inv(vg::fe_make((uint64_t)n % vg::P, 0));
 
     std::vector<int> f;
@@ -359,7 +406,7 @@ extern "C" int vg_ntt(vg_ctx *c, const vg_fe *in_, long in_len, long in_bstride,
         a.in_bstride = q == 0 ? in_bstride : n;
         a.out_bstride = n;
         a.logn = logn; a.lm = f[q]; a.kind = 0; a.logA = logA;
-        a.tw_lo = lo; a.tw_hi = hi; a.scale = 0;
+        a.tw_lo = lo; a.tw_hi = hi; a.tw_full = full; a.scale = 0;
         long logC = logA - f[q];
         a.logG = pick_logG(f[q], logC, tile_log);
         long nblocks = (n >> logA) * ((1L << logC) >> a.logG);
