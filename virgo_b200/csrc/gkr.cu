@@ -2423,23 +2423,6 @@ static bool fuse_gather(vg_gkr *g, long N)
            N > S && N >= 8;
 }
 
-// With VIRGO_TAIL_CHUNK = c (a power of two below RG_CHUNK), a group starting
-// on more than TAIL_SPLIT chunks' worth of entries uses chunks of c entries,
-// so several CTAs share its first rounds, and the few entries left continue
-// in a single-CTA group.  Off by default: on the matmul and random-circuit
-// proofs measured (c = 32 .. 256) the proof time did not change, since the
-// single-CTA tails overlap the commitment stream.
-constexpr long TAIL_SPLIT = 4;
-static long tail_chunk()
-{
-    static const long v = [] {
-        const char *e = getenv("VIRGO_TAIL_CHUNK");
-        const long x = e ? atol(e) : (long)RG_CHUNK;
-        return (x >= 2 && x <= RG_CHUNK && !(x & (x - 1))) ? x : (long)RG_CHUNK;
-    }();
-    return v;
-}
-
 // Rounds the chunks of a group starting at table length n0 with chunks of
 // `chunk` can hold (see k_round_group).
 static int group_capacity(long n0, bool nofold, long chunk)
@@ -3003,8 +2986,7 @@ extern "C" int vg_gkr_round(vg_gkr *g, vg_fe previous_random, int current_bit, v
             g->pend_n0 = g->n;
             g->pend_nofold = !fold;
             g->pend_slot0 = g->rec_n;
-            const long tc = tail_chunk();
-            g->pend_chunk = (tc < RG_CHUNK && g->n > TAIL_SPLIT * (fold ? 2 * tc : tc)) ? tc : (long)RG_CHUNK;
+            g->pend_chunk = RG_CHUNK;
         }
         g->pend_r.push_back(tofe(previous_random));
         ++g->rec_n;
