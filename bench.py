@@ -880,6 +880,8 @@ def roofline(fam, hbm_peak, peak_kind, large=None):
     gbs = f["bytes"] / (f["ms"] / 1000.0) / 1e9 if f["ms"] > 0 else 0.0
     per_launch = f["bytes"] / f["launches"]
     traffic = TRAFFIC_RATIO.get(top)
+    g = fam.get("gather_round", {"bytes": 0.0, "ms": 0.0})
+    both_b, both_ms = f["bytes"] + g["bytes"], f["ms"] + g["ms"]
     return {"bound": "hbm", "kernel": top, "achieved": round(gbs, 1), "peak": hbm_peak, "unit": "GB/s",
             "frac": round(gbs / hbm_peak, 4),
             "traffic": round(per_launch * traffic) if traffic else None,
@@ -896,6 +898,13 @@ def roofline(fam, hbm_peak, peak_kind, large=None):
                                 "note": "the round launches that move at least 100 MB each (tables of 2^21 "
                                         "entries and up), same events"}
                                if (large and top == "sumcheck_round" and large["ms"] > 0) else None),
+            "with_fused_builds": (
+                {"achieved": round(both_b / (both_ms / 1000.0) / 1e9, 1),
+                 "frac": round(both_b / (both_ms / 1000.0) / 1e9 / hbm_peak, 4),
+                 "note": "the rounds together with the gather_round family: each phase's first two rounds above "
+                         "the group start run inside its fused table build (k_gather_round2), so the family's "
+                         "largest launches are there"}
+                if top == "sumcheck_round" and g["ms"] > 0 else None),
             "alu_pipe_profile": {"frac_large_launches": 0.735, "frac_round_group": 0.33,
                                  "source": "profile-derived constants, not measured in this run: ncu "
                                            "sm__inst_executed_pipe_alu, pct of peak, of a paired round on a "

@@ -316,6 +316,10 @@ def test_bench_roofline_fields():
     assert r["traffic"] is not None and r["alu_pipe_profile"]["frac_large_launches"] > 0
     json.dumps(r)
     assert bench.roofline(fam, 6650.0, "fallback", None)["large_launches"] is None
+    assert r["with_fused_builds"] is None
+    fam["gather_round"] = {"launches": 14.0, "ms": 3.0, "bytes": 3.2e9}
+    w = bench.roofline(fam, 6650.0, "fallback", large)["with_fused_builds"]
+    assert abs(w["achieved"] - (7.5e9 + 3.2e9) / 8.3e-3 / 1e9) < 0.1
     hbm, kind = bench.peaks()
     assert hbm > 0 and kind in ("measured", "fallback")
 
