@@ -79,6 +79,15 @@ VG_HD uint64_t mulp_partial(uint64_t a, uint64_t b)
     mul64wide(a, b, lo, hi);
     return foldp((lo & P) + ((hi << 3) | (lo >> 61)));
 }
+// x = a*b mod p as (x & p) + (x >> 61), not folded further, for a*b < 2^124:
+// below 2^62 when a, b < 2^61 (x >> 61 < 2^61), below 2^61 + 2^63 when
+// a, b < 2^62.
+VG_HD uint64_t mulp_fold1(uint64_t a, uint64_t b)
+{
+    uint64_t lo, hi;
+    mul64wide(a, b, lo, hi);
+    return (lo & P) + ((hi << 3) | (lo >> 61));
+}
 
 // ---- F_{p^2} ----
 VG_HD fe operator+(fe a, fe b) { return fe_make(addp(a.real, b.real), addp(a.img, b.img)); }
@@ -86,17 +95,20 @@ VG_HD fe operator-(fe a, fe b) { return fe_make(subp(a.real, b.real), subp(a.img
 VG_HD fe operator-(fe a) { return fe_make(negp(a.real), negp(a.img)); }
 
 // (ar + i ai)(br + i bi) = (ar br - ai bi) + i((ar + ai)(br + bi) - ar br - ai bi)
-// with the three products partly reduced (below 2^61 + 8; the sums of two
-// canonical values are below 2^62, so every product is below 2^124) and the
-// differences taken as x + 4p - y (positive, below 2^64) before one fold and
-// the final canonical step.
+// For canonical inputs ac = ar br and bd = ai bi are taken once folded
+// (mulp_fold1: below 2^62), t = (ar + ai)(br + bi) (operands below 2^62, the
+// product below 2^124) folded twice (below 2^61 + 5), and the differences as
+// ac + 3p - bd (3p > 2^62 > bd; the sum below 5 2^61) and t + 5p - ac - bd
+// (5p > 2^63 > ac + bd; the sum below 6 2^61), each folded once (below
+// 2^61 + 5) before the final canonical step: the canonical product with two
+// folds fewer than folding every partial product.
 VG_HD fe operator*(fe a, fe b)
 {
-    const uint64_t ac = mulp_partial(a.real, b.real);
-    const uint64_t bd = mulp_partial(a.img, b.img);
-    const uint64_t t = mulp_partial(a.real + a.img, b.real + b.img);
-    const uint64_t re = foldp(ac + (4 * P - bd));
-    const uint64_t im = foldp(t + (4 * P - ac - bd));
+    const uint64_t ac = mulp_fold1(a.real, b.real);
+    const uint64_t bd = mulp_fold1(a.img, b.img);
+    const uint64_t t = foldp(mulp_fold1(a.real + a.img, b.real + b.img));
+    const uint64_t re = foldp(ac + (3 * P - bd));
+    const uint64_t im = foldp(t + (5 * P - ac - bd));
     return fe_make(canonp(re), canonp(im));
 }
 
