@@ -112,6 +112,20 @@ VG_HD fe operator*(fe a, fe b)
     return fe_make(canonp(re), canonp(im));
 }
 
+// x + a*b for canonical x, a, b: x joins the product's two sums before their
+// last fold (ac + 3p - bd + x.real below 6 2^61, t + 5p - ac - bd + x.img
+// below 7 2^61 + 5), so an integer add replaces a canonical one; the same
+// canonical result as x + a * b.
+VG_HD fe fe_fma(fe x, fe a, fe b)
+{
+    const uint64_t ac = mulp_fold1(a.real, b.real);
+    const uint64_t bd = mulp_fold1(a.img, b.img);
+    const uint64_t t = foldp(mulp_fold1(a.real + a.img, b.real + b.img));
+    const uint64_t re = foldp(ac + (3 * P - bd) + x.real);
+    const uint64_t im = foldp(t + (5 * P - ac - bd) + x.img);
+    return fe_make(canonp(re), canonp(im));
+}
+
 VG_HD fe fe_double(fe a) { return a + a; }
 
 // x0 + r (x1 - x0) for canonical x0, x1, r with the difference left

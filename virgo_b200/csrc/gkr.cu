@@ -186,7 +186,7 @@ struct BetaG {
     __device__ __forceinline__ fe at(long i) const
     {
         if (tab) return tab[i];
-        return f0[i & mask] * s0[i >> fh] + f1[i & mask] * s1[i >> fh];
+        return vg::fe_fma(f0[i & mask] * s0[i >> fh], f1[i & mask], s1[i >> fh]);
     }
 };
 struct BetaU {
@@ -432,8 +432,8 @@ __device__ __forceinline__ void edge1(int tk, uint32_t gv, uint32_t o, const Bet
     const fe b = bg.at(gv);
     if (bg.save) bg.save[gv] = b;   // every edge of a gate stores the same value
     switch (t) {
-    case 0: av = av + prev[o] * b; am = am + b; break;
-    case 1: am = am + prev[o] * b; break;
+    case 0: av = vg::fe_fma(av, prev[o], b); am = am + b; break;
+    case 1: am = vg::fe_fma(am, prev[o], b); break;
     case 4:
     case 5:
     case 10: am = am + b; break;
@@ -483,8 +483,8 @@ __device__ __forceinline__ void edge2(int tk, uint32_t gv, uint32_t o, const Bet
 // product skipped for a part no edge touched (it is zero)
 __device__ __forceinline__ void phase2_out(const fe (&a)[4], unsigned used, fe vu, fe &m, fe &v)
 {
-    m = (used & 2) ? a[0] + a[1] * vu : a[0];
-    v = (used & 8) ? a[2] + a[3] * vu : a[2];
+    m = (used & 2) ? vg::fe_fma(a[0], a[1], vu) : a[0];
+    v = (used & 8) ? vg::fe_fma(a[2], a[3], vu) : a[2];
 }
 
 struct EdgeView {
@@ -648,7 +648,7 @@ template <bool LAZY>
 __device__ __forceinline__ fe rg_fold(fe x0, fe x1, fe r)
 {
     if (LAZY) return vg::fold_lazy(x0, x1, r);
-    return x0 + r * (x1 - x0);
+    return vg::fe_fma(x0, r, x1 - x0);
 }
 
 // A round's sums over one pair: (m0 + ma x)(v0 + va x) + a0 + aa x has x^2
@@ -659,10 +659,15 @@ template <bool FULL = true>
 __device__ __forceinline__ void rg_sums(fe v0, fe v1, fe a0, fe a1, fe m0, fe m1, fe (&acc)[3])
 {
     const fe va = v1 - v0, ma = m1 - m0;
-    const fe p2 = ma * va, p0 = m0 * v0;
-    acc[0] = acc[0] + p2;
-    if (FULL) acc[1] = acc[1] + ((m1 * v1 - p0 - p2) + (a1 - a0));
-    acc[2] = acc[2] + p0 + a0;
+    if (FULL) {
+        const fe p2 = ma * va, p0 = m0 * v0;
+        acc[0] = acc[0] + p2;
+        acc[1] = acc[1] + ((m1 * v1 - p0 - p2) + (a1 - a0));
+        acc[2] = acc[2] + p0 + a0;
+    } else {   // each product added inside its last fold (vg::fe_fma)
+        acc[0] = vg::fe_fma(acc[0], ma, va);
+        acc[2] = vg::fe_fma(acc[2] + a0, m0, v0);
+    }
 }
 
 // The x term of a round that follows another round of its phase, from the
@@ -1008,7 +1013,7 @@ template <bool LAZY>
 __device__ __forceinline__ fe fold(fe x0, fe x1, fe r)
 {
     if (LAZY) return vg::fold_lazy(x0, x1, r);
-    return x0 + r * (x1 - x0);
+    return vg::fe_fma(x0, r, x1 - x0);
 }
 
 // The block partials are reduced by the last block to finish (a counter in
