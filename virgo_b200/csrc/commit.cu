@@ -60,7 +60,7 @@ __global__ void k_virtual_oracle(const fe *__restrict__ l, const fe *__restrict_
         long off = (long)(slice0 + s) * S + j;
         fe c0 = lq_coef[s * 2 * m] + lq_coef[s * 2 * m + m];
         fe xm = tw_pow(twf_lo, twf_hi, ((uint64_t)j * (uint64_t)m) & mask);
-        fe g = l[off] * q[off] - (xm - vg::fe_one()) * h[off];
+        fe g = vg::fe_fma(l[off] * q[off], vg::fe_one() - xm, h[off]);   // l q - (x^m - 1) h
         fe xinv = tw_pow(twi_lo, twi_hi, (uint64_t)j);
         vo[off] = ((g - c0) * mm) * xinv;
     }
@@ -86,7 +86,7 @@ __global__ void k_inner_product(const fe *__restrict__ l, const fe *__restrict__
     fe acc[1] = {vg::fe_zero()};
     for (long i = blockIdx.x * (long)blockDim.x + threadIdx.x; i < n_data + n_mask; i += (long)gridDim.x * blockDim.x) {
         long pos = i < n_data ? (i << 5) : (64 * S + (i - n_data) * gap);
-        acc[0] = acc[0] + l[pos] * q[pos];
+        acc[0] = vg::fe_fma(acc[0], l[pos], q[pos]);
     }
     block_sum<1>(acc, sm);
     if (threadIdx.x == 0) parts[blockIdx.x] = acc[0];
@@ -112,8 +112,8 @@ __global__ void __launch_bounds__(128) k_fri_fold_leaf(const fe *__restrict__ c,
     for (int s = 0; s < 65; ++s) {
         const fe *cs = c + (long)s * n;
         fe a0 = cs[k], b0 = cs[k + half], a1 = cs[k + q4], b1 = cs[k + q4 + half];
-        fe y0 = half_fe((a0 + b0) + t0 * (a0 - b0));
-        fe y1 = half_fe((a1 + b1) + t1 * (a1 - b1));
+        fe y0 = half_fe(vg::fe_fma(a0 + b0, t0, a0 - b0));
+        fe y1 = half_fe(vg::fe_fma(a1 + b1, t1, a1 - b1));
         out[(long)s * nh + k] = y0;
         out[(long)s * nh + k + q4] = y1;
         uint64_t w[8] = {y0.img, y0.real, y1.img, y1.real, h[0], h[1], h[2], h[3]};
@@ -134,7 +134,7 @@ __global__ void k_fri_fold(const fe *__restrict__ c, long n, int t, fe r, const 
         const long s = i / h, k = i - s * h;
         const fe a = c[s * n + k], b = c[s * n + k + h];
         const fe w = r * tw_pow(twi_lo, twi_hi, (uint64_t)k << t);
-        out[i] = half_fe((a + b) + w * (a - b));
+        out[i] = half_fe(vg::fe_fma(a + b, w, a - b));
     }
 }
 
