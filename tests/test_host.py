@@ -421,3 +421,20 @@ def test_replay_verifier_rejects_malformed_proof_files(tmp_path):
         open(p, "wb").write(data)
         out = subprocess.run([binary, c, m, p, str(tmp_path / "r.txt")], capture_output=True, text=True, timeout=60)
         assert out.returncode == 2 and "VGPF" in out.stderr, (name, out.stderr)
+
+
+def test_field_arithmetic_against_schoolbook(tmp_path):
+    """The F_p2 product (two folds fewer than folding every partial product),
+    x + a*b folded once (fe_fma), sums and differences of csrc/fp2.cuh, built
+    for the host, against schoolbook 128-bit arithmetic reduced by % on
+    every combination of edge values and on random inputs."""
+    import shutil
+    cxx = shutil.which("g++") or shutil.which("c++")
+    if not cxx:
+        pytest.skip("no host C++ compiler")
+    exe = str(tmp_path / "field_check")
+    subprocess.run([cxx, "-O2", "-std=c++17", "-I" + os.path.join(ROOT, "virgo_b200", "csrc"),
+                    os.path.join(ROOT, "tests", "field_check.cpp"), "-o", exe], check=True)
+    out = subprocess.run([exe, "2000000"], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stdout[-2000:]
+    assert "cases agree" in out.stdout
