@@ -53,9 +53,12 @@ __device__ __forceinline__ void sha3_256_64(const uint64_t w[8], uint64_t d[4])
     d[3] = aL3 | ((uint64_t)aH3 << 32);
 }
 
-// sha3_256_64 with the 24 rounds in a loop unrolled four times (round
-// constants from constant memory): a sixth of the fully unrolled code, for
-// kernels whose permutation body would not stay in the instruction cache
+// sha3_256_64 with the first 20 rounds in a loop unrolled four times (round
+// constants from constant memory) and the last four written out, so that the
+// last round forms only the lanes the 256-bit digest reads (row 0: theta's
+// five column sums, five lanes through rho and pi, four chi outputs, about a
+// third of a round): under half of the fully unrolled code, for kernels whose
+// permutation body would not stay in the instruction cache
 __constant__ uint32_t vg_keccak_rcl[24] = VG_KECCAK_RC_LO, vg_keccak_rch[24] = VG_KECCAK_RC_HI;
 __device__ __forceinline__ void sha3_256_64_compact(const uint64_t w[8], uint64_t d[4])
 {
@@ -68,7 +71,9 @@ __device__ __forceinline__ void sha3_256_64_compact(const uint64_t w[8], uint64_
     uint32_t aL17 = 0, aH17 = 0, aL18 = 0, aH18 = 0, aL19 = 0, aH19 = 0, aL20 = 0, aH20 = 0, aL21 = 0, aH21 = 0;
     uint32_t aL22 = 0, aH22 = 0, aL23 = 0, aH23 = 0, aL24 = 0, aH24 = 0;
 #pragma unroll 4
-    for (int r = 0; r < 24; ++r) VG_KECCAK_ROUND32(vg_keccak_rcl[r], vg_keccak_rch[r]);
+    for (int r = 0; r < 20; ++r) VG_KECCAK_ROUND32(vg_keccak_rcl[r], vg_keccak_rch[r]);
+#pragma unroll
+    for (int r = 20; r < 24; ++r) VG_KECCAK_ROUND32(vg_keccak_rcl[r], vg_keccak_rch[r]);
     d[0] = aL0 | ((uint64_t)aH0 << 32);
     d[1] = aL1 | ((uint64_t)aH1 << 32);
     d[2] = aL2 | ((uint64_t)aH2 << 32);
