@@ -76,7 +76,7 @@ HBM_BOUND = {"ntt_pass", "virtual_oracle", "eval_layer", "phase1_scatter", "phas
 # a property of the code and the circuit, not of the run.  The pipe's peak is
 # ncu's sm__inst_executed_pipe_alu.avg.peak_sustained, 2 warp instructions
 # per SM cycle, on 148 SMs at the run's median SM clock.
-ALU_WARP_INST_PER_PROOF = {"matmul256": 2.345e9}
+ALU_WARP_INST_PER_PROOF = {"matmul256": 2.319e9}
 # proofs the reference arm times per step (the step's sample)
 REF_SAMPLE_PER_STEP = 8
 ALU_PEAK_PER_SM_CYCLE = 2
